@@ -1,0 +1,128 @@
+"""ctypes binding of libfpb200.so (include/fp_capi.h).
+
+The library is the only compute path: if it is missing or no CUDA device is present every call raises
+(there is no CPU fallback). Arrays may be numpy (host, synchronous) or torch CUDA tensors (device,
+queued on torch's current stream).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libfpb200.so")
+
+FP_DEVICE, FP_SYNC = 1, 2
+FP_F64, FP_F32 = 0, 1
+STATUS = {0: "FP_OK", 1: "FP_ERR_INVALID", 2: "FP_ERR_CUDA", 3: "FP_ERR_UNSUPPORTED", 4: "FP_ERR_NOT_CONVERGED",
+          5: "FP_ERR_NAN", 6: "FP_ERR_NOMEM"}
+
+# Every symbol include/fp_capi.h declares, with its ctypes signature.
+_vp, _i, _d, _ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_longlong
+SIGNATURES = {
+    "fp_last_error": ([], ctypes.c_char_p),
+    "fp_transform_f64": ([_i, _i, _i, _i, _i, _vp, _vp, _i, _vp], _i),
+    "fp_transform_f32": ([_i, _i, _i, _i, _i, _vp, _vp, _i, _vp], _i),
+    "fp_rect_create": ([_i, _i, _d, _d, _vp, _i, _vp], _i),
+    "fp_rect_solve_f64": ([_vp, _vp, _ll, _i, _vp], _i),
+    "fp_rect_solve_f32": ([_vp, _vp, _ll, _i, _vp], _i),
+    "fp_rect_destroy": ([_vp], _i),
+}
+
+_lib = None
+
+
+class FpError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Loads libfpb200.so (raises if it was not built: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m focalors_poisson_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(rc: int, allow=()):
+    if rc != 0 and rc not in allow:
+        raise FpError(rc, lib().fp_last_error().decode())
+    return rc
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+def _stream():
+    import torch
+
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _args(x, want):
+    """(pointer, flags, stream, keepalive) for a numpy array or a torch CUDA tensor of dtype `want`."""
+    if _is_torch(x):
+        import torch
+
+        tdt = torch.float64 if want == np.float64 else torch.float32
+        if not x.is_cuda or x.dtype != tdt or not x.is_contiguous():
+            raise TypeError(f"expected a contiguous CUDA {tdt} tensor")
+        return ctypes.c_void_p(x.data_ptr()), FP_DEVICE, _stream(), x
+    a = np.ascontiguousarray(x, dtype=want)
+    return ctypes.c_void_p(a.ctypes.data), 0, None, a
+
+
+def transform(bc_yneg: int, bc_ypos: int, f, inverse: bool = False, out=None):
+    """PoissonFFT2D_* transform (forward) or transform_transpose (inverse) of an (nx, ny) field."""
+    want = np.float32 if (getattr(f, "dtype", None) in (np.float32,) or str(getattr(f, "dtype", "")) == "torch.float32") else np.float64
+    nx, ny = f.shape[-2], f.shape[-1]
+    rows = int(np.prod(f.shape[:-1]))
+    if out is None:
+        out = f.clone() if _is_torch(f) else np.empty(f.shape, dtype=want)
+    p_in, flags, stream, keep_in = _args(f, want)
+    p_out, _, _, keep_out = _args(out, want)
+    fn = lib().fp_transform_f32 if want == np.float32 else lib().fp_transform_f64
+    check(fn(bc_yneg, bc_ypos, rows, ny, int(inverse), p_in, p_out, flags, stream))
+    if not _is_torch(out) and keep_out is not out:
+        out[...] = keep_out
+    return out
+
+
+class Rect:
+    """PoissonSolver2D(nx, ny, hx, hy, bc) on the GPU: solve() works in place on (…, nx, ny) arrays."""
+
+    def __init__(self, nx, ny, hx, hy, bc, precision=FP_F64):
+        self.nx, self.ny, self.precision = nx, ny, precision
+        h = ctypes.c_void_p()
+        bca = (ctypes.c_int * 4)(*[int(b) for b in bc])
+        check(lib().fp_rect_create(nx, ny, float(hx), float(hy), bca, precision, ctypes.byref(h)))
+        self.h = h
+
+    def solve(self, f):
+        want = np.float32 if self.precision == FP_F32 else np.float64
+        if f.shape[-2:] != (self.nx, self.ny):
+            raise ValueError("field shape does not match the solver")
+        batch = int(np.prod(f.shape[:-2])) if len(f.shape) > 2 else 1
+        p, flags, stream, keep = _args(f, want)
+        fn = lib().fp_rect_solve_f32 if want == np.float32 else lib().fp_rect_solve_f64
+        check(fn(self.h, p, batch, flags, stream))
+        if not _is_torch(f) and keep is not f:
+            f[...] = keep
+        return f
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fp_rect_destroy(self.h)
+            self.h = None

@@ -1,0 +1,241 @@
+// Shared-memory complex FFT engine for one CTA.
+//
+// Layout: the whole length-M sequence lives in one shared-memory buffer of M complex values and is
+// transformed in place by mixed-radix stages (radix 2, 3, 4, 5, 7, 8). Each butterfly reads and
+// writes the same R slots, so one buffer suffices (no ping-pong), which is what lets an FP64
+// transform of length ~13k fit in the 227 KB a CTA may own.
+//
+//  * DIF stages (natural order in)  -> spectrum in mixed-radix digit-reversed order
+//  * DIT stages (digit-reversed in) -> spectrum in natural order
+//
+// A smooth length L is transformed by loading the input digit-reversed (a per-plan index table) and
+// running the DIT stages. A length with a prime factor above 7 goes through Bluestein's chirp-z
+// identity on a smooth length M >= 2L-1:  X_k = c_k * sum_n (x_n c_n) conj(c_{k-n}),
+// c_n = exp(-i pi n^2 / L): DIF of (x c), pointwise product with the (digit-reversed, 1/M-scaled)
+// transform of the chirp kernel, conjugate, DIT, conjugate, times c_k.
+//
+// All twiddles, chirps and permutations are precomputed on the host in long double and read
+// through the read-only cache.
+#pragma once
+
+#include "fp_common.cuh"
+
+namespace fpb
+{
+
+constexpr int kFftMaxStages = 20;
+
+struct FftStage
+{
+    int R;       // radix
+    int S;       // span between butterfly legs
+    int B;       // block size this stage works in (= R * S)
+    int tw_off;  // twiddles for this stage: tw[tw_off + b*R + q] = exp(-2 pi i b q / B)
+};
+
+struct FftDesc
+{
+    int      L;     // logical transform length
+    int      M;     // executed length (L, or the Bluestein length)
+    int      blue;  // 1: Bluestein
+    int      nst;
+    FftStage st[kFftMaxStages];
+};
+
+template <typename T2> struct FftTables
+{
+    const T2*  tw;     // stage twiddles
+    const T2*  chirp;  // Bluestein: c_n, n < L
+    const T2*  bhat;   // Bluestein: FFT_M(conj chirp kernel) / M, digit-reversed
+    const int* perm;   // direct: slot of input n for the DIT stages
+};
+
+// ---------------------------------------------------------------------------------------------
+// Radix butterflies, forward sign exp(-2 pi i / R)
+// ---------------------------------------------------------------------------------------------
+template <typename T2> __device__ __forceinline__ void dft2(T2* x)
+{
+    T2 a = x[0], b = x[1];
+    x[0] = a + b;
+    x[1] = a - b;
+}
+
+template <typename T2> __device__ __forceinline__ void dft4(T2* x)
+{
+    T2 s0 = x[0] + x[2], s1 = x[0] - x[2], s2 = x[1] + x[3], s3 = mul_mi(x[1] - x[3]);
+    x[0] = s0 + s2;
+    x[2] = s0 - s2;
+    x[1] = s1 + s3;
+    x[3] = s1 - s3;
+}
+
+template <typename T2> __device__ __forceinline__ void dft8(T2* x)
+{
+    typedef decltype(T2::x) T;
+    const T r = (T)0.70710678118654752440;
+    T2 e[4] = {x[0], x[2], x[4], x[6]};
+    T2 o[4] = {x[1], x[3], x[5], x[7]};
+    dft4(e);
+    dft4(o);
+    // o_k *= w8^k : w8 = (1 - i)/sqrt2, w8^2 = -i, w8^3 = -(1 + i)/sqrt2
+    T2 o1 = mk<T2>((o[1].x + o[1].y) * r, (o[1].y - o[1].x) * r);
+    T2 o2 = mul_mi(o[2]);
+    T2 o3 = mk<T2>((o[3].y - o[3].x) * r, -(o[3].x + o[3].y) * r);
+    x[0] = e[0] + o[0];
+    x[4] = e[0] - o[0];
+    x[1] = e[1] + o1;
+    x[5] = e[1] - o1;
+    x[2] = e[2] + o2;
+    x[6] = e[2] - o2;
+    x[3] = e[3] + o3;
+    x[7] = e[3] - o3;
+}
+
+template <typename T2> __device__ __forceinline__ void dft3(T2* x)
+{
+    typedef decltype(T2::x) T;
+    const T s = (T)0.86602540378443864676;
+    T2 t = x[1] + x[2], u = x[1] - x[2];
+    T2 a = mk<T2>(x[0].x - (T)0.5 * t.x, x[0].y - (T)0.5 * t.y);
+    T2 b = mk<T2>(s * u.y, -s * u.x);  // -i * s * u
+    x[0] = x[0] + t;
+    x[1] = a + b;
+    x[2] = a - b;
+}
+
+template <typename T2> __device__ __forceinline__ void dft5(T2* x)
+{
+    typedef decltype(T2::x) T;
+    const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
+    const T s1 = (T)0.95105651629515357212, s2 = (T)0.58778525229247312917;
+    T2 t1 = x[1] + x[4], t2 = x[2] + x[3], t3 = x[1] - x[4], t4 = x[2] - x[3];
+    T2 a1 = mk<T2>(x[0].x + c1 * t1.x + c2 * t2.x, x[0].y + c1 * t1.y + c2 * t2.y);
+    T2 a2 = mk<T2>(x[0].x + c2 * t1.x + c1 * t2.x, x[0].y + c2 * t1.y + c1 * t2.y);
+    T2 b1 = mk<T2>(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
+    T2 b2 = mk<T2>(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
+    x[0] = x[0] + t1 + t2;
+    x[1] = a1 + mul_mi(b1);
+    x[4] = a1 - mul_mi(b1);
+    x[2] = a2 + mul_mi(b2);
+    x[3] = a2 - mul_mi(b2);
+}
+
+template <typename T2> __device__ __forceinline__ void dft7(T2* x)
+{
+    typedef decltype(T2::x) T;
+    const T C1 = (T)0.62348980185873353053, C2 = (T)-0.22252093395631440429, C3 = (T)-0.90096886790241912624;
+    const T S1 = (T)0.78183148246802980871, S2 = (T)0.97492791218182360702, S3 = (T)0.43388373911755812048;
+    T2 t1 = x[1] + x[6], t2 = x[2] + x[5], t3 = x[3] + x[4];
+    T2 u1 = x[1] - x[6], u2 = x[2] - x[5], u3 = x[3] - x[4];
+    T2 a1 = mk<T2>(x[0].x + C1 * t1.x + C2 * t2.x + C3 * t3.x, x[0].y + C1 * t1.y + C2 * t2.y + C3 * t3.y);
+    T2 a2 = mk<T2>(x[0].x + C2 * t1.x + C3 * t2.x + C1 * t3.x, x[0].y + C2 * t1.y + C3 * t2.y + C1 * t3.y);
+    T2 a3 = mk<T2>(x[0].x + C3 * t1.x + C1 * t2.x + C2 * t3.x, x[0].y + C3 * t1.y + C1 * t2.y + C2 * t3.y);
+    // b_k = sum_m sin(2 pi m k / 7) u_m
+    T2 b1 = mk<T2>(S1 * u1.x + S2 * u2.x + S3 * u3.x, S1 * u1.y + S2 * u2.y + S3 * u3.y);
+    T2 b2 = mk<T2>(S2 * u1.x - S3 * u2.x - S1 * u3.x, S2 * u1.y - S3 * u2.y - S1 * u3.y);
+    T2 b3 = mk<T2>(S3 * u1.x - S1 * u2.x + S2 * u3.x, S3 * u1.y - S1 * u2.y + S2 * u3.y);
+    x[0] = x[0] + t1 + t2 + t3;
+    x[1] = a1 + mul_mi(b1);
+    x[6] = a1 - mul_mi(b1);
+    x[2] = a2 + mul_mi(b2);
+    x[5] = a2 - mul_mi(b2);
+    x[3] = a3 + mul_mi(b3);
+    x[4] = a3 - mul_mi(b3);
+}
+
+template <int R, typename T2> __device__ __forceinline__ void dft(T2* x)
+{
+    if constexpr (R == 2) dft2(x);
+    else if constexpr (R == 3) dft3(x);
+    else if constexpr (R == 4) dft4(x);
+    else if constexpr (R == 5) dft5(x);
+    else if constexpr (R == 7) dft7(x);
+    else dft8(x);
+}
+
+template <int R, bool DIT, typename T2>
+__device__ __forceinline__ void stage_radix(T2* buf, const FftStage st, int nbf, const T2* __restrict__ tw)
+{
+    for (int t = threadIdx.x; t < nbf; t += blockDim.x)
+    {
+        const int blk = t / st.S;
+        const int b   = t - blk * st.S;
+        T2*       p   = buf + blk * st.B + b;
+        const T2* w   = tw + st.tw_off + b * R;
+        T2        x[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) x[q] = p[q * st.S];
+        if (DIT)
+        {
+#pragma unroll
+            for (int q = 1; q < R; ++q) x[q] = cmul(x[q], __ldg(w + q));
+        }
+        dft<R>(x);
+        if (!DIT)
+        {
+#pragma unroll
+            for (int q = 1; q < R; ++q) x[q] = cmul(x[q], __ldg(w + q));
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) p[q * st.S] = x[q];
+    }
+}
+
+// Runs all stages (DIF order or DIT order) on buf. Ends with a barrier.
+template <bool DIT, typename T2> __device__ void fft_stages(T2* buf, const FftDesc& d, const T2* __restrict__ tw)
+{
+    for (int s0 = 0; s0 < d.nst; ++s0)
+    {
+        const int      s   = DIT ? d.nst - 1 - s0 : s0;
+        const FftStage st  = d.st[s];
+        const int      nbf = d.M / st.R;
+        switch (st.R)
+        {
+            case 2: stage_radix<2, DIT>(buf, st, nbf, tw); break;
+            case 3: stage_radix<3, DIT>(buf, st, nbf, tw); break;
+            case 4: stage_radix<4, DIT>(buf, st, nbf, tw); break;
+            case 5: stage_radix<5, DIT>(buf, st, nbf, tw); break;
+            case 7: stage_radix<7, DIT>(buf, st, nbf, tw); break;
+            default: stage_radix<8, DIT>(buf, st, nbf, tw); break;
+        }
+        __syncthreads();
+    }
+}
+
+// Slot in buf where input element n (n < M) must be stored before fft_execute.
+template <typename T2> __device__ __forceinline__ int fft_in_slot(const FftDesc& d, const FftTables<T2>& t, int n)
+{
+    return d.blue ? n : __ldg(t.perm + n);
+}
+// Scale applied to input n before storing (Bluestein pre-chirp); zero past L.
+template <typename T2> __device__ __forceinline__ T2 fft_in_value(const FftDesc& d, const FftTables<T2>& t, int n, T2 z)
+{
+    if (!d.blue) return z;
+    if (n >= d.L) return mk<T2>(0, 0);
+    return cmul(z, __ldg(t.chirp + n));
+}
+
+// In-place transform; on return buf holds the natural-order spectrum (direct) or its Bluestein
+// intermediate, read back through fft_out.
+template <typename T2> __device__ void fft_execute(T2* buf, const FftDesc& d, const FftTables<T2>& t)
+{
+    __syncthreads();
+    if (!d.blue)
+    {
+        fft_stages<true>(buf, d, t.tw);
+        return;
+    }
+    fft_stages<false>(buf, d, t.tw);
+    for (int k = threadIdx.x; k < d.M; k += blockDim.x) buf[k] = cconj(cmul(buf[k], __ldg(t.bhat + k)));
+    __syncthreads();
+    fft_stages<true>(buf, d, t.tw);
+}
+
+// Spectrum value X_k, 0 <= k < L, after fft_execute.
+template <typename T2> __device__ __forceinline__ T2 fft_out(const T2* buf, const FftDesc& d, const FftTables<T2>& t, int k)
+{
+    if (!d.blue) return buf[k];
+    return cmul(cconj(buf[k]), __ldg(t.chirp + k));
+}
+
+}  // namespace fpb

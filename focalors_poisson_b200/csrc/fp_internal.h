@@ -1,0 +1,131 @@
+// Host-side infrastructure shared by the C ABI implementation: error reporting, device buffers,
+// device-resident transform and rectangle plans.
+#pragma once
+
+#include "fp_plan.h"
+#include "fp_transform.cuh"
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace fpb
+{
+
+struct Error : std::runtime_error
+{
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string& msg);
+
+#define FPB_CUDA(call)                                                                                   \
+    do                                                                                                   \
+    {                                                                                                    \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            throw ::fpb::Error(e_ == cudaErrorMemoryAllocation ? 6 : 2,                                  \
+                               std::string(#call) + ": " + cudaGetErrorString(e_));                      \
+    } while (0)
+
+#define FPB_CHECK_LAUNCH() FPB_CUDA(cudaGetLastError())
+
+// Owning device allocation.
+class DevBuf
+{
+public:
+    DevBuf() = default;
+    explicit DevBuf(size_t bytes) { alloc(bytes); }
+    ~DevBuf() { release(); }
+    DevBuf(const DevBuf&)            = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_)
+    {
+        o.p_ = nullptr;
+        o.n_ = 0;
+    }
+    DevBuf& operator=(DevBuf&& o) noexcept
+    {
+        if (this != &o)
+        {
+            release();
+            p_   = o.p_;
+            n_   = o.n_;
+            o.p_ = nullptr;
+            o.n_ = 0;
+        }
+        return *this;
+    }
+    void alloc(size_t bytes)
+    {
+        release();
+        if (bytes == 0) return;
+        FPB_CUDA(cudaMalloc(&p_, bytes));
+        n_ = bytes;
+    }
+    void ensure(size_t bytes)
+    {
+        if (bytes > n_) alloc(bytes);
+    }
+    void release()
+    {
+        if (p_) cudaFree(p_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p_); }
+    void*  get() const { return p_; }
+    size_t bytes() const { return n_; }
+
+private:
+    void*  p_ = nullptr;
+    size_t n_ = 0;
+};
+
+template <typename T> DevBuf upload(const std::vector<T>& v)
+{
+    DevBuf b(v.size() * sizeof(T));
+    if (!v.empty()) FPB_CUDA(cudaMemcpy(b.get(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return b;
+}
+
+// Device-resident plan for one transform family at one row length and precision.
+template <typename T> struct DevTransform
+{
+    typedef typename Cplx<T>::type T2;
+    int     kind = 0, n = 0;
+    FftDesc fd{};
+    DevBuf  tw, chirp, bhat, perm, ta, tb;
+    T       s1 = 0, s2 = 0;
+    int     threads = 128;
+    size_t  smem    = 0;
+
+    DevTransform(int kind, int n);
+    // rows = fields * nx contiguous rows of length n; in and out may alias.
+    void run(const T* in, T* out, long long rows, bool inverse, cudaStream_t s) const;
+};
+
+// Device-resident PoissonSolver2D: transform plan + chase tables.
+template <typename T> struct DevRect
+{
+    int                              nx = 0, ny = 0;
+    double                           hx = 0, hy = 0;
+    int                              bc[4]{};
+    std::unique_ptr<DevTransform<T>> tr;
+    DevBuf                           ctab;  // nx*ny chase coefficients (see build_chase_tables)
+    DevBuf                           z1, z2;  // periodic-x Sherman-Morrison vectors (nx*ny each)
+    bool                             periodic_x = false;
+    bool                             singular   = false;  // no Dirichlet-like face: last wavenumber singular
+
+    DevRect(int nx, int ny, double hx, double hy, const int* bc);
+    // In-place solve of `batch` back-to-back fields.
+    void solve(T* f, long long batch, cudaStream_t s) const;
+};
+
+size_t max_dynamic_smem();
+
+}  // namespace fpb

@@ -1,0 +1,261 @@
+// Host-side planning: FFT stage factorisation, twiddle / chirp / permutation tables, transform
+// family tables and rectangle-solver coefficients.
+#include "fp_plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+
+namespace fpb
+{
+
+namespace
+{
+typedef std::complex<long double> cld;
+const long double kPi = 3.141592653589793238462643383279502884L;
+const double      kRefPi = 3.14159265358979323846;  // the reference's `pi` (base/pch.h:13)
+
+cld root_of_unity(long long num, long long den)  // exp(-2 pi i num / den), exact reduction
+{
+    num %= den;
+    if (num < 0) num += den;
+    long double a = -2.0L * kPi * (long double)num / (long double)den;
+    return cld(std::cos(a), std::sin(a));
+}
+
+// Radix sequence for a 7-smooth length (8s first, then 4, 2, 3, 5, 7); empty if not 7-smooth.
+std::vector<int> radices(int m)
+{
+    std::vector<int> r;
+    if (m == 1) return r;
+    while (m % 8 == 0) { r.push_back(8); m /= 8; }
+    while (m % 4 == 0) { r.push_back(4); m /= 4; }
+    while (m % 2 == 0) { r.push_back(2); m /= 2; }
+    while (m % 3 == 0) { r.push_back(3); m /= 3; }
+    while (m % 5 == 0) { r.push_back(5); m /= 5; }
+    while (m % 7 == 0) { r.push_back(7); m /= 7; }
+    if (m != 1) r.clear();
+    return r;
+}
+
+double stage_cost(int R)  // flops per element of one stage (butterfly + twiddle), rough
+{
+    switch (R)
+    {
+        case 2: return 5.0;
+        case 3: return 9.3;
+        case 4: return 8.5;
+        case 5: return 13.6;
+        case 7: return 19.0;
+        default: return 12.3;
+    }
+}
+
+// Position p of the DIF output holds X[digit_reverse(p)].
+std::vector<int> dif_order(const FftDesc& d)
+{
+    std::vector<int> idx(d.M);
+    for (int p = 0; p < d.M; ++p)
+    {
+        long long k = 0, mult = 1;
+        int       pp = p;
+        for (int s = 0; s < d.nst; ++s)
+        {
+            int k1 = pp / d.st[s].S;
+            pp -= k1 * d.st[s].S;
+            k += (long long)k1 * mult;
+            mult *= d.st[s].R;
+        }
+        idx[p] = (int)k;
+    }
+    return idx;
+}
+
+void host_dft(std::vector<cld>& x)  // natural-order forward DFT, recursive mixed radix (host only)
+{
+    const int n = (int)x.size();
+    if (n <= 1) return;
+    int p = 2;
+    while (p * p <= n && n % p) ++p;
+    if (n % p) p = n;
+    const int       m = n / p;
+    std::vector<cld> out(n);
+    std::vector<std::vector<cld>> sub(p, std::vector<cld>(m));
+    for (int r = 0; r < p; ++r)
+        for (int k = 0; k < m; ++k) sub[r][k] = x[(size_t)k * p + r];
+    for (int r = 0; r < p; ++r) host_dft(sub[r]);
+    for (int k = 0; k < n; ++k)
+    {
+        cld acc = 0;
+        for (int r = 0; r < p; ++r) acc += sub[r][k % m] * root_of_unity((long long)r * k, n);
+        out[k] = acc;
+    }
+    x.swap(out);
+}
+
+void build_stages(FftDesc& d, const std::vector<int>& rad, std::vector<cld>& tw)
+{
+    if ((int)rad.size() > kFftMaxStages) throw std::runtime_error("FFT plan: too many stages");
+    d.nst = (int)rad.size();
+    int B = d.M;
+    tw.clear();
+    for (int s = 0; s < d.nst; ++s)
+    {
+        const int R = rad[s], S = B / R;
+        d.st[s].R      = R;
+        d.st[s].S      = S;
+        d.st[s].B      = B;
+        d.st[s].tw_off = (int)tw.size();
+        for (int b = 0; b < S; ++b)
+            for (int q = 0; q < R; ++q) tw.push_back(root_of_unity((long long)b * q, B));
+        B = S;
+    }
+}
+}  // namespace
+
+int kind_of(int bn, int bp)
+{
+    if (bn == BC_PERIODIC && bp == BC_PERIODIC) return K_PP;
+    if (bn == BC_NEUMANN && bp == BC_NEUMANN) return K_NN;
+    if (dir_like(bn) && dir_like(bp)) return K_DD;
+    if (dir_like(bn) && bp == BC_NEUMANN) return K_DN;
+    if (bn == BC_NEUMANN && dir_like(bp)) return K_ND;
+    return -1;
+}
+
+int r2c_length(int kind, int n)
+{
+    switch (kind)
+    {
+        case K_DD: return 2 * n + 2;
+        case K_NN: return 2 * n;
+        case K_ND:
+        case K_DN: return 2 * n + 1;
+        default: return n;
+    }
+}
+
+HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit)
+{
+    HostFft h;
+    h.d.L = L;
+    std::vector<int> rad = radices(L);
+    if (!rad.empty() || L == 1)
+    {
+        h.d.M    = L;
+        h.d.blue = 0;
+        build_stages(h.d, rad, h.tw);
+        std::vector<int> idx = dif_order(h.d);
+        h.perm.assign(L, 0);
+        for (int p = 0; p < L; ++p) h.perm[idx[p]] = p;
+    }
+    else
+    {
+        // Smallest-cost 7-smooth M >= 2L-1.
+        int    best = -1;
+        double best_cost = 1e300;
+        for (int M = 2 * L - 1; M <= 3 * L; ++M)
+        {
+            std::vector<int> r = radices(M);
+            if (r.empty()) continue;
+            double c = 0;
+            for (int x : r) c += stage_cost(x);
+            c *= M;
+            if (c < best_cost)
+            {
+                best_cost = c;
+                best      = M;
+            }
+        }
+        if (best < 0) throw std::runtime_error("FFT plan: no Bluestein length");
+        h.d.M    = best;
+        h.d.blue = 1;
+        build_stages(h.d, radices(best), h.tw);
+        h.chirp.resize(L);
+        for (int n = 0; n < L; ++n) h.chirp[n] = root_of_unity(((long long)n * n) % (2LL * L), 2LL * L);
+        std::vector<cld> b(best, cld(0, 0));
+        for (int n = 0; n < L; ++n) b[n] = std::conj(h.chirp[n]);
+        for (int n = 1; n < L; ++n) b[best - n] = std::conj(h.chirp[n]);
+        host_dft(b);
+        std::vector<int> idx = dif_order(h.d);
+        h.bhat.resize(best);
+        for (int p = 0; p < best; ++p) h.bhat[p] = b[idx[p]] / (long double)best;
+    }
+    if ((size_t)h.d.M * elem_bytes > smem_limit)
+        throw std::runtime_error("transform length " + std::to_string(L) + " needs " +
+                                 std::to_string((size_t)h.d.M * elem_bytes) +
+                                 " bytes of shared memory, more than this build supports");
+    return h;
+}
+
+KindTables kind_tables(int kind, int n)
+{
+    KindTables t;
+    const double pi = kRefPi;
+    switch (kind)
+    {
+        case K_DD: t.s1 = std::sqrt(2.0 / (1. + n)); break;  // poisson_fft2d.cpp:22
+        case K_NN:                                             // poisson_fft2d.cpp:81-90
+            t.s1 = std::sqrt(2.0 / n);
+            t.s2 = std::sqrt(1.0 / n);
+            t.a.resize(n);
+            t.b.resize(n);
+            for (int j = 0; j < n; j++)
+            {
+                t.a[j] = std::cos(pi * (j + 1.) / n / 2);
+                t.b[j] = std::sin(pi * (j + 1.) / n / 2);
+            }
+            break;
+        case K_ND:  // poisson_fft2d.cpp:157-165
+            t.s1 = std::sqrt(4. / (2. * n + 1.));
+            t.a.resize(n);
+            t.b.resize(n);
+            for (int j = 0; j < n; j++)
+            {
+                t.a[j] = std::cos(2. * n * pi * (j + 1.) / (2. * n + 1.));
+                t.b[j] = std::sin(2. * n * pi * (j + 1.) / (2. * n + 1.));
+            }
+            break;
+        case K_DN: t.s1 = std::sqrt(4. / (2. * n + 1.)); break;  // poisson_fft2d.cpp:227
+        case K_PP:                                                 // poisson_fft2d.cpp:390-397
+            t.s1 = std::sqrt(2.0 / n);
+            t.a.resize(n);
+            t.b.resize(n);
+            for (int j = 0; j < n; j++)
+            {
+                t.a[j] = std::cos(pi * (2.0 * j + 1.0) / 4.0);
+                t.b[j] = std::sin(pi * (2.0 * j + 1.0) / 4.0);
+            }
+            break;
+        default: throw std::runtime_error("unknown transform family");
+    }
+    return t;
+}
+
+std::vector<double> cal_lambda(int n, int bn, int bp)
+{
+    const double        pi = kRefPi;
+    std::vector<double> lam(n);
+    for (int i = 1; i <= n; i++)
+    {
+        double v;
+        if (bn == BC_PERIODIC && bp == BC_PERIODIC) v = -2.0 * std::cos(2.0 * pi / n * std::floor(i / 2.0));
+        else if (bn == BC_NEUMANN && bp == BC_NEUMANN) v = -2.0 * std::cos(pi / n * i);
+        else if (dir_like(bn) && dir_like(bp)) v = +2.0 * std::cos(pi / (n + 1) * i);
+        else if ((dir_like(bn) && bp == BC_NEUMANN) || (bn == BC_NEUMANN && dir_like(bp)))
+            v = -2.0 * std::cos(2.0 * pi * i / (2 * n + 1));
+        else throw std::runtime_error("unsupported boundary pair");
+        lam[i - 1] = v;
+    }
+    return lam;
+}
+
+std::vector<double> x_diag(int ny, double hx, double hy, int bn, int bp)
+{
+    std::vector<double> lam = cal_lambda(ny, bn, bp);
+    std::vector<double> d(ny);
+    for (int j = 0; j < ny; j++) d[j] = -2.0 + hx * hx / hy / hy * (lam[j] - 2.0);
+    return d;
+}
+
+}  // namespace fpb

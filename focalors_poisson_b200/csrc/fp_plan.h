@@ -1,0 +1,78 @@
+// Host-side plans: FFT factorisation / twiddles, per-boundary-pair transform tables, rectangle
+// solver coefficients. Everything here is computed once per plan and uploaded to the device.
+#pragma once
+
+#include "fp_fft.cuh"
+
+#include <complex>
+#include <string>
+#include <vector>
+
+namespace fpb
+{
+
+// Boundary types and faces, numbered like the reference's PDEBoundaryType / LocationType
+// (base/location_boundary.h:8-16, 62-69).
+enum Bc : int
+{
+    BC_DIRICHLET  = 0,
+    BC_NEUMANN    = 1,
+    BC_PERIODIC   = 2,
+    BC_ADJACENTED = 3,
+    BC_NULL       = 4
+};
+enum Face : int
+{
+    XNEG = 0,
+    XPOS = 1,
+    YNEG = 2,
+    YPOS = 3
+};
+inline bool dir_like(int b) { return b == BC_DIRICHLET || b == BC_ADJACENTED; }
+inline int  opposite_face(int f) { return f ^ 1; }
+
+// y-transform families, one per boundary pair (PoissonSolver2DBase::create_fft,
+// pe/poisson/poisson_solver2d_base.cpp:64-91).
+enum Kind : int
+{
+    K_DD = 0,
+    K_NN = 1,
+    K_ND = 2,
+    K_DN = 3,
+    K_PP = 4
+};
+int kind_of(int bc_neg, int bc_pos);  // -1 if unsupported
+
+// Length of the real DFT the reference uses for each family (poisson_fft2d.cpp:19-465).
+int r2c_length(int kind, int n);
+
+struct HostFft
+{
+    FftDesc                               d{};
+    std::vector<std::complex<long double>> tw;
+    std::vector<std::complex<long double>> chirp;
+    std::vector<std::complex<long double>> bhat;  // digit-reversed, scaled by 1/M
+    std::vector<int>                       perm;
+};
+// Plans a length-L complex DFT whose single buffer must fit in smem_limit bytes for complex
+// elements of elem_bytes. Throws std::runtime_error if it cannot.
+HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit);
+
+// Per-family tables computed with the reference's own double expressions so that the device
+// transform reproduces the reference's values, not merely the exact transform.
+struct KindTables
+{
+    std::vector<double> a, b;  // NN: cos/sin(pi (j+1) / n / 2); ND: cos/sin(2 n pi (j+1) / (2n+1));
+                               // PP: cos/sin(pi (2j+1) / 4)
+    double s1 = 0, s2 = 0;     // DD: sqrt(2/(1+n)); NN: sqrt(2/n), sqrt(1/n); ND/DN: sqrt(4/(2n+1));
+                               // PP: sqrt(2/n)
+};
+KindTables kind_tables(int kind, int n);
+
+// Eigenvalues of the y second difference (PoissonSolver2DBase::cal_lambda,
+// pe/poisson/poisson_solver2d_base.cpp:28-62) and the chase diagonal
+// x_diag[j] = -2 + hx^2/hy^2 (lambda_j - 2) (pe/poisson/poisson_solver2d.cpp:46-51).
+std::vector<double> cal_lambda(int n, int bc_neg, int bc_pos);
+std::vector<double> x_diag(int ny, double hx, double hy, int bc_yneg, int bc_ypos);
+
+}  // namespace fpb

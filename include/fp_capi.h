@@ -1,0 +1,75 @@
+/*
+ * C ABI of libfpb200.so: the B200 (sm_100a) composite-geometry FFT / domain-decomposition Poisson
+ * solve of Focalors_Poisson's 2D path.
+ *
+ * Conventions
+ *   - Fields are row-major nx x ny float64 (or float32) arrays, value(i, j) = f[i*ny + j], exactly the
+ *     reference's field2 layout (base/field/field2.cpp:304-314).
+ *   - Boundary codes are the reference's PDEBoundaryType values (base/location_boundary.h:62-69):
+ *     0 Dirichlet, 1 Neumann, 2 Periodic, 3 Adjacented; faces are its LocationType order
+ *     (base/location_boundary.h:8-16): 0 XNegative, 1 XPositive, 2 YNegative, 3 YPositive.
+ *   - Every entry point returns an fp_status; no C++ exception crosses the ABI. fp_last_error()
+ *     describes the last failure on the calling thread.
+ *   - Pointers are host memory unless FP_DEVICE is set in `flags`, in which case they are device
+ *     memory and the work is queued on `stream` (a cudaStream_t, NULL = legacy default stream) without
+ *     a host synchronisation unless FP_SYNC is also set. Host-pointer calls are synchronous.
+ *   - There is no CPU fallback: without a usable CUDA device every compute call fails with
+ *     FP_ERR_CUDA.
+ */
+#ifndef FP_CAPI_H
+#define FP_CAPI_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fp_status
+{
+    FP_OK                = 0,
+    FP_ERR_INVALID       = 1, /* bad argument, unsupported boundary combination, bad geometry */
+    FP_ERR_CUDA          = 2, /* CUDA runtime error (no device, launch failure, ...) */
+    FP_ERR_UNSUPPORTED   = 3, /* size beyond what this build supports */
+    FP_ERR_NOT_CONVERGED = 4, /* GMRES stopped at max_iter above tol (result still written) */
+    FP_ERR_NAN           = 5, /* non-finite value met */
+    FP_ERR_NOMEM         = 6  /* device allocation failed */
+} fp_status;
+
+#define FP_DEVICE 1 /* pointers are device memory, work queued on `stream` */
+#define FP_SYNC 2   /* synchronise `stream` before returning */
+
+#define FP_F64 0
+#define FP_F32 1
+
+/* Message for the last failing call on this thread ("" if none). */
+const char* fp_last_error(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * y-direction transforms: PoissonFFT2D_{DD,NN,ND,DN,PP}::transform / transform_transpose
+ * (reference pe/poisson/poisson_fft2d.h:8-136, pe/poisson/poisson_fft2d.cpp:19-465). The family is
+ * chosen from the y boundary pair like PoissonSolver2DBase::create_fft
+ * (pe/poisson/poisson_solver2d_base.cpp:64-91). `in` and `out` may alias.
+ * ------------------------------------------------------------------------------------------- */
+int fp_transform_f64(int bc_yneg, int bc_ypos, int nx, int ny, int inverse, const double* in, double* out,
+                     int flags, void* stream);
+int fp_transform_f32(int bc_yneg, int bc_ypos, int nx, int ny, int inverse, const float* in, float* out,
+                     int flags, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Single rectangle: PoissonSolver2D(nx, ny, hx, hy, bc_xneg, bc_xpos, bc_yneg, bc_ypos) and its
+ * solve(field2&) (reference pe/poisson/poisson_solver2d.h:10-34, pe/poisson/poisson_solver2d.cpp:3-90):
+ * forward y-transform, one tridiagonal "chasing" solve per wavenumber along x, inverse transform.
+ * bc[4] in face order. `batch` fields are stored back to back (batch * nx * ny values), solved in
+ * place.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct fp_rect fp_rect;
+
+int fp_rect_create(int nx, int ny, double hx, double hy, const int* bc, int precision, fp_rect** out);
+int fp_rect_solve_f64(fp_rect* r, double* f, long long batch, int flags, void* stream);
+int fp_rect_solve_f32(fp_rect* r, float* f, long long batch, int flags, void* stream);
+int fp_rect_destroy(fp_rect* r);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FP_CAPI_H */
