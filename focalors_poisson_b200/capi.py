@@ -29,7 +29,27 @@ SIGNATURES = {
     "fp_rect_solve_f64": ([_vp, _vp, _ll, _i, _vp], _i),
     "fp_rect_solve_f32": ([_vp, _vp, _ll, _i, _vp], _i),
     "fp_rect_destroy": ([_vp], _i),
+    "fp_composite_create": ([_vp, _i, _d, _i, _i, _vp], _i),
+    "fp_composite_set_parameter": ([_vp, _i, _d, _i], _i),
+    "fp_composite_solve_f64": ([_vp, _vp, _vp, _i, _vp, _vp], _i),
+    "fp_composite_tree": ([_vp, _vp, _vp], _i),
+    "fp_composite_destroy": ([_vp], _i),
 }
+FP_GMRES_FULLFIELD, FP_CHECK_CONVERGENCE = 4, 8
+
+
+class Geometry(ctypes.Structure):
+    """struct fp_geometry"""
+
+    _fields_ = [("n_domains", ctypes.c_int), ("nx", _vp), ("ny", _vp), ("hx", _vp), ("hy", _vp), ("bc", _vp),
+                ("n_connections", ctypes.c_int), ("connections", _vp), ("root", ctypes.c_int)]
+
+
+class SolveInfo(ctypes.Structure):
+    """struct fp_solve_info"""
+
+    _fields_ = [("gmres_iterations", ctypes.c_int), ("gmres_restarts", ctypes.c_int),
+                ("gmres_residual", ctypes.c_double), ("converged", ctypes.c_int)]
 
 _lib = None
 
@@ -125,4 +145,84 @@ class Rect:
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
             _lib.fp_rect_destroy(self.h)
+            self.h = None
+
+
+class Composite:
+    """ConcatPoissonSolver2D on the GPU for a tree of rectangles.
+
+    geo: any object with nx, ny, hx, hy (per domain lists), bc (4 faces per domain) and connections
+    [(a, face of a, b)] -- e.g. focalors_poisson_b200.workloads.Geometry.
+    """
+
+    def __init__(self, geo, m=20, tol=1e-8, max_iter=100, root=-1, fullfield=False):
+        nd = len(geo.nx)
+        self.nd = nd
+        self.shapes = [(int(a), int(b)) for a, b in zip(geo.nx, geo.ny)]
+        self._arr = dict(
+            nx=np.ascontiguousarray(geo.nx, dtype=np.int32), ny=np.ascontiguousarray(geo.ny, dtype=np.int32),
+            hx=np.ascontiguousarray(geo.hx, dtype=np.float64), hy=np.ascontiguousarray(geo.hy, dtype=np.float64),
+            bc=np.ascontiguousarray(np.asarray(geo.bc, dtype=np.int32).reshape(-1)),
+            conn=np.ascontiguousarray(np.asarray(geo.connections, dtype=np.int32).reshape(-1)))
+        a = self._arr
+        g = Geometry(nd, a["nx"].ctypes.data, a["ny"].ctypes.data, a["hx"].ctypes.data, a["hy"].ctypes.data,
+                     a["bc"].ctypes.data, len(geo.connections), a["conn"].ctypes.data if len(geo.connections) else None,
+                     int(root))
+        h = ctypes.c_void_p()
+        check(lib().fp_composite_create(ctypes.byref(g), int(m), float(tol), int(max_iter),
+                                        FP_GMRES_FULLFIELD if fullfield else 0, ctypes.byref(h)))
+        self.h = h
+
+    def set_parameter(self, m, tol, max_iter):
+        check(lib().fp_composite_set_parameter(self.h, int(m), float(tol), int(max_iter)))
+
+    def tree(self):
+        root = ctypes.c_int(0)
+        lv = np.zeros(self.nd, dtype=np.int32)
+        check(lib().fp_composite_tree(self.h, ctypes.byref(root), lv.ctypes.data))
+        return root.value, lv
+
+    def solve(self, fields, ghosts=None, check_convergence=False):
+        """Solves in place. fields: list of (nx, ny) float64 numpy arrays (host) or CUDA tensors (device).
+        ghosts: None or per domain a list of 4 arrays/None (Variable2D buffer values)."""
+        if len(fields) != self.nd:
+            raise ValueError("one field per domain expected")
+        keep = []
+        ptrs = []
+        flags = 0
+        stream = None
+        for f, shp in zip(fields, self.shapes):
+            if tuple(f.shape) != shp:
+                raise ValueError(f"field shape {tuple(f.shape)} != domain shape {shp}")
+            p, fl, st, k = _args(f, np.float64)
+            if not _is_torch(f) and k is not f:
+                raise TypeError("host fields must be contiguous float64 numpy arrays (solved in place)")
+            flags |= fl
+            stream = st if st is not None else stream
+            keep.append(k)
+            ptrs.append(p.value)
+        fp = (ctypes.c_void_p * self.nd)(*ptrs)
+        gp = None
+        if ghosts is not None:
+            gl = []
+            for d in range(self.nd):
+                for face in range(4):
+                    gv = None if ghosts[d] is None else ghosts[d][face]
+                    if gv is None:
+                        gl.append(None)
+                        continue
+                    p, _, _, k = _args(gv, np.float64)
+                    keep.append(k)
+                    gl.append(p.value)
+            gp = (ctypes.c_void_p * (4 * self.nd))(*gl)
+        info = SolveInfo()
+        if check_convergence:
+            flags |= FP_CHECK_CONVERGENCE
+        check(lib().fp_composite_solve_f64(self.h, fp, gp, flags, stream, ctypes.byref(info)))
+        return dict(iterations=info.gmres_iterations, restarts=info.gmres_restarts, residual=info.gmres_residual,
+                    converged=bool(info.converged))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fp_composite_destroy(self.h)
             self.h = None

@@ -14,30 +14,19 @@ thread_local std::string g_last_error;
 }
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
-template <typename F> int guarded(F&& f)
+const char* last_error() { return g_last_error.c_str(); }
+
+void require_device()
 {
-    try
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
     {
-        f();
-        g_last_error.clear();
-        return FP_OK;
-    }
-    catch (const Error& e)
-    {
-        g_last_error = e.what();
-        return e.code;
-    }
-    catch (const std::exception& e)
-    {
-        g_last_error = e.what();
-        return FP_ERR_INVALID;
-    }
-    catch (...)
-    {
-        g_last_error = "unknown error";
-        return FP_ERR_INVALID;
+        cudaGetLastError();
+        throw Error(FP_ERR_CUDA, "no CUDA device available (libfpb200 has no CPU fallback)");
     }
 }
+
 
 namespace
 {
@@ -55,17 +44,6 @@ template <typename T> std::shared_ptr<DevTransform<T>> cached_transform(int kind
     auto p     = std::make_shared<DevTransform<T>>(kind, n);
     cache[key] = p;
     return p;
-}
-
-void require_device()
-{
-    int n = 0;
-    cudaError_t e = cudaGetDeviceCount(&n);
-    if (e != cudaSuccess || n == 0)
-    {
-        cudaGetLastError();
-        throw Error(FP_ERR_CUDA, "no CUDA device available (libfpb200 has no CPU fallback)");
-    }
 }
 
 template <typename T>

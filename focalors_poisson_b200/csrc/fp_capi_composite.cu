@@ -1,0 +1,134 @@
+// C ABI (include/fp_capi.h): composite-geometry solver.
+#include "../../include/fp_capi.h"
+#include "fp_composite.h"
+
+using namespace fpb;
+
+struct fp_composite
+{
+    std::unique_ptr<Composite> c;
+    std::vector<DevBuf>        fields, ghosts;
+};
+
+namespace
+{
+std::unique_ptr<Composite> make_composite(const fp_geometry* g, int m, double tol, int max_iter, int flags)
+{
+    if (!g || g->n_domains <= 0 || !g->nx || !g->ny || !g->hx || !g->hy || !g->bc)
+        throw Error(FP_ERR_INVALID, "incomplete geometry description");
+    if (g->n_connections > 0 && !g->connections) throw Error(FP_ERR_INVALID, "null connection list");
+    std::vector<Domain> doms(g->n_domains);
+    for (int d = 0; d < g->n_domains; ++d)
+    {
+        doms[d].nx = g->nx[d];
+        doms[d].ny = g->ny[d];
+        doms[d].hx = g->hx[d];
+        doms[d].hy = g->hy[d];
+        for (int f = 0; f < 4; ++f) doms[d].bc[f] = g->bc[4 * d + f];
+    }
+    std::vector<std::array<int, 3>> conns(g->n_connections);
+    for (int k = 0; k < g->n_connections; ++k)
+        conns[k] = {g->connections[3 * k], g->connections[3 * k + 1], g->connections[3 * k + 2]};
+    const int mode = (flags & FP_GMRES_FULLFIELD) ? GMRES_FULLFIELD : GMRES_INTERFACE;
+    return std::unique_ptr<Composite>(new Composite(doms, conns, g->root, m, tol, max_iter, mode));
+}
+}  // namespace
+
+extern "C" {
+
+int fp_composite_create(const fp_geometry* g, int m, double tol, int max_iter, int flags, fp_composite** out)
+{
+    return guarded([&] {
+        if (!out) throw Error(FP_ERR_INVALID, "null output handle");
+        *out = nullptr;
+        require_device();
+        std::unique_ptr<fp_composite> h(new fp_composite());
+        h->c = make_composite(g, m, tol, max_iter, flags);
+        *out = h.release();
+    });
+}
+
+int fp_composite_set_parameter(fp_composite* c, int m, double tol, int max_iter)
+{
+    return guarded([&] {
+        if (!c) throw Error(FP_ERR_INVALID, "null solver");
+        c->c->set_parameter(m, tol, max_iter);
+    });
+}
+
+int fp_composite_solve_f64(fp_composite* c, double* const* fields, const double* const* ghosts, int flags,
+                           void* stream, fp_solve_info* info)
+{
+    GmresInfo gi;
+    int       rc = guarded([&] {
+        if (!c) throw Error(FP_ERR_INVALID, "null solver");
+        if (!fields) throw Error(FP_ERR_INVALID, "null field list");
+        cudaStream_t s    = static_cast<cudaStream_t>(stream);
+        const auto&  doms = c->c->domains();
+        const int    nd   = (int)doms.size();
+        for (int d = 0; d < nd; ++d)
+            if (!fields[d]) throw Error(FP_ERR_INVALID, "null field pointer");
+        if (flags & FP_DEVICE)
+        {
+            c->c->solve(fields, ghosts, s, &gi);
+            if (flags & FP_SYNC) FPB_CUDA(cudaStreamSynchronize(s));
+        }
+        else
+        {
+            c->fields.resize(nd);
+            c->ghosts.resize(4 * nd);
+            std::vector<double*>       dev(nd);
+            std::vector<const double*> gdev(4 * nd, nullptr);
+            for (int d = 0; d < nd; ++d)
+            {
+                const size_t bytes = doms[d].cells() * sizeof(double);
+                c->fields[d].ensure(bytes);
+                dev[d] = c->fields[d].as<double>();
+                FPB_CUDA(cudaMemcpyAsync(dev[d], fields[d], bytes, cudaMemcpyHostToDevice, s));
+                for (int f = 0; f < 4 && ghosts; ++f)
+                {
+                    if (!ghosts[4 * d + f]) continue;
+                    const size_t gb = (size_t)(f < 2 ? doms[d].ny : doms[d].nx) * sizeof(double);
+                    c->ghosts[4 * d + f].ensure(gb);
+                    FPB_CUDA(cudaMemcpyAsync(c->ghosts[4 * d + f].get(), ghosts[4 * d + f], gb, cudaMemcpyHostToDevice,
+                                             s));
+                    gdev[4 * d + f] = c->ghosts[4 * d + f].as<double>();
+                }
+            }
+            c->c->solve(dev.data(), gdev.data(), s, &gi);
+            for (int d = 0; d < nd; ++d)
+                FPB_CUDA(cudaMemcpyAsync(fields[d], dev[d], doms[d].cells() * sizeof(double), cudaMemcpyDeviceToHost,
+                                         s));
+            FPB_CUDA(cudaStreamSynchronize(s));
+        }
+        if ((flags & FP_CHECK_CONVERGENCE) && !gi.converged)
+            throw Error(FP_ERR_NOT_CONVERGED, "GMRES stopped at max_iter above tol (residual " +
+                                                  std::to_string(gi.residual) + ")");
+    });
+    if (info)
+    {
+        info->gmres_iterations = gi.iterations;
+        info->gmres_restarts   = gi.restarts;
+        info->gmres_residual   = gi.residual;
+        info->converged        = gi.converged ? 1 : 0;
+    }
+    return rc;
+}
+
+int fp_composite_tree(const fp_composite* c, int* root, int* level_of)
+{
+    return guarded([&] {
+        if (!c || !root || !level_of) throw Error(FP_ERR_INVALID, "null argument");
+        const Tree& t = c->c->tree();
+        *root         = t.root;
+        for (size_t l = 0; l < t.levels.size(); ++l)
+            for (int d : t.levels[l]) level_of[d] = (int)l;
+    });
+}
+
+int fp_composite_destroy(fp_composite* c)
+{
+    return guarded([&] { delete c; });
+}
+
+}  // extern "C"

@@ -1,0 +1,502 @@
+// Composite-geometry solve: block elimination over the domain tree with a Schur-complement GMRES at
+// every internal node, restating ConcatPoissonSolver2D::solve (pe/concat/concat_solver2d.cpp:101-157)
+// and GMRESSolver2D (pe/concat/gmres_solver2d.cpp:39-252) on device buffers.
+//
+// GMRES works either on the node's interface unknowns (default: the Krylov vectors are the values on
+// the node's faces shared with its children, y = P x, solving (I - P A^-1 S) y = P A^-1 b and finishing
+// with x = A^-1 b + A^-1 S y), or on full fields exactly like the reference. Each operator apply is
+// one rectangle solve of the node plus the children's dense Schur matrices. The orthogonalisation is
+// the reference's modified Gram-Schmidt, the small Hessenberg least-squares problem (Givens rotations,
+// back substitution) runs on the host in FP64.
+#include "fp_composite.h"
+#include "fp_ops.cuh"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <queue>
+
+namespace fpb
+{
+
+namespace
+{
+inline unsigned grid_for(long long n, int block, int cap = 4096)
+{
+    long long g = (n + block - 1) / block;
+    return (unsigned)std::max(1LL, std::min<long long>(g, cap));
+}
+
+struct PinnedHost
+{
+    double* p = nullptr;
+    explicit PinnedHost(size_t n) { FPB_CUDA(cudaMallocHost(&p, n * sizeof(double))); }
+    ~PinnedHost()
+    {
+        if (p) cudaFreeHost(p);
+    }
+};
+}  // namespace
+
+Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root)
+{
+    if (nd <= 0) throw Error(1, "geometry has no domains");
+    std::vector<std::array<int, 4>> adj(nd, {-1, -1, -1, -1});
+    for (const auto& c : conns)
+    {
+        const int a = c[0], loc = c[1], b = c[2];
+        if (a < 0 || a >= nd || b < 0 || b >= nd || a == b || loc < 0 || loc > 3)
+            throw Error(1, "invalid connection");
+        if ((adj[a][loc] != -1 && adj[a][loc] != b) || (adj[b][loc ^ 1] != -1 && adj[b][loc ^ 1] != a))
+            throw Error(1, "a face is connected twice");
+        adj[a][loc]     = b;
+        adj[b][loc ^ 1] = a;
+    }
+    // connectivity (Geometry2D::is_single_connected, geometry2d.cpp:109-163) and acyclicity
+    long long edges = 0;
+    for (int d = 0; d < nd; ++d)
+        for (int f = 0; f < 4; ++f) edges += adj[d][f] >= 0;
+    edges /= 2;
+    {
+        std::vector<int> seen(nd, 0);
+        std::queue<int>  q;
+        q.push(0);
+        seen[0] = 1;
+        while (!q.empty())
+        {
+            int u = q.front();
+            q.pop();
+            for (int f = 0; f < 4; ++f)
+                if (adj[u][f] >= 0 && !seen[adj[u][f]])
+                {
+                    seen[adj[u][f]] = 1;
+                    q.push(adj[u][f]);
+                }
+        }
+        for (int d = 0; d < nd; ++d)
+            if (!seen[d]) throw Error(1, "Geometry is not single connected");
+    }
+    if (edges != nd - 1)
+        throw Error(1, "geometry adjacency has a cycle; the domain decomposition needs a tree of subdomains");
+    Tree t;
+    if (root < 0)
+    {
+        if (nd == 1) root = 0;
+        else
+        {
+            std::vector<int> deg(nd, 0), leaves;
+            for (int d = 0; d < nd; ++d)
+            {
+                for (int f = 0; f < 4; ++f) deg[d] += adj[d][f] >= 0;
+                if (deg[d] <= 1) leaves.push_back(d);
+            }
+            int remaining = nd;
+            while (remaining > 2 && !leaves.empty())
+            {
+                remaining -= (int)leaves.size();
+                std::vector<int> next;
+                for (int lf : leaves)
+                    for (int f = 0; f < 4; ++f)
+                        if (adj[lf][f] >= 0 && --deg[adj[lf][f]] == 1) next.push_back(adj[lf][f]);
+                leaves.swap(next);
+            }
+            root = leaves.empty() ? 0 : *std::min_element(leaves.begin(), leaves.end());
+        }
+    }
+    if (root >= nd) throw Error(1, "root index out of range");
+    t.root = root;
+    t.children.assign(nd, {});
+    t.parent.assign(nd, {-1, -1});
+    std::vector<int> stack = {root}, par(nd, -2);
+    par[root]              = -1;
+    while (!stack.empty())
+    {
+        int u = stack.back();
+        stack.pop_back();
+        for (int f = 0; f < 4; ++f)
+        {
+            int v = adj[u][f];
+            if (v < 0 || v == par[u]) continue;
+            par[v] = u;
+            t.children[u].push_back({f, v});
+            t.parent[v] = {f ^ 1, u};
+            stack.push_back(v);
+        }
+    }
+    std::vector<int> frontier = {root};
+    while (!frontier.empty())
+    {
+        t.levels.push_back(frontier);
+        std::vector<int> next;
+        for (int d : frontier)
+            for (auto& c : t.children[d]) next.push_back(c.second);
+        frontier.swap(next);
+    }
+    return t;
+}
+
+Composite::Composite(const std::vector<Domain>& doms, const std::vector<std::array<int, 3>>& conns, int root, int m,
+                     double tol, int max_iter, int mode)
+    : dom_(doms), m_(m), max_iter_(max_iter), mode_(mode), tol_(tol)
+{
+    if (m < 1 || m > 200) throw Error(1, "GMRES restart length m must be in [1, 200]");
+    if (max_iter < 1) throw Error(1, "maxIter must be positive");
+    const int nd = (int)dom_.size();
+    tree_        = build_tree(nd, conns, root);
+    for (const auto& c : conns)
+    {
+        Domain &a = dom_[c[0]], &b = dom_[c[2]];
+        a.bc[c[1]]     = BC_ADJACENTED;
+        b.bc[c[1] ^ 1] = BC_ADJACENTED;
+        const bool xdir = c[1] < 2;
+        if (xdir ? (a.ny != b.ny) : (a.nx != b.nx))
+            throw Error(1, "connected domains must share the interface length");
+    }
+    rect_.resize(nd);
+    for (int d = 0; d < nd; ++d)
+        rect_[d].reset(new DevRect<double>(dom_[d].nx, dom_[d].ny, dom_[d].hx, dom_[d].hy, dom_[d].bc));
+    temp_.resize(nd);
+    for (int d = 0; d < nd; ++d)
+        if (d != tree_.root) temp_[d].alloc(dom_[d].cells() * sizeof(double));
+    node_.resize(nd);
+    for (int d = 0; d < nd; ++d)
+    {
+        Node& nd_ = node_[d];
+        int   off = 0;
+        for (auto& c : tree_.children[d])
+        {
+            Link L;
+            L.loc   = c.first;
+            L.child = c.second;
+            L.cn    = edge_length(L.loc, dom_[d].nx, dom_[d].ny);
+            L.off   = off;
+            off += L.cn;
+            nd_.kids.push_back(std::move(L));
+        }
+        if (nd_.kids.empty()) continue;
+        nd_.n_if = off;
+        nd_.n    = (mode_ == GMRES_FULLFIELD) ? dom_[d].cells() : (long long)off;
+        nd_.R.alloc(dom_[d].cells() * sizeof(double));
+    }
+    red_.alloc((kRedBlocks + 8) * sizeof(double));
+    FPB_CUDA(cudaMemset(red_.get(), 0, red_.bytes()));
+    set_parameter(m, tol, max_iter);
+    build_schur();
+}
+
+Composite::~Composite() = default;
+
+void Composite::set_parameter(int m, double tol, int max_iter)
+{
+    if (m < 1 || m > 200) throw Error(1, "GMRES restart length m must be in [1, 200]");
+    const bool rebuild = (m != m_ || tol != tol_ || max_iter != max_iter_);
+    m_                 = m;
+    tol_               = tol;
+    max_iter_          = max_iter;
+    for (auto& nd : node_)
+    {
+        if (nd.kids.empty()) continue;
+        nd.V.alloc((size_t)(m_ + 1) * nd.n * sizeof(double));
+        nd.w.alloc(nd.n * sizeof(double));
+        nd.r.alloc(nd.n * sizeof(double));
+        nd.x.alloc(nd.n * sizeof(double));
+        nd.b.alloc(nd.n * sizeof(double));
+        nd.hcol.alloc((m_ + 2) * sizeof(double));
+        nd.tmp.alloc(64 * sizeof(double) + (size_t)(m_ + 1) * sizeof(double));
+    }
+    // Nested GMRES tolerances enter the Schur matrices of internal children, so the reference rebuilds
+    // its solver map when parameters change (concat_solver2d.cpp:7-17); do the same.
+    if (rebuild)
+    {
+        bool nested = false;
+        for (int d = 0; d < (int)node_.size(); ++d)
+            if (d != tree_.root && !node_[d].kids.empty()) nested = true;
+        bool built = false;
+        for (auto& nd : node_)
+            for (auto& L : nd.kids) built |= L.S.get() != nullptr;
+        if (nested && built) build_schur();
+    }
+}
+
+double Composite::dot(const double* a, const double* b, long long n, bool sqrt_, cudaStream_t s, double* dev_out)
+{
+    double*   partials = red_.as<double>();
+    unsigned* ticket   = reinterpret_cast<unsigned*>(partials + kRedBlocks);
+    k_dot<<<grid_for(n, kRedThreads, kRedBlocks), kRedThreads, 0, s>>>(a, b, n, partials, ticket, dev_out,
+                                                                      sqrt_ ? 1 : 0);
+    FPB_CHECK_LAUNCH();
+    return 0.0;
+}
+
+void Composite::schur_apply_into(int d, const double* vec, bool vec_is_field, double* R, cudaStream_t s)
+{
+    const Domain& D = dom_[d];
+    for (const Link& L : node_[d].kids)
+    {
+        const double* v      = vec_is_field ? vec + edge_index(L.loc, D.nx, D.ny, 0) : vec + L.off;
+        long long     stride = 1;
+        if (vec_is_field && L.loc >= 2) stride = D.ny;
+        const int warps = 8;
+        k_schur_matvec<double><<<(L.cn + warps - 1) / warps, warps * 32, 0, s>>>(L.S.as<double>(), L.cn, v, stride, R,
+                                                                                D.nx, D.ny, L.loc);
+        FPB_CHECK_LAUNCH();
+    }
+}
+
+void Composite::afun(int d, const double* v, double* out, cudaStream_t s)
+{
+    Node&         N = node_[d];
+    const Domain& D = dom_[d];
+    double*       R = N.R.as<double>();
+    FPB_CUDA(cudaMemsetAsync(R, 0, D.cells() * sizeof(double), s));
+    schur_apply_into(d, v, mode_ == GMRES_FULLFIELD, R, s);
+    rect_[d]->solve(R, 1, s);
+    if (mode_ == GMRES_FULLFIELD)
+    {
+        k_sub<<<grid_for(N.n, 256), 256, 0, s>>>(out, v, R, N.n);
+        FPB_CHECK_LAUNCH();
+        return;
+    }
+    for (const Link& L : N.kids)
+    {
+        k_edge_sub<double><<<grid_for(L.cn, 128), 128, 0, s>>>(out + L.off, v + L.off, R, D.nx, D.ny, L.loc);
+        FPB_CHECK_LAUNCH();
+    }
+}
+
+void Composite::node_solve(int d, double* f, cudaStream_t s, GmresInfo* info)
+{
+    Node& N = node_[d];
+    if (N.kids.empty())
+    {
+        rect_[d]->solve(f, 1, s);
+        return;
+    }
+    const Domain& D = dom_[d];
+    const long long n = N.n;
+    const int       m = m_;
+    double *V = N.V.as<double>(), *w = N.w.as<double>(), *r = N.r.as<double>(), *x = N.x.as<double>(),
+           *b = N.b.as<double>(), *hcol = N.hcol.as<double>(), *ydev = N.tmp.as<double>();
+
+    rect_[d]->solve(f, 1, s);  // b <- A^-1 b (gmres_solver2d.cpp:130)
+    if (mode_ == GMRES_FULLFIELD)
+        FPB_CUDA(cudaMemcpyAsync(b, f, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    else
+        for (const Link& L : N.kids)
+        {
+            k_edge_gather<double><<<grid_for(L.cn, 128), 128, 0, s>>>(b + L.off, f, D.nx, D.ny, L.loc);
+            FPB_CHECK_LAUNCH();
+        }
+    FPB_CUDA(cudaMemcpyAsync(x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+
+    thread_local std::unique_ptr<PinnedHost> host;
+    if (!host || !host->p) host.reset(new PinnedHost(512));
+    double*             hbuf = host->p;
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    bool                converged = false;
+    double              last_res  = 0;
+    int                 iters = 0, restarts = 0;
+
+    for (int outer = 0; outer < max_iter_; outer++)
+    {
+        afun(d, x, w, s);
+        k_sub<<<grid_for(n, 256), 256, 0, s>>>(r, b, w, n);
+        FPB_CHECK_LAUNCH();
+        dot(r, r, n, true, s, hcol + m + 1);
+        // Convergence is judged on the reference's full-field residual (gmres_solver2d.cpp:149-160). In
+        // interface mode the iterate is x(y) = A^-1 b + A^-1 S y, whose full-field residual is
+        // A^-1 S rho(y) for the interface residual rho: one more rectangle solve per restart.
+        if (mode_ == GMRES_INTERFACE)
+        {
+            double* R = N.R.as<double>();
+            FPB_CUDA(cudaMemsetAsync(R, 0, D.cells() * sizeof(double), s));
+            schur_apply_into(d, r, false, R, s);
+            rect_[d]->solve(R, 1, s);
+            dot(R, R, D.cells(), true, s, hcol + m);
+        }
+        FPB_CUDA(cudaMemcpyAsync(hbuf, hcol + m, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        FPB_CUDA(cudaStreamSynchronize(s));
+        const double rho  = hbuf[1];
+        const double beta = (mode_ == GMRES_INTERFACE) ? hbuf[0] : rho;
+        last_res          = beta;
+        if (!std::isfinite(beta) || !std::isfinite(rho)) throw Error(5, "non-finite GMRES residual");
+        if (beta < tol_)
+        {
+            converged = true;
+            break;
+        }
+        // Arnoldi stops on the interface estimate |g_{j+1}|, scaled by the measured ratio of the two norms.
+        const double inner_tol = (mode_ == GMRES_INTERFACE && beta > 0) ? 0.5 * tol_ * (rho / beta) : tol_;
+        restarts++;
+        std::fill(H.begin(), H.end(), 0.0);
+        std::fill(cs.begin(), cs.end(), 0.0);
+        std::fill(sn.begin(), sn.end(), 0.0);
+        std::fill(g.begin(), g.end(), 0.0);
+        k_scale_inv<<<grid_for(n, 256), 256, 0, s>>>(V, r, n, hcol + m + 1);  // V0 = r / ||r||
+        FPB_CHECK_LAUNCH();
+        g[0] = rho;
+        int j = 0;
+        for (; j < m; j++)
+        {
+            double* Vj = V + (size_t)j * n;
+            afun(d, Vj, w, s);
+            for (int i = 0; i <= j; i++)  // modified Gram-Schmidt (gmres_solver2d.cpp:183-187)
+            {
+                const double* Vi = V + (size_t)i * n;
+                dot(Vi, w, n, false, s, hcol + i);
+                k_axpy_dev<<<grid_for(n, 256), 256, 0, s>>>(w, Vi, n, hcol + i, -1.0);
+                FPB_CHECK_LAUNCH();
+            }
+            dot(w, w, n, true, s, hcol + j + 1);
+            FPB_CUDA(cudaMemcpyAsync(hbuf, hcol, (j + 2) * sizeof(double), cudaMemcpyDeviceToHost, s));
+            FPB_CUDA(cudaStreamSynchronize(s));
+            for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = hbuf[i];
+            const double h_j1j = hbuf[j + 1];
+            if (!std::isfinite(h_j1j)) throw Error(5, "non-finite GMRES Arnoldi value");
+            iters++;
+            if (h_j1j < 1e-12) break;
+            H[(size_t)(j + 1) * m + j] = h_j1j;
+            k_scale_inv<<<grid_for(n, 256), 256, 0, s>>>(V + (size_t)(j + 1) * n, w, n, hcol + j + 1);
+            FPB_CHECK_LAUNCH();
+            for (int i = 0; i < j; i++)
+            {
+                const double temp          = cs[i] * H[(size_t)i * m + j] + sn[i] * H[(size_t)(i + 1) * m + j];
+                H[(size_t)(i + 1) * m + j] = -sn[i] * H[(size_t)i * m + j] + cs[i] * H[(size_t)(i + 1) * m + j];
+                H[(size_t)i * m + j]       = temp;
+            }
+            const double hjj   = H[(size_t)j * m + j];
+            const double hj1   = H[(size_t)(j + 1) * m + j];
+            const double denom = std::hypot(hjj, hj1);
+            cs[j]              = hjj / denom;
+            sn[j]              = hj1 / denom;
+            H[(size_t)j * m + j]       = cs[j] * H[(size_t)j * m + j] + sn[j] * H[(size_t)(j + 1) * m + j];
+            H[(size_t)(j + 1) * m + j] = 0.0;
+            const double temp          = cs[j] * g[j];
+            g[j + 1]                   = -sn[j] * g[j];
+            g[j]                       = temp;
+            if (std::fabs(g[j + 1]) < inner_tol)
+            {
+                j++;
+                break;
+            }
+        }
+        std::fill(y.begin(), y.end(), 0.0);
+        for (int i = j - 1; i >= 0; i--)
+        {
+            y[i] = g[i];
+            for (int k = i + 1; k < j; k++) y[i] -= H[(size_t)i * m + k] * y[k];
+            y[i] /= H[(size_t)i * m + i];
+        }
+        if (j > 0)
+        {
+            for (int i = 0; i < j; ++i) hbuf[i] = y[i];
+            FPB_CUDA(cudaMemcpyAsync(ydev, hbuf, j * sizeof(double), cudaMemcpyHostToDevice, s));
+            k_multi_axpy<<<grid_for(n, 256), 256, 0, s>>>(x, V, n, n, ydev, j);
+            FPB_CHECK_LAUNCH();
+            FPB_CUDA(cudaStreamSynchronize(s));  // hbuf is reused next iteration
+        }
+    }
+    if (mode_ == GMRES_FULLFIELD)
+    {
+        FPB_CUDA(cudaMemcpyAsync(f, x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    else
+    {
+        double* R = N.R.as<double>();
+        FPB_CUDA(cudaMemsetAsync(R, 0, D.cells() * sizeof(double), s));
+        schur_apply_into(d, x, false, R, s);
+        rect_[d]->solve(R, 1, s);
+        k_add<double><<<grid_for(D.cells(), 256), 256, 0, s>>>(f, R, D.cells());
+        FPB_CHECK_LAUNCH();
+    }
+    if (info)
+    {
+        info->iterations += iters;
+        info->restarts += restarts;
+        info->residual  = last_res;
+        info->converged = info->converged && converged;
+    }
+}
+
+void Composite::build_schur()
+{
+    cudaStream_t s = 0;
+    for (auto lv = tree_.levels.rbegin(); lv != tree_.levels.rend(); ++lv)
+        for (int d : *lv)
+            for (Link& L : node_[d].kids)
+            {
+                const int       c     = L.child;
+                const Domain&   C     = dom_[c];
+                const int       face  = L.loc ^ 1;  // child's face toward d
+                const long long cells = C.cells();
+                L.S.alloc((size_t)L.cn * L.cn * sizeof(double));
+                const bool leaf = node_[c].kids.empty();
+                long long  nb   = leaf ? std::max(1LL, std::min<long long>(L.cn, (512LL << 20) / (cells * 8))) : 1;
+                DevBuf     work((size_t)nb * cells * sizeof(double));
+                for (int i0 = 0; i0 < L.cn; i0 += (int)nb)
+                {
+                    const int cnt = (int)std::min<long long>(nb, L.cn - i0);
+                    FPB_CUDA(cudaMemsetAsync(work.get(), 0, (size_t)cnt * cells * sizeof(double), s));
+                    k_impulses<double><<<grid_for(cnt, 128), 128, 0, s>>>(work.as<double>(), C.nx, C.ny, face, i0, cnt);
+                    FPB_CHECK_LAUNCH();
+                    if (leaf) rect_[c]->solve(work.as<double>(), cnt, s);
+                    else
+                        for (int b = 0; b < cnt; ++b) node_solve(c, work.as<double>() + (size_t)b * cells, s, nullptr);
+                    k_impulse_extract<double><<<grid_for((long long)cnt * L.cn, 256), 256, 0, s>>>(
+                        work.as<double>(), C.nx, C.ny, face, L.S.as<double>(), L.cn, i0, cnt);
+                    FPB_CHECK_LAUNCH();
+                }
+                FPB_CUDA(cudaStreamSynchronize(s));
+            }
+}
+
+void Composite::solve(double* const* fields, const double* const* ghosts, cudaStream_t s, GmresInfo* info)
+{
+    const int nd = (int)dom_.size();
+    for (int d = 0; d < nd; ++d)
+    {
+        const Domain& D = dom_[d];
+        AssembleArgs  a;
+        a.nx = D.nx;
+        a.ny = D.ny;
+        a.hx = D.hx;
+        a.hy = D.hy;
+        for (int f = 0; f < 4; ++f)
+        {
+            a.bc[f]    = D.bc[f];
+            a.ghost[f] = ghosts ? ghosts[4 * d + f] : nullptr;
+        }
+        k_assemble_scale<double><<<grid_for(D.cells(), 256, 1 << 30), 256, 0, s>>>(fields[d], a);
+        FPB_CHECK_LAUNCH();
+    }
+    auto bond = [&](double* dst, int dd, int loc, const double* src, int sd) {
+        const Domain &A = dom_[dd], &B = dom_[sd];
+        k_bond_add<double><<<grid_for(edge_length(loc, A.nx, A.ny), 128), 128, 0, s>>>(dst, A.nx, A.ny, loc, -1.0, src,
+                                                                                     B.nx, B.ny);
+        FPB_CHECK_LAUNCH();
+    };
+    const auto& T = tree_;
+    for (int l = (int)T.levels.size() - 1; l >= 1; --l)
+    {
+        for (int d : T.levels[l])
+        {
+            double* td = temp_[d].as<double>();
+            FPB_CUDA(cudaMemcpyAsync(td, fields[d], dom_[d].cells() * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            for (auto& c : T.children[d])
+            {
+                bond(td, d, c.first, temp_[c.second].as<double>(), c.second);
+                bond(fields[d], d, c.first, temp_[c.second].as<double>(), c.second);
+            }
+        }
+        for (int d : T.levels[l]) node_solve(d, temp_[d].as<double>(), s, nullptr);
+    }
+    for (auto& c : T.children[T.root]) bond(fields[T.root], T.root, c.first, temp_[c.second].as<double>(), c.second);
+    node_solve(T.root, fields[T.root], s, info);
+    for (size_t l = 1; l < T.levels.size(); ++l)
+    {
+        for (int d : T.levels[l]) bond(fields[d], d, T.parent[d].first, fields[T.parent[d].second], T.parent[d].second);
+        for (int d : T.levels[l]) node_solve(d, fields[d], s, nullptr);
+    }
+}
+
+}  // namespace fpb

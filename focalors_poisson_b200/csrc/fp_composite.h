@@ -1,0 +1,93 @@
+// Composite-geometry solver: the reference's ConcatPoissonSolver2D (pe/concat/concat_solver2d.cpp)
+// with its Schur-complement GMRES (pe/concat/gmres_solver2d.cpp) on the GPU.
+#pragma once
+
+#include "fp_internal.h"
+
+#include <array>
+#include <memory>
+#include <vector>
+
+namespace fpb
+{
+
+struct Domain
+{
+    int    nx = 0, ny = 0;
+    double hx = 0, hy = 0;
+    int    bc[4]{};  // with Adjacented on connected faces
+    long long cells() const { return (long long)nx * ny; }
+};
+
+struct Tree
+{
+    int                                   root = 0;
+    std::vector<std::vector<std::pair<int, int>>> children;  // d -> [(face of d, child)]
+    std::vector<std::pair<int, int>>      parent;            // d -> (face of d toward its parent, parent)
+    std::vector<std::vector<int>>         levels;            // BFS levels, root first
+};
+
+// Geometry2D::build_tree (base/domain/geometry2d.cpp:165-176) over TreeUtils
+// (base/domain/geometry_tree.hpp:22-200). The root is the tree centre found by leaf stripping; a tie
+// between two centres goes to the lower domain index (the reference compares addresses). Children are
+// listed in face order. Throws on a disconnected or cyclic geometry.
+Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root);
+
+struct GmresInfo
+{
+    int    iterations = 0;  // Arnoldi steps over all solves of the root node
+    int    restarts   = 0;
+    double residual   = 0;  // last residual norm of the root GMRES
+    bool   converged  = true;
+};
+
+enum GmresMode : int
+{
+    GMRES_INTERFACE = 0,  // Krylov vectors on the interface unknowns (default)
+    GMRES_FULLFIELD = 1   // Krylov vectors are full fields, like the reference
+};
+
+class Composite
+{
+public:
+    Composite(const std::vector<Domain>& doms, const std::vector<std::array<int, 3>>& conns, int root, int m,
+              double tol, int max_iter, int mode);
+    ~Composite();
+    void set_parameter(int m, double tol, int max_iter);
+    // fields[d]: device pointers (nx*ny doubles) solved in place; ghosts[4*d+face]: device or null.
+    void solve(double* const* fields, const double* const* ghosts, cudaStream_t s, GmresInfo* info);
+
+    const Tree&                tree() const { return tree_; }
+    const std::vector<Domain>& domains() const { return dom_; }
+
+private:
+    struct Link
+    {
+        int    child, loc, cn, off;
+        DevBuf S;  // cn x cn, S[j*cn + i] = child response at interface cell j to an impulse at cell i
+    };
+    struct Node
+    {
+        std::vector<Link> kids;
+        int               n_if = 0;
+        long long         n    = 0;  // Krylov vector length
+        DevBuf            V, w, r, x, b, R, hcol, tmp;
+    };
+
+    void build_schur();
+    void node_solve(int d, double* f, cudaStream_t s, GmresInfo* info);
+    void afun(int d, const double* v, double* out, cudaStream_t s);
+    void schur_apply_into(int d, const double* vec, bool vec_is_field, double* R, cudaStream_t s);
+    double dot(const double* a, const double* b, long long n, bool sqrt_, cudaStream_t s, double* dev_out);
+
+    std::vector<Domain>                          dom_;
+    Tree                                         tree_;
+    int                                          m_, max_iter_, mode_;
+    double                                       tol_;
+    std::vector<std::unique_ptr<DevRect<double>>> rect_;
+    std::vector<Node>                            node_;
+    std::vector<DevBuf>                          temp_;    // per non-root domain (upward sweep temporaries)
+    DevBuf                                       red_;     // reduction scratch: partials + ticket + results
+};
+
+}  // namespace fpb

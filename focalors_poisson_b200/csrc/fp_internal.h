@@ -21,7 +21,35 @@ struct Error : std::runtime_error
     Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
-void set_last_error(const std::string& msg);
+void        set_last_error(const std::string& msg);
+const char* last_error();
+void        require_device();
+
+// Runs f, converting exceptions to an fp_status code and the thread's last-error message.
+template <typename F> int guarded(F&& f)
+{
+    try
+    {
+        f();
+        set_last_error("");
+        return 0;
+    }
+    catch (const Error& e)
+    {
+        set_last_error(e.what());
+        return e.code;
+    }
+    catch (const std::exception& e)
+    {
+        set_last_error(e.what());
+        return 1;
+    }
+    catch (...)
+    {
+        set_last_error("unknown error");
+        return 1;
+    }
+}
 
 #define FPB_CUDA(call)                                                                                   \
     do                                                                                                   \
@@ -116,7 +144,7 @@ template <typename T> struct DevRect
     double                           hx = 0, hy = 0;
     int                              bc[4]{};
     std::unique_ptr<DevTransform<T>> tr;
-    DevBuf                           ctab;  // nx*ny chase coefficients (see build_chase_tables)
+    DevBuf                           ctab;  // nx*ny chase coefficients (meaning in fp_chase.cuh)
     DevBuf                           z1, z2;  // periodic-x Sherman-Morrison vectors (nx*ny each)
     bool                             periodic_x = false;
     bool                             singular   = false;  // no Dirichlet-like face: last wavenumber singular

@@ -1,0 +1,212 @@
+// Small device operations of the composite solve: boundary assembly and h^2 scaling, interface
+// coupling (bond_add), edge gather/scatter, dense Schur matrix-vector products, deterministic BLAS-1.
+#pragma once
+
+#include "fp_common.cuh"
+
+namespace fpb
+{
+
+// Edge element k of face `loc` of an nx x ny field: XNEG row 0, XPOS row nx-1, YNEG column 0,
+// YPOS column ny-1 (field2::*_bond_add, base/field/field2.cpp:212-302).
+__host__ __device__ __forceinline__ long long edge_index(int loc, int nx, int ny, int k)
+{
+    switch (loc)
+    {
+        case 0: return k;
+        case 1: return (long long)(nx - 1) * ny + k;
+        case 2: return (long long)k * ny;
+        default: return (long long)k * ny + (ny - 1);
+    }
+}
+__host__ __device__ __forceinline__ int edge_length(int loc, int nx, int ny) { return loc < 2 ? ny : nx; }
+
+struct AssembleArgs
+{
+    int           nx, ny;
+    double        hx, hy;
+    int           bc[4];
+    const double* ghost[4];  // may be null (zero ghost values)
+};
+
+// f = (f + boundary terms) * hx^2 in the order of ConcatPoissonSolver2D::boundary_assembly
+// (pe/concat/concat_solver2d.cpp:159-223: Dirichlet faces x-,x+,y-,y+ then Neumann faces) followed by
+// the hx^2 scaling of solve() (:111-116).
+template <typename T> __global__ void k_assemble_scale(T* __restrict__ f, const AssembleArgs a)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)a.nx * a.ny) return;
+    const int i = (int)(t / a.ny), j = (int)(t % a.ny);
+    double    v = f[t];
+    const bool on[4] = {i == 0, i == a.nx - 1, j == 0, j == a.ny - 1};
+    if (on[0] || on[1] || on[2] || on[3])
+    {
+        const int    idx[4] = {j, j, i, i};
+        const double dco[4] = {-1.0 / a.hx / a.hx, -1.0 / a.hx / a.hx, -1.0 / a.hy / a.hy, -1.0 / a.hy / a.hy};
+        const double nco[4] = {1.0 / a.hx, -1.0 / a.hx, 1.0 / a.hy, -1.0 / a.hy};
+        for (int face = 0; face < 4; ++face)
+            if (on[face] && a.bc[face] == 0) v += dco[face] * (a.ghost[face] ? a.ghost[face][idx[face]] : 0.0);
+        for (int face = 0; face < 4; ++face)
+            if (on[face] && a.bc[face] == 1) v += nco[face] * (a.ghost[face] ? a.ghost[face][idx[face]] : 0.0);
+    }
+    f[t] = (T)(v * (a.hx * a.hx));
+}
+
+// dst.bond_add(loc, a, src): dst's face `loc` += a * src's opposite face (field2.cpp:257-302).
+template <typename T>
+__global__ void k_bond_add(T* __restrict__ dst, int dnx, int dny, int loc, T a, const T* __restrict__ src, int snx,
+                           int sny)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = edge_length(loc, dnx, dny);
+    if (k >= n) return;
+    const long long di = edge_index(loc, dnx, dny, k);
+    const long long si = edge_index(loc ^ 1, snx, sny, k);
+    dst[di] += a * src[si];
+}
+
+// out[k] = v[k] - field.edge(loc)[k]   (GMRES Afun: x - ft restricted to the interface)
+template <typename T>
+__global__ void k_edge_sub(T* __restrict__ out, const T* __restrict__ v, const T* __restrict__ field, int nx, int ny,
+                           int loc)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = edge_length(loc, nx, ny);
+    if (k >= n) return;
+    out[k] = v[k] + (T)-1.0 * field[edge_index(loc, nx, ny, k)];
+}
+
+// out[k] = field.edge(loc)[k]
+template <typename T>
+__global__ void k_edge_gather(T* __restrict__ out, const T* __restrict__ field, int nx, int ny, int loc)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = edge_length(loc, nx, ny);
+    if (k >= n) return;
+    out[k] = field[edge_index(loc, nx, ny, k)];
+}
+
+// field.edge(loc)[i] += sum_j S[i*cn + j] * v[j * vstride]  -- one warp per row i
+// (SchurMat2D_*::operator*, pe/concat/schur_mat2d.cpp:18-123). v may be a field edge (vstride = the
+// edge's element stride) or a contiguous interface vector (vstride = 1).
+template <typename T>
+__global__ void k_schur_matvec(const double* __restrict__ S, int cn, const T* __restrict__ v, long long vstride,
+                               T* __restrict__ field, int nx, int ny, int loc)
+{
+    const int row  = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= cn) return;
+    const double* Sr  = S + (long long)row * cn;
+    double        acc = 0.0;
+    for (int j = lane; j < cn; j += 32) acc += (double)v[j * vstride] * Sr[j];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0)
+    {
+        const long long e = edge_index(loc, nx, ny, row);
+        field[e]          = (T)((double)field[e] + acc);
+    }
+}
+
+// Impulse batch for Schur construction: fields[b] (zeroed by the caller) gets 1 at interface cell
+// i0 + b of face `loc` (SchurMat2D_*::construct, schur_mat2d.cpp:5-16).
+template <typename T> __global__ void k_impulses(T* fields, int nx, int ny, int loc, int i0, int nb)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    fields[(long long)b * nx * ny + edge_index(loc, nx, ny, i0 + b)] = (T)1;
+}
+// S[j*cn + (i0+b)] = fields[b].edge(loc)[j]
+template <typename T>
+__global__ void k_impulse_extract(const T* fields, int nx, int ny, int loc, double* S, int cn, int i0, int nb)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nb * cn) return;
+    const int b = (int)(t / cn), j = (int)(t % cn);
+    S[(long long)j * cn + i0 + b] = (double)fields[(long long)b * nx * ny + edge_index(loc, nx, ny, j)];
+}
+
+// ---------------------------------------------------------------------------------------------
+// Deterministic BLAS-1 on FP64 vectors. Reductions: fixed grid, per-block partial sums, the last
+// block (atomic ticket, no waiting) adds the partials in index order.
+// ---------------------------------------------------------------------------------------------
+constexpr int kRedBlocks  = 256;
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double s = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sh[w];
+    return s;
+}
+
+// out[0] = sum_i a[i] * b[i]  (b == a: squared norm). partials: kRedBlocks doubles; ticket: 1 uint (zero)
+__global__ void k_dot(const double* __restrict__ a, const double* __restrict__ b, long long n, double* partials,
+                      unsigned* ticket, double* out, int take_sqrt)
+{
+    __shared__ double sh[32];
+    __shared__ bool   last;
+    double            v = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        v += a[i] * b[i];
+    const double s = block_sum(v, sh);
+    if (threadIdx.x == 0)
+    {
+        partials[blockIdx.x] = s;
+        __threadfence();
+        last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0)
+    {
+        __threadfence();
+        double tot = 0;
+        for (int k = 0; k < (int)gridDim.x; ++k) tot += ((volatile double*)partials)[k];
+        *out    = take_sqrt ? sqrt(tot) : tot;
+        *ticket = 0u;
+    }
+}
+
+// y += coef * x, coef = sign * (*c)  (coefficient read from device memory)
+__global__ void k_axpy_dev(double* __restrict__ y, const double* __restrict__ x, long long n, const double* c, double sign)
+{
+    const double a = sign * (*c);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] += a * x[i];
+}
+// y = (1 / *h) * x + 0
+__global__ void k_scale_inv(double* __restrict__ y, const double* __restrict__ x, long long n, const double* h)
+{
+    const double a = 1.0 / (*h);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = 0.0 + a * x[i];
+}
+// r = b + (-1) * ax
+__global__ void k_sub(double* __restrict__ r, const double* __restrict__ b, const double* __restrict__ ax, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        r[i] = b[i] + -1.0 * ax[i];
+}
+// x += y_0 V_0 + y_1 V_1 + ... (applied in order per element, like sequential axpys)
+__global__ void k_multi_axpy(double* __restrict__ x, const double* __restrict__ V, long long ld, long long n,
+                             const double* __restrict__ y, int k)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        double v = x[i];
+        for (int q = 0; q < k; ++q) v += y[q] * V[q * ld + i];
+        x[i] = v;
+    }
+}
+// y += x (mixed precision: T field added into a double field)
+template <typename T>
+__global__ void k_add(double* __restrict__ y, const T* __restrict__ x, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] += (double)x[i];
+}
+
+}  // namespace fpb

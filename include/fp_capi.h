@@ -68,6 +68,52 @@ int fp_rect_solve_f64(fp_rect* r, double* f, long long batch, int flags, void* s
 int fp_rect_solve_f32(fp_rect* r, float* f, long long batch, int flags, void* stream);
 int fp_rect_destroy(fp_rect* r);
 
+/* ---------------------------------------------------------------------------------------------
+ * Composite geometry: Geometry2D + Variable2D + ConcatPoissonSolver2D (reference
+ * base/domain/geometry2d.h:15-59, pe/concat/concat_solver2d.h:18-56): a tree of rectangles coupled
+ * through shared faces, solved by block elimination with a Schur-complement GMRES at every internal
+ * node (pe/concat/gmres_solver2d.cpp:123-252). The Schur matrices (pe/concat/schur_mat2d.cpp:5-106)
+ * are built at creation by batched unit-impulse solves on the device.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct fp_composite fp_composite;
+
+typedef struct fp_geometry
+{
+    int           n_domains;
+    const int*    nx;          /* cells per domain along x */
+    const int*    ny;          /* cells per domain along y */
+    const double* hx;          /* grid spacing per domain */
+    const double* hy;
+    const int*    bc;          /* 4 per domain, face order; faces named by a connection become Adjacented */
+    int           n_connections;
+    const int*    connections; /* 3 per connection (a, face of a, b): Geometry2D::connect(a, face, b) */
+    int           root;        /* -1: tree centre as TreeUtils::findOptimalRoot (ties -> lower index) */
+} fp_geometry;
+
+typedef struct fp_solve_info
+{
+    int    gmres_iterations; /* Arnoldi steps of the root GMRES in this solve */
+    int    gmres_restarts;   /* restart cycles of the root GMRES */
+    double gmres_residual;   /* last residual norm / estimate of the root GMRES */
+    int    converged;        /* 1 if every GMRES met its tolerance */
+} fp_solve_info;
+
+#define FP_GMRES_FULLFIELD 4 /* create flag: Krylov vectors are full fields, as the reference */
+#define FP_CHECK_CONVERGENCE 8 /* solve flag: return FP_ERR_NOT_CONVERGED when GMRES missed tol */
+
+/* Creation builds the tree, the per-domain rectangle plans and every Schur matrix. Defaults of the
+ * reference: m = 20, tol = 1e-8, max_iter = 100 (concat_solver2d.h:48-50). */
+int fp_composite_create(const fp_geometry* g, int m, double tol, int max_iter, int flags, fp_composite** out);
+/* ConcatPoissonSolver2D::set_parameter (concat_solver2d.cpp:7-17). */
+int fp_composite_set_parameter(fp_composite* c, int m, double tol, int max_iter);
+/* ConcatPoissonSolver2D::solve: fields[d] (RHS in, solution out, in place); ghosts[4*d + face] are the
+ * Variable2D ghost buffers (NULL = zero), length ny for x faces and nx for y faces. */
+int fp_composite_solve_f64(fp_composite* c, double* const* fields, const double* const* ghosts, int flags,
+                           void* stream, fp_solve_info* info);
+/* Tree actually used: root index and BFS level of every domain (root = 0). */
+int fp_composite_tree(const fp_composite* c, int* root, int* level_of);
+int fp_composite_destroy(fp_composite* c);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,6 +10,12 @@ def load(name):
     return np.load(os.path.join(GOLDEN, name))
 
 
+def tight_outputs(name):
+    """The reference's solution of the same case driven to GMRES tol 1e-15."""
+    z = load(name)
+    return [z[f"tight_{i}"] for i in range(len(z["nx"]))]
+
+
 def composite_case(name):
     """Returns (geometry dict, rhs list, ghosts or None, outputs list, (m, tol, max_iter), root)."""
     z = load(name)
