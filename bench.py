@@ -1,0 +1,317 @@
+"""Benchmark: composite-geometry Poisson solves per second on B200 (solves/s and HBM GB/s).
+
+Workload (the BASELINE cross configuration that fits one GPU): a cross of 5 subdomains of 2048 x 2048 cells
+(centre + 4 arms), h = 1/2048, Neumann arm tips, Dirichlet elsewhere, seeded zero-mean Gaussian RHS,
+GMRES(m=20, tol=1e-12, maxIter=100) on the interface unknowns. One step = one full composite solve
+(inputs re-filled from a resident copy first, since a solve consumes its right-hand side).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (the path does not shard), one process per GPU under torchrun.
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s and HBM GB/s (% peak), FP32+IR vs FP64 at 1e-10 rel L2, 1 B200"
+N_CELLS = 2048
+GMRES = (20, 1e-12, 100)
+SEED = 2024
+
+
+def workload_config():
+    return {
+        "workload": f"cross 5x{N_CELLS}x{N_CELLS} (centre + 4 arms), h=1/{N_CELLS}, Neumann arm tips, "
+                    f"zero-mean Gaussian RHS (seed {SEED}), GMRES(m={GMRES[0]}, tol={GMRES[1]:g}, maxIter={GMRES[2]})",
+        "cells": 5 * N_CELLS * N_CELLS,
+        "l2_policy": "inputs larger than L2 (5 x 33.5 MB FP64 fields re-filled each step)",
+    }
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU reference (the reference's own sources, oracle/_ref) -- baseline leg and --impl reference
+# ------------------------------------------------------------------------------------------------
+def reference_solver(n: int, threads: int):
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import refbind as R
+    from oracle import schur_closed_form as SC
+    from focalors_poisson_b200 import workloads as W
+
+    g = W.cross(n, neumann_tips=True)
+    rhs = W.gaussian_rhs(g, SEED)
+    lx = [a * h for a, h in zip(g.nx, g.hx)]
+    ly = [b * h for b, h in zip(g.ny, g.hy)]
+    bco = [[0 if b == 3 else b for b in row] for row in g.bc]
+    # Root Schur matrices in closed form (oracle/schur_closed_form.py): the reference's own construction
+    # needs one full solve per interface cell. The timed region is the reference's unmodified solve().
+    S = SC.root_schur_matrices(g)
+    case = R.ConcatCase(g.nx, g.ny, lx, ly, g.connections, bco, *GMRES, schur=S)
+    return case, rhs
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    from oracle import refbind as R
+
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfpref.so not built (needs the reference "
+                                                               "sources at build time)"}))
+        return
+    case, rhs = reference_solver(N_CELLS, threads)
+    budget = 150.0
+    times = []
+    for _ in range(max(0, min(args.warmup, 0))):
+        case.solve(rhs)
+    t_start = time.perf_counter()
+    while len(times) < args.steps:
+        _, t = case.solve(rhs)
+        times.append(t)
+        if time.perf_counter() - t_start + t > budget:
+            break
+    total = sum(times)
+    value = len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": len(times), "steps_requested": args.steps, "warmup": 0, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference",
+                         "sample": "full solves of the same workload on the reference's own sources (FFTW r2c via "
+                                   "the project shim), OpenMP Hybrid build, each solve one step; steps capped at "
+                                   "~150 s of CPU time; warm-up skipped (CPU)"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def cpu_baseline_sample():
+    """Bounded CPU sample for the main arm: one reference solve of the same cross at 1024^2 cells per
+    subdomain, scaled to 2048^2 by the cell ratio (4x); the scaling ignores the CPU's growth in GMRES
+    work and FFT length, so it overstates the reference's speed at 2048^2."""
+    threads = os.cpu_count() or 1
+    try:
+        from oracle import refbind as R
+
+        if not R.available():
+            return {"value": None, "unit": "solves/s", "cores": threads, "kind": "reference",
+                    "sample": "unavailable: oracle/_ref/libfpref.so not built"}
+        n = N_CELLS // 2
+        case, rhs = reference_solver(n, threads)
+        _, t = case.solve(rhs)
+        scale = (N_CELLS / n) ** 2
+        return {"value": 1.0 / (t * scale), "unit": "solves/s", "cores": threads, "kind": "reference",
+                "sample": f"one reference solve of the cross at 5x{n}x{n} ({t:.2f} s), scaled x{scale:g} by cells",
+                "sample_seconds": t}
+    except Exception as e:  # the baseline leg never blocks the GPU measurement
+        return {"value": None, "unit": "solves/s", "cores": threads, "kind": "reference", "sample": f"failed: {e}"}
+
+
+# ------------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    if args.warmup < 3:
+        args.warmup = 3
+
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from focalors_poisson_b200 import capi
+    from focalors_poisson_b200 import workloads as W
+
+    g = W.cross(N_CELLS, neumann_tips=True)
+    rhs = W.gaussian_rhs(g, SEED + rank)
+    solver = capi.Composite(g, *GMRES)
+    dev = torch.device("cuda", local)
+    pristine = [torch.tensor(r, device=dev) for r in rhs]
+    work = [torch.empty_like(p) for p in pristine]
+    stream = torch.cuda.current_stream()
+
+    def step():
+        for w, p in zip(work, pristine):
+            w.copy_(p)
+        return solver.solve(work)
+
+    infos = [step() for _ in range(args.warmup)]
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    clocks = ClockSampler(local)
+    lib = capi.lib()
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = lib.fp_launch_count()
+    print(f"[bench] library launches before the timed region: {launches0}", file=sys.stderr)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        infos.append(step())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = lib.fp_launch_count() - launches0
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = args.steps * world / (t_max / 1e3)
+
+    # e2e: the same solve through the C ABI with host buffers (H2D + solve + D2H inside the timed region)
+    host = [torch.empty(p.shape, dtype=torch.float64, pin_memory=True) for p in pristine]
+    host_np = [h.numpy() for h in host]
+    e2e_times = []
+    for it in range(args.steps + 1):
+        for h, r in zip(host_np, rhs):
+            h[...] = r
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solver.solve(host_np)  # synchronous host-pointer call
+        if it > 0:
+            e2e_times.append(time.perf_counter() - t0)
+    e2e_t = sum(e2e_times)
+    if dist is not None:
+        t = torch.tensor([e2e_t], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    field_bytes = sum(int(p.numel()) * 8 for p in pristine)
+    e2e = {"value": args.steps * world / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": field_bytes,
+           "d2h_bytes_per_step": field_bytes}
+
+    # roofline of the dominant kernel: the DD y-transform of one 2048^2 FP64 subdomain
+    x = torch.randn(N_CELLS, N_CELLS, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        capi.transform(0, 0, x, out=x)
+    torch.cuda.synchronize()
+    reps = 20
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    for _ in range(reps):
+        capi.transform(0, 0, x, out=x)
+    k1.record(stream)
+    torch.cuda.synchronize()
+    t_kernel = k0.elapsed_time(k1) / reps / 1e3
+    bytes_launch = 2 * N_CELLS * N_CELLS * 8
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_launch / t_kernel / 1e9
+    roofline = {"kernel": "k_transform<double, DD> (2048x2048 rows, in place)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": f"{peak_kind} hbm_gbs", "traffic": None,
+                "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": t_kernel * 1e3}
+
+    iters = [i["iterations"] for i in infos]
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "precision_form": "FP64 drop-in (interface GMRES)",
+        "gmres_iterations_per_solve": statistics.mean(iters) if iters else None,
+        "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample()
+    if rank == 0:
+        print(json.dumps(line))
+    del solver
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -23,6 +23,7 @@ STATUS = {0: "FP_OK", 1: "FP_ERR_INVALID", 2: "FP_ERR_CUDA", 3: "FP_ERR_UNSUPPOR
 _vp, _i, _d, _ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_longlong
 SIGNATURES = {
     "fp_last_error": ([], ctypes.c_char_p),
+    "fp_launch_count": ([], ctypes.c_longlong),
     "fp_transform_f64": ([_i, _i, _i, _i, _i, _vp, _vp, _i, _vp], _i),
     "fp_transform_f32": ([_i, _i, _i, _i, _i, _vp, _vp, _i, _vp], _i),
     "fp_rect_create": ([_i, _i, _d, _d, _vp, _i, _vp], _i),

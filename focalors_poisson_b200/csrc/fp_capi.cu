@@ -2,6 +2,7 @@
 #include "../../include/fp_capi.h"
 #include "fp_internal.h"
 
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -13,6 +14,12 @@ namespace
 thread_local std::string g_last_error;
 }
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+namespace
+{
+std::atomic<long long> g_launches{0};
+}
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 const char* last_error() { return g_last_error.c_str(); }
 
@@ -109,6 +116,8 @@ void rect_solve(fp_rect* r, R* plan, T* f, long long batch, int flags, void* str
 extern "C" {
 
 const char* fp_last_error(void) { return fpb::g_last_error.c_str(); }
+
+long long fp_launch_count(void) { return fpb::g_launches.load(); }
 
 int fp_transform_f64(int bn, int bp, int nx, int ny, int inverse, const double* in, double* out, int flags,
                      void* stream)

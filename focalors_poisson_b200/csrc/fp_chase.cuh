@@ -17,14 +17,17 @@
 namespace fpb
 {
 
+// only_last: one thread per field, handling just the last wavenumber (the singular one), for use next
+// to the chunked kernels below.
 template <typename T>
 __global__ void k_chase(T* __restrict__ f, int nx, int ny, long long batch, const T* __restrict__ ctab,
-                        const T* __restrict__ z1, const T* __restrict__ z2, int periodic, int singular)
+                        const T* __restrict__ z1, const T* __restrict__ z2, int periodic, int singular,
+                        int only_last)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= batch * ny) return;
-    const int       j   = (int)(t % ny);
-    const long long b   = t / ny;
+    if (t >= (only_last ? batch : batch * ny)) return;
+    const int       j   = only_last ? ny - 1 : (int)(t % ny);
+    const long long b   = only_last ? t : t / ny;
     T*              col = f + b * (long long)nx * ny + j;
     const long long s   = ny;
 
@@ -103,6 +106,141 @@ __global__ void k_chase(T* __restrict__ f, int nx, int ny, long long batch, cons
     const T  g2 = (yl / ((T)1 + al) - y0 / a0) / (bl / ((T)1 + al) - ((T)1 + b0) / a0);
     const T  g1 = y0 / a0 - g2 * (((T)1 + b0) / a0);
     for (int i = 0; i < nx; ++i) col[i * s] = col[i * s] - g1 * __ldg(a + i * s) - g2 * __ldg(bb + i * s);
+}
+
+}  // namespace fpb
+
+namespace fpb
+{
+
+// ---------------------------------------------------------------------------------------------
+// Chunked ("partition") form of the same Thomas solve for the standard (Dirichlet / Neumann ends)
+// systems, used when nx is a multiple of kChunk. Rows are cut into P = nx / kChunk chunks; the last
+// row of every chunk is a separator. The kChunk-1 interior rows of chunk p satisfy
+//   x_int = z_p - B_{p-1} g - B_p h,   z_p = T^-1 f_int, g = T^-1 e_first, h = T^-1 e_last,
+// with B_p the separator values; the separator equations then form a tridiagonal system of size P:
+//   -g_last B_{p-1} + (d_sep - h_last - g'_first) B_p - h'_first B_{p+1} = f_sep - z_p,last - z_{p+1},first
+// (primes: next chunk). Three launches: local interior solves (parallel over chunks and wavenumbers),
+// the separator system (parallel over wavenumbers), the correction. The result equals the sequential
+// Thomas solve up to round-off; T, g, h depend only on (chunk type, wavenumber) and are tabulated.
+// Tables (type 0 = first chunk, whose first row carries the x- Neumann change; type 1 = the others),
+// each [type][r][j], r < kChunk-1: c (Thomas factors), g, h.
+// ---------------------------------------------------------------------------------------------
+constexpr int kChunk = 32;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_chase_local(T* __restrict__ f, int nx, int ny, long long batch,
+                                                     const T* __restrict__ ctab, T* __restrict__ zend, int skip_last)
+{
+    constexpr int  Li = kChunk - 1;
+    const int      P  = nx / kChunk;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= batch * P * ny) return;
+    const int       j   = (int)(t % ny);
+    if (skip_last && j == ny - 1) return;
+    const long long bp  = t / ny;
+    const int       p   = (int)(bp % P);
+    const long long b   = bp / P;
+    const int       typ = p == 0 ? 0 : 1;
+    T*              col = f + b * (long long)nx * ny + (long long)p * kChunk * ny + j;
+    const T*        c   = ctab + (long long)typ * Li * ny + j;
+    T               y[Li];
+#pragma unroll
+    for (int r = 0; r < Li; ++r) y[r] = col[(long long)r * ny];
+    T prev = 0;
+#pragma unroll
+    for (int r = 0; r < Li; ++r)
+    {
+        prev = (y[r] - prev) * __ldg(c + (long long)r * ny);
+        y[r] = prev;
+    }
+#pragma unroll
+    for (int r = Li - 2; r >= 0; --r) y[r] = y[r] - __ldg(c + (long long)r * ny) * y[r + 1];
+#pragma unroll
+    for (int r = 0; r < Li; ++r) col[(long long)r * ny] = y[r];
+    T* ze                      = zend + ((b * P + p) * 2) * (long long)ny + j;
+    ze[0]                      = y[0];
+    ze[ny]                     = y[Li - 1];
+}
+
+// Separator system per (field, wavenumber). ends: [type][4][j] = g_first, g_last, h_first, h_last.
+template <typename T>
+__global__ void k_chase_reduced(T* __restrict__ f, int nx, int ny, long long batch, const T* __restrict__ ends,
+                                const T* __restrict__ dsep, int end_neumann, const T* __restrict__ zend,
+                                T* __restrict__ bsep, T* __restrict__ work, int skip_last)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= batch * ny) return;
+    const int       j = (int)(t % ny);
+    if (skip_last && j == ny - 1) return;
+    const long long b = t / ny;
+    const int       P = nx / kChunk;
+    const T         d = dsep[j];
+    auto e = [&](int typ, int k) { return ends[((long long)typ * 4 + k) * ny + j]; };
+    const T* ze = zend + b * (long long)P * 2 * ny + j;
+    T*       cw = work + b * (long long)P * ny + j;  // Thomas factors of the separator system
+    T*       bs = bsep + b * (long long)P * ny + j;  // right-hand sides, then the solution B_p
+    T*       fb = f + b * (long long)nx * ny + j;
+    T        yprev = 0, cprev = 0;
+    for (int p = 0; p < P; ++p)
+    {
+        const int  typ   = p == 0 ? 0 : 1;
+        const bool last  = p == P - 1;
+        const T    fsep  = fb[(long long)(p * kChunk + kChunk - 1) * ny];
+        const T    lower = p > 0 ? -e(typ, 1) : (T)0;
+        T          diag  = (last && end_neumann ? d + (T)1 : d) - e(typ, 3);
+        T          rhs   = fsep - ze[(long long)(2 * p + 1) * ny];
+        if (!last)
+        {
+            diag -= e(1, 0);
+            rhs -= ze[(long long)(2 * (p + 1)) * ny];
+        }
+        const T den  = diag - lower * cprev;
+        const T up   = last ? (T)0 : -e(1, 2);
+        const T cp   = up / den;
+        yprev        = (rhs - lower * yprev) / den;
+        cw[(long long)p * ny] = cp;
+        bs[(long long)p * ny] = yprev;
+        cprev        = cp;
+    }
+    T x = bs[(long long)(P - 1) * ny];
+    fb[(long long)(nx - 1) * ny] = x;
+    for (int p = P - 2; p >= 0; --p)
+    {
+        x                                            = bs[(long long)p * ny] - cw[(long long)p * ny] * x;
+        bs[(long long)p * ny]                        = x;
+        fb[(long long)(p * kChunk + kChunk - 1) * ny] = x;
+    }
+}
+
+// x_int = z - B_{p-1} g - B_p h on the interior rows.
+template <typename T>
+__global__ void __launch_bounds__(256) k_chase_correct(T* __restrict__ f, int nx, int ny, long long batch,
+                                                       const T* __restrict__ gtab, const T* __restrict__ htab,
+                                                       const T* __restrict__ bsep, int skip_last)
+{
+    constexpr int  Li = kChunk - 1;
+    const int      P  = nx / kChunk;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= batch * P * ny) return;
+    const int       j   = (int)(t % ny);
+    if (skip_last && j == ny - 1) return;
+    const long long bp  = t / ny;
+    const int       p   = (int)(bp % P);
+    const long long b   = bp / P;
+    const int       typ = p == 0 ? 0 : 1;
+    const T*        bs  = bsep + b * (long long)P * ny + j;
+    const T         bl  = p > 0 ? bs[(long long)(p - 1) * ny] : (T)0;
+    const T         br  = bs[(long long)p * ny];
+    T*              col = f + b * (long long)nx * ny + (long long)p * kChunk * ny + j;
+    const T*        g   = gtab + (long long)typ * Li * ny + j;
+    const T*        h   = htab + (long long)typ * Li * ny + j;
+#pragma unroll 8
+    for (int r = 0; r < Li; ++r)
+    {
+        const long long o = (long long)r * ny;
+        col[o]            = col[o] - bl * __ldg(g + o) - br * __ldg(h + o);
+    }
 }
 
 }  // namespace fpb

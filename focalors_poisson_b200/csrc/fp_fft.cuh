@@ -44,10 +44,11 @@ struct FftDesc
 
 template <typename T2> struct FftTables
 {
-    const T2*  tw;     // stage twiddles
-    const T2*  chirp;  // Bluestein: c_n, n < L
-    const T2*  bhat;   // Bluestein: FFT_M(conj chirp kernel) / M, digit-reversed
-    const int* perm;   // direct: slot of input n for the DIT stages
+    const T2*   tw;      // stage twiddles
+    const T2*   chirp;   // Bluestein: c_n, n < L
+    const T2*   bhat;    // Bluestein: FFT_M(conj chirp kernel) / M, digit-reversed
+    const int*  perm;    // direct: slot of input n for the DIT stages
+    const int4* stages;  // (R, S, B, tw_off) per stage, read through the constant-like cache
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -182,13 +183,20 @@ __device__ __forceinline__ void stage_radix(T2* buf, const FftStage st, int nbf,
 }
 
 // Runs all stages (DIF order or DIT order) on buf. Ends with a barrier.
-template <bool DIT, typename T2> __device__ void fft_stages(T2* buf, const FftDesc& d, const T2* __restrict__ tw)
+template <bool DIT, typename T2>
+__device__ void fft_stages(T2* buf, const FftDesc& d, const T2* __restrict__ tw, const int4* __restrict__ stages)
 {
-    for (int s0 = 0; s0 < d.nst; ++s0)
+    const int nst = d.nst, M = d.M;
+    for (int s0 = 0; s0 < nst; ++s0)
     {
-        const int      s   = DIT ? d.nst - 1 - s0 : s0;
-        const FftStage st  = d.st[s];
-        const int      nbf = d.M / st.R;
+        const int  s = DIT ? nst - 1 - s0 : s0;
+        const int4 q = __ldg(stages + s);
+        FftStage   st;
+        st.R          = q.x;
+        st.S          = q.y;
+        st.B          = q.z;
+        st.tw_off     = q.w;
+        const int nbf = M / st.R;
         switch (st.R)
         {
             case 2: stage_radix<2, DIT>(buf, st, nbf, tw); break;
@@ -222,13 +230,13 @@ template <typename T2> __device__ void fft_execute(T2* buf, const FftDesc& d, co
     __syncthreads();
     if (!d.blue)
     {
-        fft_stages<true>(buf, d, t.tw);
+        fft_stages<true>(buf, d, t.tw, t.stages);
         return;
     }
-    fft_stages<false>(buf, d, t.tw);
+    fft_stages<false>(buf, d, t.tw, t.stages);
     for (int k = threadIdx.x; k < d.M; k += blockDim.x) buf[k] = cconj(cmul(buf[k], __ldg(t.bhat + k)));
     __syncthreads();
-    fft_stages<true>(buf, d, t.tw);
+    fft_stages<true>(buf, d, t.tw, t.stages);
 }
 
 // Spectrum value X_k, 0 <= k < L, after fft_execute.

@@ -60,7 +60,14 @@ template <typename F> int guarded(F&& f)
                                std::string(#call) + ": " + cudaGetErrorString(e_));                      \
     } while (0)
 
-#define FPB_CHECK_LAUNCH() FPB_CUDA(cudaGetLastError())
+// Every kernel launch is followed by FPB_CHECK_LAUNCH(), which also counts it (fp_launch_count()).
+void note_launch();
+#define FPB_CHECK_LAUNCH()                                                                               \
+    do                                                                                                   \
+    {                                                                                                    \
+        ::fpb::note_launch();                                                                            \
+        FPB_CUDA(cudaGetLastError());                                                                    \
+    } while (0)
 
 // Owning device allocation.
 class DevBuf
@@ -127,7 +134,7 @@ template <typename T> struct DevTransform
     typedef typename Cplx<T>::type T2;
     int     kind = 0, n = 0;
     FftDesc fd{};
-    DevBuf  tw, chirp, bhat, perm, ta, tb;
+    DevBuf  tw, chirp, bhat, perm, stages, ta, tb, tc;
     T       s1 = 0, s2 = 0;
     int     threads = 128;
     size_t  smem    = 0;
@@ -148,10 +155,18 @@ template <typename T> struct DevRect
     DevBuf                           z1, z2;  // periodic-x Sherman-Morrison vectors (nx*ny each)
     bool                             periodic_x = false;
     bool                             singular   = false;  // no Dirichlet-like face: last wavenumber singular
+    bool                             chunked    = false;  // partition chase (nx a multiple of kChunk)
+    bool                             end_neumann = false;
+    DevBuf                           cc, cg, chh, cends, dsep;  // partition chase tables
+    mutable DevBuf                   scratch;                   // partition chase scratch (per batch)
 
     DevRect(int nx, int ny, double hx, double hy, const int* bc);
     // In-place solve of `batch` back-to-back fields.
     void solve(T* f, long long batch, cudaStream_t s) const;
+    // Scratch elements the partition chase needs for `batch` fields (0 when it is not used).
+    long long chase_scratch_elems(long long batch) const;
+    // The chase alone, with caller-provided scratch of chase_scratch_elems(batch) elements.
+    void chase(T* f, long long batch, T* scratch, cudaStream_t s) const;
 };
 
 size_t max_dynamic_smem();

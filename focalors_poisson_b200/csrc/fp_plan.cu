@@ -123,12 +123,12 @@ int kind_of(int bn, int bp)
     return -1;
 }
 
-int r2c_length(int kind, int n)
+int fft_length(int kind, int n)
 {
     switch (kind)
     {
-        case K_DD: return 2 * n + 2;
-        case K_NN: return 2 * n;
+        case K_DD: return n + 1;
+        case K_NN: return n;
         case K_ND:
         case K_DN: return 2 * n + 1;
         default: return n;
@@ -194,7 +194,11 @@ KindTables kind_tables(int kind, int n)
     const double pi = kRefPi;
     switch (kind)
     {
-        case K_DD: t.s1 = std::sqrt(2.0 / (1. + n)); break;  // poisson_fft2d.cpp:22
+        case K_DD:  // poisson_fft2d.cpp:22; folding weights of the length-(n+1) DST-I
+            t.s1 = std::sqrt(2.0 / (1. + n));
+            t.c.resize(n + 1);
+            for (int j = 0; j <= n; ++j) t.c[j] = cld(std::sin(kPi * (long double)j / (long double)(n + 1)), 0.0L);
+            break;
         case K_NN:                                             // poisson_fft2d.cpp:81-90
             t.s1 = std::sqrt(2.0 / n);
             t.s2 = std::sqrt(1.0 / n);
@@ -205,6 +209,8 @@ KindTables kind_tables(int kind, int n)
                 t.a[j] = std::cos(pi * (j + 1.) / n / 2);
                 t.b[j] = std::sin(pi * (j + 1.) / n / 2);
             }
+            t.c.resize(n);  // Makhoul post-twiddle exp(-i pi m / 2n)
+            for (int m = 0; m < n; ++m) t.c[m] = root_of_unity(m, 4LL * n);
             break;
         case K_ND:  // poisson_fft2d.cpp:157-165
             t.s1 = std::sqrt(4. / (2. * n + 1.));

@@ -43,8 +43,8 @@ enum Kind : int
 };
 int kind_of(int bc_neg, int bc_pos);  // -1 if unsupported
 
-// Length of the real DFT the reference uses for each family (poisson_fft2d.cpp:19-465).
-int r2c_length(int kind, int n);
+// Length of the complex FFT each family's device transform runs (fp_transform.cuh).
+int fft_length(int kind, int n);
 
 struct HostFft
 {
@@ -66,6 +66,7 @@ struct KindTables
                                // PP: cos/sin(pi (2j+1) / 4)
     double s1 = 0, s2 = 0;     // DD: sqrt(2/(1+n)); NN: sqrt(2/n), sqrt(1/n); ND/DN: sqrt(4/(2n+1));
                                // PP: sqrt(2/n)
+    std::vector<std::complex<long double>> c;  // DD: sin(pi j/(n+1)), j <= n; NN: exp(-i pi m / 2n), m < n
 };
 KindTables kind_tables(int kind, int n);
 

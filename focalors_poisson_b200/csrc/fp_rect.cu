@@ -56,7 +56,7 @@ template <typename T> DevTransform<T>::DevTransform(int kind_, int n_) : kind(ki
 {
     if (n < 2) throw Error(1, "row length must be at least 2");
     if (kind == K_PP && (n % 2)) throw Error(1, "periodic transform needs an even length");
-    const int L = r2c_length(kind, n);
+    const int L = fft_length(kind, n);
     HostFft   h;
     try
     {
@@ -77,16 +77,21 @@ template <typename T> DevTransform<T>::DevTransform(int kind_, int n_) : kind(ki
     {
         perm = upload(h.perm);
     }
+    std::vector<int4> st(fd.nst);
+    for (int s = 0; s < fd.nst; ++s) st[s] = make_int4(fd.st[s].R, fd.st[s].S, fd.st[s].B, fd.st[s].tw_off);
+    stages        = upload(st);
     KindTables kt = kind_tables(kind, n);
     if (!kt.a.empty())
     {
         ta = upload(convert<T>(kt.a));
         tb = upload(convert<T>(kt.b));
     }
+    if (!kt.c.empty()) tc = upload(convert_c<T2>(kt.c));
     s1      = (T)kt.s1;
     s2      = (T)kt.s2;
-    threads = std::min(512, std::max(64, ((fd.M / 8 + 31) / 32) * 32));
-    smem    = (size_t)fd.M * sizeof(T2);
+    threads = std::min(512, std::max(64, ((fd.M / 16 + 31) / 32) * 32));
+    smem    = (size_t)fd.M * sizeof(T2) + (kind == K_DD ? (size_t)2 * (n / 2 + 1) * sizeof(T) : 0);
+    if (smem > max_dynamic_smem()) throw Error(3, "transform of length " + std::to_string(n) + " needs more shared memory than a CTA has");
 }
 
 template <typename T> void DevTransform<T>::run(const T* in, T* out, long long rows, bool inverse, cudaStream_t s) const
@@ -97,7 +102,8 @@ template <typename T> void DevTransform<T>::run(const T* in, T* out, long long r
     a.rows  = rows;
     a.n     = n;
     a.fd    = fd;
-    a.ft    = FftTables<T2>{tw.as<T2>(), chirp.as<T2>(), bhat.as<T2>(), perm.as<int>()};
+    a.ft    = FftTables<T2>{tw.as<T2>(), chirp.as<T2>(), bhat.as<T2>(), perm.as<int>(), stages.as<int4>()};
+    a.tc    = tc.as<T2>();
     a.ta    = ta.as<T>();
     a.tb    = tb.as<T>();
     a.s1    = s1;
@@ -169,6 +175,43 @@ void periodic_tables(int nx, int ny, const std::vector<double>& d, std::vector<d
         }
     }
 }
+// Partition-chase tables for the interior rows (kChunk-1 of them) of a chunk: [type][r][j] Thomas
+// factors c, spikes g = T^-1 e_first and h = T^-1 e_last, and [type][4][j] end values
+// (g_first, g_last, h_first, h_last). Type 0 is the first chunk (x- Neumann change on its first row).
+void partition_tables(int ny, const std::vector<double>& d, bool start_neu, std::vector<double>& c,
+                      std::vector<double>& g, std::vector<double>& h, std::vector<double>& ends)
+{
+    const int Li = kChunk - 1;
+    c.assign((size_t)2 * Li * ny, 0.0);
+    g.assign((size_t)2 * Li * ny, 0.0);
+    h.assign((size_t)2 * Li * ny, 0.0);
+    ends.assign((size_t)2 * 4 * ny, 0.0);
+    std::vector<double> cc(Li), y(Li), x(Li);
+    for (int typ = 0; typ < 2; ++typ)
+        for (int j = 0; j < ny; ++j)
+        {
+            const double dj = d[j];
+            cc[0]           = (typ == 0 && start_neu) ? 1.0 / (dj + 1.0) : 1.0 / dj;
+            for (int r = 1; r < Li; ++r) cc[r] = 1.0 / (dj - cc[r - 1]);
+            for (int r = 0; r < Li; ++r) c[((size_t)typ * Li + r) * ny + j] = cc[r];
+            for (int which = 0; which < 2; ++which)
+            {
+                double prev = 0;
+                for (int r = 0; r < Li; ++r)
+                {
+                    const double rhs = (which == 0) ? (r == 0 ? 1.0 : 0.0) : (r == Li - 1 ? 1.0 : 0.0);
+                    prev             = (rhs - prev) * cc[r];
+                    y[r]             = prev;
+                }
+                x[Li - 1] = y[Li - 1];
+                for (int r = Li - 2; r >= 0; --r) x[r] = y[r] - cc[r] * x[r + 1];
+                std::vector<double>& dst = which == 0 ? g : h;
+                for (int r = 0; r < Li; ++r) dst[((size_t)typ * Li + r) * ny + j] = x[r];
+                ends[((size_t)typ * 4 + 2 * which + 0) * ny + j] = x[0];
+                ends[((size_t)typ * 4 + 2 * which + 1) * ny + j] = x[Li - 1];
+            }
+        }
+}
 }  // namespace
 
 template <typename T> DevRect<T>::DevRect(int nx_, int ny_, double hx_, double hy_, const int* bc_)
@@ -188,7 +231,19 @@ template <typename T> DevRect<T>::DevRect(int nx_, int ny_, double hx_, double h
     std::vector<double> d = x_diag(ny, hx, hy, bc[YNEG], bc[YPOS]);
     std::vector<double> c;
     chase_table(nx, ny, d, !xp && bc[XNEG] == BC_NEUMANN, !xp && bc[XPOS] == BC_NEUMANN, c);
-    ctab = upload(convert<T>(c));
+    ctab        = upload(convert<T>(c));
+    end_neumann = !xp && bc[XPOS] == BC_NEUMANN;
+    chunked     = !xp && nx % kChunk == 0 && nx >= 2 * kChunk;
+    if (chunked)
+    {
+        std::vector<double> pc, pg, ph, pe;
+        partition_tables(ny, d, bc[XNEG] == BC_NEUMANN, pc, pg, ph, pe);
+        cc    = upload(convert<T>(pc));
+        cg    = upload(convert<T>(pg));
+        chh   = upload(convert<T>(ph));
+        cends = upload(convert<T>(pe));
+        dsep  = upload(convert<T>(d));
+    }
     if (periodic_x)
     {
         std::vector<double> a, b;
@@ -198,16 +253,54 @@ template <typename T> DevRect<T>::DevRect(int nx_, int ny_, double hx_, double h
     }
 }
 
+template <typename T> long long DevRect<T>::chase_scratch_elems(long long batch) const
+{
+    if (!chunked) return 0;
+    const long long P = nx / kChunk;
+    return batch * P * ny * 4;  // chunk end values (2), separator solution (1), separator factors (1)
+}
+
+template <typename T> void DevRect<T>::chase(T* f, long long batch, T* scr, cudaStream_t s) const
+{
+    if (!chunked)
+    {
+        const long long nthreads = batch * ny;
+        const int       block    = 128;
+        k_chase<T><<<(unsigned)((nthreads + block - 1) / block), block, 0, s>>>(
+            f, nx, ny, batch, ctab.as<T>(), z1.as<T>(), z2.as<T>(), periodic_x ? 1 : 0, singular ? 1 : 0, 0);
+        FPB_CHECK_LAUNCH();
+        return;
+    }
+    const long long P    = nx / kChunk;
+    T*              zend = scr;
+    T*              bsep = zend + batch * P * ny * 2;
+    T*              work = bsep + batch * P * ny;
+    const int       skip = singular ? 1 : 0;
+    const long long nl   = batch * P * ny;
+    k_chase_local<T><<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(f, nx, ny, batch, cc.as<T>(), zend, skip);
+    FPB_CHECK_LAUNCH();
+    const long long nr = batch * ny;
+    k_chase_reduced<T><<<(unsigned)((nr + 127) / 128), 128, 0, s>>>(f, nx, ny, batch, cends.as<T>(), dsep.as<T>(),
+                                                                   end_neumann ? 1 : 0, zend, bsep, work, skip);
+    FPB_CHECK_LAUNCH();
+    k_chase_correct<T><<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(f, nx, ny, batch, cg.as<T>(), chh.as<T>(), bsep,
+                                                                   skip);
+    FPB_CHECK_LAUNCH();
+    if (singular)
+    {
+        k_chase<T><<<(unsigned)((batch + 127) / 128), 128, 0, s>>>(f, nx, ny, batch, ctab.as<T>(), z1.as<T>(),
+                                                                  z2.as<T>(), 0, 1, 1);
+        FPB_CHECK_LAUNCH();
+    }
+}
+
 template <typename T> void DevRect<T>::solve(T* f, long long batch, cudaStream_t s) const
 {
     if (batch <= 0) return;
     tr->run(f, f, batch * nx, false, s);
-    const long long nthreads = batch * ny;
-    const int       block    = 128;
-    k_chase<T><<<(unsigned)((nthreads + block - 1) / block), block, 0, s>>>(f, nx, ny, batch, ctab.as<T>(),
-                                                                           z1.as<T>(), z2.as<T>(),
-                                                                           periodic_x ? 1 : 0, singular ? 1 : 0);
-    FPB_CHECK_LAUNCH();
+    const long long need = chase_scratch_elems(batch);
+    if (need) scratch.ensure((size_t)need * sizeof(T));
+    chase(f, batch, scratch.as<T>(), s);
     tr->run(f, f, batch * nx, true, s);
 }
 

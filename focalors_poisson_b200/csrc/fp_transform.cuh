@@ -1,13 +1,24 @@
-// y-direction transforms of the five boundary families (DD, NN, ND, DN, PP), forward and inverse,
-// for a batch of contiguous rows. Each CTA owns one complex FFT of the family's real-DFT length L
-// (2n+2, 2n, 2n+1, 2n+1, n) in shared memory. Two real sequences ride in one complex FFT:
-//   * families that need one real DFT per row (DD, DN, forward NN / ND) pack two rows,
-//   * families that need two real DFTs of the same row (inverse NN / ND, both PP directions) pack
-//     the row's two sequences,
-// and are separated afterwards with U_k = (Z_k + conj Z_{L-k})/2, V_k = (Z_k - conj Z_{L-k})/(2i).
-// Pre- and post-processing restate the reference's per-family formulas
-// (pe/poisson/poisson_fft2d.cpp:37-45, 92-133, 167-205, 232-262, 401-465) with tables computed by
-// the same double expressions (fp_plan.cu), so results agree with the reference to FFT round-off.
+// y-direction transforms of the five boundary families (DD, NN, ND, DN, PP), forward and inverse, for
+// a batch of contiguous rows. Each CTA owns one complex FFT in shared memory. The transforms are the
+// reference's PoissonFFT2D_* matrices (pe/poisson/poisson_fft2d.cpp:19-465), evaluated with the
+// shortest complex FFT each family admits:
+//
+//   DD   DST-I of n = N+1 by the odd/even folding y_j = sin(pi j/n)(x_j + x_{n-j}) + (x_j - x_{n-j})/2:
+//        X_{2k} = -Im Y_k, X_{2k+1} = X_{2k-1} + Re Y_k (a prefix sum), Y = DFT_n(y);  L = N+1
+//   NN   DCT-II by Makhoul's reordering v = (f_0, f_2, ..., f_3, f_1), C_m = Re(e^{-i pi m/2N} V_m),
+//        modes in the reference's order (mean last, others reversed and negated); the inverse is its
+//        transpose, Re(DFT(e^{-i pi m/2N} a_m)) un-reordered;  L = N
+//   ND   forward: the reference's length-(2N+1) real DFT; inverse: its transpose Re(DFT(beta p)) with
+//        beta = sin + i cos of the reference's twiddles;  L = 2N+1
+//   DN   the reference's length-(2N+1) real DFT (the family is its own transpose);  L = 2N+1
+//   PP   the reference's two length-N real DFTs of one row packed in one complex FFT;  L = N
+//
+// Two real transforms share one complex FFT: for real-input families two rows ride as z = u + i v and
+// separate as U_k = (Z_k + conj Z_{L-k})/2, V_k = (Z_k - conj Z_{L-k})/(2i); for real-output families
+// (NN and ND inverses) two Hermitian-symmetrised rows ride as z = h_a + i h_b and come out as
+// Re Z / Im Z. Every family except PP therefore costs half a complex FFT of length L per row.
+// Family tables that the reference computes itself (ND, PP twiddles) are evaluated with its own double
+// expressions (fp_plan.cu), so results agree with the reference to FFT round-off.
 #pragma once
 
 #include "fp_fft.cuh"
@@ -24,88 +35,153 @@ template <typename T> struct TransformArgs
     int           n;     // row length (ny)
     FftDesc       fd;
     FftTables<T2> ft;
-    const T*      ta;  // family table a (cos)
-    const T*      tb;  // family table b (sin)
+    const T*      ta;  // family table a (ND: cos, PP: cos)
+    const T*      tb;  // family table b (ND: sin, PP: sin)
+    const T2*     tc;  // DD: (sin(pi j/(N+1)), 0); NN: exp(-i pi m / 2N)
     T             s1, s2;
 };
 
 template <int KIND, int INV> struct FamilyTraits
 {
-    // true: one real DFT per row, two rows per FFT; false: two real DFTs of one row
-    static constexpr bool kPairRows = (KIND == 0) || (KIND == 3) || (!INV && (KIND == 1 || KIND == 2));
+    static constexpr bool kPairRows = (KIND != 4);
 };
 
 template <typename T> __device__ __forceinline__ T alt_neg_even(int j) { return (j & 1) ? (T)1 : (T)-1; }
 template <typename T> __device__ __forceinline__ T alt_pos_even(int j) { return (j & 1) ? (T)-1 : (T)1; }
 
+// Real input value u(i) of one row for the families whose FFT input is real.
 template <typename T, int KIND, int INV>
-__device__ __forceinline__ typename Cplx<T>::type build_input(const TransformArgs<T>& a, const T* fa, const T* fb, int i)
+__device__ __forceinline__ T real_input(const TransformArgs<T>& a, const T* f, int i)
+{
+    const int n = a.n;
+    if (KIND == 0)  // DD folding, n+1 = L
+    {
+        if (i == 0) return (T)0;
+        const T xj = f[i - 1], xm = f[n - i];  // x_j, x_{L-j}
+        return a.tc[i].x * (xj + xm) + (T)0.5 * (xj - xm);
+    }
+    if (KIND == 1)  // NN forward: Makhoul reordering
+        return (2 * i < n) ? f[2 * i] : f[2 * n - 1 - 2 * i];
+    // ND forward, DN: ex[j+1] = (j even ? -1 : 1) sqrt(4/(2n+1)) f_j
+    if (i >= 1 && i <= n) return (alt_neg_even<T>(i - 1) * a.s1) * f[i - 1];
+    return (T)0;
+}
+
+// Hermitian-symmetrised input h(i) of one row for the real-output families (NN / ND inverses).
+template <typename T, int KIND>
+__device__ __forceinline__ typename Cplx<T>::type herm_input(const TransformArgs<T>& a, const T* p, int i)
+{
+    typedef typename Cplx<T>::type T2;
+    const int n = a.n;
+    if (KIND == 1)  // NN inverse: c_m = w_m a_m, a_0 = sqrt(1/n) p_{n-1}, a_m = -sqrt(2/n) p_{n-1-m}
+    {
+        auto c = [&](int m) -> T2 {
+            const T am = (m == 0) ? a.s2 * p[n - 1] : -a.s1 * p[n - 1 - m];
+            const T2 w = a.tc[m];
+            return mk<T2>(w.x * am, w.y * am);
+        };
+        const T2 c1 = c(i), c2 = c((n - i) % n);
+        return mk<T2>((T)0.5 * (c1.x + c2.x), (T)0.5 * (c1.y - c2.y));
+    }
+    // ND inverse: g_t = (sin_b + i cos_b)_{t-1} p_{t-1} for 1 <= t <= n, zero elsewhere (L = 2n+1)
+    if (i == 0) return mk<T2>(0, 0);
+    if (i <= n)
+    {
+        const T p0 = p[i - 1];
+        return mk<T2>((T)0.5 * (__ldg(a.tb + i - 1) * p0), (T)0.5 * (__ldg(a.ta + i - 1) * p0));
+    }
+    const int t  = 2 * n + 1 - i;
+    const T   p0 = p[t - 1];
+    return mk<T2>((T)0.5 * (__ldg(a.tb + t - 1) * p0), (T)-0.5 * (__ldg(a.ta + t - 1) * p0));
+}
+
+// PP: the row's two real sequences (poisson_fft2d.cpp:401-447).
+template <typename T, int INV>
+__device__ __forceinline__ typename Cplx<T>::type pp_input(const TransformArgs<T>& a, const T* f, int i)
 {
     typedef typename Cplx<T>::type T2;
     const int n = a.n;
     T         u = 0, v = 0;
-    if (KIND == 0)  // DD: ex[j+1] = f_j (length 2n+2)
-    {
-        if (i >= 1 && i <= n)
-        {
-            u = fa[i - 1];
-            v = fb ? fb[i - 1] : (T)0;
-        }
-    }
-    else if (KIND == 1 && !INV)  // NN forward: ex[j+1] = (j even ? -1 : 1) f_j
-    {
-        if (i >= 1 && i <= n)
-        {
-            const T s = alt_neg_even<T>(i - 1);
-            u         = s * fa[i - 1];
-            v         = fb ? s * fb[i - 1] : (T)0;
-        }
-    }
-    else if (KIND == 1 && INV)  // NN inverse: cos(..) p_j and sin(..) p_j
-    {
-        if (i >= 1 && i <= n)
-        {
-            const T p = fa[i - 1];
-            u         = __ldg(a.ta + i - 1) * p;
-            v         = __ldg(a.tb + i - 1) * p;
-        }
-    }
-    else if ((KIND == 2 && !INV) || KIND == 3)  // ND forward, DN both: (j even ? -1 : 1) sqrt(4/(2n+1)) f_j
-    {
-        if (i >= 1 && i <= n)
-        {
-            const T s = alt_neg_even<T>(i - 1) * a.s1;
-            u         = s * fa[i - 1];
-            v         = fb ? s * fb[i - 1] : (T)0;
-        }
-    }
-    else if (KIND == 2 && INV)  // ND inverse: sqrt(4/(2n+1)) sin(..) p_j and ... cos(..) p_j
-    {
-        if (i >= 1 && i <= n)
-        {
-            const T p = fa[i - 1];
-            u         = (a.s1 * __ldg(a.tb + i - 1)) * p;
-            v         = (a.s1 * __ldg(a.ta + i - 1)) * p;
-        }
-    }
-    else if (KIND == 4 && !INV)  // PP forward: sin input [0, f_0..f_{n-2}], cos input alternating
+    if (!INV)  // sin input [0, f_0..f_{n-2}], cos input alternating from +f_0
     {
         if (i >= 1 && i <= n - 1)
         {
-            const T f = fa[i - 1];
-            u         = f;
-            v         = alt_pos_even<T>(i - 1) * f;
+            u = f[i - 1];
+            v = alt_pos_even<T>(i - 1) * f[i - 1];
         }
     }
-    else  // PP inverse: even/odd cos parts summed into u, sin parts into v (poisson_fft2d.cpp:441-447)
+    else  // even/odd cos parts summed into u, sin parts into v
     {
         const int h = n / 2;
-        if (i < h) u += __ldg(a.ta + 2 * i) * fa[2 * i];
-        if (i >= 1 && i <= h) u += __ldg(a.ta + 2 * i - 1) * fa[2 * i - 1];
-        if (i >= 1 && i <= h) v += __ldg(a.tb + 2 * (h - i)) * fa[2 * (h - i)];
-        if (i <= h - 1) v += __ldg(a.tb + 2 * (h - 1 - i) + 1) * fa[2 * (h - 1 - i) + 1];
+        if (i < h) u += __ldg(a.ta + 2 * i) * f[2 * i];
+        if (i >= 1 && i <= h) u += __ldg(a.ta + 2 * i - 1) * f[2 * i - 1];
+        if (i >= 1 && i <= h) v += __ldg(a.tb + 2 * (h - i)) * f[2 * (h - i)];
+        if (i <= h - 1) v += __ldg(a.tb + 2 * (h - 1 - i) + 1) * f[2 * (h - 1 - i) + 1];
     }
     return mk<T2>(u, v);
+}
+
+// Inclusive prefix sums of two arrays of length K in shared memory (one CTA).
+template <typename T> __device__ void block_scan2(T* xa, T* xb, int K)
+{
+    __shared__ T wa[32], wb[32];
+    const int    T_   = blockDim.x;
+    const int    chunk = (K + T_ - 1) / T_;
+    const int    lo = min(K, threadIdx.x * chunk), hi = min(K, lo + chunk);
+    T            sa = 0, sb = 0;
+    for (int k = lo; k < hi; ++k)
+    {
+        sa += xa[k];
+        sb += xb[k];
+    }
+    // inclusive scan of the per-thread sums
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T         ia = sa, ib = sb;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const T ya = __shfl_up_sync(0xffffffffu, ia, o), yb = __shfl_up_sync(0xffffffffu, ib, o);
+        if (lane >= o)
+        {
+            ia += ya;
+            ib += yb;
+        }
+    }
+    if (lane == 31)
+    {
+        wa[warp] = ia;
+        wb[warp] = ib;
+    }
+    __syncthreads();
+    if (warp == 0)
+    {
+        const int nw = (T_ + 31) / 32;
+        T         va = lane < nw ? wa[lane] : (T)0, vb = lane < nw ? wb[lane] : (T)0;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const T ya = __shfl_up_sync(0xffffffffu, va, o), yb = __shfl_up_sync(0xffffffffu, vb, o);
+            if (lane >= o)
+            {
+                va += ya;
+                vb += yb;
+            }
+        }
+        if (lane < nw)
+        {
+            wa[lane] = va;
+            wb[lane] = vb;
+        }
+    }
+    __syncthreads();
+    T oa = ia - sa + (warp > 0 ? wa[warp - 1] : (T)0);
+    T ob = ib - sb + (warp > 0 ? wb[warp - 1] : (T)0);
+    for (int k = lo; k < hi; ++k)
+    {
+        oa += xa[k];
+        ob += xb[k];
+        xa[k] = oa;
+        xb[k] = ob;
+    }
+    __syncthreads();
 }
 
 template <typename T, int KIND, int INV>
@@ -114,110 +190,131 @@ __global__ void __launch_bounds__(512) k_transform(const TransformArgs<T> a)
     typedef typename Cplx<T>::type T2;
     extern __shared__ __align__(16) unsigned char fp_smem_raw[];
     T2*          buf = reinterpret_cast<T2*>(fp_smem_raw);
-    __shared__ T red[2][32];
     __shared__ T rowsc[2];
 
     constexpr bool kPair = FamilyTraits<KIND, INV>::kPairRows;
+    constexpr bool kHerm = INV && (KIND == 1 || KIND == 2);  // real-output families
     const int      n     = a.n;
     const int      L     = a.fd.L;
     const long long r0   = kPair ? 2LL * blockIdx.x : (long long)blockIdx.x;
     if (r0 >= a.rows) return;
-    const T* fa = a.in + r0 * n;
-    const T* fb = (kPair && r0 + 1 < a.rows) ? fa + n : nullptr;
-    T*       oa = a.out + r0 * n;
-    T*       ob = (kPair && r0 + 1 < a.rows) ? oa + n : nullptr;
+    const bool has_b = kPair && r0 + 1 < a.rows;
+    const T*   fa    = a.in + r0 * n;
+    const T*   fb    = has_b ? fa + n : fa;
+    T*         oa    = a.out + r0 * n;
+    T*         ob    = has_b ? oa + n : nullptr;
 
-    // Row scalars needed after the FFT (read before any in-place write).
-    if (threadIdx.x == 0)
-    {
-        if (KIND == 4 && !INV) rowsc[0] = fa[n - 1];  // PP forward: f(i, ny-1)
-        if (KIND == 1 && INV) rowsc[0] = fa[n - 1];   // NN inverse: p_hat(i, ny-1)
-    }
-    if (KIND == 1 && !INV)  // NN forward mean slot: sum_j sqrt(1/n) f_j
-    {
-        T sa = 0, sb = 0;
-        for (int j = threadIdx.x; j < n; j += blockDim.x)
-        {
-            sa += a.s2 * fa[j];
-            if (fb) sb += a.s2 * fb[j];
-        }
-        for (int o = 16; o > 0; o >>= 1)
-        {
-            sa += __shfl_down_sync(0xffffffffu, sa, o);
-            sb += __shfl_down_sync(0xffffffffu, sb, o);
-        }
-        if ((threadIdx.x & 31) == 0)
-        {
-            red[0][threadIdx.x >> 5] = sa;
-            red[1][threadIdx.x >> 5] = sb;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0)
-        {
-            T ta = 0, tb = 0;
-            for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w)
-            {
-                ta += red[0][w];
-                tb += red[1][w];
-            }
-            rowsc[0] = ta;
-            rowsc[1] = tb;
-        }
-    }
+    if (KIND == 4 && !INV && threadIdx.x == 0) rowsc[0] = fa[n - 1];  // PP forward: f(i, ny-1)
 
     for (int i = threadIdx.x; i < a.fd.M; i += blockDim.x)
     {
-        T2 z = (i < L) ? build_input<T, KIND, INV>(a, fa, fb, i) : mk<T2>(0, 0);
+        T2 z = mk<T2>(0, 0);
+        if (i < L)
+        {
+            if (KIND == 4) z = pp_input<T, INV>(a, fa, i);
+            else if (kHerm)
+            {
+                const T2 ha = herm_input<T, KIND>(a, fa, i);
+                const T2 hb = has_b ? herm_input<T, KIND>(a, fb, i) : mk<T2>(0, 0);
+                z           = mk<T2>(ha.x - hb.y, ha.y + hb.x);  // h_a + i h_b
+            }
+            else
+            {
+                z = mk<T2>(real_input<T, KIND, INV>(a, fa, i), has_b ? real_input<T, KIND, INV>(a, fb, i) : (T)0);
+            }
+        }
         buf[fft_in_slot(a.fd, a.ft, i)] = fft_in_value(a.fd, a.ft, i, z);
     }
     fft_execute(buf, a.fd, a.ft);
 
     const T half = (T)0.5;
+    if (KIND == 0)
+    {
+        // DD: X_{2k} = -Im Y_k (k >= 1), X_{2k+1} = Re Y_0 / 2 + sum_{q=1..k} Re Y_q; out_m = s1 X_{m+1}
+        const int K  = (n + 1) / 2;  // odd outputs X_1, X_3, ...
+        T*        ca = reinterpret_cast<T*>(buf + a.fd.M);
+        T*        cb = ca + K;
+        for (int k = threadIdx.x; k <= n / 2; k += blockDim.x)
+        {
+            const T2 Zk = fft_out(buf, a.fd, a.ft, k % L);
+            const T2 Zm = fft_out(buf, a.fd, a.ft, (L - k) % L);
+            if (k < K)
+            {
+                const T sc = (k == 0) ? (T)0.5 : (T)1;
+                ca[k]      = sc * (half * (Zk.x + Zm.x));  // Re Y^a_k
+                cb[k]      = sc * (half * (Zk.y + Zm.y));  // Re Y^b_k
+            }
+            if (k >= 1 && 2 * k <= n)
+            {
+                oa[2 * k - 1] = a.s1 * (-(half * (Zk.y - Zm.y)));  // -Im Y^a_k
+                if (ob) ob[2 * k - 1] = a.s1 * (half * (Zk.x - Zm.x));  // -Im Y^b_k
+            }
+        }
+        __syncthreads();
+        block_scan2(ca, cb, K);
+        for (int k = threadIdx.x; k < K; k += blockDim.x)
+        {
+            oa[2 * k] = a.s1 * ca[k];
+            if (ob) ob[2 * k] = a.s1 * cb[k];
+        }
+        return;
+    }
+
     for (int j = threadIdx.x; j < n; j += blockDim.x)
     {
-        const int k  = j + 1;
-        const T2  Xk = fft_out(buf, a.fd, a.ft, k % L);
-        const T2  Xm = fft_out(buf, a.fd, a.ft, (L - k) % L);
-        // U = spectrum of the real part, V = spectrum of the imaginary part
-        const T Ur = half * (Xk.x + Xm.x), Ui = half * (Xk.y - Xm.y);
-        const T Vr = half * (Xk.y + Xm.y), Vi = -half * (Xk.x - Xm.x);
-        if (KIND == 0)
+        if (KIND == 1 && !INV)
         {
-            oa[j] = -a.s1 * Ui;
-            if (ob) ob[j] = -a.s1 * Vi;
-        }
-        else if (KIND == 1 && !INV)
-        {
+            // reference slot j holds mode m = n-1-j negated and scaled, the mean (m = 0) in slot n-1
+            const int m  = (j < n - 1) ? n - 1 - j : 0;
+            const T2  Zk = fft_out(buf, a.fd, a.ft, m);
+            const T2  Zm = fft_out(buf, a.fd, a.ft, (L - m) % L);
+            const T2  w  = a.tc[m];  // (cos, -sin)(pi m / 2n)
+            const T Ur = half * (Zk.x + Zm.x), Ui = half * (Zk.y - Zm.y);
+            const T Vr = half * (Zk.y + Zm.y), Vi = -half * (Zk.x - Zm.x);
+            const T Ca = w.x * Ur - w.y * Ui, Cb = w.x * Vr - w.y * Vi;  // Re(w V)
             if (j < n - 1)
             {
-                const T c = __ldg(a.ta + j), s = __ldg(a.tb + j);
-                oa[j] = a.s1 * (-c * Ui - s * Ur);
-                if (ob) ob[j] = a.s1 * (-c * Vi - s * Vr);
+                oa[j] = -a.s1 * Ca;
+                if (ob) ob[j] = -a.s1 * Cb;
             }
             else
             {
-                oa[j] = rowsc[0];
-                if (ob) ob[j] = rowsc[1];
+                oa[j] = a.s2 * Ca;
+                if (ob) ob[j] = a.s2 * Cb;
             }
         }
         else if (KIND == 1 && INV)
         {
-            oa[j] = alt_pos_even<T>(j) * a.s1 * Xk.y + (a.s1 + a.s2) * rowsc[0];
-        }
-        else if (KIND == 2 && !INV)
-        {
-            const T c = __ldg(a.ta + j), s = __ldg(a.tb + j);
-            oa[j] = s * Ur - c * Ui;
-            if (ob) ob[j] = s * Vr - c * Vi;
+            const int  m = (j & 1) ? n - 1 - (j - 1) / 2 : j / 2;
+            const T2   Z = fft_out(buf, a.fd, a.ft, m);
+            oa[j]        = Z.x;
+            if (ob) ob[j] = Z.y;
         }
         else if (KIND == 2 && INV)
         {
-            oa[j] = alt_neg_even<T>(j) * Xk.x;
+            const T2 Z = fft_out(buf, a.fd, a.ft, j + 1);
+            const T  s = alt_neg_even<T>(j) * a.s1;
+            oa[j]      = s * Z.x;
+            if (ob) ob[j] = s * Z.y;
         }
-        else if (KIND == 3)
+        else if (KIND == 2 || KIND == 3)
         {
-            oa[j] = alt_pos_even<T>(j) * Ui;
-            if (ob) ob[j] = alt_pos_even<T>(j) * Vi;
+            const int k  = j + 1;
+            const T2  Xk = fft_out(buf, a.fd, a.ft, k % L);
+            const T2  Xm = fft_out(buf, a.fd, a.ft, (L - k) % L);
+            const T   Ur = half * (Xk.x + Xm.x), Ui = half * (Xk.y - Xm.y);
+            const T   Vr = half * (Xk.y + Xm.y), Vi = -half * (Xk.x - Xm.x);
+            if (KIND == 2)
+            {
+                const T c = __ldg(a.ta + j), s = __ldg(a.tb + j);
+                oa[j]     = s * Ur - c * Ui;
+                if (ob) ob[j] = s * Vr - c * Vi;
+            }
+            else
+            {
+                oa[j] = alt_pos_even<T>(j) * Ui;
+                if (ob) ob[j] = alt_pos_even<T>(j) * Vi;
+            }
         }
         else if (KIND == 4 && !INV)
         {
@@ -237,14 +334,16 @@ __global__ void __launch_bounds__(512) k_transform(const TransformArgs<T> a)
             const T   tc = la - half * (Ck.y + Cm.y);
             oa[j]        = a.s1 * (__ldg(a.ta + j) * ts + __ldg(a.tb + j) * tc);
         }
-        else  // PP inverse
+        else if (KIND == 4)
         {
             const int h  = n / 2;
             T         fc = 0, fs = 0;
             if (j < h)
             {
-                fc = alt_neg_even<T>(j) * Ui;
-                fs = Vr;
+                const T2 Xk = fft_out(buf, a.fd, a.ft, j + 1);
+                const T2 Xm = fft_out(buf, a.fd, a.ft, (L - j - 1) % L);
+                fc          = alt_neg_even<T>(j) * (half * (Xk.y - Xm.y));
+                fs          = half * (Xk.y + Xm.y);
             }
             else if (j <= n - 2)
             {
@@ -256,8 +355,7 @@ __global__ void __launch_bounds__(512) k_transform(const TransformArgs<T> a)
             }
             else
             {
-                const T2 Y0 = fft_out(buf, a.fd, a.ft, 0);
-                fs          = Y0.y;  // Re V_0 = Im Z_0
+                fs = fft_out(buf, a.fd, a.ft, 0).y;  // Re V_0 = Im Z_0
             }
             oa[j] = a.s1 * (fc + fs);
         }

@@ -43,6 +43,9 @@ typedef enum fp_status
 /* Message for the last failing call on this thread ("" if none). */
 const char* fp_last_error(void);
 
+/* Number of CUDA kernels this library has launched in the process so far (all threads). */
+long long fp_launch_count(void);
+
 /* ---------------------------------------------------------------------------------------------
  * y-direction transforms: PoissonFFT2D_{DD,NN,ND,DN,PP}::transform / transform_transpose
  * (reference pe/poisson/poisson_fft2d.h:8-136, pe/poisson/poisson_fft2d.cpp:19-465). The family is
