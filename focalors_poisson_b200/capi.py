@@ -30,6 +30,7 @@ SIGNATURES = {
     "fp_rect_solve_f64": ([_vp, _vp, _ll, _i, _vp], _i),
     "fp_rect_solve_f32": ([_vp, _vp, _ll, _i, _vp], _i),
     "fp_rect_destroy": ([_vp], _i),
+    "fp_rect_solve_f64_noalloc": ([_vp, _vp, _ll, _vp], _i),
     "fp_composite_create": ([_vp, _i, _d, _i, _i, _vp], _i),
     "fp_composite_set_parameter": ([_vp, _i, _d, _i], _i),
     "fp_composite_solve_f64": ([_vp, _vp, _vp, _i, _vp, _vp], _i),

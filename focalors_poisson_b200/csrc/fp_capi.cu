@@ -81,13 +81,6 @@ void transform_impl(int bn, int bp, int nx, int ny, int inverse, const T* in, T*
 
 using namespace fpb;
 
-struct fp_rect
-{
-    int                             precision = FP_F64;
-    std::unique_ptr<DevRect<double>> r64;
-    std::unique_ptr<DevRect<float>>  r32;
-    DevBuf                          staging;
-};
 
 namespace fpb
 {

@@ -172,3 +172,12 @@ template <typename T> struct DevRect
 size_t max_dynamic_smem();
 
 }  // namespace fpb
+
+// Handle behind fp_rect* (include/fp_capi.h).
+struct fp_rect
+{
+    int                                    precision = 0;  // FP_F64 or FP_F32
+    std::unique_ptr<fpb::DevRect<double>> r64;
+    std::unique_ptr<fpb::DevRect<float>>  r32;
+    fpb::DevBuf                            staging;
+};

@@ -71,6 +71,17 @@ int fp_rect_solve_f64(fp_rect* r, double* f, long long batch, int flags, void* s
 int fp_rect_solve_f32(fp_rect* r, float* f, long long batch, int flags, void* stream);
 int fp_rect_destroy(fp_rect* r);
 
+/* fp_rect_solve_f64 for callers that cannot allocate device memory when they solve: code running
+ * inside a CUDA stream capture (allocation calls are not capturable) or under another allocator's
+ * memory budget. No counterpart in the reference (its solve is host-only). Same result as
+ * fp_rect_solve_f64 with FP_DEVICE: `f` is device memory, the work is queued on `stream`, nothing is
+ * allocated or freed. Its scratch is one fixed device array of 2^21 doubles (16 MiB) that every GPU
+ * loading the library holds until exit; solves needing more (4 * batch * (nx/32) * ny doubles when nx
+ * is a multiple of 32, none otherwise) are rejected with FP_ERR_UNSUPPORTED. The first call on a
+ * device looks the array's address up (do it before any stream capture); calls that overlap on the GPU
+ * share the array and race. `r` must be an FP_F64 solver. */
+int fp_rect_solve_f64_noalloc(fp_rect* r, double* f, long long batch, void* stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Composite geometry: Geometry2D + Variable2D + ConcatPoissonSolver2D (reference
  * base/domain/geometry2d.h:15-59, pe/concat/concat_solver2d.h:18-56): a tree of rectangles coupled
