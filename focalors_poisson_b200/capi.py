@@ -37,7 +37,7 @@ SIGNATURES = {
     "fp_composite_tree": ([_vp, _vp, _vp], _i),
     "fp_composite_destroy": ([_vp], _i),
 }
-FP_GMRES_FULLFIELD, FP_CHECK_CONVERGENCE = 4, 8
+FP_GMRES_FULLFIELD, FP_CHECK_CONVERGENCE, FP_NO_INTERFACE_INVERSE = 4, 8, 16
 
 
 class Geometry(ctypes.Structure):
@@ -157,7 +157,7 @@ class Composite:
     [(a, face of a, b)] -- e.g. focalors_poisson_b200.workloads.Geometry.
     """
 
-    def __init__(self, geo, m=20, tol=1e-8, max_iter=100, root=-1, fullfield=False):
+    def __init__(self, geo, m=20, tol=1e-8, max_iter=100, root=-1, fullfield=False, interface_inverse=True):
         nd = len(geo.nx)
         self.nd = nd
         self.shapes = [(int(a), int(b)) for a, b in zip(geo.nx, geo.ny)]
@@ -171,8 +171,8 @@ class Composite:
                      a["bc"].ctypes.data, len(geo.connections), a["conn"].ctypes.data if len(geo.connections) else None,
                      int(root))
         h = ctypes.c_void_p()
-        check(lib().fp_composite_create(ctypes.byref(g), int(m), float(tol), int(max_iter),
-                                        FP_GMRES_FULLFIELD if fullfield else 0, ctypes.byref(h)))
+        flags = (FP_GMRES_FULLFIELD if fullfield else 0) | (0 if interface_inverse else FP_NO_INTERFACE_INVERSE)
+        check(lib().fp_composite_create(ctypes.byref(g), int(m), float(tol), int(max_iter), flags, ctypes.byref(h)))
         self.h = h
 
     def set_parameter(self, m, tol, max_iter):

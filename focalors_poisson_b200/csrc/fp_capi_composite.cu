@@ -30,7 +30,8 @@ std::unique_ptr<Composite> make_composite(const fp_geometry* g, int m, double to
     for (int k = 0; k < g->n_connections; ++k)
         conns[k] = {g->connections[3 * k], g->connections[3 * k + 1], g->connections[3 * k + 2]};
     const int mode = (flags & FP_GMRES_FULLFIELD) ? GMRES_FULLFIELD : GMRES_INTERFACE;
-    return std::unique_ptr<Composite>(new Composite(doms, conns, g->root, m, tol, max_iter, mode));
+    return std::unique_ptr<Composite>(
+        new Composite(doms, conns, g->root, m, tol, max_iter, mode, (flags & FP_NO_INTERFACE_INVERSE) == 0));
 }
 }  // namespace
 

@@ -11,6 +11,8 @@
 #include "fp_composite.h"
 #include "fp_ops.cuh"
 
+#include <cublas_v2.h>
+
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -136,8 +138,8 @@ Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root)
 }
 
 Composite::Composite(const std::vector<Domain>& doms, const std::vector<std::array<int, 3>>& conns, int root, int m,
-                     double tol, int max_iter, int mode)
-    : dom_(doms), m_(m), max_iter_(max_iter), mode_(mode), tol_(tol)
+                     double tol, int max_iter, int mode, bool interface_inverse)
+    : dom_(doms), m_(m), max_iter_(max_iter), mode_(mode), want_inverse_(interface_inverse), tol_(tol)
 {
     if (m < 1 || m > 200) throw Error(1, "GMRES restart length m must be in [1, 200]");
     if (max_iter < 1) throw Error(1, "maxIter must be positive");
@@ -182,6 +184,9 @@ Composite::Composite(const std::vector<Domain>& doms, const std::vector<std::arr
     FPB_CUDA(cudaMemset(red_.get(), 0, red_.bytes()));
     set_parameter(m, tol, max_iter);
     build_schur();
+    if (want_inverse_ && mode_ == GMRES_INTERFACE)
+        for (int d = 0; d < nd; ++d)
+            if (!node_[d].kids.empty() && node_[d].n_if <= kMaxInverse) build_interface_inverse(d);
 }
 
 Composite::~Composite() = default;
@@ -288,6 +293,8 @@ void Composite::node_solve(int d, double* f, cudaStream_t s, GmresInfo* info)
             FPB_CHECK_LAUNCH();
         }
     FPB_CUDA(cudaMemcpyAsync(x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+
+    if (N.has_inv && refine_with_inverse(d, f, s, info)) return;
 
     thread_local std::unique_ptr<PinnedHost> host;
     if (!host || !host->p) host.reset(new PinnedHost(512));
@@ -416,6 +423,159 @@ void Composite::node_solve(int d, double* f, cudaStream_t s, GmresInfo* info)
         info->residual  = last_res;
         info->converged = info->converged && converged;
     }
+}
+
+namespace
+{
+struct Cublas
+{
+    cublasHandle_t h = nullptr;
+    Cublas()
+    {
+        if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) throw Error(2, "cublasCreate failed");
+    }
+    ~Cublas()
+    {
+        if (h) cublasDestroy(h);
+    }
+    // C = A B for row-major n x n matrices (column-major view: C^T = B^T A^T)
+    void gemm(const double* A, const double* B, double* C, int n)
+    {
+        const double one = 1.0, zero = 0.0;
+        if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, B, n, A, n, &zero, C, n) != CUBLAS_STATUS_SUCCESS)
+            throw Error(2, "cublasDgemm failed");
+    }
+};
+}  // namespace
+
+// Dense interface operator M = I - P A^-1 E S of node d (column c = response on all of d's interface
+// cells to the c-th Schur column placed on its edge, one batched rectangle solve per block of columns)
+// and its inverse by the Newton-Schulz iteration X <- X (2I - M X), X_0 = M^T / (|M|_1 |M|_inf), which
+// converges for any nonsingular M. Only GEMMs (cuBLAS) and small kernels.
+void Composite::build_interface_inverse(int d)
+{
+    Node&           N     = node_[d];
+    const Domain&   D     = dom_[d];
+    const int       n     = N.n_if;
+    const long long cells = D.cells();
+    cudaStream_t    s     = 0;
+    DevBuf          M((size_t)n * n * sizeof(double)), X((size_t)n * n * sizeof(double)), P((size_t)n * n * sizeof(double));
+    const long long nb    = std::max(1LL, std::min<long long>(n, (512LL << 20) / (cells * 8)));
+    DevBuf          work((size_t)nb * cells * sizeof(double));
+    for (const Link& L : N.kids)
+        for (int c0 = 0; c0 < L.cn; c0 += (int)nb)
+        {
+            const int cnt = (int)std::min<long long>(nb, L.cn - c0);
+            FPB_CUDA(cudaMemsetAsync(work.get(), 0, (size_t)cnt * cells * sizeof(double), s));
+            k_edge_scatter_col<<<grid_for((long long)cnt * L.cn, 256), 256, 0, s>>>(
+                work.as<double>(), cells, D.nx, D.ny, L.loc, L.S.as<double>(), L.cn, c0, cnt);
+            FPB_CHECK_LAUNCH();
+            rect_[d]->solve(work.as<double>(), cnt, s);
+            for (const Link& Lo : N.kids)
+            {
+                k_edge_gather_col<<<grid_for((long long)cnt * Lo.cn, 256), 256, 0, s>>>(
+                    M.as<double>(), n, Lo.off, work.as<double>(), cells, D.nx, D.ny, Lo.loc, Lo.cn, L.off + c0, cnt);
+                FPB_CHECK_LAUNCH();
+            }
+        }
+    const long long nn = (long long)n * n;
+    k_identity_minus<<<grid_for(nn, 256, 1 << 30), 256, 0, s>>>(M.as<double>(), n);
+    FPB_CHECK_LAUNCH();
+    DevBuf sums(2 * (size_t)n * sizeof(double));
+    k_abs_sums<<<grid_for(n, 128), 128, 0, s>>>(M.as<double>(), n, sums.as<double>(), sums.as<double>() + n);
+    FPB_CHECK_LAUNCH();
+    std::vector<double> hs(2 * (size_t)n);
+    FPB_CUDA(cudaMemcpy(hs.data(), sums.get(), hs.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    const double ninf = *std::max_element(hs.begin(), hs.begin() + n);
+    const double n1   = *std::max_element(hs.begin() + n, hs.end());
+    if (!(ninf > 0) || !std::isfinite(ninf * n1)) throw Error(5, "interface operator is zero or not finite");
+    k_scaled_transpose<<<grid_for(nn, 256, 1 << 30), 256, 0, s>>>(X.as<double>(), M.as<double>(), n, 1.0 / (ninf * n1));
+    FPB_CHECK_LAUNCH();
+    Cublas    cb;
+    double*   partials = red_.as<double>();
+    unsigned* ticket   = reinterpret_cast<unsigned*>(partials + kRedBlocks);
+    double*   out      = partials + kRedBlocks + 2;
+    double    prev     = 1e300;
+    bool      ok       = false;
+    work.release();
+    DevBuf Xn((size_t)n * n * sizeof(double));
+    for (int it = 0; it < 200; ++it)
+    {
+        cb.gemm(M.as<double>(), X.as<double>(), P.as<double>(), n);  // P = M X
+        k_identity_residual<<<kRedBlocks, kRedThreads, 0, s>>>(P.as<double>(), n, partials, ticket, out);
+        FPB_CHECK_LAUNCH();
+        double err2 = 0;
+        FPB_CUDA(cudaMemcpy(&err2, out, sizeof(double), cudaMemcpyDeviceToHost));
+        const double err = std::sqrt(err2);  // ||I - M X||_F
+        if (!std::isfinite(err)) break;
+        if (err < 1e-13 * std::sqrt((double)n) || (err < 1e-6 && err > 0.5 * prev))
+        {
+            ok = err < 1e-6;  // converged, or stalled at round-off
+            break;
+        }
+        prev = err;
+        k_two_identity_minus<<<grid_for(nn, 256, 1 << 30), 256, 0, s>>>(P.as<double>(), n);  // P = 2I - M X
+        FPB_CHECK_LAUNCH();
+        cb.gemm(X.as<double>(), P.as<double>(), Xn.as<double>(), n);  // X <- X (2I - M X)
+        std::swap(X, Xn);
+    }
+    FPB_CUDA(cudaDeviceSynchronize());
+    if (ok)
+    {
+        N.X       = std::move(X);
+        N.Z.alloc(cells * sizeof(double));
+        N.has_inv = true;
+    }
+}
+
+// Interface solve with the precomputed inverse X of M = I - P A^-1 S, judged by the reference's test:
+// y = X g; Z = A^-1 S y; interface residual rho = g - M y = g - y + P Z; accept when the full-field
+// residual |A^-1 S rho| < tol, otherwise y += X rho and repeat (at most 4 times). On success
+// f = A^-1 b + Z. Returns false (f untouched beyond b = A^-1 b) if it did not converge; the caller then
+// runs GMRES from scratch.
+bool Composite::refine_with_inverse(int d, double* f, cudaStream_t s, GmresInfo* info)
+{
+    Node&         N = node_[d];
+    const Domain& D = dom_[d];
+    const int     n = N.n_if;
+    double *g = N.b.as<double>(), *y = N.x.as<double>(), *rho = N.r.as<double>(), *Z = N.Z.as<double>(),
+           *R = N.R.as<double>(), *hcol = N.hcol.as<double>();
+    const int warps = 8;
+    k_dense_matvec<<<(n + warps - 1) / warps, warps * 32, 0, s>>>(N.X.as<double>(), n, g, y, 0);
+    FPB_CHECK_LAUNCH();
+    double beta = 0;
+    for (int it = 0; it < 4; ++it)
+    {
+        FPB_CUDA(cudaMemsetAsync(Z, 0, D.cells() * sizeof(double), s));
+        schur_apply_into(d, y, false, Z, s);
+        rect_[d]->solve(Z, 1, s);
+        for (const Link& L : N.kids)
+        {
+            k_interface_residual<<<grid_for(L.cn, 128), 128, 0, s>>>(rho + L.off, g + L.off, y + L.off, Z, D.nx, D.ny,
+                                                                   L.loc, L.cn);
+            FPB_CHECK_LAUNCH();
+        }
+        FPB_CUDA(cudaMemsetAsync(R, 0, D.cells() * sizeof(double), s));
+        schur_apply_into(d, rho, false, R, s);
+        rect_[d]->solve(R, 1, s);
+        dot(R, R, D.cells(), true, s, hcol);
+        FPB_CUDA(cudaMemcpyAsync(&beta, hcol, sizeof(double), cudaMemcpyDeviceToHost, s));
+        FPB_CUDA(cudaStreamSynchronize(s));
+        if (!std::isfinite(beta)) break;
+        if (info) info->iterations += 1;
+        if (beta < tol_)
+        {
+            k_add<double><<<grid_for(D.cells(), 256), 256, 0, s>>>(f, Z, D.cells());
+            FPB_CHECK_LAUNCH();
+            if (info) info->residual = beta;
+            return true;
+        }
+        k_dense_matvec<<<(n + warps - 1) / warps, warps * 32, 0, s>>>(N.X.as<double>(), n, rho, y, 1);
+        FPB_CHECK_LAUNCH();
+    }
+    // not converged: restart plain GMRES from the gathered right-hand side
+    FPB_CUDA(cudaMemcpyAsync(y, g, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    return false;
 }
 
 void Composite::build_schur()

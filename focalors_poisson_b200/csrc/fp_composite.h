@@ -50,8 +50,11 @@ enum GmresMode : int
 class Composite
 {
 public:
+    // interface_inverse: build the inverse of each node's dense interface operator I - P A^-1 S at
+    // creation and use it to precondition the interface GMRES (interface mode, n_if <= kMaxInverse).
     Composite(const std::vector<Domain>& doms, const std::vector<std::array<int, 3>>& conns, int root, int m,
-              double tol, int max_iter, int mode);
+              double tol, int max_iter, int mode, bool interface_inverse = true);
+    static constexpr int kMaxInverse = 16384;
     ~Composite();
     void set_parameter(int m, double tol, int max_iter);
     // fields[d]: device pointers (nx*ny doubles) solved in place; ghosts[4*d+face]: device or null.
@@ -72,9 +75,13 @@ private:
         int               n_if = 0;
         long long         n    = 0;  // Krylov vector length
         DevBuf            V, w, r, x, b, R, hcol, tmp;
+        DevBuf            X, Z;  // interface inverse (n_if x n_if) and A^-1 S y workspace
+        bool              has_inv = false;
     };
 
     void build_schur();
+    void build_interface_inverse(int d);
+    bool refine_with_inverse(int d, double* f, cudaStream_t s, GmresInfo* info);
     void node_solve(int d, double* f, cudaStream_t s, GmresInfo* info);
     void afun(int d, const double* v, double* out, cudaStream_t s);
     void schur_apply_into(int d, const double* vec, bool vec_is_field, double* R, cudaStream_t s);
@@ -83,6 +90,7 @@ private:
     std::vector<Domain>                          dom_;
     Tree                                         tree_;
     int                                          m_, max_iter_, mode_;
+    bool                                         want_inverse_ = true;
     double                                       tol_;
     std::vector<std::unique_ptr<DevRect<double>>> rect_;
     std::vector<Node>                            node_;

@@ -210,3 +210,117 @@ __global__ void k_add(double* __restrict__ y, const T* __restrict__ x, long long
 }
 
 }  // namespace fpb
+
+namespace fpb
+{
+// ---------------------------------------------------------------------------------------------
+// Dense interface operator and its inverse (preconditioner of the interface GMRES)
+// ---------------------------------------------------------------------------------------------
+// fields[b].edge(loc)[q] = S[q*cn + c0 + b]: column c0+b of a child's Schur matrix placed on the edge
+__global__ void k_edge_scatter_col(double* fields, long long cells, int nx, int ny, int loc, const double* S, int cn,
+                                   int c0, int nb)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nb * cn) return;
+    const int b = (int)(t / cn), q = (int)(t % cn);
+    fields[b * cells + edge_index(loc, nx, ny, q)] = S[(long long)q * cn + c0 + b];
+}
+// K[(off+q)*ld + c0 + b] = fields[b].edge(loc)[q]
+__global__ void k_edge_gather_col(double* K, long long ld, int off, const double* fields, long long cells, int nx,
+                                  int ny, int loc, int cn, int c0, int nb)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nb * cn) return;
+    const int b = (int)(t / cn), q = (int)(t % cn);
+    K[(long long)(off + q) * ld + c0 + b] = fields[b * cells + edge_index(loc, nx, ny, q)];
+}
+// A = I - A (n x n)
+__global__ void k_identity_minus(double* A, int n)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * n) return;
+    const long long i = t / n, j = t % n;
+    A[t]              = (i == j ? 1.0 : 0.0) - A[t];
+}
+// A = 2I - A (n x n)
+__global__ void k_two_identity_minus(double* A, int n)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * n) return;
+    const long long i = t / n, j = t % n;
+    A[t]              = (i == j ? 2.0 : 0.0) - A[t];
+}
+// X = s * M^T (row-major n x n)
+__global__ void k_scaled_transpose(double* X, const double* M, int n, double s)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * n) return;
+    const long long i = t / n, j = t % n;
+    X[t]              = s * M[j * n + i];
+}
+// rowsum[i] = sum_j |A[i][j]| and colsum[j] = sum_i |A[i][j]| (one thread per row / column)
+__global__ void k_abs_sums(const double* A, int n, double* rowsum, double* colsum)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    double r = 0, c = 0;
+    for (int k = 0; k < n; ++k)
+    {
+        r += fabs(A[(long long)t * n + k]);
+        c += fabs(A[(long long)k * n + t]);
+    }
+    rowsum[t] = r;
+    colsum[t] = c;
+}
+// out[0] = sum_{ij} (I - P)_{ij}^2 (deterministic: per-block partials, last block adds them in order)
+__global__ void k_identity_residual(const double* __restrict__ P, int n, double* partials, unsigned* ticket,
+                                    double* out)
+{
+    __shared__ double sh[32];
+    __shared__ bool   last;
+    double            v     = 0;
+    const long long   total = (long long)n * n;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x)
+    {
+        const double e = ((t / n) == (t % n) ? 1.0 : 0.0) - P[t];
+        v += e * e;
+    }
+    const double s = block_sum(v, sh);
+    if (threadIdx.x == 0)
+    {
+        partials[blockIdx.x] = s;
+        __threadfence();
+        last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0)
+    {
+        __threadfence();
+        double tot = 0;
+        for (int k = 0; k < (int)gridDim.x; ++k) tot += ((volatile double*)partials)[k];
+        *out    = tot;
+        *ticket = 0u;
+    }
+}
+// y (+)= X g, row-major n x n, one warp per row
+__global__ void k_dense_matvec(const double* __restrict__ X, int n, const double* __restrict__ g,
+                               double* __restrict__ y, int accumulate)
+{
+    const int row  = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const double* Xr  = X + (long long)row * n;
+    double        acc = 0.0;
+    for (int j = lane; j < n; j += 32) acc += Xr[j] * g[j];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) y[row] = accumulate ? y[row] + acc : acc;
+}
+// r = g - y + field.edge(loc)   on one child's interface block
+__global__ void k_interface_residual(double* r, const double* g, const double* y, const double* field, int nx, int ny,
+                                     int loc, int cn)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cn) return;
+    r[k] = g[k] - y[k] + field[edge_index(loc, nx, ny, k)];
+}
+}  // namespace fpb

@@ -114,6 +114,11 @@ typedef struct fp_solve_info
 
 #define FP_GMRES_FULLFIELD 4 /* create flag: Krylov vectors are full fields, as the reference */
 #define FP_CHECK_CONVERGENCE 8 /* solve flag: return FP_ERR_NOT_CONVERGED when GMRES missed tol */
+/* create flag: do not build the interface inverse. By default every internal node with at most 16384
+ * interface cells gets the inverse of its dense interface operator I - P A^-1 S (batched rectangle
+ * solves + Newton-Schulz on the device at creation); a solve then starts from y = X g and refines while
+ * the reference's full-field residual test fails, falling back to plain GMRES. */
+#define FP_NO_INTERFACE_INVERSE 16
 
 /* Creation builds the tree, the per-domain rectangle plans and every Schur matrix. Defaults of the
  * reference: m = 20, tol = 1e-8, max_iter = 100 (concat_solver2d.h:48-50). */

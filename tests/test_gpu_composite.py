@@ -30,14 +30,15 @@ def test_composite_golden_fullfield(name):
 
 
 @pytest.mark.parametrize("name", COMPOSITE_CASES)
-def test_composite_golden_interface(name):
+@pytest.mark.parametrize("inverse", [True, False])
+def test_composite_golden_interface(name, inverse):
     """Interface Krylov vectors (the default) converge along a different path under the reference's own
     full-field stopping test. Driven to tol 1e-15 they agree with the reference driven to 1e-15 within
     1e-12; at the case's tol they stay within the reference's own distance from that converged answer."""
     geo, rhs, ghosts, outs, (m, tol, it), root = composite_case(name)
     tight = tight_outputs(name)
     own_err = rel_l2(outs, tight)
-    solver = capi.Composite(geometry(geo), m, 1e-15, it, root=root)
+    solver = capi.Composite(geometry(geo), m, 1e-15, it, root=root, interface_inverse=inverse)
     fields = [np.array(r, dtype=np.float64, copy=True) for r in rhs]
     solver.solve(fields, ghosts)  # 1e-15 is below the round-off floor of some cases: both stop at max_iter
     assert rel_l2(fields, tight) <= 1e-12, name
