@@ -30,7 +30,7 @@ struct FftStage
     int R;       // radix
     int S;       // span between butterfly legs
     int B;       // block size this stage works in (= R * S)
-    int tw_off;  // twiddles for this stage: tw[tw_off + b*R + q] = exp(-2 pi i b q / B)
+    int tw_off;  // twiddles for this stage: tw[tw_off + b] = exp(-2 pi i b / B); leg q uses its q-th power
 };
 
 struct FftDesc
@@ -154,6 +154,8 @@ template <int R, typename T2> __device__ __forceinline__ void dft(T2* x)
     else dft8(x);
 }
 
+// Leg q of butterfly b is rotated by w^q, w = exp(-2 pi i b / B): one table load per butterfly, the
+// powers by repeated multiplication (w^2 = w w, w^3 = w^2 w, ...; at most 7 products, a few ulp).
 template <int R, bool DIT, typename T2>
 __device__ __forceinline__ void stage_radix(T2* buf, const FftStage st, int nbf, const T2* __restrict__ tw)
 {
@@ -162,20 +164,31 @@ __device__ __forceinline__ void stage_radix(T2* buf, const FftStage st, int nbf,
         const int blk = t / st.S;
         const int b   = t - blk * st.S;
         T2*       p   = buf + blk * st.B + b;
-        const T2* w   = tw + st.tw_off + b * R;
         T2        x[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) x[q] = p[q * st.S];
-        if (DIT)
+        const bool rot = b != 0;
+        T2         w1  = rot ? __ldg(tw + st.tw_off + b) : mk<T2>(1, 0);
+        if (DIT && rot)
         {
+            T2 wq = w1;
 #pragma unroll
-            for (int q = 1; q < R; ++q) x[q] = cmul(x[q], __ldg(w + q));
+            for (int q = 1; q < R; ++q)
+            {
+                x[q] = cmul(x[q], wq);
+                wq   = cmul(wq, w1);
+            }
         }
         dft<R>(x);
-        if (!DIT)
+        if (!DIT && rot)
         {
+            T2 wq = w1;
 #pragma unroll
-            for (int q = 1; q < R; ++q) x[q] = cmul(x[q], __ldg(w + q));
+            for (int q = 1; q < R; ++q)
+            {
+                x[q] = cmul(x[q], wq);
+                wq   = cmul(wq, w1);
+            }
         }
 #pragma unroll
         for (int q = 0; q < R; ++q) p[q * st.S] = x[q];

@@ -106,8 +106,7 @@ void build_stages(FftDesc& d, const std::vector<int>& rad, std::vector<cld>& tw)
         d.st[s].S      = S;
         d.st[s].B      = B;
         d.st[s].tw_off = (int)tw.size();
-        for (int b = 0; b < S; ++b)
-            for (int q = 0; q < R; ++q) tw.push_back(root_of_unity((long long)b * q, B));
+        for (int b = 0; b < S; ++b) tw.push_back(root_of_unity(b, B));
         B = S;
     }
 }

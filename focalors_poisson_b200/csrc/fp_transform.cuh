@@ -232,7 +232,8 @@ __global__ void __launch_bounds__(512) k_transform(const TransformArgs<T> a)
     {
         // DD: X_{2k} = -Im Y_k (k >= 1), X_{2k+1} = Re Y_0 / 2 + sum_{q=1..k} Re Y_q; out_m = s1 X_{m+1}
         const int K  = (n + 1) / 2;  // odd outputs X_1, X_3, ...
-        T*        ca = reinterpret_cast<T*>(buf + a.fd.M);
+        // scan arrays: the unused tail [L, M) of a Bluestein buffer when it is long enough, else past M
+        T*        ca = reinterpret_cast<T*>(buf + ((a.fd.M - L >= K) ? L : a.fd.M));
         T*        cb = ca + K;
         for (int k = threadIdx.x; k <= n / 2; k += blockDim.x)
         {
