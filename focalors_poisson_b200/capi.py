@@ -34,10 +34,12 @@ SIGNATURES = {
     "fp_composite_create": ([_vp, _i, _d, _i, _i, _vp], _i),
     "fp_composite_set_parameter": ([_vp, _i, _d, _i], _i),
     "fp_composite_solve_f64": ([_vp, _vp, _vp, _i, _vp, _vp], _i),
+    "fp_composite_solve_f32ir": ([_vp, _vp, _vp, _i, _vp, _d, _i, _vp], _i),
+    "fp_composite_residual": ([_vp, _vp, _vp, _vp, _vp, _vp], _i),
     "fp_composite_tree": ([_vp, _vp, _vp], _i),
     "fp_composite_destroy": ([_vp], _i),
 }
-FP_GMRES_FULLFIELD, FP_CHECK_CONVERGENCE, FP_NO_INTERFACE_INVERSE = 4, 8, 16
+FP_GMRES_FULLFIELD, FP_CHECK_CONVERGENCE, FP_NO_INTERFACE_INVERSE, FP_IR_INNER_F64 = 4, 8, 16, 32
 
 
 class Geometry(ctypes.Structure):
@@ -51,7 +53,8 @@ class SolveInfo(ctypes.Structure):
     """struct fp_solve_info"""
 
     _fields_ = [("gmres_iterations", ctypes.c_int), ("gmres_restarts", ctypes.c_int),
-                ("gmres_residual", ctypes.c_double), ("converged", ctypes.c_int)]
+                ("gmres_residual", ctypes.c_double), ("converged", ctypes.c_int), ("refinements", ctypes.c_int),
+                ("rel_change", ctypes.c_double)]
 
 _lib = None
 
@@ -184,15 +187,10 @@ class Composite:
         check(lib().fp_composite_tree(self.h, ctypes.byref(root), lv.ctypes.data))
         return root.value, lv
 
-    def solve(self, fields, ghosts=None, check_convergence=False):
-        """Solves in place. fields: list of (nx, ny) float64 numpy arrays (host) or CUDA tensors (device).
-        ghosts: None or per domain a list of 4 arrays/None (Variable2D buffer values)."""
+    def _pointers(self, fields, ghosts):
         if len(fields) != self.nd:
             raise ValueError("one field per domain expected")
-        keep = []
-        ptrs = []
-        flags = 0
-        stream = None
+        keep, ptrs, flags, stream = [], [], 0, None
         for f, shp in zip(fields, self.shapes):
             if tuple(f.shape) != shp:
                 raise ValueError(f"field shape {tuple(f.shape)} != domain shape {shp}")
@@ -217,12 +215,43 @@ class Composite:
                     keep.append(k)
                     gl.append(p.value)
             gp = (ctypes.c_void_p * (4 * self.nd))(*gl)
+        return fp, gp, flags, stream, keep
+
+    @staticmethod
+    def _info(info):
+        return dict(iterations=info.gmres_iterations, restarts=info.gmres_restarts, residual=info.gmres_residual,
+                    converged=bool(info.converged), refinements=info.refinements, rel_change=info.rel_change)
+
+    def solve(self, fields, ghosts=None, check_convergence=False):
+        """ConcatPoissonSolver2D::solve in place. fields: list of (nx, ny) float64 numpy arrays (host) or CUDA
+        tensors (device). ghosts: None or per domain a list of 4 arrays/None (Variable2D buffer values)."""
+        fp, gp, flags, stream, keep = self._pointers(fields, ghosts)
         info = SolveInfo()
         if check_convergence:
             flags |= FP_CHECK_CONVERGENCE
         check(lib().fp_composite_solve_f64(self.h, fp, gp, flags, stream, ctypes.byref(info)))
-        return dict(iterations=info.gmres_iterations, restarts=info.gmres_restarts, residual=info.gmres_residual,
-                    converged=bool(info.converged))
+        return self._info(info)
+
+    def solve_ir(self, fields, ghosts=None, rel_tol=1e-12, max_refine=10, check_convergence=False, inner="f32"):
+        """The same solve by inner solves (FP32 transforms, or FP64 with inner="f64") wrapped in FP64
+        iterative refinement on the composite operator."""
+        fp, gp, flags, stream, keep = self._pointers(fields, ghosts)
+        info = SolveInfo()
+        if check_convergence:
+            flags |= FP_CHECK_CONVERGENCE
+        if inner == "f64":
+            flags |= FP_IR_INNER_F64
+        check(lib().fp_composite_solve_f32ir(self.h, fp, gp, flags, stream, float(rel_tol), int(max_refine),
+                                             ctypes.byref(info)))
+        return self._info(info)
+
+    def residual(self, u, rhs, ghosts=None):
+        """|fs - A u| / |fs| for device tensors u (solution) and rhs (unassembled right-hand side)."""
+        up, gp, _, stream, keep = self._pointers(u, ghosts)
+        rp, _, _, _, keep2 = self._pointers(rhs, None)
+        out = ctypes.c_double(0.0)
+        check(lib().fp_composite_residual(self.h, up, rp, gp, stream, ctypes.byref(out)))
+        return out.value
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

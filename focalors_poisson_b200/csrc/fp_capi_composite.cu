@@ -35,6 +35,62 @@ std::unique_ptr<Composite> make_composite(const fp_geometry* g, int m, double to
 }
 }  // namespace
 
+namespace
+{
+// Stages host or device fields, runs `body` on device pointers, copies results back for host calls.
+template <typename F>
+void with_device_fields(fp_composite* c, double* const* fields, const double* const* ghosts, int flags,
+                        cudaStream_t s, F&& body)
+{
+    if (!c) throw Error(FP_ERR_INVALID, "null solver");
+    if (!fields) throw Error(FP_ERR_INVALID, "null field list");
+    const auto& doms = c->c->domains();
+    const int   nd   = (int)doms.size();
+    for (int d = 0; d < nd; ++d)
+        if (!fields[d]) throw Error(FP_ERR_INVALID, "null field pointer");
+    if (flags & FP_DEVICE)
+    {
+        body(fields, ghosts);
+        if (flags & FP_SYNC) FPB_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    c->fields.resize(nd);
+    c->ghosts.resize(4 * nd);
+    std::vector<double*>       dev(nd);
+    std::vector<const double*> gdev(4 * nd, nullptr);
+    for (int d = 0; d < nd; ++d)
+    {
+        const size_t bytes = doms[d].cells() * sizeof(double);
+        c->fields[d].ensure(bytes);
+        dev[d] = c->fields[d].as<double>();
+        FPB_CUDA(cudaMemcpyAsync(dev[d], fields[d], bytes, cudaMemcpyHostToDevice, s));
+        for (int f = 0; f < 4 && ghosts; ++f)
+        {
+            if (!ghosts[4 * d + f]) continue;
+            const size_t gb = (size_t)(f < 2 ? doms[d].ny : doms[d].nx) * sizeof(double);
+            c->ghosts[4 * d + f].ensure(gb);
+            FPB_CUDA(cudaMemcpyAsync(c->ghosts[4 * d + f].get(), ghosts[4 * d + f], gb, cudaMemcpyHostToDevice, s));
+            gdev[4 * d + f] = c->ghosts[4 * d + f].as<double>();
+        }
+    }
+    body(dev.data(), gdev.data());
+    for (int d = 0; d < nd; ++d)
+        FPB_CUDA(cudaMemcpyAsync(fields[d], dev[d], doms[d].cells() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    FPB_CUDA(cudaStreamSynchronize(s));
+}
+
+void fill_info(fp_solve_info* info, const GmresInfo& gi, int refinements, double change)
+{
+    if (!info) return;
+    info->gmres_iterations = gi.iterations;
+    info->gmres_restarts   = gi.restarts;
+    info->gmres_residual   = gi.residual;
+    info->converged        = gi.converged ? 1 : 0;
+    info->refinements      = refinements;
+    info->rel_change       = change;
+}
+}  // namespace
+
 extern "C" {
 
 int fp_composite_create(const fp_geometry* g, int m, double tol, int max_iter, int flags, fp_composite** out)
@@ -62,58 +118,44 @@ int fp_composite_solve_f64(fp_composite* c, double* const* fields, const double*
 {
     GmresInfo gi;
     int       rc = guarded([&] {
-        if (!c) throw Error(FP_ERR_INVALID, "null solver");
-        if (!fields) throw Error(FP_ERR_INVALID, "null field list");
-        cudaStream_t s    = static_cast<cudaStream_t>(stream);
-        const auto&  doms = c->c->domains();
-        const int    nd   = (int)doms.size();
-        for (int d = 0; d < nd; ++d)
-            if (!fields[d]) throw Error(FP_ERR_INVALID, "null field pointer");
-        if (flags & FP_DEVICE)
-        {
-            c->c->solve(fields, ghosts, s, &gi);
-            if (flags & FP_SYNC) FPB_CUDA(cudaStreamSynchronize(s));
-        }
-        else
-        {
-            c->fields.resize(nd);
-            c->ghosts.resize(4 * nd);
-            std::vector<double*>       dev(nd);
-            std::vector<const double*> gdev(4 * nd, nullptr);
-            for (int d = 0; d < nd; ++d)
-            {
-                const size_t bytes = doms[d].cells() * sizeof(double);
-                c->fields[d].ensure(bytes);
-                dev[d] = c->fields[d].as<double>();
-                FPB_CUDA(cudaMemcpyAsync(dev[d], fields[d], bytes, cudaMemcpyHostToDevice, s));
-                for (int f = 0; f < 4 && ghosts; ++f)
-                {
-                    if (!ghosts[4 * d + f]) continue;
-                    const size_t gb = (size_t)(f < 2 ? doms[d].ny : doms[d].nx) * sizeof(double);
-                    c->ghosts[4 * d + f].ensure(gb);
-                    FPB_CUDA(cudaMemcpyAsync(c->ghosts[4 * d + f].get(), ghosts[4 * d + f], gb, cudaMemcpyHostToDevice,
-                                             s));
-                    gdev[4 * d + f] = c->ghosts[4 * d + f].as<double>();
-                }
-            }
-            c->c->solve(dev.data(), gdev.data(), s, &gi);
-            for (int d = 0; d < nd; ++d)
-                FPB_CUDA(cudaMemcpyAsync(fields[d], dev[d], doms[d].cells() * sizeof(double), cudaMemcpyDeviceToHost,
-                                         s));
-            FPB_CUDA(cudaStreamSynchronize(s));
-        }
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        with_device_fields(c, fields, ghosts, flags, s,
+                           [&](double* const* f, const double* const* g) { c->c->solve(f, g, s, &gi); });
         if ((flags & FP_CHECK_CONVERGENCE) && !gi.converged)
             throw Error(FP_ERR_NOT_CONVERGED, "GMRES stopped at max_iter above tol (residual " +
                                                   std::to_string(gi.residual) + ")");
     });
-    if (info)
-    {
-        info->gmres_iterations = gi.iterations;
-        info->gmres_restarts   = gi.restarts;
-        info->gmres_residual   = gi.residual;
-        info->converged        = gi.converged ? 1 : 0;
-    }
+    fill_info(info, gi, 0, 0.0);
     return rc;
+}
+
+int fp_composite_solve_f32ir(fp_composite* c, double* const* fields, const double* const* ghosts, int flags,
+                             void* stream, double rel_tol, int max_refine, fp_solve_info* info)
+{
+    GmresInfo gi;
+    int       steps  = 0;
+    double    change = 0;
+    int       rc     = guarded([&] {
+        if (!(rel_tol > 0) || max_refine < 1) throw Error(FP_ERR_INVALID, "rel_tol must be > 0 and max_refine >= 1");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        with_device_fields(c, fields, ghosts, flags, s, [&](double* const* f, const double* const* g) {
+            steps = c->c->solve_ir(f, g, s, rel_tol, max_refine, &change, &gi, (flags & FP_IR_INNER_F64) == 0);
+        });
+        if ((flags & FP_CHECK_CONVERGENCE) && steps >= max_refine && !(change <= rel_tol))
+            throw Error(FP_ERR_NOT_CONVERGED, "iterative refinement stopped at max_refine (relative change " +
+                                                  std::to_string(change) + ")");
+    });
+    fill_info(info, gi, steps, change);
+    return rc;
+}
+
+int fp_composite_residual(fp_composite* c, const double* const* u, const double* const* rhs,
+                          const double* const* ghosts, void* stream, double* rel_residual)
+{
+    return guarded([&] {
+        if (!c || !u || !rhs || !rel_residual) throw Error(FP_ERR_INVALID, "null argument");
+        *rel_residual = c->c->residual_norm(u, rhs, ghosts, static_cast<cudaStream_t>(stream));
+    });
 }
 
 int fp_composite_tree(const fp_composite* c, int* root, int* level_of)

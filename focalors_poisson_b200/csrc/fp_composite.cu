@@ -248,6 +248,12 @@ void Composite::schur_apply_into(int d, const double* vec, bool vec_is_field, do
     }
 }
 
+void Composite::rect_solve(int d, double* f, long long batch, cudaStream_t s) const
+{
+    if (mixed_) rect_[d]->solve_mixed(f, batch, s);
+    else rect_[d]->solve(f, batch, s);
+}
+
 void Composite::afun(int d, const double* v, double* out, cudaStream_t s)
 {
     Node&         N = node_[d];
@@ -274,7 +280,29 @@ void Composite::node_solve(int d, double* f, cudaStream_t s, GmresInfo* info)
     Node& N = node_[d];
     if (N.kids.empty())
     {
-        rect_[d]->solve(f, 1, s);
+        rect_solve(d, f, 1, s);
+        return;
+    }
+    if (mixed_ && N.has_inv)
+    {
+        // inner solve of iterative refinement: y = X g, f = A^-1 b + A^-1 S y, no residual test
+        const Domain& D = dom_[d];
+        double *g = N.b.as<double>(), *y = N.x.as<double>(), *Z = N.Z.as<double>();
+        rect_solve(d, f, 1, s);
+        for (const Link& L : N.kids)
+        {
+            k_edge_gather<double><<<grid_for(L.cn, 128), 128, 0, s>>>(g + L.off, f, D.nx, D.ny, L.loc);
+            FPB_CHECK_LAUNCH();
+        }
+        const int warps = 8;
+        k_dense_matvec<<<(N.n_if + warps - 1) / warps, warps * 32, 0, s>>>(N.X.as<double>(), N.n_if, g, y, 0);
+        FPB_CHECK_LAUNCH();
+        FPB_CUDA(cudaMemsetAsync(Z, 0, D.cells() * sizeof(double), s));
+        schur_apply_into(d, y, false, Z, s);
+        rect_solve(d, Z, 1, s);
+        k_add<double><<<grid_for(D.cells(), 256), 256, 0, s>>>(f, Z, D.cells());
+        FPB_CHECK_LAUNCH();
+        if (info) info->iterations += 1;
         return;
     }
     const Domain& D = dom_[d];
@@ -543,8 +571,8 @@ bool Composite::refine_with_inverse(int d, double* f, cudaStream_t s, GmresInfo*
     const int warps = 8;
     k_dense_matvec<<<(n + warps - 1) / warps, warps * 32, 0, s>>>(N.X.as<double>(), n, g, y, 0);
     FPB_CHECK_LAUNCH();
-    double beta = 0;
-    for (int it = 0; it < 4; ++it)
+    double beta = 0, prev = 1e300;
+    for (int it = 0; it < 6; ++it)
     {
         FPB_CUDA(cudaMemsetAsync(Z, 0, D.cells() * sizeof(double), s));
         schur_apply_into(d, y, false, Z, s);
@@ -563,13 +591,21 @@ bool Composite::refine_with_inverse(int d, double* f, cudaStream_t s, GmresInfo*
         FPB_CUDA(cudaStreamSynchronize(s));
         if (!std::isfinite(beta)) break;
         if (info) info->iterations += 1;
-        if (beta < tol_)
+        // accept below tol; also accept (reported as not converged) once refinement stops gaining, which
+        // happens only when tol is below the round-off floor of the problem
+        const bool stalled = it > 0 && beta > 0.5 * prev;
+        if (beta < tol_ || stalled)
         {
             k_add<double><<<grid_for(D.cells(), 256), 256, 0, s>>>(f, Z, D.cells());
             FPB_CHECK_LAUNCH();
-            if (info) info->residual = beta;
+            if (info)
+            {
+                info->residual  = beta;
+                info->converged = info->converged && beta < tol_;
+            }
             return true;
         }
+        prev = beta;
         k_dense_matvec<<<(n + warps - 1) / warps, warps * 32, 0, s>>>(N.X.as<double>(), n, rho, y, 1);
         FPB_CHECK_LAUNCH();
     }
@@ -612,6 +648,13 @@ void Composite::build_schur()
 
 void Composite::solve(double* const* fields, const double* const* ghosts, cudaStream_t s, GmresInfo* info)
 {
+    mixed_ = false;
+    assemble(fields, ghosts, s);
+    eliminate(fields, s, info);
+}
+
+void Composite::assemble(double* const* fields, const double* const* ghosts, cudaStream_t s)
+{
     const int nd = (int)dom_.size();
     for (int d = 0; d < nd; ++d)
     {
@@ -629,6 +672,10 @@ void Composite::solve(double* const* fields, const double* const* ghosts, cudaSt
         k_assemble_scale<double><<<grid_for(D.cells(), 256, 1 << 30), 256, 0, s>>>(fields[d], a);
         FPB_CHECK_LAUNCH();
     }
+}
+
+void Composite::eliminate(double* const* fields, cudaStream_t s, GmresInfo* info)
+{
     auto bond = [&](double* dst, int dd, int loc, const double* src, int sd) {
         const Domain &A = dom_[dd], &B = dom_[sd];
         k_bond_add<double><<<grid_for(edge_length(loc, A.nx, A.ny), 128), 128, 0, s>>>(dst, A.nx, A.ny, loc, -1.0, src,
@@ -657,6 +704,144 @@ void Composite::solve(double* const* fields, const double* const* ghosts, cudaSt
         for (int d : T.levels[l]) bond(fields[d], d, T.parent[d].first, fields[T.parent[d].second], T.parent[d].second);
         for (int d : T.levels[l]) node_solve(d, fields[d], s, nullptr);
     }
+}
+
+int Composite::solve_ir(double* const* fields, const double* const* ghosts, cudaStream_t s, double rel_tol,
+                        int max_refine, double* rel_change, GmresInfo* info, bool inner_fp32)
+{
+    const int nd = (int)dom_.size();
+    ensure_ir_workspace();
+    mixed_ = false;
+    assemble(fields, ghosts, s);
+    for (int d = 0; d < nd; ++d)
+    {
+        FPB_CUDA(cudaMemcpyAsync(fs_[d].get(), fields[d], dom_[d].cells() * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        FPB_CUDA(cudaMemsetAsync(u_[d].get(), 0, dom_[d].cells() * sizeof(double), s));
+    }
+    std::vector<double> hs(2 * (size_t)nd);
+    double              change = 1.0;
+    int                 steps  = 0;
+    for (; steps < max_refine;)
+    {
+        mixed_ = inner_fp32;
+        eliminate(fields, s, info);  // fields: residual in, correction out
+        mixed_ = false;
+        ++steps;
+        for (int d = 0; d < nd; ++d)
+        {
+            k_add<double><<<grid_for(dom_[d].cells(), 256), 256, 0, s>>>(u_[d].as<double>(), fields[d], dom_[d].cells());
+            FPB_CHECK_LAUNCH();
+            dot(fields[d], fields[d], dom_[d].cells(), false, s, sums_.as<double>() + 2 * d);
+            dot(u_[d].as<double>(), u_[d].as<double>(), dom_[d].cells(), false, s, sums_.as<double>() + 2 * d + 1);
+        }
+        FPB_CUDA(cudaMemcpyAsync(hs.data(), sums_.get(), hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        FPB_CUDA(cudaStreamSynchronize(s));
+        double en = 0, un = 0;
+        for (int d = 0; d < nd; ++d)
+        {
+            en += hs[2 * d];
+            un += hs[2 * d + 1];
+        }
+        if (!std::isfinite(en) || !std::isfinite(un)) throw Error(5, "non-finite value in iterative refinement");
+        const double last = change;
+        change            = un > 0 ? std::sqrt(en / un) : 0.0;
+        // stop when this correction is below tol, or when the observed contraction rate says the error left
+        // after applying it (about change * change / last) is
+        if (change <= rel_tol || (steps >= 2 && last > 0 && change * (change / last) <= rel_tol)) break;
+        std::vector<double*>       r(nd);
+        std::vector<const double*> fsp(nd), up(nd);
+        for (int d = 0; d < nd; ++d)
+        {
+            r[d]   = fields[d];
+            fsp[d] = fs_[d].as<double>();
+            up[d]  = u_[d].as<double>();
+        }
+        residual_into(r.data(), fsp.data(), up.data(), s);  // fields <- fs - A u
+    }
+    for (int d = 0; d < nd; ++d)
+        FPB_CUDA(cudaMemcpyAsync(fields[d], u_[d].get(), dom_[d].cells() * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (rel_change) *rel_change = change;
+    return steps;
+}
+
+void Composite::ensure_ir_workspace()
+{
+    const int nd = (int)dom_.size();
+    if ((int)fs_.size() == nd) return;
+    fs_.resize(nd);
+    u_.resize(nd);
+    for (int d = 0; d < nd; ++d)
+    {
+        fs_[d].alloc(dom_[d].cells() * sizeof(double));
+        u_[d].alloc(dom_[d].cells() * sizeof(double));
+    }
+    sums_.alloc(2 * (size_t)nd * sizeof(double));
+}
+
+void Composite::residual_into(double* const* r, const double* const* fs, const double* const* u, cudaStream_t s)
+{
+    const int nd = (int)dom_.size();
+    for (int d = 0; d < nd; ++d)
+    {
+        const Domain& D = dom_[d];
+        ResidualArgs  a{};
+        a.nx = D.nx;
+        a.ny = D.ny;
+        a.r2 = D.hx * D.hx / D.hy / D.hy;
+        for (int f = 0; f < 4; ++f)
+        {
+            a.bc[f] = D.bc[f];
+            a.nb[f] = nullptr;
+        }
+        for (auto& c : tree_.children[d])
+        {
+            a.nb[c.first]   = u[c.second];
+            a.nbnx[c.first] = dom_[c.second].nx;
+            a.nbny[c.first] = dom_[c.second].ny;
+        }
+        if (tree_.parent[d].second >= 0)
+        {
+            const int f = tree_.parent[d].first, p = tree_.parent[d].second;
+            a.nb[f]     = u[p];
+            a.nbnx[f]   = dom_[p].nx;
+            a.nbny[f]   = dom_[p].ny;
+        }
+        k_composite_residual<<<grid_for(D.cells(), 256, 1 << 30), 256, 0, s>>>(r[d], fs[d], u[d], a);
+        FPB_CHECK_LAUNCH();
+    }
+}
+
+double Composite::residual_norm(const double* const* u, const double* const* rhs, const double* const* ghosts,
+                                cudaStream_t s)
+{
+    const int nd = (int)dom_.size();
+    ensure_ir_workspace();
+    std::vector<double*>       fsp(nd), rp(nd);
+    std::vector<const double*> fsc(nd);
+    for (int d = 0; d < nd; ++d)
+    {
+        fsp[d] = fs_[d].as<double>();
+        fsc[d] = fsp[d];
+        rp[d]  = u_[d].as<double>();  // residual scratch
+        FPB_CUDA(cudaMemcpyAsync(fsp[d], rhs[d], dom_[d].cells() * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    assemble(fsp.data(), ghosts, s);
+    residual_into(rp.data(), fsc.data(), u, s);
+    for (int d = 0; d < nd; ++d)
+    {
+        dot(rp[d], rp[d], dom_[d].cells(), false, s, sums_.as<double>() + 2 * d);
+        dot(fsp[d], fsp[d], dom_[d].cells(), false, s, sums_.as<double>() + 2 * d + 1);
+    }
+    std::vector<double> hs(2 * (size_t)nd);
+    FPB_CUDA(cudaMemcpyAsync(hs.data(), sums_.get(), hs.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    FPB_CUDA(cudaStreamSynchronize(s));
+    double rn = 0, fn = 0;
+    for (int d = 0; d < nd; ++d)
+    {
+        rn += hs[2 * d];
+        fn += hs[2 * d + 1];
+    }
+    return fn > 0 ? std::sqrt(rn / fn) : std::sqrt(rn);
 }
 
 }  // namespace fpb

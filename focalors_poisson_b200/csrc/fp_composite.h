@@ -59,6 +59,15 @@ public:
     void set_parameter(int m, double tol, int max_iter);
     // fields[d]: device pointers (nx*ny doubles) solved in place; ghosts[4*d+face]: device or null.
     void solve(double* const* fields, const double* const* ghosts, cudaStream_t s, GmresInfo* info);
+    // Same problem by iterative refinement: inner solves with FP32 transforms (FP64 chase, FP64
+    // interface operations, the interface inverse applied once without the residual test), FP64
+    // residual of the composite operator, until |correction| <= rel_tol |u| or max_refine steps.
+    // Returns the number of refinement steps; *rel_change gets the last |correction| / |u|.
+    int solve_ir(double* const* fields, const double* const* ghosts, cudaStream_t s, double rel_tol, int max_refine,
+                 double* rel_change, GmresInfo* info, bool inner_fp32 = true);
+    // |fs - A u| / |fs| over all cells, fs = the assembled, hx^2-scaled right-hand side of (rhs, ghosts).
+    // rhs is not modified (a copy is assembled).
+    double residual_norm(const double* const* u, const double* const* rhs, const double* const* ghosts, cudaStream_t s);
 
     const Tree&                tree() const { return tree_; }
     const std::vector<Domain>& domains() const { return dom_; }
@@ -80,6 +89,11 @@ private:
     };
 
     void build_schur();
+    void assemble(double* const* fields, const double* const* ghosts, cudaStream_t s);
+    void eliminate(double* const* fields, cudaStream_t s, GmresInfo* info);
+    void rect_solve(int d, double* f, long long batch, cudaStream_t s) const;
+    void residual_into(double* const* r, const double* const* fs, const double* const* u, cudaStream_t s);
+    void ensure_ir_workspace();
     void build_interface_inverse(int d);
     bool refine_with_inverse(int d, double* f, cudaStream_t s, GmresInfo* info);
     void node_solve(int d, double* f, cudaStream_t s, GmresInfo* info);
@@ -95,6 +109,9 @@ private:
     std::vector<std::unique_ptr<DevRect<double>>> rect_;
     std::vector<Node>                            node_;
     std::vector<DevBuf>                          temp_;    // per non-root domain (upward sweep temporaries)
+    std::vector<DevBuf>                          fs_, u_;  // iterative refinement: scaled RHS, solution
+    DevBuf                                       sums_;    // per-domain reduction results
+    bool                                         mixed_ = false;  // inner solve of iterative refinement
     DevBuf                                       red_;     // reduction scratch: partials + ticket + results
 };
 

@@ -141,7 +141,9 @@ template <typename T> struct DevTransform
 
     DevTransform(int kind, int n);
     // rows = fields * nx contiguous rows of length n; in and out may alias.
-    void run(const T* in, T* out, long long rows, bool inverse, cudaStream_t s) const;
+    void run(const T* in, T* out, long long rows, bool inverse, cudaStream_t s) const { run_io<T>(in, out, rows, inverse, s); }
+    // Same with rows of another element type (FP64 rows through an FP32 transform).
+    template <typename TIO> void run_io(const TIO* in, TIO* out, long long rows, bool inverse, cudaStream_t s) const;
 };
 
 // Device-resident PoissonSolver2D: transform plan + chase tables.
@@ -163,6 +165,10 @@ template <typename T> struct DevRect
     DevRect(int nx, int ny, double hx, double hy, const int* bc);
     // In-place solve of `batch` back-to-back fields.
     void solve(T* f, long long batch, cudaStream_t s) const;
+    // FP64 plans only: the same solve with FP32 transforms (FP64 rows in and out, FP64 chase); the
+    // reduced-precision inner solve of iterative refinement. The FP32 transform plan is built on first use.
+    void solve_mixed(T* f, long long batch, cudaStream_t s) const;
+    mutable std::unique_ptr<DevTransform<float>> tr32;
     // Scratch elements the partition chase needs for `batch` fields (0 when it is not used).
     long long chase_scratch_elems(long long batch) const;
     // The chase alone, with caller-provided scratch of chase_scratch_elems(batch) elements.

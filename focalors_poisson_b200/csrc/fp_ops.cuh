@@ -324,3 +324,56 @@ __global__ void k_interface_residual(double* r, const double* g, const double* y
     r[k] = g[k] - y[k] + field[edge_index(loc, nx, ny, k)];
 }
 }  // namespace fpb
+
+namespace fpb
+{
+// ---------------------------------------------------------------------------------------------
+// FP64 residual of the composite 5-point operator (iterative refinement)
+// ---------------------------------------------------------------------------------------------
+struct ResidualArgs
+{
+    int           nx, ny;
+    double        r2;         // (hx/hy)^2
+    int           bc[4];      // with Adjacented on connected faces
+    const double* nb[4];      // neighbour fields on Adjacented faces
+    int           nbnx[4], nbny[4];
+};
+
+// r = fs - A u with (A u)_ij = u_{i-1,j} + u_{i+1,j} - 2u_ij + r2 (u_{i,j-1} + u_{i,j+1} - 2u_ij): ghosts 0
+// (Dirichlet), mirrored (Neumann), wrapped (periodic); an Adjacented face contributes the neighbour's
+// adjacent cell with coefficient 1 -- the operator ConcatPoissonSolver2D::solve inverts
+// (pe/concat/concat_solver2d.cpp:101-157, interface terms from bond_add with coefficient -1).
+__global__ void k_composite_residual(double* __restrict__ r, const double* __restrict__ fs,
+                                     const double* __restrict__ u, const ResidualArgs a)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)a.nx * a.ny) return;
+    const int    i = (int)(t / a.ny), j = (int)(t % a.ny);
+    const int    nx = a.nx, ny = a.ny;
+    const double c  = u[t];
+    double       xm, xp, ym, yp, ycoef_m = a.r2, ycoef_p = a.r2;
+    auto ghost = [&](int face, int k, double own, double wrap, double& coef) -> double {
+        switch (a.bc[face])
+        {
+            case 0: return 0.0;
+            case 1: return own;
+            case 2: return wrap;
+            default:
+            {
+                coef = 1.0;
+                return a.nb[face][edge_index(face ^ 1, a.nbnx[face], a.nbny[face], k)];
+            }
+        }
+    };
+    double dummy = 1.0;
+    xm = (i > 0) ? u[t - ny] : ghost(0, j, c, u[(long long)(nx - 1) * ny + j], dummy);
+    xp = (i < nx - 1) ? u[t + ny] : ghost(1, j, c, u[j], dummy);
+    ym = (j > 0) ? u[t - 1] : ghost(2, i, c, u[(long long)i * ny + ny - 1], ycoef_m);
+    yp = (j < ny - 1) ? u[t + 1] : ghost(3, i, c, u[(long long)i * ny], ycoef_p);
+    const double lap = xm + xp - 2.0 * c + a.r2 * ((j < ny - 1 || a.bc[3] != 3 ? yp : 0.0) +
+                                                   (j > 0 || a.bc[2] != 3 ? ym : 0.0) - 2.0 * c) +
+                       ((j == ny - 1 && a.bc[3] == 3) ? ycoef_p * yp : 0.0) +
+                       ((j == 0 && a.bc[2] == 3) ? ycoef_m * ym : 0.0);
+    r[t] = fs[t] - lap;
+}
+}  // namespace fpb

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 
 namespace fpb
 {
@@ -37,17 +38,17 @@ template <typename T2> std::vector<T2> convert_c(const std::vector<std::complex<
     return r;
 }
 
-template <typename T, int K, int I> void launch_k(const TransformArgs<T>& a, long long rows, int threads, size_t smem,
-                                                  cudaStream_t s)
+template <typename T, int K, int I, typename TIO>
+void launch_k(const TransformArgs<T, TIO>& a, long long rows, int threads, size_t smem, cudaStream_t s)
 {
     static std::once_flag once;
     std::call_once(once, [] {
-        cudaFuncSetAttribute(k_transform<T, K, I>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_transform<T, K, I, TIO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)max_dynamic_smem());
     });
     const long long grid = FamilyTraits<K, I>::kPairRows ? (rows + 1) / 2 : rows;
     if (grid <= 0) return;
-    k_transform<T, K, I><<<(unsigned)grid, threads, smem, s>>>(a);
+    k_transform<T, K, I, TIO><<<(unsigned)grid, threads, smem, s>>>(a);
     FPB_CHECK_LAUNCH();
 }
 }  // namespace
@@ -95,9 +96,11 @@ template <typename T> DevTransform<T>::DevTransform(int kind_, int n_) : kind(ki
     if (smem > max_dynamic_smem()) throw Error(3, "transform of length " + std::to_string(n) + " needs more shared memory than a CTA has");
 }
 
-template <typename T> void DevTransform<T>::run(const T* in, T* out, long long rows, bool inverse, cudaStream_t s) const
+template <typename T>
+template <typename TIO>
+void DevTransform<T>::run_io(const TIO* in, TIO* out, long long rows, bool inverse, cudaStream_t s) const
 {
-    TransformArgs<T> a;
+    TransformArgs<T, TIO> a;
     a.in    = in;
     a.out   = out;
     a.rows  = rows;
@@ -112,8 +115,8 @@ template <typename T> void DevTransform<T>::run(const T* in, T* out, long long r
     const int inv = inverse ? 1 : 0;
 #define FPB_CASE(K)                                                                                        \
     case K:                                                                                                \
-        if (inv) launch_k<T, K, 1>(a, rows, threads, smem, s);                                              \
-        else launch_k<T, K, 0>(a, rows, threads, smem, s);                                                  \
+        if (inv) launch_k<T, K, 1, TIO>(a, rows, threads, smem, s);                                         \
+        else launch_k<T, K, 0, TIO>(a, rows, threads, smem, s);                                             \
         break;
     switch (kind)
     {
@@ -295,6 +298,18 @@ template <typename T> void DevRect<T>::chase(T* f, long long batch, T* scr, cuda
     }
 }
 
+template <typename T> void DevRect<T>::solve_mixed(T* f, long long batch, cudaStream_t s) const
+{
+    if (!std::is_same<T, double>::value) throw Error(1, "mixed-precision solve needs an FP64 plan");
+    if (batch <= 0) return;
+    if (!tr32) tr32.reset(new DevTransform<float>(tr->kind, ny));
+    tr32->run_io<T>(f, f, batch * nx, false, s);
+    const long long need = chase_scratch_elems(batch);
+    if (need) scratch.ensure((size_t)need * sizeof(T));
+    chase(f, batch, scratch.as<T>(), s);
+    tr32->run_io<T>(f, f, batch * nx, true, s);
+}
+
 template <typename T> void DevRect<T>::solve(T* f, long long batch, cudaStream_t s) const
 {
     if (batch <= 0) return;
@@ -307,6 +322,7 @@ template <typename T> void DevRect<T>::solve(T* f, long long batch, cudaStream_t
 
 template struct DevTransform<double>;
 template struct DevTransform<float>;
+template void DevTransform<float>::run_io<double>(const double*, double*, long long, bool, cudaStream_t) const;
 template struct DevRect<double>;
 template struct DevRect<float>;
 

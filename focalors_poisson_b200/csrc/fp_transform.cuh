@@ -26,11 +26,13 @@
 namespace fpb
 {
 
-template <typename T> struct TransformArgs
+// T: arithmetic of the FFT; TIO: element type of the rows read and written (FP64 rows with an FP32 FFT
+// is the reduced-precision transform of the iterative-refinement path).
+template <typename T, typename TIO = T> struct TransformArgs
 {
     typedef typename Cplx<T>::type T2;
-    const T*      in;
-    T*            out;
+    const TIO*    in;
+    TIO*          out;
     long long     rows;  // rows in the batch (fields * nx)
     int           n;     // row length (ny)
     FftDesc       fd;
@@ -50,33 +52,33 @@ template <typename T> __device__ __forceinline__ T alt_neg_even(int j) { return 
 template <typename T> __device__ __forceinline__ T alt_pos_even(int j) { return (j & 1) ? (T)-1 : (T)1; }
 
 // Real input value u(i) of one row for the families whose FFT input is real.
-template <typename T, int KIND, int INV>
-__device__ __forceinline__ T real_input(const TransformArgs<T>& a, const T* f, int i)
+template <typename T, int KIND, int INV, typename TA, typename TIO>
+__device__ __forceinline__ T real_input(const TA& a, const TIO* f, int i)
 {
     const int n = a.n;
     if (KIND == 0)  // DD folding, n+1 = L
     {
         if (i == 0) return (T)0;
-        const T xj = f[i - 1], xm = f[n - i];  // x_j, x_{L-j}
+        const T xj = (T)f[i - 1], xm = (T)f[n - i];  // x_j, x_{L-j}
         return a.tc[i].x * (xj + xm) + (T)0.5 * (xj - xm);
     }
     if (KIND == 1)  // NN forward: Makhoul reordering
-        return (2 * i < n) ? f[2 * i] : f[2 * n - 1 - 2 * i];
+        return (T)((2 * i < n) ? f[2 * i] : f[2 * n - 1 - 2 * i]);
     // ND forward, DN: ex[j+1] = (j even ? -1 : 1) sqrt(4/(2n+1)) f_j
-    if (i >= 1 && i <= n) return (alt_neg_even<T>(i - 1) * a.s1) * f[i - 1];
+    if (i >= 1 && i <= n) return (alt_neg_even<T>(i - 1) * a.s1) * (T)f[i - 1];
     return (T)0;
 }
 
 // Hermitian-symmetrised input h(i) of one row for the real-output families (NN / ND inverses).
-template <typename T, int KIND>
-__device__ __forceinline__ typename Cplx<T>::type herm_input(const TransformArgs<T>& a, const T* p, int i)
+template <typename T, int KIND, typename TA, typename TIO>
+__device__ __forceinline__ typename Cplx<T>::type herm_input(const TA& a, const TIO* p, int i)
 {
     typedef typename Cplx<T>::type T2;
     const int n = a.n;
     if (KIND == 1)  // NN inverse: c_m = w_m a_m, a_0 = sqrt(1/n) p_{n-1}, a_m = -sqrt(2/n) p_{n-1-m}
     {
         auto c = [&](int m) -> T2 {
-            const T am = (m == 0) ? a.s2 * p[n - 1] : -a.s1 * p[n - 1 - m];
+            const T am = (m == 0) ? a.s2 * (T)p[n - 1] : -a.s1 * (T)p[n - 1 - m];
             const T2 w = a.tc[m];
             return mk<T2>(w.x * am, w.y * am);
         };
@@ -87,17 +89,17 @@ __device__ __forceinline__ typename Cplx<T>::type herm_input(const TransformArgs
     if (i == 0) return mk<T2>(0, 0);
     if (i <= n)
     {
-        const T p0 = p[i - 1];
+        const T p0 = (T)p[i - 1];
         return mk<T2>((T)0.5 * (__ldg(a.tb + i - 1) * p0), (T)0.5 * (__ldg(a.ta + i - 1) * p0));
     }
     const int t  = 2 * n + 1 - i;
-    const T   p0 = p[t - 1];
+    const T   p0 = (T)p[t - 1];
     return mk<T2>((T)0.5 * (__ldg(a.tb + t - 1) * p0), (T)-0.5 * (__ldg(a.ta + t - 1) * p0));
 }
 
 // PP: the row's two real sequences (poisson_fft2d.cpp:401-447).
-template <typename T, int INV>
-__device__ __forceinline__ typename Cplx<T>::type pp_input(const TransformArgs<T>& a, const T* f, int i)
+template <typename T, int INV, typename TA, typename TIO>
+__device__ __forceinline__ typename Cplx<T>::type pp_input(const TA& a, const TIO* f, int i)
 {
     typedef typename Cplx<T>::type T2;
     const int n = a.n;
@@ -106,17 +108,17 @@ __device__ __forceinline__ typename Cplx<T>::type pp_input(const TransformArgs<T
     {
         if (i >= 1 && i <= n - 1)
         {
-            u = f[i - 1];
-            v = alt_pos_even<T>(i - 1) * f[i - 1];
+            u = (T)f[i - 1];
+            v = alt_pos_even<T>(i - 1) * (T)f[i - 1];
         }
     }
     else  // even/odd cos parts summed into u, sin parts into v
     {
         const int h = n / 2;
-        if (i < h) u += __ldg(a.ta + 2 * i) * f[2 * i];
-        if (i >= 1 && i <= h) u += __ldg(a.ta + 2 * i - 1) * f[2 * i - 1];
-        if (i >= 1 && i <= h) v += __ldg(a.tb + 2 * (h - i)) * f[2 * (h - i)];
-        if (i <= h - 1) v += __ldg(a.tb + 2 * (h - 1 - i) + 1) * f[2 * (h - 1 - i) + 1];
+        if (i < h) u += __ldg(a.ta + 2 * i) * (T)f[2 * i];
+        if (i >= 1 && i <= h) u += __ldg(a.ta + 2 * i - 1) * (T)f[2 * i - 1];
+        if (i >= 1 && i <= h) v += __ldg(a.tb + 2 * (h - i)) * (T)f[2 * (h - i)];
+        if (i <= h - 1) v += __ldg(a.tb + 2 * (h - 1 - i) + 1) * (T)f[2 * (h - 1 - i) + 1];
     }
     return mk<T2>(u, v);
 }
@@ -184,8 +186,8 @@ template <typename T> __device__ void block_scan2(T* xa, T* xb, int K)
     __syncthreads();
 }
 
-template <typename T, int KIND, int INV>
-__global__ void __launch_bounds__(512) k_transform(const TransformArgs<T> a)
+template <typename T, int KIND, int INV, typename TIO = T>
+__global__ void __launch_bounds__(512) k_transform(const TransformArgs<T, TIO> a)
 {
     typedef typename Cplx<T>::type T2;
     extern __shared__ __align__(16) unsigned char fp_smem_raw[];
@@ -199,12 +201,12 @@ __global__ void __launch_bounds__(512) k_transform(const TransformArgs<T> a)
     const long long r0   = kPair ? 2LL * blockIdx.x : (long long)blockIdx.x;
     if (r0 >= a.rows) return;
     const bool has_b = kPair && r0 + 1 < a.rows;
-    const T*   fa    = a.in + r0 * n;
-    const T*   fb    = has_b ? fa + n : fa;
-    T*         oa    = a.out + r0 * n;
-    T*         ob    = has_b ? oa + n : nullptr;
+    const TIO* fa    = a.in + r0 * n;
+    const TIO* fb    = has_b ? fa + n : fa;
+    TIO*       oa    = a.out + r0 * n;
+    TIO*       ob    = has_b ? oa + n : nullptr;
 
-    if (KIND == 4 && !INV && threadIdx.x == 0) rowsc[0] = fa[n - 1];  // PP forward: f(i, ny-1)
+    if (KIND == 4 && !INV && threadIdx.x == 0) rowsc[0] = (T)fa[n - 1];  // PP forward: f(i, ny-1)
 
     for (int i = threadIdx.x; i < a.fd.M; i += blockDim.x)
     {

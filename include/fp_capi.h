@@ -110,6 +110,8 @@ typedef struct fp_solve_info
     int    gmres_restarts;   /* restart cycles of the root GMRES */
     double gmres_residual;   /* last residual norm / estimate of the root GMRES */
     int    converged;        /* 1 if every GMRES met its tolerance */
+    int    refinements;      /* fp_composite_solve_f32ir: refinement steps taken */
+    double rel_change;       /* fp_composite_solve_f32ir: last |correction| / |solution| (L2 over all cells) */
 } fp_solve_info;
 
 #define FP_GMRES_FULLFIELD 4 /* create flag: Krylov vectors are full fields, as the reference */
@@ -129,6 +131,22 @@ int fp_composite_set_parameter(fp_composite* c, int m, double tol, int max_iter)
  * Variable2D ghost buffers (NULL = zero), length ny for x faces and nx for y faces. */
 int fp_composite_solve_f64(fp_composite* c, double* const* fields, const double* const* ghosts, int flags,
                            void* stream, fp_solve_info* info);
+/* The same problem by mixed-precision iterative refinement (no counterpart in the reference, which is
+ * FP64 only): inner solves with FP32 transforms (FP64 rows, FP64 chase, FP64 interface operations),
+ * the FP64 residual of the composite 5-point operator, until |correction| <= rel_tol |solution| (or
+ * the observed contraction predicts the error left after the last correction is below rel_tol) or
+ * max_refine steps (FP_ERR_NOT_CONVERGED with FP_CHECK_CONVERGENCE if the target was missed).
+ * With FP_IR_INNER_F64 the inner solves are the FP64 ones (refinement then only removes the single
+ * FP64 solve's round-off, about eps * cond(A)). */
+#define FP_IR_INNER_F64 32
+int fp_composite_solve_f32ir(fp_composite* c, double* const* fields, const double* const* ghosts, int flags,
+                             void* stream, double rel_tol, int max_refine, fp_solve_info* info);
+/* Relative residual |fs - A u| / |fs| of a candidate solution u of the composite problem with right-hand
+ * side `rhs` and ghost buffers `ghosts` (fs = their assembled, hx^2-scaled form, the right-hand side
+ * ConcatPoissonSolver2D::solve works on; A = its composite 5-point operator). No counterpart in the
+ * reference; used to check solutions. Device pointers only (FP_DEVICE semantics); nothing is modified. */
+int fp_composite_residual(fp_composite* c, const double* const* u, const double* const* rhs,
+                          const double* const* ghosts, void* stream, double* rel_residual);
 /* Tree actually used: root index and BFS level of every domain (root = 0). */
 int fp_composite_tree(const fp_composite* c, int* root, int* level_of);
 int fp_composite_destroy(fp_composite* c);

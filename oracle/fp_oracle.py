@@ -578,3 +578,53 @@ def mock_solve(f):
     i = np.arange(nx)[:, None]
     j = np.arange(ny)[None, :]
     return f * (i * ny + j + 1)
+
+
+def composite_apply(domains, connections, bc, u):
+    """The discrete composite operator the reference's block elimination inverts, in its hx^2-scaled form
+    (concat_solver2d.cpp:101-157 with the rectangle operator of poisson_solver2d.cpp:46-51):
+    (A u)_ij = u_{i-1,j} + u_{i+1,j} - 2u_ij + (hx/hy)^2 (u_{i,j-1} + u_{i,j+1} - 2u_ij), with ghost cells
+    0 (Dirichlet), mirrored (Neumann), wrapped (periodic), and on Adjacented faces the neighbour's adjacent
+    cells entering with coefficient 1 (bond_add(loc, -1, nb) moved to the left-hand side)."""
+    nb = {(a, loc): b for a, loc, b in connections}
+    nb.update({(b, opposite(loc)): a for a, loc, b in connections})
+    out = []
+    for d, dom in enumerate(domains):
+        x = u[d]
+        nx, ny = x.shape
+        r2 = dom.hx * dom.hx / dom.hy / dom.hy
+
+        def ghost(face):
+            t = bc[d][face]
+            if face == XNEG:
+                own, wrap = x[0, :], x[nx - 1, :]
+            elif face == XPOS:
+                own, wrap = x[nx - 1, :], x[0, :]
+            elif face == YNEG:
+                own, wrap = x[:, 0], x[:, ny - 1]
+            else:
+                own, wrap = x[:, ny - 1], x[:, 0]
+            if t == D:
+                return np.zeros_like(own), 1.0
+            if t == N:
+                return own, 1.0
+            if t == P:
+                return wrap, 1.0
+            o = u[nb[(d, face)]]
+            edge = {XNEG: o[-1, :], XPOS: o[0, :], YNEG: o[:, -1], YPOS: o[:, 0]}[face]
+            return edge, 0.0
+
+        xm = np.vstack([ghost(XNEG)[0][None, :], x[:-1, :]])
+        xp = np.vstack([x[1:, :], ghost(XPOS)[0][None, :]])
+        gy0, sy0 = ghost(YNEG)
+        gy1, sy1 = ghost(YPOS)
+        ym = np.hstack([gy0[:, None], x[:, :-1]])
+        yp = np.hstack([x[:, 1:], gy1[:, None]])
+        lap = xm + xp - 2.0 * x + r2 * (yp + ym - 2.0 * x)
+        # an Adjacented y face couples with coefficient 1, not (hx/hy)^2
+        if sy0 == 0.0:
+            lap[:, 0] += (1.0 - r2) * gy0
+        if sy1 == 0.0:
+            lap[:, -1] += (1.0 - r2) * gy1
+        out.append(lap)
+    return out

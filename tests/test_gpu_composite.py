@@ -80,3 +80,33 @@ def test_cyclic_geometry_rejected():
     with pytest.raises(capi.FpError) as e:
         capi.Composite(geo)
     assert e.value.code == 1 and "cycle" in str(e.value)
+
+
+@pytest.mark.parametrize("name", COMPOSITE_CASES)
+def test_composite_f32_refinement(name):
+    """FP32-transform inner solves + FP64 iterative refinement reach the reference's converged answer to
+    1e-10 relative L2 (the target of the reduced-precision form)."""
+    geo, rhs, ghosts, outs, (m, tol, it), root = composite_case(name)
+    tight = tight_outputs(name)
+    solver = capi.Composite(geometry(geo), m, tol, it, root=root)
+    fields = [np.array(r, dtype=np.float64, copy=True) for r in rhs]
+    info = solver.solve_ir(fields, ghosts, rel_tol=1e-12, max_refine=8)
+    assert info["refinements"] >= 2, info
+    assert rel_l2(fields, tight) <= 1e-10, (name, info, rel_l2(fields, tight))
+
+
+@pytest.mark.parametrize("name", ["cross48_neumann_tips.npz", "cross24_ghosts.npz", "tree9_periodic.npz"])
+def test_composite_residual_of_reference_solution(name):
+    """The composite 5-point operator behind fp_composite_residual is the one the reference inverts: its
+    converged solutions have relative residual at round-off, a perturbed one does not."""
+    torch = torch_cuda()
+    geo, rhs, ghosts, outs, (m, tol, it), root = composite_case(name)
+    tight = tight_outputs(name)
+    solver = capi.Composite(geometry(geo), m, tol, it, root=root)
+    u = [torch.tensor(t, device="cuda") for t in tight]
+    f = [torch.tensor(r, device="cuda") for r in rhs]
+    g = None if ghosts is None else [[None if x is None else torch.tensor(x, device="cuda") for x in row]
+                                     for row in ghosts]
+    assert solver.residual(u, f, g) <= 1e-11
+    u[0][1, 1] += 1e-3 * float(u[0].abs().max())
+    assert solver.residual(u, f, g) > 1e-6
