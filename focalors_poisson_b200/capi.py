@@ -35,6 +35,8 @@ SIGNATURES = {
     "fp_composite_set_parameter": ([_vp, _i, _d, _i], _i),
     "fp_composite_solve_f64": ([_vp, _vp, _vp, _i, _vp, _vp], _i),
     "fp_composite_solve_f32ir": ([_vp, _vp, _vp, _i, _vp, _d, _i, _vp], _i),
+    "fp_composite_adjoint_f64": ([_vp, _vp, _i, _vp, _vp], _i),
+    "fp_composite_adjoint_f32ir": ([_vp, _vp, _i, _vp, _d, _i, _vp], _i),
     "fp_composite_residual": ([_vp, _vp, _vp, _vp, _vp, _vp], _i),
     "fp_composite_tree": ([_vp, _vp, _vp], _i),
     "fp_composite_destroy": ([_vp], _i),
@@ -243,6 +245,28 @@ class Composite:
             flags |= FP_IR_INNER_F64
         check(lib().fp_composite_solve_f32ir(self.h, fp, gp, flags, stream, float(rel_tol), int(max_refine),
                                              ctypes.byref(info)))
+        return self._info(info)
+
+    def adjoint(self, fields, check_convergence=False):
+        """Transposed solve in place: fields <- H A^-1 fields (the gradient with respect to the right-hand
+        side of a loss whose gradient with respect to the solution is `fields`)."""
+        fp, _, flags, stream, keep = self._pointers(fields, None)
+        info = SolveInfo()
+        if check_convergence:
+            flags |= FP_CHECK_CONVERGENCE
+        check(lib().fp_composite_adjoint_f64(self.h, fp, flags, stream, ctypes.byref(info)))
+        return self._info(info)
+
+    def adjoint_ir(self, fields, rel_tol=1e-12, max_refine=10, check_convergence=False, inner="f32"):
+        """The transposed solve by iterative refinement (FP32 or FP64 inner solves, FP64 residual)."""
+        fp, _, flags, stream, keep = self._pointers(fields, None)
+        info = SolveInfo()
+        if check_convergence:
+            flags |= FP_CHECK_CONVERGENCE
+        if inner == "f64":
+            flags |= FP_IR_INNER_F64
+        check(lib().fp_composite_adjoint_f32ir(self.h, fp, flags, stream, float(rel_tol), int(max_refine),
+                                               ctypes.byref(info)))
         return self._info(info)
 
     def residual(self, u, rhs, ghosts=None):

@@ -149,6 +149,41 @@ int fp_composite_solve_f32ir(fp_composite* c, double* const* fields, const doubl
     return rc;
 }
 
+int fp_composite_adjoint_f64(fp_composite* c, double* const* fields, int flags, void* stream, fp_solve_info* info)
+{
+    GmresInfo gi;
+    int       rc = guarded([&] {
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        with_device_fields(c, fields, nullptr, flags, s,
+                           [&](double* const* f, const double* const*) { c->c->solve_adjoint(f, s, &gi); });
+        if ((flags & FP_CHECK_CONVERGENCE) && !gi.converged)
+            throw Error(FP_ERR_NOT_CONVERGED, "GMRES stopped at max_iter above tol (residual " +
+                                                  std::to_string(gi.residual) + ")");
+    });
+    fill_info(info, gi, 0, 0.0);
+    return rc;
+}
+
+int fp_composite_adjoint_f32ir(fp_composite* c, double* const* fields, int flags, void* stream, double rel_tol,
+                               int max_refine, fp_solve_info* info)
+{
+    GmresInfo gi;
+    int       steps  = 0;
+    double    change = 0;
+    int       rc     = guarded([&] {
+        if (!(rel_tol > 0) || max_refine < 1) throw Error(FP_ERR_INVALID, "rel_tol must be > 0 and max_refine >= 1");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        with_device_fields(c, fields, nullptr, flags, s, [&](double* const* f, const double* const*) {
+            steps = c->c->solve_adjoint_ir(f, s, rel_tol, max_refine, &change, &gi, (flags & FP_IR_INNER_F64) == 0);
+        });
+        if ((flags & FP_CHECK_CONVERGENCE) && steps >= max_refine && !(change <= rel_tol))
+            throw Error(FP_ERR_NOT_CONVERGED, "iterative refinement stopped at max_refine (relative change " +
+                                                  std::to_string(change) + ")");
+    });
+    fill_info(info, gi, steps, change);
+    return rc;
+}
+
 int fp_composite_residual(fp_composite* c, const double* const* u, const double* const* rhs,
                           const double* const* ghosts, void* stream, double* rel_residual)
 {

@@ -709,10 +709,16 @@ void Composite::eliminate(double* const* fields, cudaStream_t s, GmresInfo* info
 int Composite::solve_ir(double* const* fields, const double* const* ghosts, cudaStream_t s, double rel_tol,
                         int max_refine, double* rel_change, GmresInfo* info, bool inner_fp32)
 {
-    const int nd = (int)dom_.size();
     ensure_ir_workspace();
     mixed_ = false;
     assemble(fields, ghosts, s);
+    return refine(fields, s, rel_tol, max_refine, rel_change, info, inner_fp32);
+}
+
+int Composite::refine(double* const* fields, cudaStream_t s, double rel_tol, int max_refine, double* rel_change,
+                      GmresInfo* info, bool inner_fp32)
+{
+    const int nd = (int)dom_.size();
     for (int d = 0; d < nd; ++d)
     {
         FPB_CUDA(cudaMemcpyAsync(fs_[d].get(), fields[d], dom_[d].cells() * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -761,6 +767,50 @@ int Composite::solve_ir(double* const* fields, const double* const* ghosts, cuda
     for (int d = 0; d < nd; ++d)
         FPB_CUDA(cudaMemcpyAsync(fields[d], u_[d].get(), dom_[d].cells() * sizeof(double), cudaMemcpyDeviceToDevice, s));
     if (rel_change) *rel_change = change;
+    return steps;
+}
+
+// The operator ConcatPoissonSolver2D::solve inverts is A u = H (f + b(ghosts)), H = diag(hx_d^2) per domain,
+// A the composite 5-point operator of k_composite_residual. A is symmetric: inside a domain the x and y
+// stencils are symmetric for every boundary type (Dirichlet ghosts move to the right-hand side, Neumann
+// mirrors, periodic wraps), and every interface couples the two adjacent cells with coefficient 1 in both
+// equations (bond_add with coefficient -1 on both sides, pe/concat/concat_solver2d.cpp:101-157). The map
+// f -> u is therefore A^-1 H, and its transpose is H A^-1: the same elimination applied to the unscaled,
+// unassembled vector, then scaled by hx_d^2. Without any Dirichlet face A is singular and the forward solve
+// picks one particular solution, which has no such transpose: refused.
+void Composite::require_nonsingular() const
+{
+    for (const Domain& D : dom_)
+        for (int f = 0; f < 4; ++f)
+            if (D.bc[f] == 0) return;
+    throw Error(3, "adjoint solve needs a Dirichlet face: the composite operator is singular");
+}
+
+void Composite::scale_by_h2(double* const* fields, cudaStream_t s)
+{
+    for (size_t d = 0; d < dom_.size(); ++d)
+    {
+        k_scale<<<grid_for(dom_[d].cells(), 256), 256, 0, s>>>(fields[d], dom_[d].hx * dom_[d].hx, dom_[d].cells());
+        FPB_CHECK_LAUNCH();
+    }
+}
+
+void Composite::solve_adjoint(double* const* fields, cudaStream_t s, GmresInfo* info)
+{
+    require_nonsingular();
+    mixed_ = false;
+    eliminate(fields, s, info);
+    scale_by_h2(fields, s);
+}
+
+int Composite::solve_adjoint_ir(double* const* fields, cudaStream_t s, double rel_tol, int max_refine,
+                                double* rel_change, GmresInfo* info, bool inner_fp32)
+{
+    require_nonsingular();
+    ensure_ir_workspace();
+    mixed_    = false;
+    const int steps = refine(fields, s, rel_tol, max_refine, rel_change, info, inner_fp32);
+    scale_by_h2(fields, s);
     return steps;
 }
 

@@ -65,6 +65,12 @@ public:
     // Returns the number of refinement steps; *rel_change gets the last |correction| / |u|.
     int solve_ir(double* const* fields, const double* const* ghosts, cudaStream_t s, double rel_tol, int max_refine,
                  double* rel_change, GmresInfo* info, bool inner_fp32 = true);
+    // Transposed solve (adjoint of fields -> solution, ghosts held fixed): g <- H A^-1 g in place, H =
+    // diag(hx^2) per domain, A the composite operator (symmetric). FP_ERR_UNSUPPORTED without a Dirichlet face.
+    void solve_adjoint(double* const* fields, cudaStream_t s, GmresInfo* info);
+    // The same by iterative refinement (FP32 or FP64 inner solves, FP64 residual), as solve_ir.
+    int solve_adjoint_ir(double* const* fields, cudaStream_t s, double rel_tol, int max_refine, double* rel_change,
+                         GmresInfo* info, bool inner_fp32 = true);
     // |fs - A u| / |fs| over all cells, fs = the assembled, hx^2-scaled right-hand side of (rhs, ghosts).
     // rhs is not modified (a copy is assembled).
     double residual_norm(const double* const* u, const double* const* rhs, const double* const* ghosts, cudaStream_t s);
@@ -94,6 +100,10 @@ private:
     void rect_solve(int d, double* f, long long batch, cudaStream_t s) const;
     void residual_into(double* const* r, const double* const* fs, const double* const* u, cudaStream_t s);
     void ensure_ir_workspace();
+    int  refine(double* const* fields, cudaStream_t s, double rel_tol, int max_refine, double* rel_change,
+                GmresInfo* info, bool inner_fp32);  // fields: assembled, scaled RHS in, solution out
+    void require_nonsingular() const;
+    void scale_by_h2(double* const* fields, cudaStream_t s);
     void build_interface_inverse(int d);
     bool refine_with_inverse(int d, double* f, cudaStream_t s, GmresInfo* info);
     void node_solve(int d, double* f, cudaStream_t s, GmresInfo* info);

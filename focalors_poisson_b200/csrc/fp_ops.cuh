@@ -201,6 +201,12 @@ __global__ void k_multi_axpy(double* __restrict__ x, const double* __restrict__ 
         x[i] = v;
     }
 }
+// y *= a
+__global__ void k_scale(double* __restrict__ y, double a, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] *= a;
+}
 // y += x (mixed precision: T field added into a double field)
 template <typename T>
 __global__ void k_add(double* __restrict__ y, const T* __restrict__ x, long long n)

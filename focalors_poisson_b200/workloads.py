@@ -163,3 +163,59 @@ def gaussian_bumps_rhs(g: Geometry, seed: int, n_bumps: int = 32) -> list:
             f += amp[k] * np.exp(-((X - cx[k]) ** 2 + (Y - cy[k]) ** 2) / (2.0 * w[k] ** 2))
         out.append(f)
     return out
+
+
+def adjoint_case(n: int = 512, seed: int = 2024, probes: int = 64):
+    """Differentiable-solve workload: cross 5 x n^2, h = 1/n, homogeneous Dirichlet outer faces; RHS
+    f ~ N(0,1) (seed), per-cell source scale s ~ U(0.5, 1.5) (seed+1), target u_t ~ N(0,1) (seed+2), loss
+    0.5 |u - u_t|^2 with u the solution for s*f; `probes` random cells (domain, i, j) (seed+3) for the
+    finite-difference check."""
+    g = cross(n)
+    f = gaussian_rhs(g, seed, zero_mean=False)
+    rng = np.random.default_rng(seed + 1)
+    s = [rng.uniform(0.5, 1.5, (a, b)) for a, b in zip(g.nx, g.ny)]
+    rng = np.random.default_rng(seed + 2)
+    ut = [rng.standard_normal((a, b)) for a, b in zip(g.nx, g.ny)]
+    rng = np.random.default_rng(seed + 3)
+    dom = rng.integers(0, g.n_domains, probes)
+    pts = [(int(d), int(rng.integers(0, g.nx[d])), int(rng.integers(0, g.ny[d]))) for d in dom]
+    return g, f, s, ut, pts
+
+
+SIDES = tuple(range(64, 1025, 32))  # {64, 96, ..., 1024}: 31 side lengths
+
+
+def lt_problem(seed: int) -> Geometry:
+    """One problem of the batched-uneven workload: an L (3 subdomains) or T (4 subdomains) shape, free side
+    lengths drawn uniformly from SIDES with numpy default_rng(seed), homogeneous Dirichlet outer faces,
+    one grid step h = 1/max(side) for every subdomain. Centre C (index 0) is the tree root.
+
+      L: C (a x b); X at C's x+ face (c x b); Y at C's y+ face (a x d)
+      T: C (a x b); W at C's x- face (c x b); E at C's x+ face (e x b); N at C's y+ face (a x d)
+    """
+    rng = np.random.default_rng(seed)
+    shape = "L" if rng.integers(0, 2) == 0 else "T"
+    draw = lambda: int(SIDES[rng.integers(0, len(SIDES))])  # noqa: E731
+    a, b, c, d = draw(), draw(), draw(), draw()
+    if shape == "L":
+        nx, ny = [a, c, a], [b, b, d]
+        conns = [(0, XPOS, 1), (0, YPOS, 2)]
+        names = ["C", "X", "Y"]
+    else:
+        e = draw()
+        nx, ny = [a, c, e, a], [b, b, b, d]
+        conns = [(0, XNEG, 1), (0, XPOS, 2), (0, YPOS, 3)]
+        names = ["C", "W", "E", "N"]
+    h = 1.0 / max(nx + ny)
+    nd = len(nx)
+    return Geometry(nx, ny, [h] * nd, [h] * nd, [[DIRICHLET] * 4 for _ in range(nd)], conns, [(0.0, 0.0)] * nd,
+                    names)
+
+
+def batched_uneven(count: int = 512, seed: int = 2024):
+    """The batched-uneven workload: `count` independent L/T problems (problem p uses seed + p) and their
+    seeded N(0,1) right-hand sides (seed + p + 1000003)."""
+    geos = [lt_problem(seed + p) for p in range(count)]
+    rhs = [gaussian_rhs(g, seed + p + 1000003, zero_mean=False) for p, g in enumerate(geos)]
+    return geos, rhs
+

@@ -141,6 +141,17 @@ int fp_composite_solve_f64(fp_composite* c, double* const* fields, const double*
 #define FP_IR_INNER_F64 32
 int fp_composite_solve_f32ir(fp_composite* c, double* const* fields, const double* const* ghosts, int flags,
                              void* stream, double rel_tol, int max_refine, fp_solve_info* info);
+/* Adjoint (transposed) solve of the map rhs -> solution with the ghost buffers held fixed: the gradient
+ * of a loss L(u) with respect to the right-hand side is fp_composite_adjoint_*(dL/du). In place:
+ * fields <- H A^-1 fields, H = diag(hx_d^2) per domain, A the composite 5-point operator that
+ * ConcatPoissonSolver2D::solve inverts (pe/concat/concat_solver2d.cpp:101-157), which is symmetric, so
+ * the transposed solve runs through the same kernels as the forward one. No counterpart in the reference
+ * (it has no gradients). Geometries without a Dirichlet face (singular A) give FP_ERR_UNSUPPORTED.
+ * _f32ir: by iterative refinement, same rel_tol / max_refine / FP_IR_INNER_F64 meaning as
+ * fp_composite_solve_f32ir. Same host/device field semantics as the solves. */
+int fp_composite_adjoint_f64(fp_composite* c, double* const* fields, int flags, void* stream, fp_solve_info* info);
+int fp_composite_adjoint_f32ir(fp_composite* c, double* const* fields, int flags, void* stream, double rel_tol,
+                               int max_refine, fp_solve_info* info);
 /* Relative residual |fs - A u| / |fs| of a candidate solution u of the composite problem with right-hand
  * side `rhs` and ghost buffers `ghosts` (fs = their assembled, hx^2-scaled form, the right-hand side
  * ConcatPoissonSolver2D::solve works on; A = its composite 5-point operator). No counterpart in the

@@ -485,7 +485,9 @@ class ConcatPoissonSolver2D:
     """ConcatPoissonSolver2D (pe/concat/concat_solver2d.cpp). domains[i].bc holds the boundary type of each
     face; adjacented faces are overridden from the connections (variable2d.cpp:25-45)."""
 
-    def __init__(self, domains, connections, m=20, tol=1e-8, max_iter=100, root=None):
+    def __init__(self, domains, connections, m=20, tol=1e-8, max_iter=100, root=None, schur=None):
+        """schur: optional per-domain-index Schur matrices to use instead of building them by impulse
+        solves (e.g. oracle/schur_closed_form.py for large leaves)."""
         self.domains = domains
         self.tree = build_tree(len(domains), connections, root)
         self.bc = []
@@ -507,7 +509,8 @@ class ConcatPoissonSolver2D:
                     g = GMRESSolver2D(m, tol, max_iter, ps.solve)
                     for loc, c in self.tree.children[d]:
                         cd_ = domains[c]
-                        g.S.append((loc, schur_matrix(loc, cd_.nx, cd_.ny, self.solvers[c])))
+                        S = schur[c] if schur is not None and schur[c] is not None else None
+                        g.S.append((loc, S if S is not None else schur_matrix(loc, cd_.nx, cd_.ny, self.solvers[c])))
                     self.solvers[d] = g.solve
                     self.gmres = g if d == self.tree.root else getattr(self, "gmres", None)
                 else:

@@ -76,7 +76,7 @@ def parse_printed_blocks(stdout):
     separator lines ('----...' and 'Testing ...')."""
     blocks, cur = [], []
     for line in stdout.splitlines():
-        if line.startswith("-") or line.startswith("Testing"):
+        if (line.strip() and set(line.strip()) == {"-"}) or line.startswith("Testing"):
             if cur:
                 blocks.append(np.asarray(cur))
             cur = []
