@@ -40,8 +40,14 @@ SIGNATURES = {
     "fp_composite_residual": ([_vp, _vp, _vp, _vp, _vp, _vp], _i),
     "fp_composite_tree": ([_vp, _vp, _vp], _i),
     "fp_composite_destroy": ([_vp], _i),
+    "fp_batch_create": ([_vp, _i, _i, _vp], _i),
+    "fp_batch_solve": ([_vp, _vp, _vp, _i, _vp, _i], _i),
+    "fp_batch_residuals": ([_vp, _vp, _vp, _vp, _vp, _vp], _i),
+    "fp_batch_info": ([_vp, _vp, _vp, _vp, _vp], _i),
+    "fp_batch_destroy": ([_vp], _i),
 }
 FP_GMRES_FULLFIELD, FP_CHECK_CONVERGENCE, FP_NO_INTERFACE_INVERSE, FP_IR_INNER_F64 = 4, 8, 16, 32
+FP_BATCH_F32, FP_BATCH_NO_AUTOTUNE, FP_BATCH_GRAPH = 64, 128, 256
 
 
 class Geometry(ctypes.Structure):
@@ -281,3 +287,80 @@ class Composite:
         if getattr(self, "h", None) and _lib is not None:
             _lib.fp_composite_destroy(self.h)
             self.h = None
+
+
+class Batch:
+    """Batched composite solves (fp_batch_*): `problems` is a list of geometries (as for Composite), each a
+    root with leaves on full faces, Dirichlet outer faces, nx a multiple of 32. Fields are CUDA float64
+    tensors, one per subdomain, problems back to back (flat list)."""
+
+    def __init__(self, problems, precision="f64", autotune=True):
+        self.keep = []
+        geos = (Geometry * len(problems))()
+        self.shapes = []
+        for p, geo in enumerate(problems):
+            arr = dict(
+                nx=np.ascontiguousarray(geo.nx, dtype=np.int32), ny=np.ascontiguousarray(geo.ny, dtype=np.int32),
+                hx=np.ascontiguousarray(geo.hx, dtype=np.float64), hy=np.ascontiguousarray(geo.hy, dtype=np.float64),
+                bc=np.ascontiguousarray(np.asarray(geo.bc, dtype=np.int32).reshape(-1)),
+                conn=np.ascontiguousarray(np.asarray(geo.connections, dtype=np.int32).reshape(-1)))
+            self.keep.append(arr)
+            nc = len(geo.connections)
+            geos[p] = Geometry(len(geo.nx), arr["nx"].ctypes.data, arr["ny"].ctypes.data, arr["hx"].ctypes.data,
+                               arr["hy"].ctypes.data, arr["bc"].ctypes.data, nc,
+                               arr["conn"].ctypes.data if nc else None, -1)
+            self.shapes += [(int(a), int(b)) for a, b in zip(geo.nx, geo.ny)]
+        flags = (FP_BATCH_F32 if precision == "f32" else 0) | (0 if autotune else FP_BATCH_NO_AUTOTUNE)
+        h = ctypes.c_void_p()
+        check(lib().fp_batch_create(geos, len(problems), flags, ctypes.byref(h)))
+        self.h = h
+        self.n_problems = len(problems)
+        self.n_domains = len(self.shapes)
+
+    def _ptrs(self, fields):
+        if len(fields) != self.n_domains:
+            raise ValueError(f"{self.n_domains} fields expected")
+        ptrs = []
+        for f, shp in zip(fields, self.shapes):
+            if tuple(f.shape) != shp:
+                raise ValueError(f"field shape {tuple(f.shape)} != subdomain shape {shp}")
+            p, fl, _, _ = _args(f, np.float64)
+            if not fl & FP_DEVICE:
+                raise TypeError("batched solves take CUDA tensors")
+            ptrs.append(p.value)
+        return (ctypes.c_void_p * self.n_domains)(*ptrs)
+
+    def _ghosts(self, ghosts):
+        if ghosts is None:
+            return None
+        gl = []
+        for d in range(self.n_domains):
+            for face in range(4):
+                g = None if ghosts[d] is None else ghosts[d][face]
+                gl.append(None if g is None else _args(g, np.float64)[0].value)
+        return (ctypes.c_void_p * (4 * self.n_domains))(*gl)
+
+    def solve(self, fields, ghosts=None, steps=0, graph=False, sync=False):
+        """In place. steps == 0: one solve in the storage precision; steps >= 1: FP64 iterative refinement
+        with that many inner solves. graph: capture once, replay afterwards (same tensors and steps)."""
+        flags = FP_DEVICE | (FP_BATCH_GRAPH if graph else 0) | (FP_SYNC if sync else 0)
+        check(lib().fp_batch_solve(self.h, self._ptrs(fields), self._ghosts(ghosts), flags, _stream(), int(steps)))
+
+    def residuals(self, u, rhs, ghosts=None):
+        out = np.zeros(self.n_problems)
+        check(lib().fp_batch_residuals(self.h, self._ptrs(u), self._ptrs(rhs), self._ghosts(ghosts), _stream(),
+                                       out.ctypes.data))
+        return out
+
+    def info(self):
+        npb, nd, gk = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        shape = (ctypes.c_int * 3)()
+        check(lib().fp_batch_info(self.h, ctypes.byref(npb), ctypes.byref(nd), shape, ctypes.byref(gk)))
+        return dict(n_problems=npb.value, n_domains=nd.value, dst_threads=shape[0], dst_blocks_per_sm=shape[1],
+                    chase_threads=shape[2], graph_kernels=gk.value)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fp_batch_destroy(self.h)
+            self.h = None
+

@@ -1,0 +1,1664 @@
+// Batched composite solves (fp_batch.h). Host plan + heterogeneous persistent kernels.
+#include "fp_batch.h"
+#include "fp_chase.cuh"
+#include "fp_ops.cuh"
+
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <numeric>
+
+namespace fpb
+{
+
+// =============================================================================================
+// Device side
+// =============================================================================================
+
+// Largest s with prefix[s] <= x (prefix ascending, prefix[0] = 0).
+__device__ __forceinline__ int seg_of(const long long* __restrict__ prefix, int n, long long x)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// sqrt(2/(n+1)) sin(pi (k+1)(j+1)/(n+1)): DST-I basis vector k at point j (the reference's DD transform,
+// pe/poisson/poisson_fft2d.cpp:19-57, is this orthonormal matrix).
+__device__ __forceinline__ double dst_basis(int n, int k, int j)
+{
+    const long long q = (long long)(k + 1) * (j + 1) % (2LL * (n + 1));
+    return sqrt(2.0 / (n + 1)) * sinpi((double)q / (double)(n + 1));
+}
+
+// ---------------------------------------------------------------------------------------------
+// DST-I (the DD family, self-inverse) of rows of many lengths in one persistent launch
+// ---------------------------------------------------------------------------------------------
+template <typename T> struct BPlan
+{
+    typedef typename Cplx<T>::type T2;
+    int        n, L, M, blue, nst;
+    const T2*  tw;
+    const T2*  chirp;
+    const T2*  bhat;
+    const int* perm;
+    const int4* stages;
+    const T2*  tc;
+    T          s1;
+};
+
+struct DstSeg
+{
+    const void* in;
+    void*       out;
+    int         rows, plan;
+};
+
+// One work item = two rows of one segment (z = u + i v through one complex FFT of length n+1, see
+// fp_transform.cuh). ACC: out (FP64) += result instead of out = result.
+template <typename T, typename TIN, typename TOUT, bool ACC>
+__global__ void __launch_bounds__(512) k_b_dst(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix,
+                                               int nseg, long long nitems, const BPlan<T>* __restrict__ plans)
+{
+    typedef typename Cplx<T>::type T2;
+    extern __shared__ __align__(16) unsigned char fp_smem_raw[];
+    T2*       buf  = reinterpret_cast<T2*>(fp_smem_raw);
+    const T   half = (T)0.5;
+    for (long long it = blockIdx.x; it < nitems; it += gridDim.x)
+    {
+        const int      s  = seg_of(prefix, nseg, it);
+        const DstSeg   sg = segs[s];
+        const BPlan<T> P  = plans[sg.plan];
+        const int      n  = P.n;
+        const long long r0    = 2 * (it - prefix[s]);
+        const bool      has_b = r0 + 1 < sg.rows;
+        const TIN*      fa    = static_cast<const TIN*>(sg.in) + r0 * n;
+        const TIN*      fb    = has_b ? fa + n : fa;
+        TOUT*           oa    = static_cast<TOUT*>(sg.out) + r0 * n;
+        TOUT*           ob    = has_b ? oa + n : nullptr;
+        FftDesc         d;
+        d.L    = P.L;
+        d.M    = P.M;
+        d.blue = P.blue;
+        d.nst  = P.nst;
+        const FftTables<T2> ft{P.tw, P.chirp, P.bhat, P.perm, P.stages};
+        const int           L = P.L;
+        for (int i = threadIdx.x; i < P.M; i += blockDim.x)
+        {
+            T2 z = mk<T2>(0, 0);
+            if (i < L && i > 0)
+            {
+                const T c  = P.tc[i].x;
+                const T xa = (T)fa[i - 1], xma = (T)fa[n - i];
+                const T va = c * (xa + xma) + half * (xa - xma);
+                T       vb = 0;
+                if (has_b)
+                {
+                    const T xb = (T)fb[i - 1], xmb = (T)fb[n - i];
+                    vb         = c * (xb + xmb) + half * (xb - xmb);
+                }
+                z = mk<T2>(va, vb);
+            }
+            buf[fft_in_slot(d, ft, i)] = fft_in_value(d, ft, i, z);
+        }
+        fft_execute(buf, d, ft);
+        const int K  = (n + 1) / 2;
+        T*        ca = reinterpret_cast<T*>(buf + ((P.M - L >= K) ? L : P.M));
+        T*        cb = ca + K;
+        auto put = [&](TOUT* o, int idx, T v) {
+            if (ACC) o[idx] = (TOUT)((double)o[idx] + (double)v);
+            else o[idx] = (TOUT)v;
+        };
+        for (int k = threadIdx.x; k <= n / 2; k += blockDim.x)
+        {
+            const T2 Zk = fft_out(buf, d, ft, k % L);
+            const T2 Zm = fft_out(buf, d, ft, (L - k) % L);
+            if (k < K)
+            {
+                const T sc = (k == 0) ? (T)0.5 : (T)1;
+                ca[k]      = sc * (half * (Zk.x + Zm.x));
+                cb[k]      = sc * (half * (Zk.y + Zm.y));
+            }
+            if (k >= 1 && 2 * k <= n)
+            {
+                put(oa, 2 * k - 1, P.s1 * (-(half * (Zk.y - Zm.y))));
+                if (ob) put(ob, 2 * k - 1, P.s1 * (half * (Zk.x - Zm.x)));
+            }
+        }
+        __syncthreads();
+        block_scan2(ca, cb, K);
+        for (int k = threadIdx.x; k < K; k += blockDim.x)
+        {
+            put(oa, 2 * k, P.s1 * ca[k]);
+            if (ob) put(ob, 2 * k, P.s1 * cb[k]);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Partition chase (fp_chase.cuh) over many subdomains, out of place, with right-hand-side
+// modifiers: rhs(i, k) = in(i, k) + sum_rows [i == row] c v[k] + sum_cols c s[i] psi_k(j)
+// (a row term is a spectral vector on one row; a column term is a physical column of values at
+// column j, whose y-DST is s[i] psi_k(j)).
+// ---------------------------------------------------------------------------------------------
+constexpr int kMaxMods = 4;
+
+template <typename T> struct ChaseTabDev
+{
+    const T* cc;
+    const T* cg;
+    const T* chh;
+    const T* cends;
+    const T* dsep;
+};
+
+template <typename T> struct ChaseSeg
+{
+    const T* in;
+    T*       out;
+    int      nx, ny, tab;
+    T*       zend;  // scratch: 2 P ny
+    T*       bsep;  // P ny
+    T*       work;  // P ny
+    int      nrow, ncol;
+    int      row_i[kMaxMods];
+    const double* row_v[kMaxMods];
+    double   row_c[kMaxMods];
+    int      col_j[kMaxMods];
+    const double* col_s[kMaxMods];
+    double   col_c[kMaxMods];
+};
+
+template <typename T> struct ModCtx
+{
+    double psi[kMaxMods];
+};
+
+template <typename T>
+__device__ __forceinline__ void mod_init(const ChaseSeg<T>& sg, int k, ModCtx<T>& m)
+{
+    for (int c = 0; c < sg.ncol; ++c) m.psi[c] = sg.col_c[c] * dst_basis(sg.ny, k, sg.col_j[c]);
+}
+template <typename T>
+__device__ __forceinline__ T mod_rhs(const ChaseSeg<T>& sg, const ModCtx<T>& m, int i, int k, T raw)
+{
+    if (sg.nrow == 0 && sg.ncol == 0) return raw;
+    double v = (double)raw;
+    for (int r = 0; r < sg.nrow; ++r)
+        if (sg.row_i[r] == i) v += sg.row_c[r] * sg.row_v[r][k];
+    for (int c = 0; c < sg.ncol; ++c) v += m.psi[c] * sg.col_s[c][i];
+    return (T)v;
+}
+
+// blocks of segment s: prefix (in blocks); per segment P*ny threads (local / correct) or ny (reduced)
+template <typename T>
+__global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __restrict__ segs,
+                                                       const long long* __restrict__ prefix, int nseg,
+                                                       const ChaseTabDev<T>* __restrict__ tabs)
+{
+    constexpr int Li = kChunk - 1;
+    const int     s  = seg_of(prefix, nseg, blockIdx.x);
+    const ChaseSeg<T> sg = segs[s];
+    const long long t  = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
+    const int       ny = sg.ny, P = sg.nx / kChunk;
+    if (t >= (long long)P * ny) return;
+    const int j   = (int)(t % ny);
+    const int p   = (int)(t / ny);
+    const int typ = p == 0 ? 0 : 1;
+    const ChaseTabDev<T> tb = tabs[sg.tab];
+    ModCtx<T>            mc;
+    mod_init(sg, j, mc);
+    const T* col = sg.in + (long long)p * kChunk * ny + j;
+    T*       out = sg.out + (long long)p * kChunk * ny + j;
+    const T* c   = tb.cc + (long long)typ * Li * ny + j;
+    T        y[Li];
+#pragma unroll
+    for (int r = 0; r < Li; ++r) y[r] = mod_rhs(sg, mc, p * kChunk + r, j, col[(long long)r * ny]);
+    T prev = 0;
+#pragma unroll
+    for (int r = 0; r < Li; ++r)
+    {
+        prev = (y[r] - prev) * __ldg(c + (long long)r * ny);
+        y[r] = prev;
+    }
+#pragma unroll
+    for (int r = Li - 2; r >= 0; --r) y[r] = y[r] - __ldg(c + (long long)r * ny) * y[r + 1];
+#pragma unroll
+    for (int r = 0; r < Li; ++r) out[(long long)r * ny] = y[r];
+    T* ze  = sg.zend + (long long)(p * 2) * ny + j;
+    ze[0]  = y[0];
+    ze[ny] = y[Li - 1];
+}
+
+template <typename T>
+__global__ void k_b_chase_reduced(const ChaseSeg<T>* __restrict__ segs, const long long* __restrict__ prefix,
+                                  int nseg, const ChaseTabDev<T>* __restrict__ tabs)
+{
+    const int         s  = seg_of(prefix, nseg, blockIdx.x);
+    const ChaseSeg<T> sg = segs[s];
+    const long long   t  = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
+    const int         ny = sg.ny, nx = sg.nx, P = nx / kChunk;
+    if (t >= ny) return;
+    const int            j  = (int)t;
+    const ChaseTabDev<T> tb = tabs[sg.tab];
+    ModCtx<T>            mc;
+    mod_init(sg, j, mc);
+    const T d = tb.dsep[j];
+    auto e = [&](int typ, int k) { return tb.cends[((long long)typ * 4 + k) * ny + j]; };
+    const T* ze = sg.zend + j;
+    T*       cw = sg.work + j;
+    T*       bs = sg.bsep + j;
+    T        yprev = 0, cprev = 0;
+    for (int p = 0; p < P; ++p)
+    {
+        const int  typ   = p == 0 ? 0 : 1;
+        const bool last  = p == P - 1;
+        const int  isep  = p * kChunk + kChunk - 1;
+        const T    fsep  = mod_rhs(sg, mc, isep, j, sg.in[(long long)isep * ny + j]);
+        const T    lower = p > 0 ? -e(typ, 1) : (T)0;
+        T          diag  = d - e(typ, 3);
+        T          rhs   = fsep - ze[(long long)(2 * p + 1) * ny];
+        if (!last)
+        {
+            diag -= e(1, 0);
+            rhs -= ze[(long long)(2 * (p + 1)) * ny];
+        }
+        const T den = diag - lower * cprev;
+        const T up  = last ? (T)0 : -e(1, 2);
+        const T cp  = up / den;
+        yprev       = (rhs - lower * yprev) / den;
+        cw[(long long)p * ny] = cp;
+        bs[(long long)p * ny] = yprev;
+        cprev                 = cp;
+    }
+    T x = bs[(long long)(P - 1) * ny];
+    sg.out[(long long)(nx - 1) * ny + j] = x;
+    for (int p = P - 2; p >= 0; --p)
+    {
+        x                                                  = bs[(long long)p * ny] - cw[(long long)p * ny] * x;
+        bs[(long long)p * ny]                              = x;
+        sg.out[(long long)(p * kChunk + kChunk - 1) * ny + j] = x;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_b_chase_correct(const ChaseSeg<T>* __restrict__ segs,
+                                                         const long long* __restrict__ prefix, int nseg,
+                                                         const ChaseTabDev<T>* __restrict__ tabs)
+{
+    constexpr int     Li = kChunk - 1;
+    const int         s  = seg_of(prefix, nseg, blockIdx.x);
+    const ChaseSeg<T> sg = segs[s];
+    const long long   t  = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
+    const int         ny = sg.ny, P = sg.nx / kChunk;
+    if (t >= (long long)P * ny) return;
+    const int            j   = (int)(t % ny);
+    const int            p   = (int)(t / ny);
+    const int            typ = p == 0 ? 0 : 1;
+    const ChaseTabDev<T> tb  = tabs[sg.tab];
+    const T*             bs  = sg.bsep + j;
+    const T              bl  = p > 0 ? bs[(long long)(p - 1) * ny] : (T)0;
+    const T              br  = bs[(long long)p * ny];
+    T*                   col = sg.out + (long long)p * kChunk * ny + j;
+    const T*             g   = tb.cg + (long long)typ * Li * ny + j;
+    const T*             h   = tb.chh + (long long)typ * Li * ny + j;
+#pragma unroll 8
+    for (int r = 0; r < Li; ++r)
+    {
+        const long long o = (long long)r * ny;
+        col[o]            = col[o] - bl * __ldg(g + o) - br * __ldg(h + o);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Small per-subdomain / per-problem kernels
+// ---------------------------------------------------------------------------------------------
+// out[i] = coef * sum_k psi_k(j) X(i, k): the physical value at column j of a y-spectral field.
+template <typename T> struct ColReq
+{
+    const T* X;
+    int      nx, ny, j;
+    double*  out;
+    double   coef;
+};
+template <typename T>
+__global__ void k_b_colvals(const ColReq<T>* __restrict__ reqs, const long long* __restrict__ prefix, int nreq)
+{
+    const long long w    = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int       lane = threadIdx.x & 31;
+    if (w >= prefix[nreq]) return;
+    const int       q = seg_of(prefix, nreq, w);
+    const ColReq<T> R = reqs[q];
+    const int       i = (int)(w - prefix[q]);
+    const T*        row = R.X + (long long)i * R.ny;
+    double          acc = 0;
+    for (int k = lane; k < R.ny; k += 32) acc += dst_basis(R.ny, k, R.j) * (double)row[k];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) R.out[i] = R.coef * acc;
+}
+
+// out[k] = coef * X(i, k)
+template <typename T> struct RowReq
+{
+    const T* X;
+    int      ny, i;
+    double*  out;
+    double   coef;
+};
+template <typename T>
+__global__ void k_b_rowcopy(const RowReq<T>* __restrict__ reqs, const long long* __restrict__ prefix, int nreq)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= prefix[nreq]) return;
+    const int       q = seg_of(prefix, nreq, t);
+    const RowReq<T> R = reqs[q];
+    const int       k = (int)(t - prefix[q]);
+    R.out[k]          = R.coef * (double)R.X[(long long)R.i * R.ny + k];
+}
+
+// Interface solve of one problem in the spectral bases (see fp_batch.h). Edges: x-edges e (root faces
+// x- / x+, rows ie[e]) with y-spectral unknowns (ny), y-edges Y (root faces y- / y+, columns jy[Y]) with
+// x-spectral unknowns (nx).
+struct BIface
+{
+    int           nx, ny, nxe, nye;
+    int           ie[2], jy[2];
+    double        r;
+    const double* alpha;  // nx: x eigenvalues - 2 ... (root)
+    const double* beta;   // ny
+    const double* sig[2];   // x-edge leaf responses (ny)
+    const double* sigp[2];  // y-edge leaf responses (nx)
+    const double* invxx;    // ny blocks of nxe x nxe
+    const double* invyy;    // nx blocks of nye x nye (used when nxe == 0)
+    const double* rinv;     // (nye nx)^2 column-major (when nxe > 0 and nye > 0)
+    double*       gX;   // nxe * ny
+    double*       gY;   // nye * nx (x-spectral)
+    double*       zX;   // nxe * ny
+    double*       rhsY; // nye * nx
+    double*       yX;   // nxe * ny
+    double*       yY;   // nye * nx (x-spectral)
+    double*       sY;   // nye * nx: sigma' yY (x-spectral)
+    double*       bX;   // nxe * ny: -leaf edge rows (y-spectral), root right-hand side terms
+    double*       bX2;  // nxe * ny: bX + sigma yX
+};
+
+__device__ __forceinline__ double chi_edge(int n, int m, int i) { return dst_basis(n, m, i); }
+
+// zX = invXX gX, thread per (problem, k)
+__global__ void k_if_zx(const BIface* __restrict__ P, const long long* __restrict__ prefix, int np)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= prefix[np]) return;
+    const int    p = seg_of(prefix, np, t);
+    const BIface F = P[p];
+    const int    k = (int)(t - prefix[p]);
+    const int    E = F.nxe;
+    const double* B = F.invxx + (long long)k * E * E;
+    for (int e = 0; e < E; ++e)
+    {
+        double v = 0;
+        for (int e2 = 0; e2 < E; ++e2) v += B[e * E + e2] * F.gX[e2 * F.ny + k];
+        F.zX[e * F.ny + k] = v;
+    }
+}
+
+// rhsY[Y][m] = gY[Y][m] + sum_{e,k} chi_m(ie) psi_k(jY) sig_e[k] zX[e][k] / (alpha_m + r beta_k);
+// warp per (problem, Y, m)
+__global__ void k_if_rhsy(const BIface* __restrict__ P, const long long* __restrict__ prefix, int np)
+{
+    const long long w    = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int       lane = threadIdx.x & 31;
+    if (w >= prefix[np]) return;
+    const int    p  = seg_of(prefix, np, w);
+    const BIface F  = P[p];
+    const int    q  = (int)(w - prefix[p]);
+    const int    Y  = q / F.nx, m = q - Y * F.nx;
+    const double am = F.alpha[m];
+    double       acc = 0;
+    for (int e = 0; e < F.nxe; ++e)
+    {
+        const double cm = chi_edge(F.nx, m, F.ie[e]);
+        for (int k = lane; k < F.ny; k += 32)
+            acc += cm * dst_basis(F.ny, k, F.jy[Y]) * F.sig[e][k] * F.zX[e * F.ny + k] / (am + F.r * F.beta[k]);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) F.rhsY[Y * F.nx + m] = F.gY[Y * F.nx + m] + acc;
+}
+
+// yY = Rinv rhsY (thread per row) or, without x-edges, the per-m blocks; sY = sigma' yY
+__global__ void k_if_yy(const BIface* __restrict__ P, const long long* __restrict__ prefix, int np)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= prefix[np]) return;
+    const int    p = seg_of(prefix, np, t);
+    const BIface F = P[p];
+    const int    q = (int)(t - prefix[p]);  // row of the nye*nx system
+    const int    n = F.nye * F.nx;
+    double       v = 0;
+    if (F.nxe > 0)
+    {
+        for (int c = 0; c < n; ++c) v += F.rinv[(long long)c * n + q] * F.rhsY[c];
+    }
+    else
+    {
+        const int Y = q / F.nx, m = q - Y * F.nx, E = F.nye;
+        const double* B = F.invyy + (long long)m * E * E;
+        for (int Y2 = 0; Y2 < E; ++Y2) v += B[Y * E + Y2] * F.rhsY[Y2 * F.nx + m];
+    }
+    F.yY[q] = v;
+    const int Y = q / F.nx, m = q - Y * F.nx;
+    F.sY[q]    = F.sigp[Y][m] * v;
+}
+
+// yX[e][k] = sum_e' invXX_k(e, e') (gX[e'][k] + sum_{Y,m} chi_m(ie') psi_k(jY) sig'_Y[m] yY[Y][m] /
+// (alpha_m + r beta_k)); bX2 = bX + sig yX. Warp per (problem, k).
+__global__ void k_if_yx(const BIface* __restrict__ P, const long long* __restrict__ prefix, int np)
+{
+    const long long w    = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int       lane = threadIdx.x & 31;
+    if (w >= prefix[np]) return;
+    const int    p  = seg_of(prefix, np, w);
+    const BIface F  = P[p];
+    const int    k  = (int)(w - prefix[p]);
+    const double bk = F.r * F.beta[k];
+    double       t[2] = {0, 0};
+    for (int Y = 0; Y < F.nye; ++Y)
+    {
+        const double pk = dst_basis(F.ny, k, F.jy[Y]);
+        for (int m = lane; m < F.nx; m += 32)
+        {
+            const double base = pk * F.sigp[Y][m] * F.yY[Y * F.nx + m] / (F.alpha[m] + bk);
+            for (int e = 0; e < F.nxe; ++e) t[e] += chi_edge(F.nx, m, F.ie[e]) * base;
+        }
+    }
+    for (int e = 0; e < 2; ++e)
+        for (int o = 16; o > 0; o >>= 1) t[e] += __shfl_down_sync(0xffffffffu, t[e], o);
+    if (lane == 0)
+    {
+        const int     E = F.nxe;
+        const double* B = F.invxx + (long long)k * E * E;
+        for (int e = 0; e < E; ++e)
+        {
+            double v = 0;
+            for (int e2 = 0; e2 < E; ++e2) v += B[e * E + e2] * (F.gX[e2 * F.ny + k] + t[e2]);
+            F.yX[e * F.ny + k]  = v;
+            F.bX2[e * F.ny + k] = F.bX[e * F.ny + k] + F.sig[e][k] * v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Setup kernels: closed-form spectral responses
+// ---------------------------------------------------------------------------------------------
+// out[q] = sum_{m < n} w(m) / (eig_a[m] + rr * eig_b[q]), w(m) = chi_m(ia) chi_m(ib) over n points:
+// the Green's function of a Dirichlet tridiagonal line between points ia and ib, per transverse mode q.
+struct GreenReq
+{
+    int           n, ia, ib, nq;
+    const double* eig_a;  // n
+    const double* eig_b;  // nq
+    double        rr;
+    double*       out;    // nq
+};
+__global__ void k_green(const GreenReq* __restrict__ reqs, const long long* __restrict__ prefix, int nreq)
+{
+    const long long w    = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int       lane = threadIdx.x & 31;
+    if (w >= prefix[nreq]) return;
+    const int      q0 = seg_of(prefix, nreq, w);
+    const GreenReq R  = reqs[q0];
+    const int      q  = (int)(w - prefix[q0]);
+    const double   b  = R.rr * R.eig_b[q];
+    double         acc = 0;
+    for (int m = lane; m < R.n; m += 32)
+        acc += dst_basis(R.n, m, R.ia) * dst_basis(R.n, m, R.ib) / (R.eig_a[m] + b);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) R.out[q] = acc;
+}
+
+// A[(Y,m),(e,k)] (column-major, ld = nY) and B[(e,k),(Y,m)] = sum_e' invXX_k(e,e') M_XY(e',k; Y,m)
+// (column-major, ld = nX) of one problem, for R = M_YY - A B.
+__global__ void k_cross_AB(const BIface F, double* A, double* B)
+{
+    const int       nY = F.nye * F.nx, nX = F.nxe * F.ny;
+    const long long t  = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nY * nX) return;
+    const int row = (int)(t % nY), col = (int)(t / nY);  // A: row (Y, m), col (e, k)
+    {
+        const int Y = row / F.nx, m = row - Y * F.nx, e = col / F.ny, k = col - e * F.ny;
+        A[(long long)col * nY + row] = -chi_edge(F.nx, m, F.ie[e]) * dst_basis(F.ny, k, F.jy[Y]) * F.sig[e][k] /
+                                       (F.alpha[m] + F.r * F.beta[k]);
+    }
+    {
+        // B: row (e, k) = t % nX, col (Y, m) = t / nX
+        const int brow = (int)(t % nX), bcol = (int)(t / nX);
+        const int e = brow / F.ny, k = brow - e * F.ny, Y = bcol / F.nx, m = bcol - Y * F.nx;
+        const int E = F.nxe;
+        double    v = 0;
+        for (int e2 = 0; e2 < E; ++e2)
+            v += F.invxx[(long long)k * E * E + e * E + e2] *
+                 (-chi_edge(F.nx, m, F.ie[e2]) * dst_basis(F.ny, k, F.jy[Y]) * F.sigp[Y][m] /
+                  (F.alpha[m] + F.r * F.beta[k]));
+        B[(long long)bcol * nX + brow] = v;
+    }
+}
+
+// R = M_YY (column-major nY x nY): identity minus the per-m y-edge couplings H_m(jY, jY') sig'_Y'[m]
+__global__ void k_myy(const BIface F, const double* H /* 2x2 blocks per m: H[(Y*2+Y2)*nx + m] */, double* R)
+{
+    const int       nY = F.nye * F.nx;
+    const long long t  = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nY * nY) return;
+    const int row = (int)(t % nY), col = (int)(t / nY);
+    const int Y = row / F.nx, m = row - Y * F.nx, Y2 = col / F.nx, m2 = col - Y2 * F.nx;
+    double    v = (row == col) ? 1.0 : 0.0;
+    if (m == m2) v -= H[(long long)(Y * 2 + Y2) * F.nx + m] * F.sigp[Y2][m];
+    R[t] = v;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Elementwise over many subdomains
+// ---------------------------------------------------------------------------------------------
+struct AsmSeg
+{
+    double*      f;
+    double*      copy;  // when non-null: copy = assembled f (f untouched)
+    AssembleArgs a;
+};
+__global__ void k_b_assemble(const AsmSeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg)
+{
+    const int    s  = seg_of(prefix, nseg, blockIdx.x);
+    const AsmSeg sg = segs[s];
+    const long long t = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)sg.a.nx * sg.a.ny) return;
+    if (sg.copy)
+    {
+        sg.copy[t] = sg.f[t];
+        assemble_at(sg.copy, t, sg.a);
+    }
+    else
+        assemble_at(sg.f, t, sg.a);
+}
+
+struct ResSeg
+{
+    double*       r;
+    const double* fs;
+    const double* u;
+    ResidualArgs  a;
+    double*       partial;  // per block: sum r^2 (or null)
+    double*       partial_f;  // per block: sum fs^2 (or null)
+};
+__global__ void __launch_bounds__(256) k_b_residual(const ResSeg* __restrict__ segs, const long long* __restrict__ prefix,
+                                                    int nseg)
+{
+    __shared__ double sh[32];
+    const int    s  = seg_of(prefix, nseg, blockIdx.x);
+    const ResSeg sg = segs[s];
+    const long long t = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
+    double       rr = 0, ff = 0;
+    if (t < (long long)sg.a.nx * sg.a.ny)
+    {
+        const double v = sg.fs[t] - composite_lap(sg.u, t, sg.a);
+        if (sg.r) sg.r[t] = v;
+        rr = v * v;
+        ff = sg.fs[t] * sg.fs[t];
+    }
+    if (sg.partial)
+    {
+        const double a = block_sum(rr, sh);
+        __syncthreads();
+        const double b = block_sum(ff, sh);
+        if (threadIdx.x == 0)
+        {
+            sg.partial[blockIdx.x - prefix[s]]   = a;
+            sg.partial_f[blockIdx.x - prefix[s]] = b;
+        }
+    }
+}
+
+struct CopySeg
+{
+    double*       dst;
+    const double* src;
+    long long     n;
+};
+__global__ void k_b_copy(const CopySeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg)
+{
+    const int     s  = seg_of(prefix, nseg, blockIdx.x);
+    const CopySeg sg = segs[s];
+    const long long t = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
+    if (t < sg.n) sg.dst[t] = sg.src[t];
+}
+
+}  // namespace fpb
+
+// =============================================================================================
+// Host side
+// =============================================================================================
+namespace fpb
+{
+namespace
+{
+
+struct Segments  // a device work list: records + block/item prefix
+{
+    DevBuf    recs, prefix;
+    int       n     = 0;
+    long long total = 0;  // items (or blocks, or threads) over all records
+    template <typename R> void set(const std::vector<R>& r, const std::vector<long long>& counts)
+    {
+        n = (int)r.size();
+        std::vector<long long> p(r.size() + 1, 0);
+        for (size_t i = 0; i < r.size(); ++i) p[i + 1] = p[i] + counts[i];
+        total  = p.back();
+        recs   = upload(r);
+        prefix = upload(p);
+    }
+    template <typename R> const R* as() const { return recs.as<R>(); }
+    const long long*              pre() const { return prefix.as<long long>(); }
+};
+
+int grid_of(long long threads, int block) { return (int)std::max<long long>(1, (threads + block - 1) / block); }
+
+int sm_count()
+{
+    static int v = [] {
+        int dev = 0, n = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n;
+    }();
+    return v;
+}
+
+template <typename T> struct PlanSet  // DST plans by row length
+{
+    std::map<int, int>                           index;
+    std::vector<std::unique_ptr<DevTransform<T>>> tr;
+    DevBuf                                       dev;
+    size_t                                       smem = 0;
+    int get(int n)
+    {
+        auto it = index.find(n);
+        if (it != index.end()) return it->second;
+        tr.emplace_back(new DevTransform<T>(K_DD, n));
+        smem = std::max(smem, tr.back()->smem);
+        return index[n] = (int)tr.size() - 1;
+    }
+    void finish()
+    {
+        std::vector<BPlan<T>> v;
+        for (auto& t : tr)
+        {
+            BPlan<T> p;
+            p.n      = t->n;
+            p.L      = t->fd.L;
+            p.M      = t->fd.M;
+            p.blue   = t->fd.blue;
+            p.nst    = t->fd.nst;
+            p.tw     = t->tw.template as<typename BPlan<T>::T2>();
+            p.chirp  = t->chirp.template as<typename BPlan<T>::T2>();
+            p.bhat   = t->bhat.template as<typename BPlan<T>::T2>();
+            p.perm   = t->perm.template as<int>();
+            p.stages = t->stages.template as<int4>();
+            p.tc     = t->tc.template as<typename BPlan<T>::T2>();
+            p.s1     = t->s1;
+            v.push_back(p);
+        }
+        dev = upload(v);
+    }
+};
+
+template <typename T, typename TIN, typename TOUT, bool ACC> void prep_dst()
+{
+    static bool attr = false;
+    if (!attr)
+    {
+        FPB_CUDA(cudaFuncSetAttribute(k_b_dst<T, TIN, TOUT, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)max_dynamic_smem()));
+        attr = true;
+    }
+}
+
+template <typename T, typename TIN, typename TOUT, bool ACC>
+void launch_dst(const Segments& sg, const PlanSet<T>& ps, const BatchTiming& tm, cudaStream_t s)
+{
+    if (sg.total == 0) return;
+    prep_dst<T, TIN, TOUT, ACC>();
+    const long long grid = std::min<long long>(sg.total, (long long)sm_count() * tm.dst_blocks_per_sm);
+    k_b_dst<T, TIN, TOUT, ACC><<<(unsigned)grid, tm.dst_threads, ps.smem, s>>>(
+        sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, ps.dev.template as<BPlan<T>>());
+    FPB_CHECK_LAUNCH();
+}
+
+}  // namespace
+
+template <typename TS> class BatchImpl final : public BatchBase
+{
+public:
+    BatchImpl(const std::vector<BatchProblemDesc>& probs);
+    ~BatchImpl() override
+    {
+        if (graph_) cudaGraphExecDestroy(graph_);
+    }
+    void solve(double* const* fields, const double* const* ghosts, int steps, cudaStream_t s) override;
+    void solve_graph(double* const* fields, const double* const* ghosts, int steps, cudaStream_t s) override;
+    void residuals(const double* const* u, const double* const* rhs, const double* const* ghosts, cudaStream_t s,
+                   double* out) override;
+    int           n_problems() const override { return (int)prob_.size(); }
+    int           n_domains() const override { return (int)dom_.size(); }
+    const Domain& domain(int g) const override { return dom_[g].d; }
+    BatchTiming   timing() const override { return tm_; }
+    void          autotune(cudaStream_t s) override;
+    long long     graph_kernels() const override { return graph_kernels_; }
+
+private:
+    struct Dom
+    {
+        Domain    d;
+        int       prob = 0, role = 0;  // role 0: root, 1: leaf
+        int       leaf_face = -1;      // leaf: its face toward the root; root: -1
+        int       root_face = -1;      // leaf: the root's face it is attached to
+        int       plan = 0, tab = 0;
+        long long off  = 0;            // element offset in W / X / fs / u / r
+    };
+    struct Prob
+    {
+        int    root = 0, g0 = 0, nd = 0;
+        int    xe[2] = {-1, -1}, ye[2] = {-1, -1};  // leaves (global index) on the x / y edges, in edge order
+        int    nxe = 0, nye = 0;
+        BIface F{};
+        DevBuf mem;  // spectral vectors and interface work (doubles)
+        DevBuf rinv;
+    };
+
+    void   build_spectral();
+    void   build_static_lists();
+    void   build_chase_lists();
+    void   chase_run(const Segments& lc, const Segments& red, cudaStream_t s);
+    void   inner(const Segments& dst_in, const Segments& dst_out, bool acc, cudaStream_t s);
+    void   set_user_lists(double* const* fields, const double* const* ghosts, int steps);
+    ResSeg res_seg(size_t g, double* r, const double* fs, const double* const* u_user);
+    void   run(int steps, cudaStream_t s);
+
+    std::vector<DevBuf>                       eig_keep_;  // eigenvalue arrays referenced by BIface
+    std::vector<Dom>                          dom_;
+    std::vector<Prob>                         prob_;
+    long long                                 cells_ = 0;
+    PlanSet<TS>                               plans_;
+    PlanSet<double>                           eplans_;  // FP64 DSTs of edge vectors (length nx of roots)
+    std::map<std::pair<int, double>, int>     tab_index_;
+    std::vector<std::unique_ptr<DevRect<TS>>> tabs_;
+    DevBuf                                    tabs_dev_;
+    DevBuf                                    W_, X_, fs_, u_, r_, chs_;  // work, chase out, IR, chase scratch
+    DevBuf                                    edge_;  // bY, gYp, sYp, yYp per y-edge (nx each), per problem
+    std::vector<ChaseSeg<TS>>                 chase1_leaf_, chase1_root_, chase2_all_;
+    Segments                                  l1_lc_, l1_red_, r1_lc_, r1_red_, a2_lc_, a2_red_;
+    Segments                                  leaf_rows_, leaf_cols_, root_rows_, root_cols_;
+    Segments                                  edst_g_, edst_out_;         // FP64 edge DSTs
+    Segments                                  ifk_, ifym_, ifrow_, ifkw_;  // interface work lists
+    std::vector<DstSeg>                       dst_W_in_rec_, dst_X_out_rec_;
+    std::vector<long long>                    dst_counts_;
+    Segments                                  dst_fs_, dst_r_, dst_out_u_;
+    Segments                                  res_, asm_user_, dst_user_in_, dst_user_out_, copy_out_;
+    std::vector<double*>                      user_ptrs_;
+    std::vector<const double*>                user_ghosts_;
+    int                                       user_steps_ = -1;
+    BatchTiming                               tm_;
+    cudaGraphExec_t                           graph_         = nullptr;
+    long long                                 graph_kernels_ = 0;
+};
+
+template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDesc>& probs)
+{
+    if (probs.empty()) throw Error(1, "empty batch");
+    for (size_t p = 0; p < probs.size(); ++p)
+    {
+        const auto& P  = probs[p];
+        const int   nd = (int)P.doms.size();
+        if (nd <= 0) throw Error(1, "problem " + std::to_string(p) + " has no domains");
+        Tree t = build_tree(nd, P.conns, -1);
+        Prob pr;
+        pr.g0   = (int)dom_.size();
+        pr.nd   = nd;
+        pr.root = pr.g0 + t.root;
+        for (int d = 0; d < nd; ++d)
+        {
+            Dom D;
+            D.d    = P.doms[d];
+            D.prob = (int)p;
+            const Domain& q = D.d;
+            if (q.nx % kChunk != 0 || q.nx < 2 * kChunk)
+                throw Error(3, "batched solve needs nx a multiple of 32 and >= 64 in every subdomain");
+            if (q.ny < 2) throw Error(1, "each subdomain needs at least 2 cells per direction");
+            for (int f = 0; f < 4; ++f)
+                if (q.bc[f] != BC_DIRICHLET && q.bc[f] != BC_ADJACENTED)
+                    throw Error(3, "batched solve supports Dirichlet outer faces only");
+            D.role = d == t.root ? 0 : 1;
+            if (D.role == 1)
+            {
+                if (!t.children[d].empty() || t.parent[d].second != t.root)
+                    throw Error(3, "batched solve needs every subdomain attached to the root (depth-1 tree)");
+                D.leaf_face = t.parent[d].first;
+                D.root_face = D.leaf_face ^ 1;
+            }
+            D.off = cells_;
+            cells_ += q.cells();
+            dom_.push_back(D);
+        }
+        for (auto& c : t.children[t.root])
+        {
+            const int face = c.first, g = pr.g0 + c.second;
+            const Domain& R = dom_[pr.root].d;
+            const Domain& L = dom_[g].d;
+            if (face < 2)
+            {
+                if (L.ny != R.ny || L.hy != R.hy) throw Error(1, "x-connected subdomains must share ny and hy");
+                pr.xe[pr.nxe++] = g;
+            }
+            else
+            {
+                if (L.nx != R.nx || L.hx != R.hx) throw Error(1, "y-connected subdomains must share nx and hx");
+                pr.ye[pr.nye++] = g;
+            }
+        }
+        prob_.push_back(std::move(pr));
+    }
+    for (auto& D : dom_)
+    {
+        D.plan = plans_.get(D.d.ny);
+        const double r  = D.d.hx * D.d.hx / D.d.hy / D.d.hy;
+        auto         key = std::make_pair(D.d.ny, r);
+        auto         it  = tab_index_.find(key);
+        if (it == tab_index_.end())
+        {
+            const int bc0[4] = {0, 0, 0, 0};
+            tabs_.emplace_back(new DevRect<TS>(2 * kChunk, D.d.ny, D.d.hx, D.d.hy, bc0));
+            it = tab_index_.emplace(key, (int)tabs_.size() - 1).first;
+        }
+        D.tab = it->second;
+    }
+    plans_.finish();
+    std::vector<ChaseTabDev<TS>> tv;
+    for (auto& t : tabs_)
+        tv.push_back({t->cc.template as<TS>(), t->cg.template as<TS>(), t->chh.template as<TS>(),
+                      t->cends.template as<TS>(), t->dsep.template as<TS>()});
+    tabs_dev_ = upload(tv);
+    W_.alloc((size_t)cells_ * sizeof(TS));
+    X_.alloc((size_t)cells_ * sizeof(TS));
+    long long sep = 0;
+    for (auto& D : dom_) sep += (long long)(D.d.nx / kChunk) * D.d.ny * 4;
+    chs_.alloc((size_t)sep * sizeof(TS));
+    build_spectral();
+    build_static_lists();
+    prep_dst<TS, double, TS, false>();
+    prep_dst<TS, TS, double, false>();
+    prep_dst<TS, TS, double, true>();
+    prep_dst<TS, TS, TS, false>();
+    prep_dst<double, double, double, false>();
+}
+
+// Closed-form spectral responses, interface inverses and the reduced cross systems.
+template <typename TS> void BatchImpl<TS>::build_spectral()
+{
+    // eigenvalues (cal_lambda - 2, the reference's own formula) per distinct length
+    std::map<int, DevBuf> eig;
+    auto eig_of = [&](int n) -> const double* {
+        auto it = eig.find(n);
+        if (it == eig.end())
+        {
+            std::vector<double> l = cal_lambda(n, BC_DIRICHLET, BC_DIRICHLET);
+            for (auto& v : l) v -= 2.0;
+            it = eig.emplace(n, upload(l)).first;
+        }
+        return it->second.template as<double>();
+    };
+    // Per problem: doubles laid out as sig[2](ny) sigp[2](nx) gX/zX/yX/bX/bX2 (2 ny each) gY/rhsY/yY/sY
+    // (2 nx each), G blocks (ny * 4), H blocks (nx * 4), invxx (ny * 4), invyy (nx * 4)
+    std::vector<GreenReq> greq;
+    std::vector<long long> gcnt;
+    struct Host
+    {
+        std::vector<double> G, H, sig, sigp;
+    };
+    for (auto& pr : prob_)
+    {
+        const Domain& R  = dom_[pr.root].d;
+        const int     nx = R.nx, ny = R.ny;
+        const size_t  nd = 2 * ny + 2 * nx + 5 * 2 * ny + 4 * 2 * nx + 4 * ny + 4 * nx + 4 * ny + 4 * nx;
+        pr.mem.alloc(nd * sizeof(double));
+        FPB_CUDA(cudaMemset(pr.mem.get(), 0, nd * sizeof(double)));
+        double* b = pr.mem.template as<double>();
+        BIface& F = pr.F;
+        F.nx = nx;
+        F.ny = ny;
+        F.nxe = pr.nxe;
+        F.nye = pr.nye;
+        F.r   = R.hx * R.hx / R.hy / R.hy;
+        F.alpha = eig_of(nx);
+        F.beta  = eig_of(ny);
+        double* sig  = b;
+        double* sigp = sig + 2 * ny;
+        double* v    = sigp + 2 * nx;
+        F.gX  = v;
+        F.zX  = v + 2 * ny;
+        F.yX  = v + 4 * ny;
+        F.bX  = v + 6 * ny;
+        F.bX2 = v + 8 * ny;
+        v += 10 * ny;
+        F.gY   = v;
+        F.rhsY = v + 2 * nx;
+        F.yY   = v + 4 * nx;
+        F.sY   = v + 6 * nx;
+        v += 8 * nx;
+        double* Gd = v;  // G[(e*2+e2)*ny + k]
+        double* Hd = v + 4 * ny;
+        double* ix = Hd + 4 * nx;
+        double* iy = ix + 4 * ny;
+        F.invxx    = ix;
+        F.invyy    = iy;
+        for (int e = 0; e < pr.nxe; ++e)
+        {
+            const Dom& L = dom_[pr.xe[e]];
+            F.ie[e]      = L.root_face == XNEG ? 0 : nx - 1;
+            F.sig[e]     = sig + e * ny;
+            const int il = L.leaf_face == XNEG ? 0 : L.d.nx - 1;
+            greq.push_back({L.d.nx, il, il, ny, eig_of(L.d.nx), F.beta, L.d.hx * L.d.hx / L.d.hy / L.d.hy,
+                            sig + e * ny});
+            gcnt.push_back(ny);
+            for (int e2 = 0; e2 < pr.nxe; ++e2)
+            {
+                const Dom& L2 = dom_[pr.xe[e2]];
+                const int  i2 = L2.root_face == XNEG ? 0 : nx - 1;
+                greq.push_back({nx, F.ie[e], i2, ny, F.alpha, F.beta, F.r, Gd + (e * 2 + e2) * ny});
+                gcnt.push_back(ny);
+            }
+        }
+        for (int Y = 0; Y < pr.nye; ++Y)
+        {
+            const Dom& L = dom_[pr.ye[Y]];
+            F.jy[Y]      = L.root_face == YNEG ? 0 : ny - 1;
+            F.sigp[Y]    = sigp + Y * nx;
+            const int jl = L.leaf_face == YNEG ? 0 : L.d.ny - 1;
+            // sig'_m = sum_k psi_k(jl)^2 / (alpha_m + r_l beta^l_k): sum index over the leaf's ny
+            const double rl = L.d.hx * L.d.hx / L.d.hy / L.d.hy;
+            {
+                // eig_a = r_l * beta^l, so that k_green's form eig_a[k] + 1 * alpha_m applies
+                std::vector<double> l = cal_lambda(L.d.ny, BC_DIRICHLET, BC_DIRICHLET);
+                for (auto& q : l) q = rl * (q - 2.0);
+                eig_keep_.push_back(upload(l));
+                greq.push_back({L.d.ny, jl, jl, nx, eig_keep_.back().template as<double>(), F.alpha, 1.0,
+                                sigp + Y * nx});
+            }
+            gcnt.push_back(nx);
+            for (int Y2 = 0; Y2 < pr.nye; ++Y2)
+            {
+                const Dom& L2 = dom_[pr.ye[Y2]];
+                const int  j2 = L2.root_face == YNEG ? 0 : ny - 1;
+                std::vector<double> l = cal_lambda(ny, BC_DIRICHLET, BC_DIRICHLET);
+                for (auto& q : l) q = F.r * (q - 2.0);
+                eig_keep_.push_back(upload(l));
+                greq.push_back({ny, F.jy[Y], j2, nx, eig_keep_.back().template as<double>(), F.alpha, 1.0,
+                                Hd + (Y * 2 + Y2) * nx});
+                gcnt.push_back(nx);
+            }
+        }
+    }
+    if (!greq.empty())
+    {
+        Segments g;
+        g.set(greq, gcnt);
+        k_green<<<grid_of(g.total * 32, 256), 256>>>(g.as<GreenReq>(), g.pre(), g.n);
+        FPB_CHECK_LAUNCH();
+        FPB_CUDA(cudaDeviceSynchronize());
+    }
+    // interface inverses (host, tiny) and reduced cross systems (device)
+    cublasHandle_t     cb = nullptr;
+    cusolverDnHandle_t cs = nullptr;
+    DevBuf             A, B, piv, info, work;
+    for (auto& pr : prob_)
+    {
+        BIface&   F  = pr.F;
+        const int nx = F.nx, ny = F.ny;
+        double*   b  = pr.mem.template as<double>();
+        double*   Gd = b + 2 * ny + 2 * nx + 10 * ny + 8 * nx;
+        double*   Hd = Gd + 4 * ny;
+        std::vector<double> G(4 * ny), H(4 * nx), sg(2 * ny), sp(2 * nx);
+        FPB_CUDA(cudaMemcpy(G.data(), Gd, G.size() * 8, cudaMemcpyDeviceToHost));
+        FPB_CUDA(cudaMemcpy(H.data(), Hd, H.size() * 8, cudaMemcpyDeviceToHost));
+        FPB_CUDA(cudaMemcpy(sg.data(), b, sg.size() * 8, cudaMemcpyDeviceToHost));
+        FPB_CUDA(cudaMemcpy(sp.data(), b + 2 * ny, sp.size() * 8, cudaMemcpyDeviceToHost));
+        auto inv_blocks = [](int E, int n, const std::vector<double>& Gm, const std::vector<double>& s) {
+            // M = I - G(e, e2) s_e2 per mode; returns row-major E x E inverses per mode
+            std::vector<double> out((size_t)n * E * E, 0.0);
+            for (int q = 0; q < n; ++q)
+            {
+                if (E == 1)
+                {
+                    out[q] = 1.0 / (1.0 - Gm[q] * s[q]);
+                }
+                else if (E == 2)
+                {
+                    const double a = 1.0 - Gm[0 * n + q] * s[q], bb = -Gm[1 * n + q] * s[n + q];
+                    const double c = -Gm[2 * n + q] * s[q], d = 1.0 - Gm[3 * n + q] * s[n + q];
+                    const double det = a * d - bb * c;
+                    out[(size_t)q * 4 + 0] = d / det;
+                    out[(size_t)q * 4 + 1] = -bb / det;
+                    out[(size_t)q * 4 + 2] = -c / det;
+                    out[(size_t)q * 4 + 3] = a / det;
+                }
+            }
+            return out;
+        };
+        if (F.nxe > 0)
+        {
+            std::vector<double> ix = inv_blocks(F.nxe, ny, G, sg);
+            FPB_CUDA(cudaMemcpy(const_cast<double*>(F.invxx), ix.data(), ix.size() * 8, cudaMemcpyHostToDevice));
+        }
+        if (F.nye > 0 && F.nxe == 0)
+        {
+            std::vector<double> iy = inv_blocks(F.nye, nx, H, sp);
+            FPB_CUDA(cudaMemcpy(const_cast<double*>(F.invyy), iy.data(), iy.size() * 8, cudaMemcpyHostToDevice));
+        }
+        if (F.nxe > 0 && F.nye > 0)
+        {
+            const int nY = F.nye * nx, nX = F.nxe * ny;
+            if (!cb)
+            {
+                if (cublasCreate(&cb) != CUBLAS_STATUS_SUCCESS) throw Error(2, "cublasCreate failed");
+                if (cusolverDnCreate(&cs) != CUSOLVER_STATUS_SUCCESS) throw Error(2, "cusolverDnCreate failed");
+            }
+            A.ensure((size_t)nY * nX * 8);
+            B.ensure((size_t)nY * nX * 8);
+            pr.rinv.alloc((size_t)nY * nY * 8);
+            DevBuf Rm((size_t)nY * nY * 8);
+            k_cross_AB<<<grid_of((long long)nY * nX, 256), 256>>>(F, A.as<double>(), B.as<double>());
+            FPB_CHECK_LAUNCH();
+            k_myy<<<grid_of((long long)nY * nY, 256), 256>>>(F, Hd, Rm.as<double>());
+            FPB_CHECK_LAUNCH();
+            const double m1 = -1.0, one = 1.0;
+            if (cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, nY, nY, nX, &m1, A.as<double>(), nY, B.as<double>(), nX,
+                            &one, Rm.as<double>(), nY) != CUBLAS_STATUS_SUCCESS)
+                throw Error(2, "cublasDgemm failed");
+            int lw = 0;
+            if (cusolverDnDgetrf_bufferSize(cs, nY, nY, Rm.as<double>(), nY, &lw) != CUSOLVER_STATUS_SUCCESS)
+                throw Error(2, "cusolverDnDgetrf_bufferSize failed");
+            work.ensure((size_t)std::max(lw, 1) * 8);
+            piv.ensure((size_t)nY * 4);
+            info.ensure(4);
+            if (cusolverDnDgetrf(cs, nY, nY, Rm.as<double>(), nY, work.as<double>(), piv.as<int>(), info.as<int>()) !=
+                CUSOLVER_STATUS_SUCCESS)
+                throw Error(2, "cusolverDnDgetrf failed");
+            std::vector<double> I((size_t)nY * nY, 0.0);
+            for (int q = 0; q < nY; ++q) I[(size_t)q * nY + q] = 1.0;
+            FPB_CUDA(cudaMemcpy(pr.rinv.get(), I.data(), I.size() * 8, cudaMemcpyHostToDevice));
+            if (cusolverDnDgetrs(cs, CUBLAS_OP_N, nY, nY, Rm.as<double>(), nY, piv.as<int>(), pr.rinv.template as<double>(), nY,
+                                 info.as<int>()) != CUSOLVER_STATUS_SUCCESS)
+                throw Error(2, "cusolverDnDgetrs failed");
+            int hinfo = 0;
+            FPB_CUDA(cudaMemcpy(&hinfo, info.get(), 4, cudaMemcpyDeviceToHost));
+            if (hinfo != 0) throw Error(5, "singular reduced interface system");
+            F.rinv = pr.rinv.template as<double>();
+        }
+    }
+    FPB_CUDA(cudaDeviceSynchronize());
+    if (cs) cusolverDnDestroy(cs);
+    if (cb) cublasDestroy(cb);
+    for (auto& kv : eig) eig_keep_.push_back(std::move(kv.second));  // alpha / beta stay referenced
+}
+
+template <typename TS> void BatchImpl<TS>::build_static_lists()
+{
+    const int nP = (int)prob_.size();
+    // per-problem y-edge vectors: bY, gYp, sYp, yYp (nx each) for up to 2 y-edges
+    std::vector<long long> eoff(nP + 1, 0);
+    for (int p = 0; p < nP; ++p) eoff[p + 1] = eoff[p] + (long long)8 * prob_[p].F.nx;
+    edge_.alloc((size_t)std::max<long long>(eoff[nP], 1) * sizeof(double));
+    FPB_CUDA(cudaMemset(edge_.get(), 0, (size_t)std::max<long long>(eoff[nP], 1) * sizeof(double)));
+    auto ev = [&](int p, int Y, int which) {  // which: 0 bY, 1 gYp, 2 sYp, 3 yYp
+        return edge_.as<double>() + eoff[p] + (long long)(Y * 4 + which) * prob_[p].F.nx;
+    };
+    TS*       W = W_.as<TS>();
+    TS*       X = X_.as<TS>();
+    // chase scratch offsets
+    std::vector<long long> soff(dom_.size() + 1, 0);
+    for (size_t g = 0; g < dom_.size(); ++g)
+        soff[g + 1] = soff[g] + (long long)(dom_[g].d.nx / kChunk) * dom_[g].d.ny * 4;
+    auto base_seg = [&](int g, const TS* in, TS* out) {
+        ChaseSeg<TS> c{};
+        const Dom&   D = dom_[g];
+        const long long P = D.d.nx / kChunk;
+        c.in   = in;
+        c.out  = out;
+        c.nx   = D.d.nx;
+        c.ny   = D.d.ny;
+        c.tab  = D.tab;
+        c.zend = chs_.as<TS>() + soff[g];
+        c.bsep = c.zend + 2 * P * D.d.ny;
+        c.work = c.bsep + P * D.d.ny;
+        return c;
+    };
+    std::vector<ChaseSeg<TS>> l1, r1, a2;
+    std::vector<RowReq<TS>>   lr, rr;
+    std::vector<ColReq<TS>>   lc, rc;
+    std::vector<DstSeg>       eg, eo;
+    std::vector<BIface>       fk, fy, fr, fw;
+    std::vector<long long>    ck, cy, cr, cw, lrc, rrc, lcc, rcc;
+    for (int p = 0; p < nP; ++p)
+    {
+        Prob&     pr = prob_[p];
+        BIface&   F  = pr.F;
+        const int gr = pr.root;
+        const long long ro = dom_[gr].off;
+        for (int e = 0; e < pr.nxe; ++e)
+        {
+            const int   g = pr.xe[e];
+            const Dom&  L = dom_[g];
+            const int   il = L.leaf_face == XNEG ? 0 : L.d.nx - 1;
+            l1.push_back(base_seg(g, W + L.off, X + L.off));
+            lr.push_back({X + L.off, L.d.ny, il, F.bX + e * F.ny, -1.0});
+            rr.push_back({X + ro, F.ny, F.ie[e], F.gX + e * F.ny, 1.0});
+            ChaseSeg<TS> c = base_seg(g, W + L.off, X + L.off);
+            c.nrow         = 1;
+            c.row_i[0]     = il;
+            c.row_v[0]     = F.yX + e * F.ny;
+            c.row_c[0]     = -1.0;
+            a2.push_back(c);
+        }
+        for (int Y = 0; Y < pr.nye; ++Y)
+        {
+            const int  g  = pr.ye[Y];
+            const Dom& L  = dom_[g];
+            const int  jl = L.leaf_face == YNEG ? 0 : L.d.ny - 1;
+            l1.push_back(base_seg(g, W + L.off, X + L.off));
+            lc.push_back({X + L.off, L.d.nx, L.d.ny, jl, ev(p, Y, 0), -1.0});
+            rc.push_back({X + ro, F.nx, F.ny, F.jy[Y], ev(p, Y, 1), 1.0});
+            eg.push_back({ev(p, Y, 1), F.gY + Y * F.nx, 1, eplans_.get(F.nx)});
+            eo.push_back({F.sY + Y * F.nx, ev(p, Y, 2), 1, eplans_.get(F.nx)});
+            eo.push_back({F.yY + Y * F.nx, ev(p, Y, 3), 1, eplans_.get(F.nx)});
+            ChaseSeg<TS> c = base_seg(g, W + L.off, X + L.off);
+            c.ncol         = 1;
+            c.col_j[0]     = jl;
+            c.col_s[0]     = ev(p, Y, 3);
+            c.col_c[0]     = -1.0;
+            a2.push_back(c);
+        }
+        // root: first chase with the b' terms, second with b' + S y
+        ChaseSeg<TS> c1 = base_seg(gr, W + ro, X + ro), c2 = c1;
+        for (int e = 0; e < pr.nxe; ++e)
+        {
+            c1.row_i[c1.nrow] = F.ie[e];
+            c1.row_v[c1.nrow] = F.bX + e * F.ny;
+            c1.row_c[c1.nrow++] = 1.0;
+            c2.row_i[c2.nrow] = F.ie[e];
+            c2.row_v[c2.nrow] = F.bX2 + e * F.ny;
+            c2.row_c[c2.nrow++] = 1.0;
+        }
+        for (int Y = 0; Y < pr.nye; ++Y)
+        {
+            c1.col_j[c1.ncol] = F.jy[Y];
+            c1.col_s[c1.ncol] = ev(p, Y, 0);
+            c1.col_c[c1.ncol++] = 1.0;
+            c2.col_j[c2.ncol] = F.jy[Y];
+            c2.col_s[c2.ncol] = ev(p, Y, 0);
+            c2.col_c[c2.ncol++] = 1.0;
+            c2.col_j[c2.ncol] = F.jy[Y];
+            c2.col_s[c2.ncol] = ev(p, Y, 2);
+            c2.col_c[c2.ncol++] = 1.0;
+        }
+        if (pr.nxe + pr.nye > 0) r1.push_back(c1);
+        a2.push_back(c2);
+        if (pr.nxe > 0)
+        {
+            fk.push_back(F);
+            ck.push_back(F.ny);
+            fw.push_back(F);
+            cw.push_back(F.ny);
+        }
+        if (pr.nye > 0)
+        {
+            fy.push_back(F);
+            cy.push_back((long long)F.nye * F.nx);
+            fr.push_back(F);
+            cr.push_back((long long)F.nye * F.nx);
+        }
+    }
+    eplans_.finish();
+    chase1_leaf_ = l1;
+    chase1_root_ = r1;
+    chase2_all_  = a2;
+    build_chase_lists();
+    for (auto& q : lr) lrc.push_back(q.ny);
+    for (auto& q : rr) rrc.push_back(q.ny);
+    for (auto& q : lc) lcc.push_back(q.nx);
+    for (auto& q : rc) rcc.push_back(q.nx);
+    leaf_rows_.set(lr, lrc);
+    root_rows_.set(rr, rrc);
+    leaf_cols_.set(lc, lcc);
+    root_cols_.set(rc, rcc);
+    std::vector<long long> one_e(eg.size(), 1), one_o(eo.size(), 1);
+    edst_g_.set(eg, one_e);
+    edst_out_.set(eo, one_o);
+    ifk_.set(fk, ck);
+    ifkw_.set(fw, cw);
+    ifym_.set(fy, cy);
+    ifrow_.set(fr, cr);
+    // DST lists over all subdomains between internal buffers
+    std::vector<DstSeg>    dfs, dr, dou;
+    std::vector<long long> dc;
+    for (auto& D : dom_)
+    {
+        dc.push_back((D.d.nx + 1) / 2);
+        dfs.push_back({nullptr, W + D.off, D.d.nx, D.plan});
+        dou.push_back({X + D.off, nullptr, D.d.nx, D.plan});
+    }
+    dst_W_in_rec_  = dfs;
+    dst_X_out_rec_ = dou;
+    dst_counts_    = dc;
+}
+
+template <typename TS> void BatchImpl<TS>::build_chase_lists()
+{
+    const int bt = tm_.chase_threads;
+    auto mk = [&](const std::vector<ChaseSeg<TS>>& v, Segments& lc, Segments& red) {
+        std::vector<long long> a, b;
+        for (auto& c : v)
+        {
+            a.push_back(((long long)(c.nx / kChunk) * c.ny + bt - 1) / bt);
+            b.push_back((c.ny + 127) / 128);
+        }
+        lc.set(v, a);
+        red.set(v, b);
+    };
+    mk(chase1_leaf_, l1_lc_, l1_red_);
+    mk(chase1_root_, r1_lc_, r1_red_);
+    mk(chase2_all_, a2_lc_, a2_red_);
+}
+
+template <typename TS> void BatchImpl<TS>::chase_run(const Segments& lc, const Segments& red, cudaStream_t s)
+{
+    if (lc.n == 0) return;
+    const ChaseTabDev<TS>* tabs = tabs_dev_.as<ChaseTabDev<TS>>();
+    k_b_chase_local<TS><<<(unsigned)lc.total, tm_.chase_threads, 0, s>>>(lc.as<ChaseSeg<TS>>(), lc.pre(), lc.n, tabs);
+    FPB_CHECK_LAUNCH();
+    k_b_chase_reduced<TS><<<(unsigned)red.total, 128, 0, s>>>(red.as<ChaseSeg<TS>>(), red.pre(), red.n, tabs);
+    FPB_CHECK_LAUNCH();
+    k_b_chase_correct<TS><<<(unsigned)lc.total, tm_.chase_threads, 0, s>>>(lc.as<ChaseSeg<TS>>(), lc.pre(), lc.n, tabs);
+    FPB_CHECK_LAUNCH();
+}
+
+// One inner solve: dst_in (FP64 rows -> W), ..., X -> dst_out (FP64 rows; += when acc).
+template <typename TS> void BatchImpl<TS>::inner(const Segments& dst_in, const Segments& dst_out, bool acc, cudaStream_t s)
+{
+    launch_dst<TS, double, TS, false>(dst_in, plans_, tm_, s);
+    chase_run(l1_lc_, l1_red_, s);
+    if (leaf_rows_.n)
+    {
+        k_b_rowcopy<TS><<<grid_of(leaf_rows_.total, 256), 256, 0, s>>>(leaf_rows_.as<RowReq<TS>>(), leaf_rows_.pre(),
+                                                                    leaf_rows_.n);
+        FPB_CHECK_LAUNCH();
+    }
+    if (leaf_cols_.n)
+    {
+        k_b_colvals<TS><<<grid_of(leaf_cols_.total * 32, 256), 256, 0, s>>>(leaf_cols_.as<ColReq<TS>>(),
+                                                                         leaf_cols_.pre(), leaf_cols_.n);
+        FPB_CHECK_LAUNCH();
+    }
+    chase_run(r1_lc_, r1_red_, s);
+    if (root_rows_.n)
+    {
+        k_b_rowcopy<TS><<<grid_of(root_rows_.total, 256), 256, 0, s>>>(root_rows_.as<RowReq<TS>>(), root_rows_.pre(),
+                                                                    root_rows_.n);
+        FPB_CHECK_LAUNCH();
+    }
+    if (root_cols_.n)
+    {
+        k_b_colvals<TS><<<grid_of(root_cols_.total * 32, 256), 256, 0, s>>>(root_cols_.as<ColReq<TS>>(),
+                                                                         root_cols_.pre(), root_cols_.n);
+        FPB_CHECK_LAUNCH();
+    }
+    launch_dst<double, double, double, false>(edst_g_, eplans_, tm_, s);
+    if (ifk_.n)
+    {
+        k_if_zx<<<grid_of(ifk_.total, 128), 128, 0, s>>>(ifk_.as<BIface>(), ifk_.pre(), ifk_.n);
+        FPB_CHECK_LAUNCH();
+    }
+    if (ifym_.n)
+    {
+        k_if_rhsy<<<grid_of(ifym_.total * 32, 256), 256, 0, s>>>(ifym_.as<BIface>(), ifym_.pre(), ifym_.n);
+        FPB_CHECK_LAUNCH();
+        k_if_yy<<<grid_of(ifrow_.total, 128), 128, 0, s>>>(ifrow_.as<BIface>(), ifrow_.pre(), ifrow_.n);
+        FPB_CHECK_LAUNCH();
+    }
+    if (ifkw_.n)
+    {
+        k_if_yx<<<grid_of(ifkw_.total * 32, 256), 256, 0, s>>>(ifkw_.as<BIface>(), ifkw_.pre(), ifkw_.n);
+        FPB_CHECK_LAUNCH();
+    }
+    launch_dst<double, double, double, false>(edst_out_, eplans_, tm_, s);
+    chase_run(a2_lc_, a2_red_, s);
+    if (acc) launch_dst<TS, TS, double, true>(dst_out, plans_, tm_, s);
+    else launch_dst<TS, TS, double, false>(dst_out, plans_, tm_, s);
+}
+
+template <typename TS>
+void BatchImpl<TS>::set_user_lists(double* const* fields, const double* const* ghosts, int steps)
+{
+    const int nd = (int)dom_.size();
+    std::vector<double*>       f(fields, fields + nd);
+    std::vector<const double*> gh;
+    if (ghosts) gh.assign(ghosts, ghosts + 4 * nd);
+    if (f == user_ptrs_ && gh == user_ghosts_ && steps == user_steps_) return;
+    if (graph_)
+    {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+    FPB_CUDA(cudaDeviceSynchronize());  // the lists below may still be read by queued work
+    user_ptrs_   = f;
+    user_ghosts_ = gh;
+    user_steps_  = steps;
+    const bool ir = steps > 0;
+    if (ir && !fs_.get())
+    {
+        fs_.alloc((size_t)cells_ * 8);
+        u_.alloc((size_t)cells_ * 8);
+        r_.alloc((size_t)cells_ * 8);
+        // IR lists between internal buffers
+        std::vector<DstSeg> a = dst_W_in_rec_, b = dst_W_in_rec_, c = dst_X_out_rec_;
+        for (size_t g = 0; g < dom_.size(); ++g)
+        {
+            a[g].in  = fs_.as<double>() + dom_[g].off;
+            b[g].in  = r_.as<double>() + dom_[g].off;
+            c[g].out = u_.as<double>() + dom_[g].off;
+        }
+        dst_fs_.set(a, dst_counts_);
+        dst_r_.set(b, dst_counts_);
+        dst_out_u_.set(c, dst_counts_);
+        std::vector<ResSeg>    rs;
+        std::vector<long long> rc;
+        for (size_t g = 0; g < dom_.size(); ++g) rs.push_back(res_seg(g, r_.as<double>(), fs_.as<double>(), nullptr));
+        for (auto& q : rs) rc.push_back((q.a.nx * (long long)q.a.ny + 255) / 256);
+        res_.set(rs, rc);
+    }
+    std::vector<AsmSeg>    as;
+    std::vector<long long> ac;
+    std::vector<DstSeg>    di = dst_W_in_rec_, dout = dst_X_out_rec_;
+    std::vector<CopySeg>   cp;
+    std::vector<long long> cc;
+    for (int g = 0; g < nd; ++g)
+    {
+        const Domain& D = dom_[g].d;
+        AsmSeg        q{};
+        q.f    = f[g];
+        q.copy = ir ? fs_.as<double>() + dom_[g].off : nullptr;
+        q.a.nx = D.nx;
+        q.a.ny = D.ny;
+        q.a.hx = D.hx;
+        q.a.hy = D.hy;
+        for (int k = 0; k < 4; ++k)
+        {
+            q.a.bc[k]    = D.bc[k];
+            q.a.ghost[k] = gh.empty() ? nullptr : gh[4 * g + k];
+        }
+        as.push_back(q);
+        ac.push_back((D.cells() + 255) / 256);
+        di[g].in   = f[g];
+        dout[g].out = f[g];
+        cp.push_back({f[g], ir ? u_.as<double>() + dom_[g].off : nullptr, D.cells()});
+        cc.push_back((D.cells() + 255) / 256);
+    }
+    asm_user_.set(as, ac);
+    dst_user_in_.set(di, dst_counts_);
+    dst_user_out_.set(dout, dst_counts_);
+    if (ir) copy_out_.set(cp, cc);
+}
+
+template <typename TS> ResSeg BatchImpl<TS>::res_seg(size_t g, double* r, const double* fs, const double* const* u_user)
+{
+    const Domain& D = dom_[g].d;
+    ResSeg        q{};
+    auto          U = [&](size_t h) -> const double* { return u_user ? u_user[h] : u_.as<double>() + dom_[h].off; };
+    q.r    = r ? r + dom_[g].off : nullptr;
+    q.fs   = fs + dom_[g].off;
+    q.u    = U(g);
+    q.a.nx = D.nx;
+    q.a.ny = D.ny;
+    q.a.r2 = D.hx * D.hx / D.hy / D.hy;
+    for (int f = 0; f < 4; ++f)
+    {
+        q.a.bc[f] = D.bc[f];
+        q.a.nb[f] = nullptr;
+    }
+    const Dom& d = dom_[g];
+    const Prob& pr = prob_[d.prob];
+    if (d.role == 1)
+    {
+        const Dom& R        = dom_[pr.root];
+        q.a.nb[d.leaf_face] = U(pr.root);
+        q.a.nbnx[d.leaf_face] = R.d.nx;
+        q.a.nbny[d.leaf_face] = R.d.ny;
+    }
+    else
+    {
+        for (int h = pr.g0; h < pr.g0 + pr.nd; ++h)
+        {
+            if (dom_[h].role != 1) continue;
+            const int f   = dom_[h].root_face;
+            q.a.nb[f]     = U(h);
+            q.a.nbnx[f]   = dom_[h].d.nx;
+            q.a.nbny[f]   = dom_[h].d.ny;
+        }
+    }
+    return q;
+}
+
+template <typename TS> void BatchImpl<TS>::run(int steps, cudaStream_t s)
+{
+    k_b_assemble<<<(unsigned)asm_user_.total, 256, 0, s>>>(asm_user_.as<AsmSeg>(), asm_user_.pre(), asm_user_.n);
+    FPB_CHECK_LAUNCH();
+    if (steps == 0)
+    {
+        inner(dst_user_in_, dst_user_out_, false, s);
+        return;
+    }
+    inner(dst_fs_, dst_out_u_, false, s);
+    for (int k = 1; k < steps; ++k)
+    {
+        k_b_residual<<<(unsigned)res_.total, 256, 0, s>>>(res_.as<ResSeg>(), res_.pre(), res_.n);
+        FPB_CHECK_LAUNCH();
+        inner(dst_r_, dst_out_u_, true, s);
+    }
+    k_b_copy<<<(unsigned)copy_out_.total, 256, 0, s>>>(copy_out_.as<CopySeg>(), copy_out_.pre(), copy_out_.n);
+    FPB_CHECK_LAUNCH();
+}
+
+template <typename TS>
+void BatchImpl<TS>::solve(double* const* fields, const double* const* ghosts, int steps, cudaStream_t s)
+{
+    if (!fields) throw Error(1, "null field list");
+    for (int g = 0; g < (int)dom_.size(); ++g)
+        if (!fields[g]) throw Error(1, "null field pointer");
+    if (steps < 0 || steps > 64) throw Error(1, "steps must be in [0, 64]");
+    set_user_lists(fields, ghosts, steps);
+    run(steps, s);
+}
+
+template <typename TS> void BatchImpl<TS>::solve_graph(double* const* fields, const double* const* ghosts, int steps,
+                                                       cudaStream_t s)
+{
+    if (!fields) throw Error(1, "null field list");
+    if (steps < 0 || steps > 64) throw Error(1, "steps must be in [0, 64]");
+    set_user_lists(fields, ghosts, steps);
+    if (!graph_)
+    {
+        cudaStream_t cap;
+        FPB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaGraph_t g     = nullptr;
+        const long long before = launches_noted();
+        FPB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        try
+        {
+            run(steps, cap);
+        }
+        catch (...)
+        {
+            cudaStreamEndCapture(cap, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaStreamDestroy(cap);
+            throw;
+        }
+        FPB_CUDA(cudaStreamEndCapture(cap, &g));
+        graph_kernels_ = launches_noted() - before;
+        const cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
+        cudaGraphDestroy(g);
+        cudaStreamDestroy(cap);
+        FPB_CUDA(e);
+    }
+    FPB_CUDA(cudaGraphLaunch(graph_, s));
+    note_launches(graph_kernels_);
+}
+
+template <typename TS>
+void BatchImpl<TS>::residuals(const double* const* u, const double* const* rhs, const double* const* ghosts,
+                              cudaStream_t s, double* out)
+{
+    const int nd = (int)dom_.size();
+    DevBuf    fs((size_t)cells_ * 8);
+    std::vector<AsmSeg>    as;
+    std::vector<ResSeg>    rs;
+    std::vector<long long> ac, bo(nd + 1, 0);
+    for (int g = 0; g < nd; ++g)
+    {
+        const Domain& D = dom_[g].d;
+        AsmSeg        q{};
+        q.f    = const_cast<double*>(rhs[g]);
+        q.copy = fs.as<double>() + dom_[g].off;
+        q.a.nx = D.nx;
+        q.a.ny = D.ny;
+        q.a.hx = D.hx;
+        q.a.hy = D.hy;
+        for (int k = 0; k < 4; ++k)
+        {
+            q.a.bc[k]    = D.bc[k];
+            q.a.ghost[k] = ghosts ? ghosts[4 * g + k] : nullptr;
+        }
+        as.push_back(q);
+        ac.push_back((D.cells() + 255) / 256);
+        bo[g + 1] = bo[g] + ac.back();
+    }
+    DevBuf pa((size_t)bo[nd] * 8), pf((size_t)bo[nd] * 8);
+    for (int g = 0; g < nd; ++g)
+    {
+        ResSeg q      = res_seg(g, nullptr, fs.as<double>(), u);
+        q.fs          = fs.as<double>() + dom_[g].off;
+        q.partial     = pa.as<double>() + bo[g];
+        q.partial_f   = pf.as<double>() + bo[g];
+        rs.push_back(q);
+    }
+    Segments A, R;
+    A.set(as, ac);
+    R.set(rs, ac);
+    k_b_assemble<<<(unsigned)A.total, 256, 0, s>>>(A.as<AsmSeg>(), A.pre(), A.n);
+    FPB_CHECK_LAUNCH();
+    k_b_residual<<<(unsigned)R.total, 256, 0, s>>>(R.as<ResSeg>(), R.pre(), R.n);
+    FPB_CHECK_LAUNCH();
+    std::vector<double> ha(bo[nd]), hf(bo[nd]);
+    FPB_CUDA(cudaMemcpyAsync(ha.data(), pa.get(), ha.size() * 8, cudaMemcpyDeviceToHost, s));
+    FPB_CUDA(cudaMemcpyAsync(hf.data(), pf.get(), hf.size() * 8, cudaMemcpyDeviceToHost, s));
+    FPB_CUDA(cudaStreamSynchronize(s));
+    for (size_t p = 0; p < prob_.size(); ++p)
+    {
+        double rr = 0, ff = 0;
+        for (int g = prob_[p].g0; g < prob_[p].g0 + prob_[p].nd; ++g)
+            for (long long b = bo[g]; b < bo[g + 1]; ++b)
+            {
+                rr += ha[b];
+                ff += hf[b];
+            }
+        out[p] = ff > 0 ? std::sqrt(rr / ff) : std::sqrt(rr);
+    }
+}
+
+// Launch shapes by measurement: the DST over all subdomains (threads per CTA x CTAs per SM) and the
+// chase (threads per CTA), each candidate timed with CUDA events on the real work lists (contents of
+// the work buffers are irrelevant to the timing; they are zeroed first).
+template <typename TS> void BatchImpl<TS>::autotune(cudaStream_t s)
+{
+    FPB_CUDA(cudaMemsetAsync(W_.get(), 0, (size_t)cells_ * sizeof(TS), s));
+    FPB_CUDA(cudaMemsetAsync(X_.get(), 0, (size_t)cells_ * sizeof(TS), s));
+    std::vector<DstSeg> rec = dst_X_out_rec_;
+    for (size_t g = 0; g < dom_.size(); ++g) rec[g].out = W_.as<TS>() + dom_[g].off;
+    Segments sg;
+    sg.set(rec, dst_counts_);
+    cudaEvent_t e0, e1;
+    FPB_CUDA(cudaEventCreate(&e0));
+    FPB_CUDA(cudaEventCreate(&e1));
+    auto time_it = [&](auto&& fn) {
+        fn();
+        FPB_CUDA(cudaEventRecord(e0, s));
+        for (int r = 0; r < 3; ++r) fn();
+        FPB_CUDA(cudaEventRecord(e1, s));
+        FPB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        FPB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms;
+    };
+    BatchTiming best = tm_;
+    float       bt   = 1e30f;
+    for (int th : {128, 256, 512})
+        for (int bps : {1, 2, 4, 8})
+        {
+            tm_.dst_threads       = th;
+            tm_.dst_blocks_per_sm = bps;
+            int occ = 0;
+            prep_dst<TS, TS, TS, false>();
+            FPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_dst<TS, TS, TS, false>, th, plans_.smem));
+            if (occ < bps) continue;
+            const float t = time_it([&] { launch_dst<TS, TS, TS, false>(sg, plans_, tm_, s); });
+            if (t < bt)
+            {
+                bt   = t;
+                best = tm_;
+            }
+        }
+    tm_ = best;
+    bt  = 1e30f;
+    for (int th : {128, 256})
+    {
+        tm_.chase_threads = th;
+        build_chase_lists();
+        const float t = time_it([&] { chase_run(a2_lc_, a2_red_, s); });
+        if (t < bt)
+        {
+            bt                 = t;
+            best.chase_threads = th;
+        }
+    }
+    tm_ = best;
+    build_chase_lists();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (graph_)
+    {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+}
+
+std::unique_ptr<BatchBase> make_batch(const std::vector<BatchProblemDesc>& probs, int precision)
+{
+    if (precision == 1) return std::unique_ptr<BatchBase>(new BatchImpl<float>(probs));
+    return std::unique_ptr<BatchBase>(new BatchImpl<double>(probs));
+}
+
+}  // namespace fpb

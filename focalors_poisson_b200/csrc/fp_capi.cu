@@ -20,6 +20,8 @@ namespace
 std::atomic<long long> g_launches{0};
 }
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launches_noted() { return (long long)g_launches.load(std::memory_order_relaxed); }
 
 const char* last_error() { return g_last_error.c_str(); }
 

@@ -61,7 +61,9 @@ template <typename F> int guarded(F&& f)
     } while (0)
 
 // Every kernel launch is followed by FPB_CHECK_LAUNCH(), which also counts it (fp_launch_count()).
-void note_launch();
+void      note_launch();
+void      note_launches(long long n);  // kernels of a replayed CUDA graph
+long long launches_noted();
 #define FPB_CHECK_LAUNCH()                                                                               \
     do                                                                                                   \
     {                                                                                                    \

@@ -1,5 +1,6 @@
 // Small device operations of the composite solve: boundary assembly and h^2 scaling, interface
 // coupling (bond_add), edge gather/scatter, dense Schur matrix-vector products, deterministic BLAS-1.
+// Included by more than one translation unit: the non-template kernels have internal linkage.
 #pragma once
 
 #include "fp_common.cuh"
@@ -32,10 +33,8 @@ struct AssembleArgs
 // f = (f + boundary terms) * hx^2 in the order of ConcatPoissonSolver2D::boundary_assembly
 // (pe/concat/concat_solver2d.cpp:159-223: Dirichlet faces x-,x+,y-,y+ then Neumann faces) followed by
 // the hx^2 scaling of solve() (:111-116).
-template <typename T> __global__ void k_assemble_scale(T* __restrict__ f, const AssembleArgs a)
+template <typename T> __device__ __forceinline__ void assemble_at(T* __restrict__ f, long long t, const AssembleArgs& a)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)a.nx * a.ny) return;
     const int i = (int)(t / a.ny), j = (int)(t % a.ny);
     double    v = f[t];
     const bool on[4] = {i == 0, i == a.nx - 1, j == 0, j == a.ny - 1};
@@ -50,6 +49,12 @@ template <typename T> __global__ void k_assemble_scale(T* __restrict__ f, const 
             if (on[face] && a.bc[face] == 1) v += nco[face] * (a.ghost[face] ? a.ghost[face][idx[face]] : 0.0);
     }
     f[t] = (T)(v * (a.hx * a.hx));
+}
+template <typename T> __global__ void k_assemble_scale(T* __restrict__ f, const AssembleArgs a)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)a.nx * a.ny) return;
+    assemble_at(f, t, a);
 }
 
 // dst.bond_add(loc, a, src): dst's face `loc` += a * src's opposite face (field2.cpp:257-302).
@@ -144,7 +149,7 @@ __device__ __forceinline__ double block_sum(double v, double* sh)
 }
 
 // out[0] = sum_i a[i] * b[i]  (b == a: squared norm). partials: kRedBlocks doubles; ticket: 1 uint (zero)
-__global__ void k_dot(const double* __restrict__ a, const double* __restrict__ b, long long n, double* partials,
+static __global__ void k_dot(const double* __restrict__ a, const double* __restrict__ b, long long n, double* partials,
                       unsigned* ticket, double* out, int take_sqrt)
 {
     __shared__ double sh[32];
@@ -171,27 +176,27 @@ __global__ void k_dot(const double* __restrict__ a, const double* __restrict__ b
 }
 
 // y += coef * x, coef = sign * (*c)  (coefficient read from device memory)
-__global__ void k_axpy_dev(double* __restrict__ y, const double* __restrict__ x, long long n, const double* c, double sign)
+static __global__ void k_axpy_dev(double* __restrict__ y, const double* __restrict__ x, long long n, const double* c, double sign)
 {
     const double a = sign * (*c);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         y[i] += a * x[i];
 }
 // y = (1 / *h) * x + 0
-__global__ void k_scale_inv(double* __restrict__ y, const double* __restrict__ x, long long n, const double* h)
+static __global__ void k_scale_inv(double* __restrict__ y, const double* __restrict__ x, long long n, const double* h)
 {
     const double a = 1.0 / (*h);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         y[i] = 0.0 + a * x[i];
 }
 // r = b + (-1) * ax
-__global__ void k_sub(double* __restrict__ r, const double* __restrict__ b, const double* __restrict__ ax, long long n)
+static __global__ void k_sub(double* __restrict__ r, const double* __restrict__ b, const double* __restrict__ ax, long long n)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         r[i] = b[i] + -1.0 * ax[i];
 }
 // x += y_0 V_0 + y_1 V_1 + ... (applied in order per element, like sequential axpys)
-__global__ void k_multi_axpy(double* __restrict__ x, const double* __restrict__ V, long long ld, long long n,
+static __global__ void k_multi_axpy(double* __restrict__ x, const double* __restrict__ V, long long ld, long long n,
                              const double* __restrict__ y, int k)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -202,7 +207,7 @@ __global__ void k_multi_axpy(double* __restrict__ x, const double* __restrict__ 
     }
 }
 // y *= a
-__global__ void k_scale(double* __restrict__ y, double a, long long n)
+static __global__ void k_scale(double* __restrict__ y, double a, long long n)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         y[i] *= a;
@@ -223,7 +228,7 @@ namespace fpb
 // Dense interface operator and its inverse (preconditioner of the interface GMRES)
 // ---------------------------------------------------------------------------------------------
 // fields[b].edge(loc)[q] = S[q*cn + c0 + b]: column c0+b of a child's Schur matrix placed on the edge
-__global__ void k_edge_scatter_col(double* fields, long long cells, int nx, int ny, int loc, const double* S, int cn,
+static __global__ void k_edge_scatter_col(double* fields, long long cells, int nx, int ny, int loc, const double* S, int cn,
                                    int c0, int nb)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -232,7 +237,7 @@ __global__ void k_edge_scatter_col(double* fields, long long cells, int nx, int 
     fields[b * cells + edge_index(loc, nx, ny, q)] = S[(long long)q * cn + c0 + b];
 }
 // K[(off+q)*ld + c0 + b] = fields[b].edge(loc)[q]
-__global__ void k_edge_gather_col(double* K, long long ld, int off, const double* fields, long long cells, int nx,
+static __global__ void k_edge_gather_col(double* K, long long ld, int off, const double* fields, long long cells, int nx,
                                   int ny, int loc, int cn, int c0, int nb)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -241,7 +246,7 @@ __global__ void k_edge_gather_col(double* K, long long ld, int off, const double
     K[(long long)(off + q) * ld + c0 + b] = fields[b * cells + edge_index(loc, nx, ny, q)];
 }
 // A = I - A (n x n)
-__global__ void k_identity_minus(double* A, int n)
+static __global__ void k_identity_minus(double* A, int n)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)n * n) return;
@@ -249,7 +254,7 @@ __global__ void k_identity_minus(double* A, int n)
     A[t]              = (i == j ? 1.0 : 0.0) - A[t];
 }
 // A = 2I - A (n x n)
-__global__ void k_two_identity_minus(double* A, int n)
+static __global__ void k_two_identity_minus(double* A, int n)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)n * n) return;
@@ -257,7 +262,7 @@ __global__ void k_two_identity_minus(double* A, int n)
     A[t]              = (i == j ? 2.0 : 0.0) - A[t];
 }
 // X = s * M^T (row-major n x n)
-__global__ void k_scaled_transpose(double* X, const double* M, int n, double s)
+static __global__ void k_scaled_transpose(double* X, const double* M, int n, double s)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)n * n) return;
@@ -265,7 +270,7 @@ __global__ void k_scaled_transpose(double* X, const double* M, int n, double s)
     X[t]              = s * M[j * n + i];
 }
 // rowsum[i] = sum_j |A[i][j]| and colsum[j] = sum_i |A[i][j]| (one thread per row / column)
-__global__ void k_abs_sums(const double* A, int n, double* rowsum, double* colsum)
+static __global__ void k_abs_sums(const double* A, int n, double* rowsum, double* colsum)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
@@ -279,7 +284,7 @@ __global__ void k_abs_sums(const double* A, int n, double* rowsum, double* colsu
     colsum[t] = c;
 }
 // out[0] = sum_{ij} (I - P)_{ij}^2 (deterministic: per-block partials, last block adds them in order)
-__global__ void k_identity_residual(const double* __restrict__ P, int n, double* partials, unsigned* ticket,
+static __global__ void k_identity_residual(const double* __restrict__ P, int n, double* partials, unsigned* ticket,
                                     double* out)
 {
     __shared__ double sh[32];
@@ -309,7 +314,7 @@ __global__ void k_identity_residual(const double* __restrict__ P, int n, double*
     }
 }
 // y (+)= X g, row-major n x n, one warp per row
-__global__ void k_dense_matvec(const double* __restrict__ X, int n, const double* __restrict__ g,
+static __global__ void k_dense_matvec(const double* __restrict__ X, int n, const double* __restrict__ g,
                                double* __restrict__ y, int accumulate)
 {
     const int row  = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
@@ -322,7 +327,7 @@ __global__ void k_dense_matvec(const double* __restrict__ X, int n, const double
     if (lane == 0) y[row] = accumulate ? y[row] + acc : acc;
 }
 // r = g - y + field.edge(loc)   on one child's interface block
-__global__ void k_interface_residual(double* r, const double* g, const double* y, const double* field, int nx, int ny,
+static __global__ void k_interface_residual(double* r, const double* g, const double* y, const double* field, int nx, int ny,
                                      int loc, int cn)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -349,11 +354,8 @@ struct ResidualArgs
 // (Dirichlet), mirrored (Neumann), wrapped (periodic); an Adjacented face contributes the neighbour's
 // adjacent cell with coefficient 1 -- the operator ConcatPoissonSolver2D::solve inverts
 // (pe/concat/concat_solver2d.cpp:101-157, interface terms from bond_add with coefficient -1).
-__global__ void k_composite_residual(double* __restrict__ r, const double* __restrict__ fs,
-                                     const double* __restrict__ u, const ResidualArgs a)
+__device__ __forceinline__ double composite_lap(const double* __restrict__ u, long long t, const ResidualArgs& a)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)a.nx * a.ny) return;
     const int    i = (int)(t / a.ny), j = (int)(t % a.ny);
     const int    nx = a.nx, ny = a.ny;
     const double c  = u[t];
@@ -380,6 +382,13 @@ __global__ void k_composite_residual(double* __restrict__ r, const double* __res
                                                    (j > 0 || a.bc[2] != 3 ? ym : 0.0) - 2.0 * c) +
                        ((j == ny - 1 && a.bc[3] == 3) ? ycoef_p * yp : 0.0) +
                        ((j == 0 && a.bc[2] == 3) ? ycoef_m * ym : 0.0);
-    r[t] = fs[t] - lap;
+    return lap;
+}
+static __global__ void k_composite_residual(double* __restrict__ r, const double* __restrict__ fs,
+                                     const double* __restrict__ u, const ResidualArgs a)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)a.nx * a.ny) return;
+    r[t] = fs[t] - composite_lap(u, t, a);
 }
 }  // namespace fpb

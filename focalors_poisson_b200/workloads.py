@@ -185,9 +185,9 @@ def adjoint_case(n: int = 512, seed: int = 2024, probes: int = 64):
 SIDES = tuple(range(64, 1025, 32))  # {64, 96, ..., 1024}: 31 side lengths
 
 
-def lt_problem(seed: int) -> Geometry:
+def lt_problem(seed: int, sides=SIDES) -> Geometry:
     """One problem of the batched-uneven workload: an L (3 subdomains) or T (4 subdomains) shape, free side
-    lengths drawn uniformly from SIDES with numpy default_rng(seed), homogeneous Dirichlet outer faces,
+    lengths drawn uniformly from `sides` with numpy default_rng(seed), homogeneous Dirichlet outer faces,
     one grid step h = 1/max(side) for every subdomain. Centre C (index 0) is the tree root.
 
       L: C (a x b); X at C's x+ face (c x b); Y at C's y+ face (a x d)
@@ -195,7 +195,7 @@ def lt_problem(seed: int) -> Geometry:
     """
     rng = np.random.default_rng(seed)
     shape = "L" if rng.integers(0, 2) == 0 else "T"
-    draw = lambda: int(SIDES[rng.integers(0, len(SIDES))])  # noqa: E731
+    draw = lambda: int(sides[rng.integers(0, len(sides))])  # noqa: E731
     a, b, c, d = draw(), draw(), draw(), draw()
     if shape == "L":
         nx, ny = [a, c, a], [b, b, d]

@@ -162,6 +162,37 @@ int fp_composite_residual(fp_composite* c, const double* const* u, const double*
 int fp_composite_tree(const fp_composite* c, int* root, int* level_of);
 int fp_composite_destroy(fp_composite* c);
 
+/* ---------------------------------------------------------------------------------------------------
+ * Batched composite solves: many independent ConcatPoissonSolver2D problems of uneven sizes solved
+ * together (pe/concat/concat_solver2d.cpp:101-157 per problem), every stage one launch over all problems.
+ * No counterpart in the reference, which solves one geometry per solver object; each problem is what a
+ * ConcatPoissonSolver2D over that geometry computes (the converged solution of its Schur GMRES).
+ * Supported problems: a root rectangle with leaf rectangles attached on full faces (depth-1 tree: L, T,
+ * cross), every outer face Dirichlet, nx of every subdomain a multiple of 32 and >= 64; others give
+ * FP_ERR_UNSUPPORTED. The interface system is solved exactly in the DST bases (closed-form responses,
+ * one dense reduced system per problem whose inverse is built at creation).
+ * ------------------------------------------------------------------------------------------------- */
+typedef struct fp_batch fp_batch;
+#define FP_BATCH_F32 64          /* create flag: FP32 storage and arithmetic in the inner solves */
+#define FP_BATCH_NO_AUTOTUNE 128 /* create flag: keep the default launch shapes (no timing at creation) */
+#define FP_BATCH_GRAPH 256       /* solve flag: capture the launch sequence into a CUDA graph once per
+                                    (field pointers, steps) and replay it on later calls */
+/* problems[p].root is ignored (the reference's rule picks the root). */
+int fp_batch_create(const fp_geometry* problems, int n_problems, int flags, fp_batch** out);
+/* fields: device pointers (FP_DEVICE required), one per subdomain, problems back to back in creation
+ * order; solved in place. ghosts: 4 device pointers per subdomain (or null entries / null). steps == 0:
+ * one solve in the storage precision; steps >= 1: that many inner solves in FP64 iterative refinement
+ * (FP64 residual of the composite operator). Queued on `stream`; FP_SYNC waits. */
+int fp_batch_solve(fp_batch* b, double* const* fields, const double* const* ghosts, int flags, void* stream,
+                   int steps);
+/* Per-problem |fs - A u| / |fs| (as fp_composite_residual); rel_residuals: host array of n_problems. */
+int fp_batch_residuals(fp_batch* b, const double* const* u, const double* const* rhs, const double* const* ghosts,
+                       void* stream, double* rel_residuals);
+/* Counts, the autotuned launch shape (DST threads per CTA, DST CTAs per SM, chase threads per CTA) and the
+ * number of kernels in the captured graph (0 before the first FP_BATCH_GRAPH solve). */
+int fp_batch_info(const fp_batch* b, int* n_problems, int* n_domains, int* launch_shape, long long* graph_kernels);
+int fp_batch_destroy(fp_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -158,6 +158,22 @@ def lt_shapes():
         composite(f"lt_shape_{seed}.npz", g, W.gaussian_rhs(g, 40 + seed, zero_mean=False), 20, 1e-12, 100)
 
 
+def batch_lt():
+    """Small problems of the batched-uneven workload (L and T shapes, sides 64 / 96 / 128), one of them
+    with non-zero Dirichlet ghost values."""
+    for k, seed in enumerate((11, 12, 13, 14)):
+        g = W.lt_problem(seed, sides=(64, 96, 128))
+        rhs = W.gaussian_rhs(g, 500 + seed, zero_mean=False)
+        ghosts = None
+        if k == 3:
+            rng = np.random.default_rng(600)
+            ghosts = [[None if g.bc[i][f] == ADJ or any(c[0] == i and c[1] == f or c[2] == i and c[1] == (f ^ 1)
+                                                         for c in g.connections)
+                       else rng.standard_normal(g.ny[i] if f < 2 else g.nx[i]) for f in range(4)]
+                      for i in range(g.n_domains)]
+        composite(f"batch_lt_{k}.npz", g, rhs, 20, 1e-12, 200, ghosts=ghosts)
+
+
 def tree9():
     g = W.tree9(16)
     composite("tree9_periodic.npz", g, W.gaussian_bumps_rhs(g, 9), 20, 1e-12, 100)
@@ -183,5 +199,6 @@ if __name__ == "__main__":
     cross_neumann()
     cross_ghosts()
     lt_shapes()
+    batch_lt()
     tree9()
     mocks()
