@@ -47,7 +47,7 @@ SIGNATURES = {
     "fp_batch_destroy": ([_vp], _i),
 }
 FP_GMRES_FULLFIELD, FP_CHECK_CONVERGENCE, FP_NO_INTERFACE_INVERSE, FP_IR_INNER_F64 = 4, 8, 16, 32
-FP_BATCH_F32, FP_BATCH_NO_AUTOTUNE, FP_BATCH_GRAPH = 64, 128, 256
+FP_BATCH_F32, FP_BATCH_NO_AUTOTUNE, FP_BATCH_GRAPH, FP_NO_SPECTRAL = 64, 128, 256, 512
 
 
 class Geometry(ctypes.Structure):
@@ -168,7 +168,8 @@ class Composite:
     [(a, face of a, b)] -- e.g. focalors_poisson_b200.workloads.Geometry.
     """
 
-    def __init__(self, geo, m=20, tol=1e-8, max_iter=100, root=-1, fullfield=False, interface_inverse=True):
+    def __init__(self, geo, m=20, tol=1e-8, max_iter=100, root=-1, fullfield=False, interface_inverse=True,
+                 spectral=True):
         nd = len(geo.nx)
         self.nd = nd
         self.shapes = [(int(a), int(b)) for a, b in zip(geo.nx, geo.ny)]
@@ -182,7 +183,8 @@ class Composite:
                      a["bc"].ctypes.data, len(geo.connections), a["conn"].ctypes.data if len(geo.connections) else None,
                      int(root))
         h = ctypes.c_void_p()
-        flags = (FP_GMRES_FULLFIELD if fullfield else 0) | (0 if interface_inverse else FP_NO_INTERFACE_INVERSE)
+        flags = (FP_GMRES_FULLFIELD if fullfield else 0) | (0 if interface_inverse else FP_NO_INTERFACE_INVERSE) | \
+            (0 if spectral else FP_NO_SPECTRAL)
         check(lib().fp_composite_create(ctypes.byref(g), int(m), float(tol), int(max_iter), flags, ctypes.byref(h)))
         self.h = h
 

@@ -184,18 +184,19 @@ template <typename T> struct ModCtx
 };
 
 template <typename T>
-__device__ __forceinline__ void mod_init(const ChaseSeg<T>& sg, int k, ModCtx<T>& m)
+__device__ __forceinline__ void mod_init(const ChaseSeg<T>* __restrict__ sg, int ncol, int k, ModCtx<T>& m)
 {
-    for (int c = 0; c < sg.ncol; ++c) m.psi[c] = sg.col_c[c] * dst_basis(sg.ny, k, sg.col_j[c]);
+    for (int c = 0; c < ncol; ++c) m.psi[c] = sg->col_c[c] * dst_basis(sg->ny, k, sg->col_j[c]);
 }
 template <typename T>
-__device__ __forceinline__ T mod_rhs(const ChaseSeg<T>& sg, const ModCtx<T>& m, int i, int k, T raw)
+__device__ __forceinline__ T mod_rhs(const ChaseSeg<T>* __restrict__ sg, int nrow, int ncol, const ModCtx<T>& m, int i,
+                                     int k, T raw)
 {
-    if (sg.nrow == 0 && sg.ncol == 0) return raw;
+    if (nrow == 0 && ncol == 0) return raw;
     double v = (double)raw;
-    for (int r = 0; r < sg.nrow; ++r)
-        if (sg.row_i[r] == i) v += sg.row_c[r] * sg.row_v[r][k];
-    for (int c = 0; c < sg.ncol; ++c) v += m.psi[c] * sg.col_s[c][i];
+    for (int r = 0; r < nrow; ++r)
+        if (sg->row_i[r] == i) v += sg->row_c[r] * sg->row_v[r][k];
+    for (int c = 0; c < ncol; ++c) v += m.psi[c] * sg->col_s[c][i];
     return (T)v;
 }
 
@@ -205,24 +206,23 @@ __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __rest
                                                        const long long* __restrict__ prefix, int nseg,
                                                        const ChaseTabDev<T>* __restrict__ tabs)
 {
-    constexpr int Li = kChunk - 1;
-    const int     s  = seg_of(prefix, nseg, blockIdx.x);
-    const ChaseSeg<T> sg = segs[s];
-    const long long t  = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
-    const int       ny = sg.ny, P = sg.nx / kChunk;
-    if (t >= (long long)P * ny) return;
-    const int j   = (int)(t % ny);
-    const int p   = (int)(t / ny);
+    constexpr int      Li = kChunk - 1;
+    const int          s  = seg_of(prefix, nseg, blockIdx.x);
+    const ChaseSeg<T>* sg = segs + s;
+    const int          ny = sg->ny, P = sg->nx / kChunk;
+    const int          t  = (int)(blockIdx.x - prefix[s]) * blockDim.x + threadIdx.x;
+    if (t >= P * ny) return;
+    const int j = t % ny, p = t / ny;
     const int typ = p == 0 ? 0 : 1;
-    const ChaseTabDev<T> tb = tabs[sg.tab];
-    ModCtx<T>            mc;
-    mod_init(sg, j, mc);
-    const T* col = sg.in + (long long)p * kChunk * ny + j;
-    T*       out = sg.out + (long long)p * kChunk * ny + j;
-    const T* c   = tb.cc + (long long)typ * Li * ny + j;
+    const int nrow = sg->nrow, ncol = sg->ncol;
+    ModCtx<T> mc;
+    mod_init(sg, ncol, j, mc);
+    const T* col = sg->in + (long long)p * kChunk * ny + j;
+    T*       out = sg->out + (long long)p * kChunk * ny + j;
+    const T* c   = tabs[sg->tab].cc + (long long)typ * Li * ny + j;
     T        y[Li];
 #pragma unroll
-    for (int r = 0; r < Li; ++r) y[r] = mod_rhs(sg, mc, p * kChunk + r, j, col[(long long)r * ny]);
+    for (int r = 0; r < Li; ++r) y[r] = mod_rhs(sg, nrow, ncol, mc, p * kChunk + r, j, col[(long long)r * ny]);
     T prev = 0;
 #pragma unroll
     for (int r = 0; r < Li; ++r)
@@ -234,59 +234,78 @@ __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __rest
     for (int r = Li - 2; r >= 0; --r) y[r] = y[r] - __ldg(c + (long long)r * ny) * y[r + 1];
 #pragma unroll
     for (int r = 0; r < Li; ++r) out[(long long)r * ny] = y[r];
-    T* ze  = sg.zend + (long long)(p * 2) * ny + j;
+    T* ze  = sg->zend + (long long)(p * 2) * ny + j;
     ze[0]  = y[0];
     ze[ny] = y[Li - 1];
 }
 
+// Separator system per subdomain and wavenumber (see k_chase_reduced): loop-invariant table entries
+// hoisted, the per-chunk loads issued ahead of the recurrence.
 template <typename T>
 __global__ void k_b_chase_reduced(const ChaseSeg<T>* __restrict__ segs, const long long* __restrict__ prefix,
                                   int nseg, const ChaseTabDev<T>* __restrict__ tabs)
 {
-    const int         s  = seg_of(prefix, nseg, blockIdx.x);
-    const ChaseSeg<T> sg = segs[s];
-    const long long   t  = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
-    const int         ny = sg.ny, nx = sg.nx, P = nx / kChunk;
+    constexpr int      kAhead = 8;
+    const int          s  = seg_of(prefix, nseg, blockIdx.x);
+    const ChaseSeg<T>* sg = segs + s;
+    const long long    t  = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
+    const int          ny = sg->ny, nx = sg->nx, P = nx / kChunk;
     if (t >= ny) return;
-    const int            j  = (int)t;
-    const ChaseTabDev<T> tb = tabs[sg.tab];
+    const int            j    = (int)t;
+    const ChaseTabDev<T> tb   = tabs[sg->tab];
+    const int            nrow = sg->nrow, ncol = sg->ncol;
     ModCtx<T>            mc;
-    mod_init(sg, j, mc);
-    const T d = tb.dsep[j];
-    auto e = [&](int typ, int k) { return tb.cends[((long long)typ * 4 + k) * ny + j]; };
-    const T* ze = sg.zend + j;
-    T*       cw = sg.work + j;
-    T*       bs = sg.bsep + j;
+    mod_init(sg, ncol, j, mc);
+    const T d    = tb.dsep[j];
+    const T e0_3 = tb.cends[(0 * 4 + 3) * (long long)ny + j];
+    const T e1_0 = tb.cends[(1 * 4 + 0) * (long long)ny + j], e1_1 = tb.cends[(1 * 4 + 1) * (long long)ny + j];
+    const T e1_2 = tb.cends[(1 * 4 + 2) * (long long)ny + j], e1_3 = tb.cends[(1 * 4 + 3) * (long long)ny + j];
+    const T* ze  = sg->zend + j;
+    T*       cw  = sg->work + j;
+    T*       bs  = sg->bsep + j;
+    const T* in  = sg->in;
+    T*       out = sg->out;
     T        yprev = 0, cprev = 0;
-    for (int p = 0; p < P; ++p)
+    for (int p0 = 0; p0 < P; p0 += kAhead)
     {
-        const int  typ   = p == 0 ? 0 : 1;
-        const bool last  = p == P - 1;
-        const int  isep  = p * kChunk + kChunk - 1;
-        const T    fsep  = mod_rhs(sg, mc, isep, j, sg.in[(long long)isep * ny + j]);
-        const T    lower = p > 0 ? -e(typ, 1) : (T)0;
-        T          diag  = d - e(typ, 3);
-        T          rhs   = fsep - ze[(long long)(2 * p + 1) * ny];
-        if (!last)
+        T rhs_v[kAhead];
+#pragma unroll
+        for (int q = 0; q < kAhead; ++q)
         {
-            diag -= e(1, 0);
-            rhs -= ze[(long long)(2 * (p + 1)) * ny];
+            const int p = p0 + q;
+            if (p < P)
+            {
+                const int isep = p * kChunk + kChunk - 1;
+                T r = mod_rhs(sg, nrow, ncol, mc, isep, j, in[(long long)isep * ny + j]) - ze[(long long)(2 * p + 1) * ny];
+                if (p < P - 1) r -= ze[(long long)(2 * (p + 1)) * ny];
+                rhs_v[q] = r;
+            }
         }
-        const T den = diag - lower * cprev;
-        const T up  = last ? (T)0 : -e(1, 2);
-        const T cp  = up / den;
-        yprev       = (rhs - lower * yprev) / den;
-        cw[(long long)p * ny] = cp;
-        bs[(long long)p * ny] = yprev;
-        cprev                 = cp;
+#pragma unroll
+        for (int q = 0; q < kAhead; ++q)
+        {
+            const int p = p0 + q;
+            if (p >= P) break;
+            const bool last  = p == P - 1;
+            const T    lower = p > 0 ? -e1_1 : (T)0;
+            T          diag  = d - (p == 0 ? e0_3 : e1_3);
+            if (!last) diag -= e1_0;
+            const T den = diag - lower * cprev;
+            const T up  = last ? (T)0 : -e1_2;
+            const T cp  = up / den;
+            yprev       = (rhs_v[q] - lower * yprev) / den;
+            cw[(long long)p * ny] = cp;
+            bs[(long long)p * ny] = yprev;
+            cprev                 = cp;
+        }
     }
     T x = bs[(long long)(P - 1) * ny];
-    sg.out[(long long)(nx - 1) * ny + j] = x;
+    out[(long long)(nx - 1) * ny + j] = x;
     for (int p = P - 2; p >= 0; --p)
     {
         x                                                  = bs[(long long)p * ny] - cw[(long long)p * ny] * x;
         bs[(long long)p * ny]                              = x;
-        sg.out[(long long)(p * kChunk + kChunk - 1) * ny + j] = x;
+        out[(long long)(p * kChunk + kChunk - 1) * ny + j] = x;
     }
 }
 
@@ -295,20 +314,19 @@ __global__ void __launch_bounds__(256) k_b_chase_correct(const ChaseSeg<T>* __re
                                                          const long long* __restrict__ prefix, int nseg,
                                                          const ChaseTabDev<T>* __restrict__ tabs)
 {
-    constexpr int     Li = kChunk - 1;
-    const int         s  = seg_of(prefix, nseg, blockIdx.x);
-    const ChaseSeg<T> sg = segs[s];
-    const long long   t  = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
-    const int         ny = sg.ny, P = sg.nx / kChunk;
-    if (t >= (long long)P * ny) return;
-    const int            j   = (int)(t % ny);
-    const int            p   = (int)(t / ny);
+    constexpr int      Li = kChunk - 1;
+    const int          s  = seg_of(prefix, nseg, blockIdx.x);
+    const ChaseSeg<T>* sg = segs + s;
+    const int          ny = sg->ny, P = sg->nx / kChunk;
+    const int          t  = (int)(blockIdx.x - prefix[s]) * blockDim.x + threadIdx.x;
+    if (t >= P * ny) return;
+    const int            j   = t % ny, p = t / ny;
     const int            typ = p == 0 ? 0 : 1;
-    const ChaseTabDev<T> tb  = tabs[sg.tab];
-    const T*             bs  = sg.bsep + j;
+    const ChaseTabDev<T> tb  = tabs[sg->tab];
+    const T*             bs  = sg->bsep + j;
     const T              bl  = p > 0 ? bs[(long long)(p - 1) * ny] : (T)0;
     const T              br  = bs[(long long)p * ny];
-    T*                   col = sg.out + (long long)p * kChunk * ny + j;
+    T*                   col = sg->out + (long long)p * kChunk * ny + j;
     const T*             g   = tb.cg + (long long)typ * Li * ny + j;
     const T*             h   = tb.chh + (long long)typ * Li * ny + j;
 #pragma unroll 8
@@ -576,17 +594,18 @@ struct AsmSeg
 };
 __global__ void k_b_assemble(const AsmSeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg)
 {
-    const int    s  = seg_of(prefix, nseg, blockIdx.x);
-    const AsmSeg sg = segs[s];
-    const long long t = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
-    if (t >= (long long)sg.a.nx * sg.a.ny) return;
-    if (sg.copy)
+    const int     s  = seg_of(prefix, nseg, blockIdx.x);
+    const AsmSeg* sg = segs + s;
+    const int     t  = (int)(blockIdx.x - prefix[s]) * blockDim.x + threadIdx.x;
+    if (t >= sg->a.nx * sg->a.ny) return;
+    double* copy = sg->copy;
+    if (copy)
     {
-        sg.copy[t] = sg.f[t];
-        assemble_at(sg.copy, t, sg.a);
+        copy[t] = sg->f[t];
+        assemble_at(copy, t, sg->a);
     }
     else
-        assemble_at(sg.f, t, sg.a);
+        assemble_at(sg->f, t, sg->a);
 }
 
 struct ResSeg
@@ -602,26 +621,26 @@ __global__ void __launch_bounds__(256) k_b_residual(const ResSeg* __restrict__ s
                                                     int nseg)
 {
     __shared__ double sh[32];
-    const int    s  = seg_of(prefix, nseg, blockIdx.x);
-    const ResSeg sg = segs[s];
-    const long long t = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
-    double       rr = 0, ff = 0;
-    if (t < (long long)sg.a.nx * sg.a.ny)
+    const int     s  = seg_of(prefix, nseg, blockIdx.x);
+    const ResSeg* sg = segs + s;
+    const int     t  = (int)(blockIdx.x - prefix[s]) * blockDim.x + threadIdx.x;
+    double        rr = 0, ff = 0;
+    if (t < sg->a.nx * sg->a.ny)
     {
-        const double v = sg.fs[t] - composite_lap(sg.u, t, sg.a);
-        if (sg.r) sg.r[t] = v;
+        const double v = sg->fs[t] - composite_lap(sg->u, t, sg->a);
+        if (sg->r) sg->r[t] = v;
         rr = v * v;
-        ff = sg.fs[t] * sg.fs[t];
+        ff = sg->fs[t] * sg->fs[t];
     }
-    if (sg.partial)
+    if (sg->partial)
     {
         const double a = block_sum(rr, sh);
         __syncthreads();
         const double b = block_sum(ff, sh);
         if (threadIdx.x == 0)
         {
-            sg.partial[blockIdx.x - prefix[s]]   = a;
-            sg.partial_f[blockIdx.x - prefix[s]] = b;
+            sg->partial[blockIdx.x - prefix[s]]   = a;
+            sg->partial_f[blockIdx.x - prefix[s]] = b;
         }
     }
 }
@@ -1519,6 +1538,7 @@ template <typename TS> void BatchImpl<TS>::solve_graph(double* const* fields, co
         }
         FPB_CUDA(cudaStreamEndCapture(cap, &g));
         graph_kernels_ = launches_noted() - before;
+        note_launches(-graph_kernels_);  // captured, not executed: counted when the graph is replayed
         const cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
         cudaGraphDestroy(g);
         cudaStreamDestroy(cap);

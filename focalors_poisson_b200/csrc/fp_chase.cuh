@@ -164,44 +164,60 @@ __global__ void __launch_bounds__(256) k_chase_local(T* __restrict__ f, int nx, 
 }
 
 // Separator system per (field, wavenumber). ends: [type][4][j] = g_first, g_last, h_first, h_last.
+// The table entries are loop-invariant (chunk type 1 for every chunk after the first) and the per-chunk
+// loads do not depend on the recurrence, so they are issued ahead of it in groups of kAhead.
 template <typename T>
 __global__ void k_chase_reduced(T* __restrict__ f, int nx, int ny, long long batch, const T* __restrict__ ends,
                                 const T* __restrict__ dsep, int end_neumann, const T* __restrict__ zend,
                                 T* __restrict__ bsep, T* __restrict__ work, int skip_last)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int   kAhead = 8;
+    const long long t      = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= batch * ny) return;
-    const int       j = (int)(t % ny);
+    const int j = (int)(t % ny);
     if (skip_last && j == ny - 1) return;
     const long long b = t / ny;
     const int       P = nx / kChunk;
     const T         d = dsep[j];
-    auto e = [&](int typ, int k) { return ends[((long long)typ * 4 + k) * ny + j]; };
+    const T  e0_3 = ends[(0 * 4 + 3) * (long long)ny + j];
+    const T  e1_0 = ends[(1 * 4 + 0) * (long long)ny + j], e1_1 = ends[(1 * 4 + 1) * (long long)ny + j];
+    const T  e1_2 = ends[(1 * 4 + 2) * (long long)ny + j], e1_3 = ends[(1 * 4 + 3) * (long long)ny + j];
     const T* ze = zend + b * (long long)P * 2 * ny + j;
     T*       cw = work + b * (long long)P * ny + j;  // Thomas factors of the separator system
     T*       bs = bsep + b * (long long)P * ny + j;  // right-hand sides, then the solution B_p
     T*       fb = f + b * (long long)nx * ny + j;
     T        yprev = 0, cprev = 0;
-    for (int p = 0; p < P; ++p)
+    for (int p0 = 0; p0 < P; p0 += kAhead)
     {
-        const int  typ   = p == 0 ? 0 : 1;
-        const bool last  = p == P - 1;
-        const T    fsep  = fb[(long long)(p * kChunk + kChunk - 1) * ny];
-        const T    lower = p > 0 ? -e(typ, 1) : (T)0;
-        T          diag  = (last && end_neumann ? d + (T)1 : d) - e(typ, 3);
-        T          rhs   = fsep - ze[(long long)(2 * p + 1) * ny];
-        if (!last)
+        T rhs_v[kAhead];
+#pragma unroll
+        for (int q = 0; q < kAhead; ++q)
         {
-            diag -= e(1, 0);
-            rhs -= ze[(long long)(2 * (p + 1)) * ny];
+            const int p = p0 + q;
+            if (p < P)
+            {
+                T r = fb[(long long)(p * kChunk + kChunk - 1) * ny] - ze[(long long)(2 * p + 1) * ny];
+                if (p < P - 1) r -= ze[(long long)(2 * (p + 1)) * ny];
+                rhs_v[q] = r;
+            }
         }
-        const T den  = diag - lower * cprev;
-        const T up   = last ? (T)0 : -e(1, 2);
-        const T cp   = up / den;
-        yprev        = (rhs - lower * yprev) / den;
-        cw[(long long)p * ny] = cp;
-        bs[(long long)p * ny] = yprev;
-        cprev        = cp;
+#pragma unroll
+        for (int q = 0; q < kAhead; ++q)
+        {
+            const int p = p0 + q;
+            if (p >= P) break;
+            const bool last  = p == P - 1;
+            const T    lower = p > 0 ? -e1_1 : (T)0;
+            T          diag  = (last && end_neumann ? d + (T)1 : d) - (p == 0 ? e0_3 : e1_3);
+            if (!last) diag -= e1_0;
+            const T den = diag - lower * cprev;
+            const T up  = last ? (T)0 : -e1_2;
+            const T cp  = up / den;
+            yprev       = (rhs_v[q] - lower * yprev) / den;
+            cw[(long long)p * ny] = cp;
+            bs[(long long)p * ny] = yprev;
+            cprev                 = cp;
+        }
     }
     T x = bs[(long long)(P - 1) * ny];
     fb[(long long)(nx - 1) * ny] = x;

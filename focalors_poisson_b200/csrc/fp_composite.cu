@@ -338,7 +338,7 @@ void Composite::node_solve(int d, double* f, cudaStream_t s, GmresInfo* info)
         k_sub<<<grid_for(n, 256), 256, 0, s>>>(r, b, w, n);
         FPB_CHECK_LAUNCH();
         dot(r, r, n, true, s, hcol + m + 1);
-        // Convergence is judged on the reference's full-field residual (gmres_solver2d.cpp:149-160). In
+        // Convergence is decided on the reference's full-field residual (gmres_solver2d.cpp:149-160). In
         // interface mode the iterate is x(y) = A^-1 b + A^-1 S y, whose full-field residual is
         // A^-1 S rho(y) for the interface residual rho: one more rectangle solve per restart.
         if (mode_ == GMRES_INTERFACE)
@@ -556,7 +556,7 @@ void Composite::build_interface_inverse(int d)
     }
 }
 
-// Interface solve with the precomputed inverse X of M = I - P A^-1 S, judged by the reference's test:
+// Interface solve with the precomputed inverse X of M = I - P A^-1 S, accepted by the reference's test:
 // y = X g; Z = A^-1 S y; interface residual rho = g - M y = g - y + P Z; accept when the full-field
 // residual |A^-1 S rho| < tol, otherwise y += X rho and repeat (at most 4 times). On success
 // f = A^-1 b + Z. Returns false (f untouched beyond b = A^-1 b) if it did not converge; the caller then

@@ -35,7 +35,7 @@ struct AssembleArgs
 // the hx^2 scaling of solve() (:111-116).
 template <typename T> __device__ __forceinline__ void assemble_at(T* __restrict__ f, long long t, const AssembleArgs& a)
 {
-    const int i = (int)(t / a.ny), j = (int)(t % a.ny);
+    const int i = (int)t / a.ny, j = (int)t - i * a.ny;  // a subdomain holds fewer than 2^31 cells
     double    v = f[t];
     const bool on[4] = {i == 0, i == a.nx - 1, j == 0, j == a.ny - 1};
     if (on[0] || on[1] || on[2] || on[3])
@@ -356,7 +356,7 @@ struct ResidualArgs
 // (pe/concat/concat_solver2d.cpp:101-157, interface terms from bond_add with coefficient -1).
 __device__ __forceinline__ double composite_lap(const double* __restrict__ u, long long t, const ResidualArgs& a)
 {
-    const int    i = (int)(t / a.ny), j = (int)(t % a.ny);
+    const int    i = (int)t / a.ny, j = (int)t - i * a.ny;  // a subdomain holds fewer than 2^31 cells
     const int    nx = a.nx, ny = a.ny;
     const double c  = u[t];
     double       xm, xp, ym, yp, ycoef_m = a.r2, ycoef_p = a.r2;

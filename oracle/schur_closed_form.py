@@ -1,7 +1,7 @@
 """Closed-form Schur matrices of leaf subdomains (numpy), for setting up the reference's solver at sizes
 where its own construction is impractical on CPU.
 
-TEST / BASELINE INFRASTRUCTURE. The reference builds S for a child attached at face `loc` of its parent
+TEST AND CPU-BASELINE INFRASTRUCTURE. The reference builds S for a child attached at face `loc` of its parent
 with one full child solve per interface cell (pe/concat/schur_mat2d.cpp:5-106). For a leaf child the
 response is separable:
 

@@ -7,7 +7,7 @@ Run here (where the reference checkout and oracle/_ref/libfpref.so exist):
 Every output array is produced by the reference's C++ (oracle/ref_harness.cpp over the unmodified
 reference sources). Inputs follow the reference's own validation drivers where one exists
 (case/validation/2d/poisson_solver_reference.cpp, concat_solver_reference.cpp, gmres_reference.cpp,
-shur_mat_reference.cpp) and the BASELINE workload shapes otherwise (seeded, synthetic), at sizes small
+shur_mat_reference.cpp) and the benchmark workloads' shapes otherwise (seeded, synthetic), at sizes small
 enough to commit. Files are .npz (little-endian float64 / int32 arrays).
 """
 from __future__ import annotations
