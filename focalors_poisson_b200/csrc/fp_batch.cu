@@ -40,21 +40,9 @@ __device__ __forceinline__ double dst_basis(int n, int k, int j)
 }
 
 // ---------------------------------------------------------------------------------------------
-// DST-I (the DD family, self-inverse) of rows of many lengths in one persistent launch
+// y-transforms of rows of many lengths in one persistent launch (one family and direction per launch;
+// the per-row work is transform_rows of fp_transform.cuh)
 // ---------------------------------------------------------------------------------------------
-template <typename T> struct BPlan
-{
-    typedef typename Cplx<T>::type T2;
-    int        n, L, M, blue, nst;
-    const T2*  tw;
-    const T2*  chirp;
-    const T2*  bhat;
-    const int* perm;
-    const int4* stages;
-    const T2*  tc;
-    T          s1;
-};
-
 struct DstSeg
 {
     const void* in;
@@ -62,85 +50,30 @@ struct DstSeg
     int         rows, plan;
 };
 
-// One work item = two rows of one segment (z = u + i v through one complex FFT of length n+1, see
-// fp_transform.cuh). ACC: out (FP64) += result instead of out = result.
-template <typename T, typename TIN, typename TOUT, bool ACC>
-__global__ void __launch_bounds__(512) k_b_dst(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix,
-                                               int nseg, long long nitems, const BPlan<T>* __restrict__ plans)
+// One work item = the rows one FFT carries (two for the pairing families) of one segment.
+// ACC: out (FP64) += result instead of out = result.
+template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC>
+__global__ void __launch_bounds__(512) k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix,
+                                                 int nseg, long long nitems, const XformArgs<T>* __restrict__ plans)
 {
     typedef typename Cplx<T>::type T2;
     extern __shared__ __align__(16) unsigned char fp_smem_raw[];
-    T2*       buf  = reinterpret_cast<T2*>(fp_smem_raw);
-    const T   half = (T)0.5;
+    T2*            buf = reinterpret_cast<T2*>(fp_smem_raw);
+    __shared__ T   rowsc[2];
+    constexpr bool kPair = FamilyTraits<KIND, INV>::kPairRows;
     for (long long it = blockIdx.x; it < nitems; it += gridDim.x)
     {
-        const int      s  = seg_of(prefix, nseg, it);
-        const DstSeg   sg = segs[s];
-        const BPlan<T> P  = plans[sg.plan];
-        const int      n  = P.n;
-        const long long r0    = 2 * (it - prefix[s]);
-        const bool      has_b = r0 + 1 < sg.rows;
-        const TIN*      fa    = static_cast<const TIN*>(sg.in) + r0 * n;
-        const TIN*      fb    = has_b ? fa + n : fa;
-        TOUT*           oa    = static_cast<TOUT*>(sg.out) + r0 * n;
-        TOUT*           ob    = has_b ? oa + n : nullptr;
-        FftDesc         d;
-        d.L    = P.L;
-        d.M    = P.M;
-        d.blue = P.blue;
-        d.nst  = P.nst;
-        const FftTables<T2> ft{P.tw, P.chirp, P.bhat, P.perm, P.stages};
-        const int           L = P.L;
-        for (int i = threadIdx.x; i < P.M; i += blockDim.x)
-        {
-            T2 z = mk<T2>(0, 0);
-            if (i < L && i > 0)
-            {
-                const T c  = P.tc[i].x;
-                const T xa = (T)fa[i - 1], xma = (T)fa[n - i];
-                const T va = c * (xa + xma) + half * (xa - xma);
-                T       vb = 0;
-                if (has_b)
-                {
-                    const T xb = (T)fb[i - 1], xmb = (T)fb[n - i];
-                    vb         = c * (xb + xmb) + half * (xb - xmb);
-                }
-                z = mk<T2>(va, vb);
-            }
-            buf[fft_in_slot(d, ft, i)] = fft_in_value(d, ft, i, z);
-        }
-        fft_execute(buf, d, ft);
-        const int K  = (n + 1) / 2;
-        T*        ca = reinterpret_cast<T*>(buf + ((P.M - L >= K) ? L : P.M));
-        T*        cb = ca + K;
-        auto put = [&](TOUT* o, int idx, T v) {
-            if (ACC) o[idx] = (TOUT)((double)o[idx] + (double)v);
-            else o[idx] = (TOUT)v;
-        };
-        for (int k = threadIdx.x; k <= n / 2; k += blockDim.x)
-        {
-            const T2 Zk = fft_out(buf, d, ft, k % L);
-            const T2 Zm = fft_out(buf, d, ft, (L - k) % L);
-            if (k < K)
-            {
-                const T sc = (k == 0) ? (T)0.5 : (T)1;
-                ca[k]      = sc * (half * (Zk.x + Zm.x));
-                cb[k]      = sc * (half * (Zk.y + Zm.y));
-            }
-            if (k >= 1 && 2 * k <= n)
-            {
-                put(oa, 2 * k - 1, P.s1 * (-(half * (Zk.y - Zm.y))));
-                if (ob) put(ob, 2 * k - 1, P.s1 * (half * (Zk.x - Zm.x)));
-            }
-        }
-        __syncthreads();
-        block_scan2(ca, cb, K);
-        for (int k = threadIdx.x; k < K; k += blockDim.x)
-        {
-            put(oa, 2 * k, P.s1 * ca[k]);
-            if (ob) put(ob, 2 * k, P.s1 * cb[k]);
-        }
-        __syncthreads();
+        const int           s  = seg_of(prefix, nseg, it);
+        const DstSeg&       sg = segs[s];
+        const XformArgs<T>& P  = plans[sg.plan];
+        const int           n  = P.n;
+        const long long     r0 = kPair ? 2 * (it - prefix[s]) : (it - prefix[s]);
+        const bool          has_b = kPair && r0 + 1 < sg.rows;
+        const TIN*          fa    = static_cast<const TIN*>(sg.in) + r0 * n;
+        const TIN*          fb    = has_b ? fa + n : fa;
+        TOUT*               oa    = static_cast<TOUT*>(sg.out) + r0 * n;
+        TOUT*               ob    = has_b ? oa + n : nullptr;
+        transform_rows<T, KIND, INV, TIN, TOUT, ACC>(P, fa, fb, oa, ob, has_b, buf, rowsc);
     }
 }
 
@@ -159,6 +92,7 @@ template <typename T> struct ChaseTabDev
     const T* chh;
     const T* cends;
     const T* dsep;
+    int      end_neu;  // x+ face Neumann: last separator diagonal d + 1 (x- Neumann is in the type-0 tables)
 };
 
 template <typename T> struct ChaseSeg
@@ -175,6 +109,7 @@ template <typename T> struct ChaseSeg
     double   row_c[kMaxMods];
     int      col_j[kMaxMods];
     const double* col_s[kMaxMods];
+    const double* col_tab[kMaxMods];  // y-basis values at column col_j (null: the DST-I basis)
     double   col_c[kMaxMods];
 };
 
@@ -186,7 +121,8 @@ template <typename T> struct ModCtx
 template <typename T>
 __device__ __forceinline__ void mod_init(const ChaseSeg<T>* __restrict__ sg, int ncol, int k, ModCtx<T>& m)
 {
-    for (int c = 0; c < ncol; ++c) m.psi[c] = sg->col_c[c] * dst_basis(sg->ny, k, sg->col_j[c]);
+    for (int c = 0; c < ncol; ++c)
+        m.psi[c] = sg->col_c[c] * (sg->col_tab[c] ? sg->col_tab[c][k] : dst_basis(sg->ny, k, sg->col_j[c]));
 }
 template <typename T>
 __device__ __forceinline__ T mod_rhs(const ChaseSeg<T>* __restrict__ sg, int nrow, int ncol, const ModCtx<T>& m, int i,
@@ -288,7 +224,7 @@ __global__ void k_b_chase_reduced(const ChaseSeg<T>* __restrict__ segs, const lo
             if (p >= P) break;
             const bool last  = p == P - 1;
             const T    lower = p > 0 ? -e1_1 : (T)0;
-            T          diag  = d - (p == 0 ? e0_3 : e1_3);
+            T          diag  = (last && tb.end_neu ? d + (T)1 : d) - (p == 0 ? e0_3 : e1_3);
             if (!last) diag -= e1_0;
             const T den = diag - lower * cprev;
             const T up  = last ? (T)0 : -e1_2;
@@ -343,10 +279,11 @@ __global__ void __launch_bounds__(256) k_b_chase_correct(const ChaseSeg<T>* __re
 // out[i] = coef * sum_k psi_k(j) X(i, k): the physical value at column j of a y-spectral field.
 template <typename T> struct ColReq
 {
-    const T* X;
-    int      nx, ny, j;
-    double*  out;
-    double   coef;
+    const T*      X;
+    int           nx, ny, j;
+    double*       out;
+    double        coef;
+    const double* tab;  // y-basis values at column j (null: the DST-I basis)
 };
 template <typename T>
 __global__ void k_b_colvals(const ColReq<T>* __restrict__ reqs, const long long* __restrict__ prefix, int nreq)
@@ -359,7 +296,7 @@ __global__ void k_b_colvals(const ColReq<T>* __restrict__ reqs, const long long*
     const int       i = (int)(w - prefix[q]);
     const T*        row = R.X + (long long)i * R.ny;
     double          acc = 0;
-    for (int k = lane; k < R.ny; k += 32) acc += dst_basis(R.ny, k, R.j) * (double)row[k];
+    for (int k = lane; k < R.ny; k += 32) acc += (R.tab ? R.tab[k] : dst_basis(R.ny, k, R.j)) * (double)row[k];
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if (lane == 0) R.out[i] = R.coef * acc;
 }
@@ -407,6 +344,9 @@ struct BIface
     double*       sY;   // nye * nx: sigma' yY (x-spectral)
     double*       bX;   // nxe * ny: -leaf edge rows (y-spectral), root right-hand side terms
     double*       bX2;  // nxe * ny: bX + sigma yX
+    const double* K;    // nx * ny: K[m ny + k] = 1 / (alpha_m + r beta_k), the root's inverse in the 2D basis
+    double*       vxy;  // [e][Y] ny: psi_k(jY) sig_e[k] zX[e][k]
+    double*       wxy;  // [e][Y] nx: chi_m(ie) sig'_Y[m] yY[Y][m]
 };
 
 __device__ __forceinline__ double chi_edge(int n, int m, int i) { return dst_basis(n, m, i); }
@@ -426,6 +366,8 @@ __global__ void k_if_zx(const BIface* __restrict__ P, const long long* __restric
         double v = 0;
         for (int e2 = 0; e2 < E; ++e2) v += B[e * E + e2] * F.gX[e2 * F.ny + k];
         F.zX[e * F.ny + k] = v;
+        for (int Y = 0; Y < F.nye; ++Y)
+            F.vxy[(e * 2 + Y) * F.ny + k] = dst_basis(F.ny, k, F.jy[Y]) * F.sig[e][k] * v;
     }
 }
 
@@ -436,17 +378,18 @@ __global__ void k_if_rhsy(const BIface* __restrict__ P, const long long* __restr
     const long long w    = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int       lane = threadIdx.x & 31;
     if (w >= prefix[np]) return;
-    const int    p  = seg_of(prefix, np, w);
-    const BIface F  = P[p];
-    const int    q  = (int)(w - prefix[p]);
-    const int    Y  = q / F.nx, m = q - Y * F.nx;
-    const double am = F.alpha[m];
-    double       acc = 0;
+    const int     p  = seg_of(prefix, np, w);
+    const BIface& F  = P[p];
+    const int     q  = (int)(w - prefix[p]);
+    const int     Y  = q / F.nx, m = q - Y * F.nx;
+    double        acc = 0;
     for (int e = 0; e < F.nxe; ++e)
     {
-        const double cm = chi_edge(F.nx, m, F.ie[e]);
-        for (int k = lane; k < F.ny; k += 32)
-            acc += cm * dst_basis(F.ny, k, F.jy[Y]) * F.sig[e][k] * F.zX[e * F.ny + k] / (am + F.r * F.beta[k]);
+        const double* Km = F.K + (long long)m * F.ny;
+        const double* v  = F.vxy + (e * 2 + Y) * F.ny;
+        double        a  = 0;
+        for (int k = lane; k < F.ny; k += 32) a += Km[k] * v[k];
+        acc += chi_edge(F.nx, m, F.ie[e]) * a;
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if (lane == 0) F.rhsY[Y * F.nx + m] = F.gY[Y * F.nx + m] + acc;
@@ -475,43 +418,48 @@ __global__ void k_if_yy(const BIface* __restrict__ P, const long long* __restric
     F.yY[q] = v;
     const int Y = q / F.nx, m = q - Y * F.nx;
     F.sY[q]    = F.sigp[Y][m] * v;
+    for (int e = 0; e < F.nxe; ++e) F.wxy[(e * 2 + Y) * F.nx + m] = chi_edge(F.nx, m, F.ie[e]) * F.sY[q];
 }
 
-// yX[e][k] = sum_e' invXX_k(e, e') (gX[e'][k] + sum_{Y,m} chi_m(ie') psi_k(jY) sig'_Y[m] yY[Y][m] /
-// (alpha_m + r beta_k)); bX2 = bX + sig yX. Warp per (problem, k).
+// yX[e][k] = sum_e' invXX_k(e, e') (gX[e'][k] + sum_Y psi_k(jY) sum_m K[m][k] wxy[e'][Y][m]); bX2 = bX + sig yX.
+// Thread per (problem, k): a warp reads 32 consecutive k of each K row.
 __global__ void k_if_yx(const BIface* __restrict__ P, const long long* __restrict__ prefix, int np)
 {
-    const long long w    = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int       lane = threadIdx.x & 31;
-    if (w >= prefix[np]) return;
-    const int    p  = seg_of(prefix, np, w);
-    const BIface F  = P[p];
-    const int    k  = (int)(w - prefix[p]);
-    const double bk = F.r * F.beta[k];
-    double       t[2] = {0, 0};
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= prefix[np]) return;
+    const int     p = seg_of(prefix, np, t);
+    const BIface& F = P[p];
+    const int     k = (int)(t - prefix[p]);
+    double        tt[2] = {0, 0};
     for (int Y = 0; Y < F.nye; ++Y)
     {
+        double acc[2] = {0, 0};
+        for (int m = 0; m < F.nx; ++m)
+        {
+            const double Kmk = F.K[(long long)m * F.ny + k];
+            for (int e = 0; e < F.nxe; ++e) acc[e] += Kmk * F.wxy[(e * 2 + Y) * F.nx + m];
+        }
         const double pk = dst_basis(F.ny, k, F.jy[Y]);
-        for (int m = lane; m < F.nx; m += 32)
-        {
-            const double base = pk * F.sigp[Y][m] * F.yY[Y * F.nx + m] / (F.alpha[m] + bk);
-            for (int e = 0; e < F.nxe; ++e) t[e] += chi_edge(F.nx, m, F.ie[e]) * base;
-        }
+        for (int e = 0; e < F.nxe; ++e) tt[e] += pk * acc[e];
     }
-    for (int e = 0; e < 2; ++e)
-        for (int o = 16; o > 0; o >>= 1) t[e] += __shfl_down_sync(0xffffffffu, t[e], o);
-    if (lane == 0)
+    const int     E = F.nxe;
+    const double* B = F.invxx + (long long)k * E * E;
+    for (int e = 0; e < E; ++e)
     {
-        const int     E = F.nxe;
-        const double* B = F.invxx + (long long)k * E * E;
-        for (int e = 0; e < E; ++e)
-        {
-            double v = 0;
-            for (int e2 = 0; e2 < E; ++e2) v += B[e * E + e2] * (F.gX[e2 * F.ny + k] + t[e2]);
-            F.yX[e * F.ny + k]  = v;
-            F.bX2[e * F.ny + k] = F.bX[e * F.ny + k] + F.sig[e][k] * v;
-        }
+        double v = 0;
+        for (int e2 = 0; e2 < E; ++e2) v += B[e * E + e2] * (F.gX[e2 * F.ny + k] + tt[e2]);
+        F.yX[e * F.ny + k]  = v;
+        F.bX2[e * F.ny + k] = F.bX[e * F.ny + k] + F.sig[e][k] * v;
     }
+}
+
+// K[m ny + k] = 1 / (alpha_m + r beta_k) of one problem's root
+__global__ void k_root_inverse(const BIface F, double* K)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)F.nx * F.ny) return;
+    const int m = (int)(t / F.ny), k = (int)(t - (long long)m * F.ny);
+    K[t]        = 1.0 / (F.alpha[m] + F.r * F.beta[k]);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -526,6 +474,7 @@ struct GreenReq
     const double* eig_b;  // nq
     double        rr;
     double*       out;    // nq
+    const double* wts;    // n weights w(m) (null: the DST-I products chi_m(ia) chi_m(ib))
 };
 __global__ void k_green(const GreenReq* __restrict__ reqs, const long long* __restrict__ prefix, int nreq)
 {
@@ -538,9 +487,35 @@ __global__ void k_green(const GreenReq* __restrict__ reqs, const long long* __re
     const double   b  = R.rr * R.eig_b[q];
     double         acc = 0;
     for (int m = lane; m < R.n; m += 32)
-        acc += dst_basis(R.n, m, R.ia) * dst_basis(R.n, m, R.ib) / (R.eig_a[m] + b);
+        acc += (R.wts ? R.wts[m] : dst_basis(R.n, m, R.ia) * dst_basis(R.n, m, R.ib)) / (R.eig_a[m] + b);
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if (lane == 0) R.out[q] = acc;
+}
+
+// out[k] = (T_k^-1)(i', i') for T_k = tridiag(1, D, 1) of n rows, D = d[k] (+1 on a Neumann end row):
+// the response of a subdomain at its interface row i' (0 or n-1) to an impulse there, per y-mode k, by
+// eliminating from the far end (a continued fraction).
+struct EndReq
+{
+    int           n, at_start, neu_lo, neu_hi, nq;
+    const double* d;
+    double*       out;
+};
+__global__ void k_green_end(const EndReq* __restrict__ reqs, const long long* __restrict__ prefix, int nreq)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= prefix[nreq]) return;
+    const int    q = seg_of(prefix, nreq, t);
+    const EndReq R = reqs[q];
+    const int    k = (int)(t - prefix[q]);
+    const double d = R.d[k];
+    auto D = [&](int i) { return d + ((i == 0 && R.neu_lo) || (i == R.n - 1 && R.neu_hi) ? 1.0 : 0.0); };
+    double c = 0.0;
+    if (R.at_start)
+        for (int i = R.n - 1; i >= 1; --i) c = 1.0 / (D(i) - c);
+    else
+        for (int i = 0; i <= R.n - 2; ++i) c = 1.0 / (D(i) - c);
+    R.out[k] = 1.0 / (D(R.at_start ? 0 : R.n - 1) - c);
 }
 
 // A[(Y,m),(e,k)] (column-major, ld = nY) and B[(e,k),(Y,m)] = sum_e' invXX_k(e,e') M_XY(e',k; Y,m)
@@ -645,6 +620,41 @@ __global__ void __launch_bounds__(256) k_b_residual(const ResSeg* __restrict__ s
     }
 }
 
+// u (+)= c over many subdomains with per-block partial sums of c^2 and (new) u^2
+struct AddSeg
+{
+    double*       u;
+    const double* c;
+    long long     n;
+    double*       pc;  // per block
+    double*       pu;
+};
+__global__ void __launch_bounds__(256) k_b_add_norms(const AddSeg* __restrict__ segs, const long long* __restrict__ prefix,
+                                                     int nseg, int first)
+{
+    __shared__ double sh[32];
+    const int     s  = seg_of(prefix, nseg, blockIdx.x);
+    const AddSeg* sg = segs + s;
+    const long long t = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
+    double        cc = 0, uu = 0;
+    if (t < sg->n)
+    {
+        const double c = sg->c[t];
+        const double u = first ? c : sg->u[t] + c;
+        sg->u[t]       = u;
+        cc             = c * c;
+        uu             = u * u;
+    }
+    const double a = block_sum(cc, sh);
+    __syncthreads();
+    const double b = block_sum(uu, sh);
+    if (threadIdx.x == 0)
+    {
+        sg->pc[blockIdx.x - prefix[s]] = a;
+        sg->pu[blockIdx.x - prefix[s]] = b;
+    }
+}
+
 struct CopySeg
 {
     double*       dst;
@@ -699,64 +709,123 @@ int sm_count()
     return v;
 }
 
-template <typename T> struct PlanSet  // DST plans by row length
+template <typename T> struct PlanSet  // transform plans by (family, row length)
 {
-    std::map<int, int>                           index;
+    std::map<std::pair<int, int>, int>            index;
     std::vector<std::unique_ptr<DevTransform<T>>> tr;
-    DevBuf                                       dev;
-    size_t                                       smem = 0;
-    int get(int n)
+    DevBuf                                        dev;
+    size_t                                        smem = 0;
+    int get(int kind, int n)
     {
-        auto it = index.find(n);
+        auto key = std::make_pair(kind, n);
+        auto it  = index.find(key);
         if (it != index.end()) return it->second;
-        tr.emplace_back(new DevTransform<T>(K_DD, n));
+        tr.emplace_back(new DevTransform<T>(kind, n));
         smem = std::max(smem, tr.back()->smem);
-        return index[n] = (int)tr.size() - 1;
+        return index[key] = (int)tr.size() - 1;
     }
     void finish()
     {
-        std::vector<BPlan<T>> v;
+        std::vector<XformArgs<T>> v;
         for (auto& t : tr)
         {
-            BPlan<T> p;
-            p.n      = t->n;
-            p.L      = t->fd.L;
-            p.M      = t->fd.M;
-            p.blue   = t->fd.blue;
-            p.nst    = t->fd.nst;
-            p.tw     = t->tw.template as<typename BPlan<T>::T2>();
-            p.chirp  = t->chirp.template as<typename BPlan<T>::T2>();
-            p.bhat   = t->bhat.template as<typename BPlan<T>::T2>();
-            p.perm   = t->perm.template as<int>();
-            p.stages = t->stages.template as<int4>();
-            p.tc     = t->tc.template as<typename BPlan<T>::T2>();
-            p.s1     = t->s1;
-            v.push_back(p);
+            typedef typename Cplx<T>::type T2;
+            XformArgs<T> x{};
+            x.n  = t->n;
+            x.fd = t->fd;
+            x.ft = FftTables<T2>{t->tw.template as<T2>(), t->chirp.template as<T2>(), t->bhat.template as<T2>(),
+                                 t->perm.template as<int>(), t->stages.template as<int4>()};
+            x.ta = t->ta.template as<T>();
+            x.tb = t->tb.template as<T>();
+            x.tc = t->tc.template as<T2>();
+            x.s1 = t->s1;
+            x.s2 = t->s2;
+            v.push_back(x);
         }
         dev = upload(v);
     }
 };
 
-template <typename T, typename TIN, typename TOUT, bool ACC> void prep_dst()
+// A transform work list split by family: one launch per family present, each sized for the shared memory
+// of its own largest plan.
+struct XList
+{
+    struct Part
+    {
+        int      kind = 0;
+        size_t   smem = 0;
+        Segments seg;
+    };
+    std::vector<Part> parts;
+    template <typename T> void set(const std::vector<DstSeg>& recs, const std::vector<int>& kinds, const PlanSet<T>& ps)
+    {
+        parts.clear();
+        for (int k : {K_DD, K_ND, K_DN})
+        {
+            std::vector<DstSeg>    r;
+            std::vector<long long> c;
+            size_t                 sm = 0;
+            for (size_t i = 0; i < recs.size(); ++i)
+                if (kinds[i] == k)
+                {
+                    r.push_back(recs[i]);
+                    c.push_back((recs[i].rows + 1) / 2);
+                    sm = std::max(sm, ps.tr[recs[i].plan]->smem);
+                }
+            if (r.empty()) continue;
+            parts.emplace_back();
+            parts.back().kind = k;
+            parts.back().smem = sm;
+            parts.back().seg.set(r, c);
+        }
+    }
+};
+
+template <typename T, int K, int I, typename TIN, typename TOUT, bool ACC> void prep_x()
 {
     static bool attr = false;
     if (!attr)
     {
-        FPB_CUDA(cudaFuncSetAttribute(k_b_dst<T, TIN, TOUT, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        FPB_CUDA(cudaFuncSetAttribute(k_b_xform<T, K, I, TIN, TOUT, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)max_dynamic_smem()));
         attr = true;
     }
 }
 
-template <typename T, typename TIN, typename TOUT, bool ACC>
-void launch_dst(const Segments& sg, const PlanSet<T>& ps, const BatchTiming& tm, cudaStream_t s)
+template <typename T, int K, int I, typename TIN, typename TOUT, bool ACC>
+void launch_x1(const Segments& sg, const PlanSet<T>& ps, const BatchTiming& tm, cudaStream_t s, size_t smem = 0)
 {
     if (sg.total == 0) return;
-    prep_dst<T, TIN, TOUT, ACC>();
+    prep_x<T, K, I, TIN, TOUT, ACC>();
     const long long grid = std::min<long long>(sg.total, (long long)sm_count() * tm.dst_blocks_per_sm);
-    k_b_dst<T, TIN, TOUT, ACC><<<(unsigned)grid, tm.dst_threads, ps.smem, s>>>(
-        sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, ps.dev.template as<BPlan<T>>());
+    k_b_xform<T, K, I, TIN, TOUT, ACC><<<(unsigned)grid, tm.dst_threads, smem ? smem : ps.smem, s>>>(
+        sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, ps.dev.template as<XformArgs<T>>());
     FPB_CHECK_LAUNCH();
+}
+
+// DD and DN are their own inverses (the same kernel path); ND has a distinct inverse.
+template <typename T, typename TIN, typename TOUT, bool ACC>
+void launch_x(const XList& L, bool inverse, const PlanSet<T>& ps, const BatchTiming& tm, cudaStream_t s)
+{
+    for (auto& part : L.parts)
+    {
+        switch (part.kind)
+        {
+            case K_DD: launch_x1<T, K_DD, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem); break;
+            case K_DN: launch_x1<T, K_DN, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem); break;
+            default:
+                if (inverse) launch_x1<T, K_ND, 1, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem);
+                else launch_x1<T, K_ND, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem);
+        }
+    }
+}
+
+template <typename T, typename TIN, typename TOUT, bool ACC> void prep_x_all()
+{
+    prep_x<T, K_DD, 0, TIN, TOUT, ACC>();
+    prep_x<T, K_DN, 0, TIN, TOUT, ACC>();
+    prep_x<T, K_ND, 0, TIN, TOUT, ACC>();
+    prep_x<T, K_ND, 1, TIN, TOUT, ACC>();
 }
 
 }  // namespace
@@ -779,6 +848,8 @@ public:
     BatchTiming   timing() const override { return tm_; }
     void          autotune(cudaStream_t s) override;
     long long     graph_kernels() const override { return graph_kernels_; }
+    int           refine(double* const* fields, const double* const* ghosts, double rel_tol, int max_refine,
+                         cudaStream_t s, double* rel_change) override;
 
 private:
     struct Dom
@@ -787,7 +858,7 @@ private:
         int       prob = 0, role = 0;  // role 0: root, 1: leaf
         int       leaf_face = -1;      // leaf: its face toward the root; root: -1
         int       root_face = -1;      // leaf: the root's face it is attached to
-        int       plan = 0, tab = 0;
+        int       plan = 0, tab = 0, kind = K_DD;
         long long off  = 0;            // element offset in W / X / fs / u / r
     };
     struct Prob
@@ -798,13 +869,15 @@ private:
         BIface F{};
         DevBuf mem;  // spectral vectors and interface work (doubles)
         DevBuf rinv;
+        DevBuf K;    // root inverse in the 2D basis (problems with both x- and y-edges)
     };
 
     void   build_spectral();
     void   build_static_lists();
     void   build_chase_lists();
     void   chase_run(const Segments& lc, const Segments& red, cudaStream_t s);
-    void   inner(const Segments& dst_in, const Segments& dst_out, bool acc, cudaStream_t s);
+    void   inner(const XList& dst_in, const XList& dst_out, bool acc, cudaStream_t s);
+    const double* basis_col(int kind, int n, int j);
     void   set_user_lists(double* const* fields, const double* const* ghosts, int steps);
     ResSeg res_seg(size_t g, double* r, const double* fs, const double* const* u_user);
     void   run(int steps, cudaStream_t s);
@@ -826,9 +899,12 @@ private:
     Segments                                  edst_g_, edst_out_;         // FP64 edge DSTs
     Segments                                  ifk_, ifym_, ifrow_, ifkw_;  // interface work lists
     std::vector<DstSeg>                       dst_W_in_rec_, dst_X_out_rec_;
-    std::vector<long long>                    dst_counts_;
-    Segments                                  dst_fs_, dst_r_, dst_out_u_;
-    Segments                                  res_, asm_user_, dst_user_in_, dst_user_out_, copy_out_;
+    std::vector<int>                          dst_kinds_;
+    XList                                     dst_fs_, dst_r_, dst_out_u_, dst_out_r_, dst_user_in_, dst_user_out_;
+    Segments                                  res_, asm_user_, copy_out_;
+    Segments                                  addn_;  // u += r with norms (adaptive refinement)
+    DevBuf                                    addp_;
+    std::map<std::tuple<int, int, int>, DevBuf> basis_;  // y-basis column tables (family, n, column)
     std::vector<double*>                      user_ptrs_;
     std::vector<const double*>                user_ghosts_;
     int                                       user_steps_ = -1;
@@ -859,17 +935,28 @@ template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDe
             if (q.nx % kChunk != 0 || q.nx < 2 * kChunk)
                 throw Error(3, "batched solve needs nx a multiple of 32 and >= 64 in every subdomain");
             if (q.ny < 2) throw Error(1, "each subdomain needs at least 2 cells per direction");
+            auto dl = [](int b) { return b == BC_DIRICHLET || b == BC_ADJACENTED; };
             for (int f = 0; f < 4; ++f)
-                if (q.bc[f] != BC_DIRICHLET && q.bc[f] != BC_ADJACENTED)
-                    throw Error(3, "batched solve supports Dirichlet outer faces only");
+                if (q.bc[f] != BC_DIRICHLET && q.bc[f] != BC_ADJACENTED && q.bc[f] != BC_NEUMANN)
+                    throw Error(3, "spectral solve supports Dirichlet and Neumann outer faces only");
             D.role = d == t.root ? 0 : 1;
-            if (D.role == 1)
+            if (D.role == 0)
+            {
+                for (int f = 0; f < 4; ++f)
+                    if (!dl(q.bc[f])) throw Error(3, "spectral solve needs Dirichlet faces on the root subdomain");
+            }
+            else
             {
                 if (!t.children[d].empty() || t.parent[d].second != t.root)
-                    throw Error(3, "batched solve needs every subdomain attached to the root (depth-1 tree)");
+                    throw Error(3, "spectral solve needs every subdomain attached to the root (depth-1 tree)");
                 D.leaf_face = t.parent[d].first;
                 D.root_face = D.leaf_face ^ 1;
+                // the leaf's faces along the interface carry the root's transform basis
+                const int a0 = D.leaf_face < 2 ? YNEG : XNEG;
+                if (!dl(q.bc[a0]) || !dl(q.bc[a0 + 1]))
+                    throw Error(3, "spectral solve needs Dirichlet faces on a leaf's sides along the interface");
             }
+            D.kind = kind_of(q.bc[YNEG], q.bc[YPOS]);
             D.off = cells_;
             cells_ += q.cells();
             dom_.push_back(D);
@@ -894,14 +981,17 @@ template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDe
     }
     for (auto& D : dom_)
     {
-        D.plan = plans_.get(D.d.ny);
-        const double r  = D.d.hx * D.d.hx / D.d.hy / D.d.hy;
-        auto         key = std::make_pair(D.d.ny, r);
+        D.plan = plans_.get(D.kind, D.d.ny);
+        // chase tables depend on (ny, hx^2/hy^2, y family, x- / x+ Neumann)
+        int bcd[4];
+        for (int f = 0; f < 4; ++f) bcd[f] = D.d.bc[f] == BC_ADJACENTED ? BC_DIRICHLET : D.d.bc[f];
+        const double r   = D.d.hx * D.d.hx / D.d.hy / D.d.hy;
+        const int    sig = bcd[0] + 4 * bcd[1] + 16 * bcd[2] + 64 * bcd[3];
+        auto         key = std::make_pair(D.d.ny * 256 + sig, r);
         auto         it  = tab_index_.find(key);
         if (it == tab_index_.end())
         {
-            const int bc0[4] = {0, 0, 0, 0};
-            tabs_.emplace_back(new DevRect<TS>(2 * kChunk, D.d.ny, D.d.hx, D.d.hy, bc0));
+            tabs_.emplace_back(new DevRect<TS>(2 * kChunk, D.d.ny, D.d.hx, D.d.hy, bcd));
             it = tab_index_.emplace(key, (int)tabs_.size() - 1).first;
         }
         D.tab = it->second;
@@ -910,7 +1000,7 @@ template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDe
     std::vector<ChaseTabDev<TS>> tv;
     for (auto& t : tabs_)
         tv.push_back({t->cc.template as<TS>(), t->cg.template as<TS>(), t->chh.template as<TS>(),
-                      t->cends.template as<TS>(), t->dsep.template as<TS>()});
+                      t->cends.template as<TS>(), t->dsep.template as<TS>(), t->end_neumann ? 1 : 0});
     tabs_dev_ = upload(tv);
     W_.alloc((size_t)cells_ * sizeof(TS));
     X_.alloc((size_t)cells_ * sizeof(TS));
@@ -919,11 +1009,11 @@ template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDe
     chs_.alloc((size_t)sep * sizeof(TS));
     build_spectral();
     build_static_lists();
-    prep_dst<TS, double, TS, false>();
-    prep_dst<TS, TS, double, false>();
-    prep_dst<TS, TS, double, true>();
-    prep_dst<TS, TS, TS, false>();
-    prep_dst<double, double, double, false>();
+    prep_x_all<TS, double, TS, false>();
+    prep_x_all<TS, TS, double, false>();
+    prep_x_all<TS, TS, double, true>();
+    prep_x_all<TS, TS, TS, false>();
+    prep_x<double, K_DD, 0, double, double, false>();
 }
 
 // Closed-form spectral responses, interface inverses and the reduced cross systems.
@@ -943,8 +1033,10 @@ template <typename TS> void BatchImpl<TS>::build_spectral()
     };
     // Per problem: doubles laid out as sig[2](ny) sigp[2](nx) gX/zX/yX/bX/bX2 (2 ny each) gY/rhsY/yY/sY
     // (2 nx each), G blocks (ny * 4), H blocks (nx * 4), invxx (ny * 4), invyy (nx * 4)
-    std::vector<GreenReq> greq;
+    std::vector<GreenReq>  greq;
     std::vector<long long> gcnt;
+    std::vector<EndReq>    ereq;
+    std::vector<long long> ecnt;
     struct Host
     {
         std::vector<double> G, H, sig, sigp;
@@ -953,7 +1045,7 @@ template <typename TS> void BatchImpl<TS>::build_spectral()
     {
         const Domain& R  = dom_[pr.root].d;
         const int     nx = R.nx, ny = R.ny;
-        const size_t  nd = 2 * ny + 2 * nx + 5 * 2 * ny + 4 * 2 * nx + 4 * ny + 4 * nx + 4 * ny + 4 * nx;
+        const size_t  nd = 2 * ny + 2 * nx + 5 * 2 * ny + 4 * 2 * nx + 4 * ny + 4 * nx + 4 * ny + 4 * nx + 4 * ny + 4 * nx;
         pr.mem.alloc(nd * sizeof(double));
         FPB_CUDA(cudaMemset(pr.mem.get(), 0, nd * sizeof(double)));
         double* b = pr.mem.template as<double>();
@@ -985,15 +1077,20 @@ template <typename TS> void BatchImpl<TS>::build_spectral()
         double* iy = ix + 4 * ny;
         F.invxx    = ix;
         F.invyy    = iy;
+        F.vxy      = iy + 4 * nx;
+        F.wxy      = F.vxy + 4 * ny;
         for (int e = 0; e < pr.nxe; ++e)
         {
             const Dom& L = dom_[pr.xe[e]];
             F.ie[e]      = L.root_face == XNEG ? 0 : nx - 1;
             F.sig[e]     = sig + e * ny;
-            const int il = L.leaf_face == XNEG ? 0 : L.d.nx - 1;
-            greq.push_back({L.d.nx, il, il, ny, eig_of(L.d.nx), F.beta, L.d.hx * L.d.hx / L.d.hy / L.d.hy,
+            // the leaf's response at its interface row: Dirichlet tridiagonal with the leaf's own x- / x+
+            // Neumann ends, per y-mode of the shared (DD) basis
+            eig_keep_.push_back(upload(x_diag(ny, L.d.hx, L.d.hy, BC_DIRICHLET, BC_DIRICHLET)));
+            ereq.push_back({L.d.nx, L.leaf_face == XNEG ? 1 : 0, L.d.bc[XNEG] == BC_NEUMANN ? 1 : 0,
+                            L.d.bc[XPOS] == BC_NEUMANN ? 1 : 0, ny, eig_keep_.back().template as<double>(),
                             sig + e * ny});
-            gcnt.push_back(ny);
+            ecnt.push_back(ny);
             for (int e2 = 0; e2 < pr.nxe; ++e2)
             {
                 const Dom& L2 = dom_[pr.xe[e2]];
@@ -1011,12 +1108,25 @@ template <typename TS> void BatchImpl<TS>::build_spectral()
             // sig'_m = sum_k psi_k(jl)^2 / (alpha_m + r_l beta^l_k): sum index over the leaf's ny
             const double rl = L.d.hx * L.d.hx / L.d.hy / L.d.hy;
             {
-                // eig_a = r_l * beta^l, so that k_green's form eig_a[k] + 1 * alpha_m applies
-                std::vector<double> l = cal_lambda(L.d.ny, BC_DIRICHLET, BC_DIRICHLET);
+                // eig_a = r_l * beta^l (the leaf's own y family), so that k_green's form eig_a[k] + 1 * alpha_m
+                // applies; weights: the squared y-basis value at the interface row
+                const int yn = L.d.bc[YNEG] == BC_ADJACENTED ? BC_DIRICHLET : L.d.bc[YNEG];
+                const int yp = L.d.bc[YPOS] == BC_ADJACENTED ? BC_DIRICHLET : L.d.bc[YPOS];
+                std::vector<double> l = cal_lambda(L.d.ny, yn, yp);
                 for (auto& q : l) q = rl * (q - 2.0);
                 eig_keep_.push_back(upload(l));
-                greq.push_back({L.d.ny, jl, jl, nx, eig_keep_.back().template as<double>(), F.alpha, 1.0,
-                                sigp + Y * nx});
+                const double* eg = eig_keep_.back().template as<double>();
+                const double* wt = nullptr;
+                if (L.kind != K_DD)
+                {
+                    const double*       tab = basis_col(L.kind, L.d.ny, jl);
+                    std::vector<double> w(L.d.ny);
+                    FPB_CUDA(cudaMemcpy(w.data(), tab, w.size() * 8, cudaMemcpyDeviceToHost));
+                    for (auto& q : w) q = q * q;
+                    eig_keep_.push_back(upload(w));
+                    wt = eig_keep_.back().template as<double>();
+                }
+                greq.push_back({L.d.ny, jl, jl, nx, eg, F.alpha, 1.0, sigp + Y * nx, wt});
             }
             gcnt.push_back(nx);
             for (int Y2 = 0; Y2 < pr.nye; ++Y2)
@@ -1037,6 +1147,14 @@ template <typename TS> void BatchImpl<TS>::build_spectral()
         Segments g;
         g.set(greq, gcnt);
         k_green<<<grid_of(g.total * 32, 256), 256>>>(g.as<GreenReq>(), g.pre(), g.n);
+        FPB_CHECK_LAUNCH();
+        FPB_CUDA(cudaDeviceSynchronize());
+    }
+    if (!ereq.empty())
+    {
+        Segments g;
+        g.set(ereq, ecnt);
+        k_green_end<<<grid_of(g.total, 128), 128>>>(g.as<EndReq>(), g.pre(), g.n);
         FPB_CHECK_LAUNCH();
         FPB_CUDA(cudaDeviceSynchronize());
     }
@@ -1090,6 +1208,10 @@ template <typename TS> void BatchImpl<TS>::build_spectral()
         }
         if (F.nxe > 0 && F.nye > 0)
         {
+            pr.K.alloc((size_t)nx * ny * 8);
+            F.K = pr.K.template as<double>();
+            k_root_inverse<<<grid_of((long long)nx * ny, 256), 256>>>(F, pr.K.template as<double>());
+            FPB_CHECK_LAUNCH();
             const int nY = F.nye * nx, nX = F.nxe * ny;
             if (!cb)
             {
@@ -1133,6 +1255,25 @@ template <typename TS> void BatchImpl<TS>::build_spectral()
     if (cs) cusolverDnDestroy(cs);
     if (cb) cublasDestroy(cb);
     for (auto& kv : eig) eig_keep_.push_back(std::move(kv.second));  // alpha / beta stay referenced
+}
+
+// Column j of the forward y-transform matrix of `kind` at length n (every family is orthonormal with the
+// transpose as inverse, so this is also row j of the inverse): the FP64 transform of the unit vector e_j.
+// Null for DD, whose basis dst_basis() evaluates directly.
+template <typename TS> const double* BatchImpl<TS>::basis_col(int kind, int n, int j)
+{
+    if (kind == K_DD) return nullptr;
+    auto key = std::make_tuple(kind, n, j);
+    auto it  = basis_.find(key);
+    if (it != basis_.end()) return it->second.template as<double>();
+    DevTransform<double> tr(kind, n);
+    std::vector<double>  e(n, 0.0);
+    e[j]      = 1.0;
+    DevBuf in = upload(e);
+    DevBuf out((size_t)n * 8);
+    tr.run(in.as<double>(), out.as<double>(), 1, false, 0);
+    FPB_CUDA(cudaDeviceSynchronize());
+    return (basis_[key] = std::move(out)).template as<double>();
 }
 
 template <typename TS> void BatchImpl<TS>::build_static_lists()
@@ -1199,15 +1340,16 @@ template <typename TS> void BatchImpl<TS>::build_static_lists()
             const Dom& L  = dom_[g];
             const int  jl = L.leaf_face == YNEG ? 0 : L.d.ny - 1;
             l1.push_back(base_seg(g, W + L.off, X + L.off));
-            lc.push_back({X + L.off, L.d.nx, L.d.ny, jl, ev(p, Y, 0), -1.0});
-            rc.push_back({X + ro, F.nx, F.ny, F.jy[Y], ev(p, Y, 1), 1.0});
-            eg.push_back({ev(p, Y, 1), F.gY + Y * F.nx, 1, eplans_.get(F.nx)});
-            eo.push_back({F.sY + Y * F.nx, ev(p, Y, 2), 1, eplans_.get(F.nx)});
-            eo.push_back({F.yY + Y * F.nx, ev(p, Y, 3), 1, eplans_.get(F.nx)});
+            lc.push_back({X + L.off, L.d.nx, L.d.ny, jl, ev(p, Y, 0), -1.0, basis_col(L.kind, L.d.ny, jl)});
+            rc.push_back({X + ro, F.nx, F.ny, F.jy[Y], ev(p, Y, 1), 1.0, nullptr});
+            eg.push_back({ev(p, Y, 1), F.gY + Y * F.nx, 1, eplans_.get(K_DD, F.nx)});
+            eo.push_back({F.sY + Y * F.nx, ev(p, Y, 2), 1, eplans_.get(K_DD, F.nx)});
+            eo.push_back({F.yY + Y * F.nx, ev(p, Y, 3), 1, eplans_.get(K_DD, F.nx)});
             ChaseSeg<TS> c = base_seg(g, W + L.off, X + L.off);
             c.ncol         = 1;
             c.col_j[0]     = jl;
             c.col_s[0]     = ev(p, Y, 3);
+            c.col_tab[0]   = basis_col(L.kind, L.d.ny, jl);
             c.col_c[0]     = -1.0;
             a2.push_back(c);
         }
@@ -1271,18 +1413,18 @@ template <typename TS> void BatchImpl<TS>::build_static_lists()
     ifkw_.set(fw, cw);
     ifym_.set(fy, cy);
     ifrow_.set(fr, cr);
-    // DST lists over all subdomains between internal buffers
-    std::vector<DstSeg>    dfs, dr, dou;
-    std::vector<long long> dc;
+    // transform lists over all subdomains between internal buffers (split by family where used)
+    std::vector<DstSeg> dfs, dou;
+    std::vector<int>    kinds;
     for (auto& D : dom_)
     {
-        dc.push_back((D.d.nx + 1) / 2);
+        kinds.push_back(D.kind);
         dfs.push_back({nullptr, W + D.off, D.d.nx, D.plan});
         dou.push_back({X + D.off, nullptr, D.d.nx, D.plan});
     }
     dst_W_in_rec_  = dfs;
     dst_X_out_rec_ = dou;
-    dst_counts_    = dc;
+    dst_kinds_     = kinds;
 }
 
 template <typename TS> void BatchImpl<TS>::build_chase_lists()
@@ -1316,9 +1458,9 @@ template <typename TS> void BatchImpl<TS>::chase_run(const Segments& lc, const S
 }
 
 // One inner solve: dst_in (FP64 rows -> W), ..., X -> dst_out (FP64 rows; += when acc).
-template <typename TS> void BatchImpl<TS>::inner(const Segments& dst_in, const Segments& dst_out, bool acc, cudaStream_t s)
+template <typename TS> void BatchImpl<TS>::inner(const XList& dst_in, const XList& dst_out, bool acc, cudaStream_t s)
 {
-    launch_dst<TS, double, TS, false>(dst_in, plans_, tm_, s);
+    launch_x<TS, double, TS, false>(dst_in, false, plans_, tm_, s);
     chase_run(l1_lc_, l1_red_, s);
     if (leaf_rows_.n)
     {
@@ -1345,7 +1487,7 @@ template <typename TS> void BatchImpl<TS>::inner(const Segments& dst_in, const S
                                                                          root_cols_.pre(), root_cols_.n);
         FPB_CHECK_LAUNCH();
     }
-    launch_dst<double, double, double, false>(edst_g_, eplans_, tm_, s);
+    launch_x1<double, K_DD, 0, double, double, false>(edst_g_, eplans_, tm_, s);
     if (ifk_.n)
     {
         k_if_zx<<<grid_of(ifk_.total, 128), 128, 0, s>>>(ifk_.as<BIface>(), ifk_.pre(), ifk_.n);
@@ -1360,13 +1502,13 @@ template <typename TS> void BatchImpl<TS>::inner(const Segments& dst_in, const S
     }
     if (ifkw_.n)
     {
-        k_if_yx<<<grid_of(ifkw_.total * 32, 256), 256, 0, s>>>(ifkw_.as<BIface>(), ifkw_.pre(), ifkw_.n);
+        k_if_yx<<<grid_of(ifkw_.total, 128), 128, 0, s>>>(ifkw_.as<BIface>(), ifkw_.pre(), ifkw_.n);
         FPB_CHECK_LAUNCH();
     }
-    launch_dst<double, double, double, false>(edst_out_, eplans_, tm_, s);
+    launch_x1<double, K_DD, 0, double, double, false>(edst_out_, eplans_, tm_, s);
     chase_run(a2_lc_, a2_red_, s);
-    if (acc) launch_dst<TS, TS, double, true>(dst_out, plans_, tm_, s);
-    else launch_dst<TS, TS, double, false>(dst_out, plans_, tm_, s);
+    if (acc) launch_x<TS, TS, double, true>(dst_out, true, plans_, tm_, s);
+    else launch_x<TS, TS, double, false>(dst_out, true, plans_, tm_, s);
 }
 
 template <typename TS>
@@ -1400,9 +1542,27 @@ void BatchImpl<TS>::set_user_lists(double* const* fields, const double* const* g
             b[g].in  = r_.as<double>() + dom_[g].off;
             c[g].out = u_.as<double>() + dom_[g].off;
         }
-        dst_fs_.set(a, dst_counts_);
-        dst_r_.set(b, dst_counts_);
-        dst_out_u_.set(c, dst_counts_);
+        dst_fs_.set(a, dst_kinds_, plans_);
+        dst_r_.set(b, dst_kinds_, plans_);
+        dst_out_u_.set(c, dst_kinds_, plans_);
+        std::vector<DstSeg> d = dst_X_out_rec_;
+        for (size_t g = 0; g < dom_.size(); ++g) d[g].out = r_.as<double>() + dom_[g].off;
+        dst_out_r_.set(d, dst_kinds_, plans_);
+        std::vector<AddSeg>    ad;
+        std::vector<long long> acn;
+        long long              nb = 0;
+        for (size_t g = 0; g < dom_.size(); ++g) nb += (dom_[g].d.cells() + 255) / 256;
+        addp_.alloc((size_t)2 * nb * 8);
+        long long b0 = 0;
+        for (size_t g = 0; g < dom_.size(); ++g)
+        {
+            const long long blocks = (dom_[g].d.cells() + 255) / 256;
+            ad.push_back({u_.as<double>() + dom_[g].off, r_.as<double>() + dom_[g].off, dom_[g].d.cells(),
+                          addp_.as<double>() + b0, addp_.as<double>() + nb + b0});
+            acn.push_back(blocks);
+            b0 += blocks;
+        }
+        addn_.set(ad, acn);
         std::vector<ResSeg>    rs;
         std::vector<long long> rc;
         for (size_t g = 0; g < dom_.size(); ++g) rs.push_back(res_seg(g, r_.as<double>(), fs_.as<double>(), nullptr));
@@ -1437,8 +1597,8 @@ void BatchImpl<TS>::set_user_lists(double* const* fields, const double* const* g
         cc.push_back((D.cells() + 255) / 256);
     }
     asm_user_.set(as, ac);
-    dst_user_in_.set(di, dst_counts_);
-    dst_user_out_.set(dout, dst_counts_);
+    dst_user_in_.set(di, dst_kinds_, plans_);
+    dst_user_out_.set(dout, dst_kinds_, plans_);
     if (ir) copy_out_.set(cp, cc);
 }
 
@@ -1549,6 +1709,51 @@ template <typename TS> void BatchImpl<TS>::solve_graph(double* const* fields, co
 }
 
 template <typename TS>
+int BatchImpl<TS>::refine(double* const* fields, const double* const* ghosts, double rel_tol, int max_refine,
+                         cudaStream_t s, double* rel_change)
+{
+    if (!fields) throw Error(1, "null field list");
+    if (!(rel_tol > 0) || max_refine < 1) throw Error(1, "rel_tol must be > 0 and max_refine >= 1");
+    set_user_lists(fields, ghosts, 1);
+    k_b_assemble<<<(unsigned)asm_user_.total, 256, 0, s>>>(asm_user_.as<AsmSeg>(), asm_user_.pre(), asm_user_.n);
+    FPB_CHECK_LAUNCH();
+    const long long     nb = (long long)(addp_.bytes() / 16);
+    std::vector<double> hp((size_t)2 * nb);
+    double              change = 1.0;
+    int                 steps  = 0;
+    while (steps < max_refine)
+    {
+        inner(steps == 0 ? dst_fs_ : dst_r_, dst_out_r_, false, s);  // r <- correction
+        k_b_add_norms<<<(unsigned)addn_.total, 256, 0, s>>>(addn_.as<AddSeg>(), addn_.pre(), addn_.n, steps == 0);
+        FPB_CHECK_LAUNCH();
+        ++steps;
+        FPB_CUDA(cudaMemcpyAsync(hp.data(), addp_.get(), hp.size() * 8, cudaMemcpyDeviceToHost, s));
+        FPB_CUDA(cudaStreamSynchronize(s));
+        double cn = 0, un = 0;
+        for (long long b = 0; b < nb; ++b)
+        {
+            cn += hp[b];
+            un += hp[nb + b];
+        }
+        if (!std::isfinite(cn) || !std::isfinite(un)) throw Error(5, "non-finite value in iterative refinement");
+        const double last = change;
+        change            = un > 0 ? std::sqrt(cn / un) : 0.0;
+        // stop when this correction is below rel_tol, or the observed contraction predicts the error left
+        // after applying it (about change * change / last) is
+        if (change <= rel_tol || (steps >= 2 && last > 0 && change * (change / last) <= rel_tol)) break;
+        if (steps < max_refine)
+        {
+            k_b_residual<<<(unsigned)res_.total, 256, 0, s>>>(res_.as<ResSeg>(), res_.pre(), res_.n);
+            FPB_CHECK_LAUNCH();
+        }
+    }
+    k_b_copy<<<(unsigned)copy_out_.total, 256, 0, s>>>(copy_out_.as<CopySeg>(), copy_out_.pre(), copy_out_.n);
+    FPB_CHECK_LAUNCH();
+    if (rel_change) *rel_change = change;
+    return steps;
+}
+
+template <typename TS>
 void BatchImpl<TS>::residuals(const double* const* u, const double* const* rhs, const double* const* ghosts,
                               cudaStream_t s, double* out)
 {
@@ -1618,8 +1823,8 @@ template <typename TS> void BatchImpl<TS>::autotune(cudaStream_t s)
     FPB_CUDA(cudaMemsetAsync(X_.get(), 0, (size_t)cells_ * sizeof(TS), s));
     std::vector<DstSeg> rec = dst_X_out_rec_;
     for (size_t g = 0; g < dom_.size(); ++g) rec[g].out = W_.as<TS>() + dom_[g].off;
-    Segments sg;
-    sg.set(rec, dst_counts_);
+    XList sg;
+    sg.set(rec, dst_kinds_, plans_);
     cudaEvent_t e0, e1;
     FPB_CUDA(cudaEventCreate(&e0));
     FPB_CUDA(cudaEventCreate(&e1));
@@ -1641,10 +1846,10 @@ template <typename TS> void BatchImpl<TS>::autotune(cudaStream_t s)
             tm_.dst_threads       = th;
             tm_.dst_blocks_per_sm = bps;
             int occ = 0;
-            prep_dst<TS, TS, TS, false>();
-            FPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_dst<TS, TS, TS, false>, th, plans_.smem));
+            FPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_xform<TS, K_DD, 0, TS, TS, false>, th,
+                                                                   plans_.smem));
             if (occ < bps) continue;
-            const float t = time_it([&] { launch_dst<TS, TS, TS, false>(sg, plans_, tm_, s); });
+            const float t = time_it([&] { launch_x<TS, TS, TS, false>(sg, false, plans_, tm_, s); });
             if (t < bt)
             {
                 bt   = t;

@@ -1,14 +1,16 @@
 // Batched composite solves: many independent ConcatPoissonSolver2D problems of uneven sizes solved in
 // lockstep, every stage one launch over all problems (heterogeneous work lists, persistent kernels).
 //
-// Scope: each problem is a root rectangle with leaf rectangles attached on full faces (a depth-1 tree,
-// the L / T / cross shapes), every outer face Dirichlet and nx of every subdomain a multiple of 32
-// (>= 64). Then every subdomain operator has Dirichlet-like faces on all sides and is diagonalised by
-// DST-I in both directions, so the interface operator I - P A^-1 S of the reference's Schur GMRES
+// Scope: each problem is a root rectangle with Dirichlet faces and leaf rectangles attached on full faces
+// (a depth-1 tree: the L / T / cross shapes), each leaf's sides along its interface Dirichlet, its far
+// face Dirichlet or Neumann, and nx of every subdomain a multiple of 32 (>= 64). The root operator is
+// then diagonalised by DST-I in both directions and every leaf shares the root's basis along its
+// interface, so the interface operator I - P A^-1 S of the reference's Schur GMRES
 // (pe/concat/gmres_solver2d.cpp:90-104) is known in closed form: diagonal in the y-DST basis on the
-// root's x faces, diagonal in the x-DST basis on its y faces, plus a dense cross block. The batch solves
-// it exactly (a small reduced system per problem, its inverse built at creation), which is the solution
-// the reference's GMRES converges to.
+// root's x faces (leaf responses by continued fractions, Neumann ends included), diagonal in the x-DST
+// basis on its y faces (leaf responses from the leaf's own y family, DD / ND / DN), plus a dense cross
+// block. The batch solves it exactly (a small reduced system per problem, its inverse built at
+// creation), which is the solution the reference's GMRES converges to.
 #pragma once
 
 #include "fp_composite.h"
@@ -43,6 +45,11 @@ public:
     // The same launch sequence captured once into a CUDA graph (per field pointers and steps) and replayed.
     virtual void solve_graph(double* const* fields, const double* const* ghosts, int steps, cudaStream_t s) = 0;
     virtual long long graph_kernels() const = 0;  // kernels in the captured graph
+    // Iterative refinement until |correction| <= rel_tol |u| over all cells (or the observed contraction
+    // predicts it after the last correction), at most max_refine inner solves; synchronises the stream
+    // after every step. Returns the steps taken; *rel_change the last |correction| / |u|.
+    virtual int refine(double* const* fields, const double* const* ghosts, double rel_tol, int max_refine,
+                       cudaStream_t s, double* rel_change) = 0;
     // Per-problem |fs - A u| / |fs| (fs: assembled, hx^2-scaled right-hand side); out: host, n_problems.
     virtual void residuals(const double* const* u, const double* const* rhs, const double* const* ghosts,
                            cudaStream_t s, double* out) = 0;

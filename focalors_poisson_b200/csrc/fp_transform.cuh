@@ -28,19 +28,24 @@ namespace fpb
 
 // T: arithmetic of the FFT; TIO: element type of the rows read and written (FP64 rows with an FP32 FFT
 // is the reduced-precision transform of the iterative-refinement path).
-template <typename T, typename TIO = T> struct TransformArgs
+// Everything a transform of one row length needs except the rows themselves.
+template <typename T> struct XformArgs
 {
     typedef typename Cplx<T>::type T2;
-    const TIO*    in;
-    TIO*          out;
-    long long     rows;  // rows in the batch (fields * nx)
-    int           n;     // row length (ny)
+    int           n;  // row length (ny)
     FftDesc       fd;
     FftTables<T2> ft;
     const T*      ta;  // family table a (ND: cos, PP: cos)
     const T*      tb;  // family table b (ND: sin, PP: sin)
     const T2*     tc;  // DD: (sin(pi j/(N+1)), 0); NN: exp(-i pi m / 2N)
     T             s1, s2;
+};
+
+template <typename T, typename TIO = T> struct TransformArgs : XformArgs<T>
+{
+    const TIO* in;
+    TIO*       out;
+    long long  rows;  // rows in the batch (fields * nx)
 };
 
 template <int KIND, int INV> struct FamilyTraits
@@ -186,25 +191,21 @@ template <typename T> __device__ void block_scan2(T* xa, T* xb, int K)
     __syncthreads();
 }
 
-template <typename T, int KIND, int INV, typename TIO = T>
-__global__ void __launch_bounds__(512) k_transform(const TransformArgs<T, TIO> a)
+// One work item: rows fa (and fb, when has_b and the family pairs rows) of length a.n transformed into
+// oa (ob). buf: the item's shared-memory FFT buffer; rowsc: two scratch values. ACC: out += result
+// (FP64 accumulation of a correction) instead of out = result. Ends with the CTA synchronised.
+template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC>
+__device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN* fa, const TIN* fb, TOUT* oa, TOUT* ob,
+                                               bool has_b, typename Cplx<T>::type* buf, T* rowsc)
 {
     typedef typename Cplx<T>::type T2;
-    extern __shared__ __align__(16) unsigned char fp_smem_raw[];
-    T2*          buf = reinterpret_cast<T2*>(fp_smem_raw);
-    __shared__ T rowsc[2];
-
-    constexpr bool kPair = FamilyTraits<KIND, INV>::kPairRows;
     constexpr bool kHerm = INV && (KIND == 1 || KIND == 2);  // real-output families
     const int      n     = a.n;
     const int      L     = a.fd.L;
-    const long long r0   = kPair ? 2LL * blockIdx.x : (long long)blockIdx.x;
-    if (r0 >= a.rows) return;
-    const bool has_b = kPair && r0 + 1 < a.rows;
-    const TIO* fa    = a.in + r0 * n;
-    const TIO* fb    = has_b ? fa + n : fa;
-    TIO*       oa    = a.out + r0 * n;
-    TIO*       ob    = has_b ? oa + n : nullptr;
+    auto put = [&](TOUT* o, int idx, T v) {
+        if (ACC) o[idx] = (TOUT)((double)o[idx] + (double)v);
+        else o[idx] = (TOUT)v;
+    };
 
     if (KIND == 4 && !INV && threadIdx.x == 0) rowsc[0] = (T)fa[n - 1];  // PP forward: f(i, ny-1)
 
@@ -249,17 +250,18 @@ __global__ void __launch_bounds__(512) k_transform(const TransformArgs<T, TIO> a
             }
             if (k >= 1 && 2 * k <= n)
             {
-                oa[2 * k - 1] = a.s1 * (-(half * (Zk.y - Zm.y)));  // -Im Y^a_k
-                if (ob) ob[2 * k - 1] = a.s1 * (half * (Zk.x - Zm.x));  // -Im Y^b_k
+                put(oa, 2 * k - 1, a.s1 * (-(half * (Zk.y - Zm.y))));  // -Im Y^a_k
+                if (ob) put(ob, 2 * k - 1, a.s1 * (half * (Zk.x - Zm.x)));  // -Im Y^b_k
             }
         }
         __syncthreads();
         block_scan2(ca, cb, K);
         for (int k = threadIdx.x; k < K; k += blockDim.x)
         {
-            oa[2 * k] = a.s1 * ca[k];
-            if (ob) ob[2 * k] = a.s1 * cb[k];
+            put(oa, 2 * k, a.s1 * ca[k]);
+            if (ob) put(ob, 2 * k, a.s1 * cb[k]);
         }
+        __syncthreads();
         return;
     }
 
@@ -277,28 +279,28 @@ __global__ void __launch_bounds__(512) k_transform(const TransformArgs<T, TIO> a
             const T Ca = w.x * Ur - w.y * Ui, Cb = w.x * Vr - w.y * Vi;  // Re(w V)
             if (j < n - 1)
             {
-                oa[j] = -a.s1 * Ca;
-                if (ob) ob[j] = -a.s1 * Cb;
+                put(oa, j, -a.s1 * Ca);
+                if (ob) put(ob, j, -a.s1 * Cb);
             }
             else
             {
-                oa[j] = a.s2 * Ca;
-                if (ob) ob[j] = a.s2 * Cb;
+                put(oa, j, a.s2 * Ca);
+                if (ob) put(ob, j, a.s2 * Cb);
             }
         }
         else if (KIND == 1 && INV)
         {
             const int  m = (j & 1) ? n - 1 - (j - 1) / 2 : j / 2;
             const T2   Z = fft_out(buf, a.fd, a.ft, m);
-            oa[j]        = Z.x;
-            if (ob) ob[j] = Z.y;
+            put(oa, j, Z.x);
+            if (ob) put(ob, j, Z.y);
         }
         else if (KIND == 2 && INV)
         {
             const T2 Z = fft_out(buf, a.fd, a.ft, j + 1);
             const T  s = alt_neg_even<T>(j) * a.s1;
-            oa[j]      = s * Z.x;
-            if (ob) ob[j] = s * Z.y;
+            put(oa, j, s * Z.x);
+            if (ob) put(ob, j, s * Z.y);
         }
         else if (KIND == 2 || KIND == 3)
         {
@@ -310,13 +312,13 @@ __global__ void __launch_bounds__(512) k_transform(const TransformArgs<T, TIO> a
             if (KIND == 2)
             {
                 const T c = __ldg(a.ta + j), s = __ldg(a.tb + j);
-                oa[j]     = s * Ur - c * Ui;
-                if (ob) ob[j] = s * Vr - c * Vi;
+                put(oa, j, s * Ur - c * Ui);
+                if (ob) put(ob, j, s * Vr - c * Vi);
             }
             else
             {
-                oa[j] = alt_pos_even<T>(j) * Ui;
-                if (ob) ob[j] = alt_pos_even<T>(j) * Vi;
+                put(oa, j, alt_pos_even<T>(j) * Ui);
+                if (ob) put(ob, j, alt_pos_even<T>(j) * Vi);
             }
         }
         else if (KIND == 4 && !INV)
@@ -335,7 +337,7 @@ __global__ void __launch_bounds__(512) k_transform(const TransformArgs<T, TIO> a
             const T2  Ck = fft_out(buf, a.fd, a.ft, kc);
             const T2  Cm = fft_out(buf, a.fd, a.ft, (L - kc) % L);
             const T   tc = la - half * (Ck.y + Cm.y);
-            oa[j]        = a.s1 * (__ldg(a.ta + j) * ts + __ldg(a.tb + j) * tc);
+            put(oa, j, a.s1 * (__ldg(a.ta + j) * ts + __ldg(a.tb + j) * tc));
         }
         else if (KIND == 4)
         {
@@ -360,9 +362,30 @@ __global__ void __launch_bounds__(512) k_transform(const TransformArgs<T, TIO> a
             {
                 fs = fft_out(buf, a.fd, a.ft, 0).y;  // Re V_0 = Im Z_0
             }
-            oa[j] = a.s1 * (fc + fs);
+            put(oa, j, a.s1 * (fc + fs));
         }
     }
+    __syncthreads();
+}
+
+template <typename T, int KIND, int INV, typename TIO = T>
+__global__ void __launch_bounds__(512) k_transform(const TransformArgs<T, TIO> a)
+{
+    typedef typename Cplx<T>::type T2;
+    extern __shared__ __align__(16) unsigned char fp_smem_raw[];
+    T2*          buf = reinterpret_cast<T2*>(fp_smem_raw);
+    __shared__ T rowsc[2];
+
+    constexpr bool  kPair = FamilyTraits<KIND, INV>::kPairRows;
+    const int       n     = a.n;
+    const long long r0    = kPair ? 2LL * blockIdx.x : (long long)blockIdx.x;
+    if (r0 >= a.rows) return;
+    const bool has_b = kPair && r0 + 1 < a.rows;
+    const TIO* fa    = a.in + r0 * n;
+    const TIO* fb    = has_b ? fa + n : fa;
+    TIO*       oa    = a.out + r0 * n;
+    TIO*       ob    = has_b ? oa + n : nullptr;
+    transform_rows<T, KIND, INV, TIO, TIO, false>(a, fa, fb, oa, ob, has_b, buf, rowsc);
 }
 
 }  // namespace fpb
