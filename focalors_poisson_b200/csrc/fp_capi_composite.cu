@@ -1,5 +1,6 @@
 // C ABI (include/fp_capi.h): composite-geometry solver.
 #include "../../include/fp_capi.h"
+#include "fp_batch.h"
 #include "fp_composite.h"
 
 using namespace fpb;
@@ -8,6 +9,10 @@ struct fp_composite
 {
     std::unique_ptr<Composite> c;
     std::vector<DevBuf>        fields, ghosts;
+    // Spectral direct path (fp_batch.h) for geometries it covers: a batch of this one problem in FP64
+    // (solves) and, built on first use, in FP32 (inner solves of refinement).
+    BatchProblemDesc           desc;
+    std::unique_ptr<BatchBase> sp64, sp32;
 };
 
 namespace
@@ -101,6 +106,37 @@ int fp_composite_create(const fp_geometry* g, int m, double tol, int max_iter, i
         require_device();
         std::unique_ptr<fp_composite> h(new fp_composite());
         h->c = make_composite(g, m, tol, max_iter, flags);
+        if (!(flags & (FP_GMRES_FULLFIELD | FP_NO_SPECTRAL)))
+        {
+            for (int d = 0; d < g->n_domains; ++d)
+            {
+                Domain D;
+                D.nx = g->nx[d];
+                D.ny = g->ny[d];
+                D.hx = g->hx[d];
+                D.hy = g->hy[d];
+                for (int f = 0; f < 4; ++f) D.bc[f] = g->bc[4 * d + f];
+                h->desc.doms.push_back(D);
+            }
+            for (int k = 0; k < g->n_connections; ++k)
+            {
+                const int a = g->connections[3 * k], f = g->connections[3 * k + 1], b = g->connections[3 * k + 2];
+                h->desc.conns.push_back({a, f, b});
+                h->desc.doms[a].bc[f]     = BC_ADJACENTED;
+                h->desc.doms[b].bc[f ^ 1] = BC_ADJACENTED;
+            }
+            try
+            {
+                h->sp64 = make_batch({h->desc}, 0);
+                h->sp64->autotune(0);
+                FPB_CUDA(cudaDeviceSynchronize());
+            }
+            catch (const Error& e)
+            {
+                if (e.code != FP_ERR_UNSUPPORTED) throw;
+                h->sp64.reset();  // outside the spectral path's scope: Schur GMRES
+            }
+        }
         *out = h.release();
     });
 }
@@ -119,8 +155,10 @@ int fp_composite_solve_f64(fp_composite* c, double* const* fields, const double*
     GmresInfo gi;
     int       rc = guarded([&] {
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        with_device_fields(c, fields, ghosts, flags, s,
-                           [&](double* const* f, const double* const* g) { c->c->solve(f, g, s, &gi); });
+        with_device_fields(c, fields, ghosts, flags, s, [&](double* const* f, const double* const* g) {
+            if (c->sp64) c->sp64->solve(f, g, 0, s);  // exact interface solve: nothing to converge
+            else c->c->solve(f, g, s, &gi);
+        });
         if ((flags & FP_CHECK_CONVERGENCE) && !gi.converged)
             throw Error(FP_ERR_NOT_CONVERGED, "GMRES stopped at max_iter above tol (residual " +
                                                   std::to_string(gi.residual) + ")");
@@ -139,7 +177,18 @@ int fp_composite_solve_f32ir(fp_composite* c, double* const* fields, const doubl
         if (!(rel_tol > 0) || max_refine < 1) throw Error(FP_ERR_INVALID, "rel_tol must be > 0 and max_refine >= 1");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         with_device_fields(c, fields, ghosts, flags, s, [&](double* const* f, const double* const* g) {
-            steps = c->c->solve_ir(f, g, s, rel_tol, max_refine, &change, &gi, (flags & FP_IR_INNER_F64) == 0);
+            const bool f32 = (flags & FP_IR_INNER_F64) == 0;
+            if (c->sp64)
+            {
+                if (f32 && !c->sp32)
+                {
+                    c->sp32 = make_batch({c->desc}, 1);
+                    c->sp32->autotune(s);
+                }
+                steps = (f32 ? c->sp32 : c->sp64)->refine(f, g, rel_tol, max_refine, s, &change);
+            }
+            else
+                steps = c->c->solve_ir(f, g, s, rel_tol, max_refine, &change, &gi, f32);
         });
         if ((flags & FP_CHECK_CONVERGENCE) && steps >= max_refine && !(change <= rel_tol))
             throw Error(FP_ERR_NOT_CONVERGED, "iterative refinement stopped at max_refine (relative change " +

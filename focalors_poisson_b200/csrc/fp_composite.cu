@@ -183,10 +183,18 @@ Composite::Composite(const std::vector<Domain>& doms, const std::vector<std::arr
     red_.alloc((kRedBlocks + 8) * sizeof(double));
     FPB_CUDA(cudaMemset(red_.get(), 0, red_.bytes()));
     set_parameter(m, tol, max_iter);
+}
+
+// Schur matrices and interface inverses are built on the first solve that needs them (a geometry solved by
+// the spectral path never does).
+void Composite::ensure_built()
+{
+    if (built_) return;
     build_schur();
     if (want_inverse_ && mode_ == GMRES_INTERFACE)
-        for (int d = 0; d < nd; ++d)
+        for (int d = 0; d < (int)dom_.size(); ++d)
             if (!node_[d].kids.empty() && node_[d].n_if <= kMaxInverse) build_interface_inverse(d);
+    built_ = true;
 }
 
 Composite::~Composite() = default;
@@ -676,6 +684,7 @@ void Composite::assemble(double* const* fields, const double* const* ghosts, cud
 
 void Composite::eliminate(double* const* fields, cudaStream_t s, GmresInfo* info)
 {
+    ensure_built();
     auto bond = [&](double* dst, int dd, int loc, const double* src, int sd) {
         const Domain &A = dom_[dd], &B = dom_[sd];
         k_bond_add<double><<<grid_for(edge_length(loc, A.nx, A.ny), 128), 128, 0, s>>>(dst, A.nx, A.ny, loc, -1.0, src,

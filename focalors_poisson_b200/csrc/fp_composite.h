@@ -95,6 +95,8 @@ private:
     };
 
     void build_schur();
+    void ensure_built();
+    bool built_ = false;
     void assemble(double* const* fields, const double* const* ghosts, cudaStream_t s);
     void eliminate(double* const* fields, cudaStream_t s, GmresInfo* info);
     void rect_solve(int d, double* f, long long batch, cudaStream_t s) const;

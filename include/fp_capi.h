@@ -121,6 +121,12 @@ typedef struct fp_solve_info
  * solves + Newton-Schulz on the device at creation); a solve then starts from y = X g and refines while
  * the reference's full-field residual test fails, falling back to plain GMRES. */
 #define FP_NO_INTERFACE_INVERSE 16
+/* create flag: never use the spectral direct path. By default a geometry inside that path's scope (see
+ * fp_batch_create: a Dirichlet root with leaves on full faces, nx of every subdomain a multiple of 32 and
+ * >= 64) is solved by the exact spectral interface solve of the batched solver, one transform pass per
+ * subdomain each way, instead of the Schur GMRES; the answer is the converged solution of the reference's
+ * GMRES, so its GMRES parameters do not apply (fp_solve_info reports 0 iterations). */
+#define FP_NO_SPECTRAL 512
 
 /* Creation builds the tree, the per-domain rectangle plans and every Schur matrix. Defaults of the
  * reference: m = 20, tol = 1e-8, max_iter = 100 (concat_solver2d.h:48-50). */
@@ -167,9 +173,9 @@ int fp_composite_destroy(fp_composite* c);
  * together (pe/concat/concat_solver2d.cpp:101-157 per problem), every stage one launch over all problems.
  * No counterpart in the reference, which solves one geometry per solver object; each problem is what a
  * ConcatPoissonSolver2D over that geometry computes (the converged solution of its Schur GMRES).
- * Supported problems: a root rectangle with leaf rectangles attached on full faces (depth-1 tree: L, T,
- * cross), every outer face Dirichlet, nx of every subdomain a multiple of 32 and >= 64; others give
- * FP_ERR_UNSUPPORTED. The interface system is solved exactly in the DST bases (closed-form responses,
+ * Supported problems: a root rectangle with Dirichlet faces and leaf rectangles attached on full faces
+ * (depth-1 tree: L, T, cross), each leaf's sides along its interface Dirichlet and its far face Dirichlet
+ * or Neumann, nx of every subdomain a multiple of 32 and >= 64; others give FP_ERR_UNSUPPORTED. The interface system is solved exactly in the DST bases (closed-form responses,
  * one dense reduced system per problem whose inverse is built at creation).
  * ------------------------------------------------------------------------------------------------- */
 typedef struct fp_batch fp_batch;

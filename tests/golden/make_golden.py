@@ -152,6 +152,18 @@ def cross_ghosts():
     composite("cross24_ghosts.npz", g, W.gaussian_rhs(g, 8, zero_mean=False), 20, 1e-12, 100, ghosts=ghosts)
 
 
+def cross64():
+    """Cross 5 x 64^2 (a size the spectral path covers) with Neumann arm tips: quarter-wave (ND / DN)
+    y-families on the y-arms, Neumann chase ends on the x-arms; once with zero ghosts, once with non-zero
+    Dirichlet and Neumann ghost values."""
+    g = W.cross(64, neumann_tips=True)
+    composite("cross64_neumann_tips.npz", g, W.gaussian_rhs(g, 17), 20, 1e-12, 200)
+    rng = np.random.default_rng(404)
+    ghosts = [[None if g.bc[i][f] == ADJ else rng.standard_normal(g.ny[i] if f < 2 else g.nx[i]) for f in range(4)]
+              for i in range(5)]
+    composite("cross64_ghosts.npz", g, W.gaussian_rhs(g, 18, zero_mean=False), 20, 1e-12, 200, ghosts=ghosts)
+
+
 def lt_shapes():
     for seed in range(4):
         g = W.lt_shape(seed, sides=[8, 12, 16, 20, 24, 32])
@@ -200,5 +212,6 @@ if __name__ == "__main__":
     cross_ghosts()
     lt_shapes()
     batch_lt()
+    cross64()
     tree9()
     mocks()

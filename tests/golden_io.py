@@ -34,7 +34,8 @@ def composite_case(name):
 
 COMPOSITE_CASES = ["concat_fixture6.npz", "concat_fixture6_tight.npz", "cross128_dirichlet.npz",
                    "cross48_neumann_tips.npz", "cross24_ghosts.npz", "lt_shape_0.npz", "lt_shape_1.npz",
-                   "lt_shape_2.npz", "lt_shape_3.npz", "tree9_periodic.npz"]
+                   "lt_shape_2.npz", "lt_shape_3.npz", "tree9_periodic.npz", "cross64_neumann_tips.npz",
+                   "cross64_ghosts.npz"]
 
 
 def rel_l2(a_list, b_list):

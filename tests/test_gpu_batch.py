@@ -1,5 +1,6 @@
-"""GPU parity of the batched composite solves (fp_batch_*): small L/T problems against the reference's own
-converged solutions (tests/golden/batch_lt_*.npz), larger ones against the single-problem C-ABI solve,
+"""GPU parity of the batched composite solves (fp_batch_*): small L/T problems and 64^2 crosses with Neumann
+arm tips and ghost values against the reference's own converged solutions (tests/golden/batch_lt_*.npz,
+cross64_*.npz), larger ones against the single-problem C-ABI Schur GMRES solve,
 graph capture/replay, per-problem residuals, the unsupported cases, and the full batched-uneven workload
 (512 L/T problems, sides 64..1024) checked through residuals and sampled problems."""
 import types
@@ -14,7 +15,7 @@ from focalors_poisson_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 
-GOLDEN = [f"batch_lt_{k}.npz" for k in range(4)]
+GOLDEN = [f"batch_lt_{k}.npz" for k in range(4)] + ["cross64_neumann_tips.npz", "cross64_ghosts.npz"]
 
 
 def _golden_problems():
@@ -61,7 +62,7 @@ def test_batch_matches_single_problem_solves():
     torch.cuda.synchronize()
     for p, (g, got) in enumerate(zip(probs, _split([x.cpu().numpy() for x in f], probs))):
         want = [np.array(r, copy=True) for r in _split(rhs, probs)[p]]
-        capi.Composite(g, 20, 1e-14, 200).solve(want)
+        capi.Composite(g, 20, 1e-14, 200, spectral=False).solve(want)
         assert rel_l2(got, want) <= 1e-11, (p, rel_l2(got, want))
 
 
@@ -90,9 +91,15 @@ def test_batch_rejects_unsupported():
     g = W.lt_problem(1, sides=(64,))
     bad = types.SimpleNamespace(**{k: getattr(g, k) for k in ("nx", "ny", "hx", "hy", "connections")})
     bad.bc = [list(r) for r in g.bc]
-    bad.bc[1][W.XPOS] = W.NEUMANN
+    bad.bc[0][W.YNEG] = W.NEUMANN  # Neumann on the root
     with pytest.raises(capi.FpError) as e:
         capi.Batch([bad])
+    assert e.value.code == 3
+    side = types.SimpleNamespace(**{k: getattr(g, k) for k in ("nx", "ny", "hx", "hy", "connections")})
+    side.bc = [list(r) for r in g.bc]
+    side.bc[1][W.YNEG] = W.NEUMANN  # Neumann on an x-leaf's side along the interface
+    with pytest.raises(capi.FpError) as e:
+        capi.Batch([side])
     assert e.value.code == 3
     odd = types.SimpleNamespace(nx=[48, 48], ny=[32, 32], hx=[0.1, 0.1], hy=[0.1, 0.1], bc=[[0] * 4] * 2,
                                 connections=[(0, W.XPOS, 1)])
@@ -122,7 +129,7 @@ def test_batched_uneven_workload_512():
         starts = np.cumsum([0] + [len(g.nx) for g in probs])
         for p in (0, 17, 255, 511):
             want = [np.array(x, copy=True) for x in rhs[p]]
-            capi.Composite(probs[p], 20, 1e-14, 200).solve(want)
+            capi.Composite(probs[p], 20, 1e-14, 200, spectral=False).solve(want)
             got = [f[starts[p] + d].cpu().numpy() for d in range(len(probs[p].nx))]
             assert rel_l2(got, want) <= etol, (precision, p, rel_l2(got, want))
         del b, f

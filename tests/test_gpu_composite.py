@@ -110,3 +110,28 @@ def test_composite_residual_of_reference_solution(name):
     assert solver.residual(u, f, g) <= 1e-11
     u[0][1, 1] += 1e-3 * float(u[0].abs().max())
     assert solver.residual(u, f, g) > 1e-6
+
+
+@pytest.mark.parametrize("n", [256, 1024])
+def test_spectral_path_matches_schur_gmres(n):
+    """A cross with Neumann arm tips is inside the spectral path's scope: its direct solve equals the Schur
+    GMRES driven to tol 1e-14 (FP_NO_SPECTRAL), and its FP32 refinement reaches the same answer."""
+    torch = torch_cuda()
+    g = W.cross(n, neumann_tips=True)
+    rhs = W.gaussian_rhs(g, 31)
+    spec = capi.Composite(g, 20, 1e-12, 100)
+    gm = capi.Composite(g, 20, 1e-14, 200, spectral=False)
+    a = [torch.tensor(r, device="cuda") for r in rhs]
+    b = [x.clone() for x in a]
+    c = [x.clone() for x in a]
+    info = spec.solve(a)
+    assert info["converged"] and info["iterations"] == 0  # no Krylov iteration on the spectral path
+    gm.solve(b)
+    spec.solve_ir(c, rel_tol=1e-13, max_refine=8)
+    torch.cuda.synchronize()
+    got, want, ir = ([x.cpu().numpy() for x in v] for v in (a, b, c))
+    # every FP64 answer carries round-off of order eps * cond(A) (~5e-11 at 1024^2)
+    tol = 1e-11 if n <= 256 else 1e-10
+    assert rel_l2(got, want) <= tol, rel_l2(got, want)
+    assert rel_l2(ir, want) <= tol, rel_l2(ir, want)
+
