@@ -347,7 +347,14 @@ struct BIface
     const double* K;    // nx * ny: K[m ny + k] = 1 / (alpha_m + r beta_k), the root's inverse in the 2D basis
     double*       vxy;  // [e][Y] ny: psi_k(jY) sig_e[k] zX[e][k]
     double*       wxy;  // [e][Y] nx: chi_m(ie) sig'_Y[m] yY[Y][m]
+    int           yy_chunks, yx_chunks;  // column chunks of the two dense products (both edge kinds)
+    double*       part_yy;  // [chunk][nye nx] partial sums of Rinv rhsY
+    double*       part_yx;  // [chunk][e*2+Y][ny] partial sums of K^T wxy
 };
+
+// Dense products of the interface solve run as 32-row tiles x column chunks, 8 warps per tile splitting
+// the chunk's columns; partial sums are added in a fixed order by the finishing kernel (reproducible).
+constexpr int kIfTile = 32, kIfWarps = 8, kIfChunkYY = 1024, kIfChunkYX = 512;
 
 __device__ __forceinline__ double chi_edge(int n, int m, int i) { return dst_basis(n, m, i); }
 
@@ -395,19 +402,46 @@ __global__ void k_if_rhsy(const BIface* __restrict__ P, const long long* __restr
     if (lane == 0) F.rhsY[Y * F.nx + m] = F.gY[Y * F.nx + m] + acc;
 }
 
-// yY = Rinv rhsY (thread per row) or, without x-edges, the per-m blocks; sY = sigma' yY
+// Partial sums of yY = Rinv rhsY (problems with both edge kinds): block = (row tile, column chunk); lane =
+// row (Rinv is column-major: a warp reads 32 consecutive rows of one column), warp = every 8th column.
+__global__ void __launch_bounds__(256) k_if_yy_part(const BIface* __restrict__ P, const long long* __restrict__ prefix,
+                                                    int np)
+{
+    __shared__ double red[kIfWarps][kIfTile];
+    const int     p    = seg_of(prefix, np, blockIdx.x);
+    const BIface& F    = P[p];
+    const int     b    = (int)(blockIdx.x - prefix[p]);
+    const int     tile = b / F.yy_chunks, chunk = b - tile * F.yy_chunks;
+    const int     lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int     n    = F.nye * F.nx;
+    const int     q    = tile * kIfTile + lane;
+    const int     c1   = min(n, (chunk + 1) * kIfChunkYY);
+    double        acc  = 0;
+    if (q < n)
+        for (int c = chunk * kIfChunkYY + warp; c < c1; c += kIfWarps) acc += F.rinv[(long long)c * n + q] * F.rhsY[c];
+    red[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0 && q < n)
+    {
+        double v = 0;
+        for (int w = 0; w < kIfWarps; ++w) v += red[w][lane];
+        F.part_yy[(long long)chunk * n + q] = v;
+    }
+}
+
+// yY (sum of the partials, or the per-m blocks without x-edges); sY = sigma' yY; wxy for the yx product
 __global__ void k_if_yy(const BIface* __restrict__ P, const long long* __restrict__ prefix, int np)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= prefix[np]) return;
-    const int    p = seg_of(prefix, np, t);
-    const BIface F = P[p];
-    const int    q = (int)(t - prefix[p]);  // row of the nye*nx system
-    const int    n = F.nye * F.nx;
-    double       v = 0;
+    const int     p = seg_of(prefix, np, t);
+    const BIface& F = P[p];
+    const int     q = (int)(t - prefix[p]);  // row of the nye*nx system
+    const int     n = F.nye * F.nx;
+    double        v = 0;
     if (F.nxe > 0)
     {
-        for (int c = 0; c < n; ++c) v += F.rinv[(long long)c * n + q] * F.rhsY[c];
+        for (int c = 0; c < F.yy_chunks; ++c) v += F.part_yy[(long long)c * n + q];
     }
     else
     {
@@ -421,8 +455,39 @@ __global__ void k_if_yy(const BIface* __restrict__ P, const long long* __restric
     for (int e = 0; e < F.nxe; ++e) F.wxy[(e * 2 + Y) * F.nx + m] = chi_edge(F.nx, m, F.ie[e]) * F.sY[q];
 }
 
+// Partial sums of sum_m K[m][k] wxy[e][Y][m] (problems with both edge kinds): block = (k tile, m chunk);
+// lane = k (a warp reads 32 consecutive k of one K row), warp = every 8th m.
+__global__ void __launch_bounds__(256) k_if_yx_part(const BIface* __restrict__ P, const long long* __restrict__ prefix,
+                                                    int np)
+{
+    __shared__ double red[kIfWarps][4][kIfTile];
+    const int     p    = seg_of(prefix, np, blockIdx.x);
+    const BIface& F    = P[p];
+    const int     b    = (int)(blockIdx.x - prefix[p]);
+    const int     tile = b / F.yx_chunks, chunk = b - tile * F.yx_chunks;
+    const int     lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int     k    = tile * kIfTile + lane;
+    const int     m1   = min(F.nx, (chunk + 1) * kIfChunkYX);
+    double        acc[4] = {0, 0, 0, 0};
+    if (k < F.ny)
+        for (int m = chunk * kIfChunkYX + warp; m < m1; m += kIfWarps)
+        {
+            const double Kmk = F.K[(long long)m * F.ny + k];
+            for (int e = 0; e < F.nxe; ++e)
+                for (int Y = 0; Y < F.nye; ++Y) acc[e * 2 + Y] += Kmk * F.wxy[(e * 2 + Y) * F.nx + m];
+        }
+    for (int i = 0; i < 4; ++i) red[warp][i][lane] = acc[i];
+    __syncthreads();
+    if (warp == 0 && k < F.ny)
+        for (int i = 0; i < 4; ++i)
+        {
+            double v = 0;
+            for (int w = 0; w < kIfWarps; ++w) v += red[w][i][lane];
+            F.part_yx[((long long)chunk * 4 + i) * F.ny + k] = v;
+        }
+}
+
 // yX[e][k] = sum_e' invXX_k(e, e') (gX[e'][k] + sum_Y psi_k(jY) sum_m K[m][k] wxy[e'][Y][m]); bX2 = bX + sig yX.
-// Thread per (problem, k): a warp reads 32 consecutive k of each K row.
 __global__ void k_if_yx(const BIface* __restrict__ P, const long long* __restrict__ prefix, int np)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -433,14 +498,13 @@ __global__ void k_if_yx(const BIface* __restrict__ P, const long long* __restric
     double        tt[2] = {0, 0};
     for (int Y = 0; Y < F.nye; ++Y)
     {
-        double acc[2] = {0, 0};
-        for (int m = 0; m < F.nx; ++m)
-        {
-            const double Kmk = F.K[(long long)m * F.ny + k];
-            for (int e = 0; e < F.nxe; ++e) acc[e] += Kmk * F.wxy[(e * 2 + Y) * F.nx + m];
-        }
         const double pk = dst_basis(F.ny, k, F.jy[Y]);
-        for (int e = 0; e < F.nxe; ++e) tt[e] += pk * acc[e];
+        for (int e = 0; e < F.nxe; ++e)
+        {
+            double a = 0;
+            for (int c = 0; c < F.yx_chunks; ++c) a += F.part_yx[((long long)c * 4 + e * 2 + Y) * F.ny + k];
+            tt[e] += pk * a;
+        }
     }
     const int     E = F.nxe;
     const double* B = F.invxx + (long long)k * E * E;
@@ -870,6 +934,7 @@ private:
         DevBuf mem;  // spectral vectors and interface work (doubles)
         DevBuf rinv;
         DevBuf K;    // root inverse in the 2D basis (problems with both x- and y-edges)
+        DevBuf part; // partial sums of the interface's dense products
     };
 
     void   build_spectral();
@@ -898,6 +963,7 @@ private:
     Segments                                  leaf_rows_, leaf_cols_, root_rows_, root_cols_;
     Segments                                  edst_g_, edst_out_;         // FP64 edge DSTs
     Segments                                  ifk_, ifym_, ifrow_, ifkw_;  // interface work lists
+    Segments                                  ifyyp_, ifyxp_;              // partial-product blocks
     std::vector<DstSeg>                       dst_W_in_rec_, dst_X_out_rec_;
     std::vector<int>                          dst_kinds_;
     XList                                     dst_fs_, dst_r_, dst_out_u_, dst_out_r_, dst_user_in_, dst_user_out_;
@@ -1208,6 +1274,13 @@ template <typename TS> void BatchImpl<TS>::build_spectral()
         }
         if (F.nxe > 0 && F.nye > 0)
         {
+            const int nYp = F.nye * nx;
+            F.yy_chunks   = (nYp + kIfChunkYY - 1) / kIfChunkYY;
+            F.yx_chunks   = (nx + kIfChunkYX - 1) / kIfChunkYX;
+            pr.part.alloc(((size_t)F.yy_chunks * nYp + (size_t)F.yx_chunks * 4 * ny) * 8);
+            FPB_CUDA(cudaMemset(pr.part.get(), 0, pr.part.bytes()));
+            F.part_yy = pr.part.template as<double>();
+            F.part_yx = F.part_yy + (size_t)F.yy_chunks * nYp;
             pr.K.alloc((size_t)nx * ny * 8);
             F.K = pr.K.template as<double>();
             k_root_inverse<<<grid_of((long long)nx * ny, 256), 256>>>(F, pr.K.template as<double>());
@@ -1409,6 +1482,21 @@ template <typename TS> void BatchImpl<TS>::build_static_lists()
     std::vector<long long> one_e(eg.size(), 1), one_o(eo.size(), 1);
     edst_g_.set(eg, one_e);
     edst_out_.set(eo, one_o);
+    {
+        std::vector<BIface>    py, px;
+        std::vector<long long> cy2, cx2;
+        for (auto& pr : prob_)
+            if (pr.F.nxe > 0 && pr.F.nye > 0)
+            {
+                const BIface& F = pr.F;
+                py.push_back(F);
+                cy2.push_back((long long)((F.nye * F.nx + kIfTile - 1) / kIfTile) * F.yy_chunks);
+                px.push_back(F);
+                cx2.push_back((long long)((F.ny + kIfTile - 1) / kIfTile) * F.yx_chunks);
+            }
+        ifyyp_.set(py, cy2);
+        ifyxp_.set(px, cx2);
+    }
     ifk_.set(fk, ck);
     ifkw_.set(fw, cw);
     ifym_.set(fy, cy);
@@ -1497,11 +1585,21 @@ template <typename TS> void BatchImpl<TS>::inner(const XList& dst_in, const XLis
     {
         k_if_rhsy<<<grid_of(ifym_.total * 32, 256), 256, 0, s>>>(ifym_.as<BIface>(), ifym_.pre(), ifym_.n);
         FPB_CHECK_LAUNCH();
+        if (ifyyp_.n)
+        {
+            k_if_yy_part<<<(unsigned)ifyyp_.total, 256, 0, s>>>(ifyyp_.as<BIface>(), ifyyp_.pre(), ifyyp_.n);
+            FPB_CHECK_LAUNCH();
+        }
         k_if_yy<<<grid_of(ifrow_.total, 128), 128, 0, s>>>(ifrow_.as<BIface>(), ifrow_.pre(), ifrow_.n);
         FPB_CHECK_LAUNCH();
     }
     if (ifkw_.n)
     {
+        if (ifyxp_.n)
+        {
+            k_if_yx_part<<<(unsigned)ifyxp_.total, 256, 0, s>>>(ifyxp_.as<BIface>(), ifyxp_.pre(), ifyxp_.n);
+            FPB_CHECK_LAUNCH();
+        }
         k_if_yx<<<grid_of(ifkw_.total, 128), 128, 0, s>>>(ifkw_.as<BIface>(), ifkw_.pre(), ifkw_.n);
         FPB_CHECK_LAUNCH();
     }
