@@ -4,7 +4,8 @@ Workload (the largest cross configuration that fits one GPU): a cross of 5 subdo
 (centre + 4 arms), h = 1/2048, Neumann arm tips, Dirichlet elsewhere, seeded zero-mean Gaussian RHS,
 GMRES(m=20, tol=1e-14, maxIter=100) on the interface unknowns. One step = one full composite solve
 (inputs re-filled from a resident copy first, since a solve consumes its right-hand side). Three forms are
-timed (FP64, FP64 + refinement, FP32 transforms + FP64 refinement); the headline is the fastest whose
+timed (FP64, FP64 + refinement, FP32 + FP64 refinement, FP64 solve + FP32 corrections); the headline is the
+fastest whose
 answer is within 1e-10 relative L2 of the refined solution. A second section (`batched_uneven`) times the
 512-problem batched workload the same way (N = 1 only; --no-batched skips it).
 
@@ -34,6 +35,7 @@ N_CELLS = 2048
 GMRES = (20, 1e-14, 100)
 SEED = 2024
 IR_REL_TOL = 1e-11
+INNER = {"f64ir": "f64", "f32ir": "f32", "mixedir": "mixed"}
 
 
 def workload_config():
@@ -359,7 +361,7 @@ def main():
                 w.copy_(p)
             if form == "f64":
                 return solver.solve(work)
-            return solver.solve_ir(work, rel_tol=IR_REL_TOL, max_refine=10, inner="f32" if form == "f32ir" else "f64")
+            return solver.solve_ir(work, rel_tol=IR_REL_TOL, max_refine=10, inner=INNER[form])
 
         infos = [step() for _ in range(args.warmup)]
         torch.cuda.synchronize()
@@ -385,7 +387,7 @@ def main():
         return {"ms": ms, "value": args.steps * world / (ms / 1e3), "launches": int(launches), "clocks": clk,
                 "infos": infos[-args.steps:], "solution": [w.clone() for w in work]}
 
-    forms_run = ("f64", "f64ir", "f32ir")
+    forms_run = ("f64", "f64ir", "f32ir", "mixedir")
     res = {form: run_form(form) for form in forms_run}
     # accuracy arbiter: the FP64 residual of the composite operator and, as "exact", the refinement solve
     # driven to |correction| <= 1e-14 |u| (the single FP64 solve has a round-off floor ~ eps * cond(A))
@@ -422,7 +424,7 @@ def main():
         if head == "f64":
             solver.solve(host_np)  # synchronous host-pointer call
         else:
-            solver.solve_ir(host_np, rel_tol=IR_REL_TOL, max_refine=10, inner="f32" if head == "f32ir" else "f64")
+            solver.solve_ir(host_np, rel_tol=IR_REL_TOL, max_refine=10, inner=INNER[head])
         if it > 0:
             e2e_times.append(time.perf_counter() - t0)
     e2e_t = sum(e2e_times)
@@ -470,11 +472,13 @@ def main():
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None,
-        "dtype": {"f64": "f64", "f64ir": "f64", "f32ir": "f32 transforms + f64 refinement"}[head],
+        "dtype": {"f64": "f64", "f64ir": "f64", "f32ir": "f32 transforms + f64 refinement",
+                  "mixedir": "f64 solve + f32 corrections, f64 refinement"}[head],
         "data": "synthetic", "config": workload_config(),
         "precision_form": {"f64": "FP64 drop-in (interface-preconditioned Schur GMRES)",
                            "f64ir": "FP64 solves + FP64 iterative refinement",
-                           "f32ir": "FP32 transforms + FP64 iterative refinement"}[head],
+                           "f32ir": "FP32 transforms + FP64 iterative refinement",
+                           "mixedir": "FP64 solve, then FP32-storage corrections in FP64 iterative refinement"}[head],
         "forms": forms, "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

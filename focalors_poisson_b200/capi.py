@@ -47,7 +47,7 @@ SIGNATURES = {
     "fp_batch_destroy": ([_vp], _i),
 }
 FP_GMRES_FULLFIELD, FP_CHECK_CONVERGENCE, FP_NO_INTERFACE_INVERSE, FP_IR_INNER_F64 = 4, 8, 16, 32
-FP_BATCH_F32, FP_BATCH_NO_AUTOTUNE, FP_BATCH_GRAPH, FP_NO_SPECTRAL = 64, 128, 256, 512
+FP_BATCH_F32, FP_BATCH_NO_AUTOTUNE, FP_BATCH_GRAPH, FP_NO_SPECTRAL, FP_IR_FIRST_F64 = 64, 128, 256, 512, 1024
 
 
 class Geometry(ctypes.Structure):
@@ -243,14 +243,16 @@ class Composite:
         return self._info(info)
 
     def solve_ir(self, fields, ghosts=None, rel_tol=1e-12, max_refine=10, check_convergence=False, inner="f32"):
-        """The same solve by inner solves (FP32 transforms, or FP64 with inner="f64") wrapped in FP64
-        iterative refinement on the composite operator."""
+        """The same solve by inner solves (FP32 transforms, FP64 with inner="f64", or inner="mixed": the FP64
+        solve first, then FP32 corrections) wrapped in FP64 iterative refinement on the composite operator."""
         fp, gp, flags, stream, keep = self._pointers(fields, ghosts)
         info = SolveInfo()
         if check_convergence:
             flags |= FP_CHECK_CONVERGENCE
         if inner == "f64":
             flags |= FP_IR_INNER_F64
+        elif inner == "mixed":
+            flags |= FP_IR_FIRST_F64
         check(lib().fp_composite_solve_f32ir(self.h, fp, gp, flags, stream, float(rel_tol), int(max_refine),
                                              ctypes.byref(info)))
         return self._info(info)

@@ -913,7 +913,8 @@ public:
     void          autotune(cudaStream_t s) override;
     long long     graph_kernels() const override { return graph_kernels_; }
     int           refine(double* const* fields, const double* const* ghosts, double rel_tol, int max_refine,
-                         cudaStream_t s, double* rel_change) override;
+                         cudaStream_t s, double* rel_change, BatchBase* first) override;
+    void          solve_assembled(const double* const* in, double* const* out, cudaStream_t s) override;
 
 private:
     struct Dom
@@ -971,6 +972,9 @@ private:
     Segments                                  addn_;  // u += r with norms (adaptive refinement)
     DevBuf                                    addp_;
     std::map<std::tuple<int, int, int>, DevBuf> basis_;  // y-basis column tables (family, n, column)
+    std::vector<const double*>                ext_in_;     // solve_assembled: last pointer sets and lists
+    std::vector<double*>                      ext_out_;
+    XList                                     ext_in_list_, ext_out_list_;
     std::vector<double*>                      user_ptrs_;
     std::vector<const double*>                user_ghosts_;
     int                                       user_steps_ = -1;
@@ -1807,8 +1811,31 @@ template <typename TS> void BatchImpl<TS>::solve_graph(double* const* fields, co
 }
 
 template <typename TS>
+void BatchImpl<TS>::solve_assembled(const double* const* in, double* const* out, cudaStream_t s)
+{
+    const int                  nd = (int)dom_.size();
+    std::vector<const double*> vi(in, in + nd);
+    std::vector<double*>       vo(out, out + nd);
+    if (vi != ext_in_ || vo != ext_out_)
+    {
+        FPB_CUDA(cudaDeviceSynchronize());  // the lists below may still be read by queued work
+        std::vector<DstSeg> a = dst_W_in_rec_, b = dst_X_out_rec_;
+        for (int g = 0; g < nd; ++g)
+        {
+            a[g].in  = vi[g];
+            b[g].out = vo[g];
+        }
+        ext_in_list_.set(a, dst_kinds_, plans_);
+        ext_out_list_.set(b, dst_kinds_, plans_);
+        ext_in_  = vi;
+        ext_out_ = vo;
+    }
+    inner(ext_in_list_, ext_out_list_, false, s);
+}
+
+template <typename TS>
 int BatchImpl<TS>::refine(double* const* fields, const double* const* ghosts, double rel_tol, int max_refine,
-                         cudaStream_t s, double* rel_change)
+                         cudaStream_t s, double* rel_change, BatchBase* first)
 {
     if (!fields) throw Error(1, "null field list");
     if (!(rel_tol > 0) || max_refine < 1) throw Error(1, "rel_tol must be > 0 and max_refine >= 1");
@@ -1821,7 +1848,19 @@ int BatchImpl<TS>::refine(double* const* fields, const double* const* ghosts, do
     int                 steps  = 0;
     while (steps < max_refine)
     {
-        inner(steps == 0 ? dst_fs_ : dst_r_, dst_out_r_, false, s);  // r <- correction
+        if (steps == 0 && first)
+        {
+            std::vector<const double*> fi(dom_.size());
+            std::vector<double*>       ro(dom_.size());
+            for (size_t g = 0; g < dom_.size(); ++g)
+            {
+                fi[g] = fs_.as<double>() + dom_[g].off;
+                ro[g] = r_.as<double>() + dom_[g].off;
+            }
+            first->solve_assembled(fi.data(), ro.data(), s);  // r <- first solution
+        }
+        else
+            inner(steps == 0 ? dst_fs_ : dst_r_, dst_out_r_, false, s);  // r <- correction
         k_b_add_norms<<<(unsigned)addn_.total, 256, 0, s>>>(addn_.as<AddSeg>(), addn_.pre(), addn_.n, steps == 0);
         FPB_CHECK_LAUNCH();
         ++steps;

@@ -48,8 +48,13 @@ public:
     // Iterative refinement until |correction| <= rel_tol |u| over all cells (or the observed contraction
     // predicts it after the last correction), at most max_refine inner solves; synchronises the stream
     // after every step. Returns the steps taken; *rel_change the last |correction| / |u|.
+    // first: when given, the first inner solve runs on that solver (same problems; e.g. the FP64 solve
+    // followed by FP32 corrections).
     virtual int refine(double* const* fields, const double* const* ghosts, double rel_tol, int max_refine,
-                       cudaStream_t s, double* rel_change) = 0;
+                       cudaStream_t s, double* rel_change, BatchBase* first = nullptr) = 0;
+    // One inner solve of already assembled, hx^2-scaled right-hand sides `in` (one pointer per subdomain)
+    // into `out` (stored, not accumulated); in and out may alias.
+    virtual void solve_assembled(const double* const* in, double* const* out, cudaStream_t s) = 0;
     // Per-problem |fs - A u| / |fs| (fs: assembled, hx^2-scaled right-hand side); out: host, n_problems.
     virtual void residuals(const double* const* u, const double* const* rhs, const double* const* ghosts,
                            cudaStream_t s, double* out) = 0;

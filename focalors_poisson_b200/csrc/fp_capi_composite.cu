@@ -185,7 +185,8 @@ int fp_composite_solve_f32ir(fp_composite* c, double* const* fields, const doubl
                     c->sp32 = make_batch({c->desc}, 1);
                     c->sp32->autotune(s);
                 }
-                steps = (f32 ? c->sp32 : c->sp64)->refine(f, g, rel_tol, max_refine, s, &change);
+                BatchBase* first = (f32 && (flags & FP_IR_FIRST_F64)) ? c->sp64.get() : nullptr;
+                steps = (f32 ? c->sp32 : c->sp64)->refine(f, g, rel_tol, max_refine, s, &change, first);
             }
             else
                 steps = c->c->solve_ir(f, g, s, rel_tol, max_refine, &change, &gi, f32);

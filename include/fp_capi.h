@@ -145,6 +145,10 @@ int fp_composite_solve_f64(fp_composite* c, double* const* fields, const double*
  * With FP_IR_INNER_F64 the inner solves are the FP64 ones (refinement then only removes the single
  * FP64 solve's round-off, about eps * cond(A)). */
 #define FP_IR_INNER_F64 32
+/* With FP32 inner solves: make the first inner solve the FP64 one (its answer already carries only FP64
+ * round-off, eps * cond(A)), so that one or two FP32 corrections finish the refinement. Spectral path only;
+ * ignored on the Schur GMRES path. */
+#define FP_IR_FIRST_F64 1024
 int fp_composite_solve_f32ir(fp_composite* c, double* const* fields, const double* const* ghosts, int flags,
                              void* stream, double rel_tol, int max_refine, fp_solve_info* info);
 /* Adjoint (transposed) solve of the map rhs -> solution with the ghost buffers held fixed: the gradient

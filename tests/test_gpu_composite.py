@@ -124,14 +124,18 @@ def test_spectral_path_matches_schur_gmres(n):
     a = [torch.tensor(r, device="cuda") for r in rhs]
     b = [x.clone() for x in a]
     c = [x.clone() for x in a]
+    d = [x.clone() for x in a]
     info = spec.solve(a)
     assert info["converged"] and info["iterations"] == 0  # no Krylov iteration on the spectral path
     gm.solve(b)
     spec.solve_ir(c, rel_tol=1e-13, max_refine=8)
+    mixed = spec.solve_ir(d, rel_tol=1e-13, max_refine=8, inner="mixed")
     torch.cuda.synchronize()
-    got, want, ir = ([x.cpu().numpy() for x in v] for v in (a, b, c))
+    got, want, ir, mx = ([x.cpu().numpy() for x in v] for v in (a, b, c, d))
     # every FP64 answer carries round-off of order eps * cond(A) (~5e-11 at 1024^2)
     tol = 1e-11 if n <= 256 else 1e-10
     assert rel_l2(got, want) <= tol, rel_l2(got, want)
     assert rel_l2(ir, want) <= tol, rel_l2(ir, want)
+    assert rel_l2(mx, want) <= tol, rel_l2(mx, want)
+    assert rel_l2(mx, ir) <= 1e-11 and mixed["refinements"] <= 3, (rel_l2(mx, ir), mixed)
 
