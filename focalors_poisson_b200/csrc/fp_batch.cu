@@ -137,6 +137,9 @@ __device__ __forceinline__ T mod_rhs(const ChaseSeg<T>* __restrict__ sg, int nro
 }
 
 // blocks of segment s: prefix (in blocks); per segment P*ny threads (local / correct) or ny (reduced)
+// Interior rows of the chunks. Modifiers: a row term can only fall on interior row 0 of chunk 0 (row
+// nx-1 is the last separator, handled by k_b_chase_reduced); column terms add s_c[i] psi_c(j) to every
+// row, applied as one pass per term over the thread's 31 rows.
 template <typename T>
 __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __restrict__ segs,
                                                        const long long* __restrict__ prefix, int nseg,
@@ -150,15 +153,23 @@ __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __rest
     if (t >= P * ny) return;
     const int j = t % ny, p = t / ny;
     const int typ = p == 0 ? 0 : 1;
-    const int nrow = sg->nrow, ncol = sg->ncol;
-    ModCtx<T> mc;
-    mod_init(sg, ncol, j, mc);
-    const T* col = sg->in + (long long)p * kChunk * ny + j;
-    T*       out = sg->out + (long long)p * kChunk * ny + j;
-    const T* c   = tabs[sg->tab].cc + (long long)typ * Li * ny + j;
-    T        y[Li];
+    const T*  col = sg->in + (long long)p * kChunk * ny + j;
+    T*        out = sg->out + (long long)p * kChunk * ny + j;
+    const T*  c   = tabs[sg->tab].cc + (long long)typ * Li * ny + j;
+    T         y[Li];
 #pragma unroll
-    for (int r = 0; r < Li; ++r) y[r] = mod_rhs(sg, nrow, ncol, mc, p * kChunk + r, j, col[(long long)r * ny]);
+    for (int r = 0; r < Li; ++r) y[r] = col[(long long)r * ny];
+    const int ncol = sg->ncol;
+    for (int q = 0; q < ncol; ++q)
+    {
+        const double  ps = sg->col_c[q] * (sg->col_tab[q] ? sg->col_tab[q][j] : dst_basis(ny, j, sg->col_j[q]));
+        const double* sv = sg->col_s[q] + p * kChunk;
+#pragma unroll
+        for (int r = 0; r < Li; ++r) y[r] = (T)((double)y[r] + ps * sv[r]);
+    }
+    if (p == 0)
+        for (int q = 0; q < sg->nrow; ++q)
+            if (sg->row_i[q] == 0) y[0] = (T)((double)y[0] + sg->row_c[q] * sg->row_v[q][j]);
     T prev = 0;
 #pragma unroll
     for (int r = 0; r < Li; ++r)
@@ -625,6 +636,8 @@ __global__ void k_myy(const BIface F, const double* H /* 2x2 blocks per m: H[(Y*
 // ---------------------------------------------------------------------------------------------
 // Elementwise over many subdomains
 // ---------------------------------------------------------------------------------------------
+constexpr int kAsmCells = 1024;  // cells per block of k_b_assemble
+
 struct AsmSeg
 {
     double*      f;
@@ -633,18 +646,23 @@ struct AsmSeg
 };
 __global__ void k_b_assemble(const AsmSeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg)
 {
-    const int     s  = seg_of(prefix, nseg, blockIdx.x);
-    const AsmSeg* sg = segs + s;
-    const int     t  = (int)(blockIdx.x - prefix[s]) * blockDim.x + threadIdx.x;
-    if (t >= sg->a.nx * sg->a.ny) return;
-    double* copy = sg->copy;
-    if (copy)
+    const int     s    = seg_of(prefix, nseg, blockIdx.x);
+    const AsmSeg* sg   = segs + s;
+    const int     n    = sg->a.nx * sg->a.ny;
+    const int     t0   = (int)(blockIdx.x - prefix[s]) * kAsmCells;
+    const int     t1   = min(n, t0 + kAsmCells);
+    double*       copy = sg->copy;
+    double*       f    = sg->f;
+    for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x)
     {
-        copy[t] = sg->f[t];
-        assemble_at(copy, t, sg->a);
+        if (copy)
+        {
+            copy[t] = f[t];
+            assemble_at(copy, t, sg->a);
+        }
+        else
+            assemble_at(f, t, sg->a);
     }
-    else
-        assemble_at(sg->f, t, sg->a);
 }
 
 struct ResSeg
@@ -1692,7 +1710,7 @@ void BatchImpl<TS>::set_user_lists(double* const* fields, const double* const* g
             q.a.ghost[k] = gh.empty() ? nullptr : gh[4 * g + k];
         }
         as.push_back(q);
-        ac.push_back((D.cells() + 255) / 256);
+        ac.push_back((D.cells() + kAsmCells - 1) / kAsmCells);
         di[g].in   = f[g];
         dout[g].out = f[g];
         cp.push_back({f[g], ir ? u_.as<double>() + dom_[g].off : nullptr, D.cells()});
@@ -1918,6 +1936,8 @@ void BatchImpl<TS>::residuals(const double* const* u, const double* const* rhs, 
         ac.push_back((D.cells() + 255) / 256);
         bo[g + 1] = bo[g] + ac.back();
     }
+    std::vector<long long> acb;
+    for (int g = 0; g < nd; ++g) acb.push_back((dom_[g].d.cells() + kAsmCells - 1) / kAsmCells);
     DevBuf pa((size_t)bo[nd] * 8), pf((size_t)bo[nd] * 8);
     for (int g = 0; g < nd; ++g)
     {
@@ -1928,7 +1948,7 @@ void BatchImpl<TS>::residuals(const double* const* u, const double* const* rhs, 
         rs.push_back(q);
     }
     Segments A, R;
-    A.set(as, ac);
+    A.set(as, acb);
     R.set(rs, ac);
     k_b_assemble<<<(unsigned)A.total, 256, 0, s>>>(A.as<AsmSeg>(), A.pre(), A.n);
     FPB_CHECK_LAUNCH();
@@ -1977,15 +1997,17 @@ template <typename TS> void BatchImpl<TS>::autotune(cudaStream_t s)
     };
     BatchTiming best = tm_;
     float       bt   = 1e30f;
-    for (int th : {128, 256, 512})
-        for (int bps : {1, 2, 4, 8})
+    for (int th : {128, 192, 256, 384, 512})
+    {
+        int occ = 0;
+        FPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_xform<TS, K_DD, 0, TS, TS, false>, th,
+                                                               plans_.smem));
+        // persistent grids of 1, 2, 4, the occupancy limit CTAs per SM, or one CTA per work item (1 << 20)
+        for (int bps : {1, 2, 4, occ, 1 << 20})
         {
+            if (bps < 1 || (bps > occ && bps != (1 << 20))) continue;
             tm_.dst_threads       = th;
             tm_.dst_blocks_per_sm = bps;
-            int occ = 0;
-            FPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_xform<TS, K_DD, 0, TS, TS, false>, th,
-                                                                   plans_.smem));
-            if (occ < bps) continue;
             const float t = time_it([&] { launch_x<TS, TS, TS, false>(sg, false, plans_, tm_, s); });
             if (t < bt)
             {
@@ -1993,6 +2015,7 @@ template <typename TS> void BatchImpl<TS>::autotune(cudaStream_t s)
                 best = tm_;
             }
         }
+    }
     tm_ = best;
     bt  = 1e30f;
     for (int th : {128, 256})

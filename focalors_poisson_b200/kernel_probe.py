@@ -3,7 +3,7 @@
     python -m focalors_poisson_b200.kernel_probe transform --family DD --n 2048 [--dtype f64] [--inverse]
     python -m focalors_poisson_b200.kernel_probe rect --n 2048 --bc 0 0 0 0 [--dtype f32]
     python -m focalors_poisson_b200.kernel_probe transform ... --launches 1     # one launch, for ncu -c 1
-    python -m focalors_poisson_b200.kernel_probe composite --n 2048 [--form f64|f64ir|f32ir] [--launches K]
+    python -m focalors_poisson_b200.kernel_probe composite --n 2048 [--form f64|f64ir|f32ir|mixedir] [--launches K]
     python -m focalors_poisson_b200.kernel_probe batch --problems 512 [--precision f64|f32] [--steps S]
 
 With --launches 1 the composite and batch modes print how many library kernels ran before the final call,
@@ -26,7 +26,7 @@ def main():
 
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["transform", "rect", "composite", "batch"])
-    ap.add_argument("--form", default="f64", choices=["f64", "f64ir", "f32ir"])
+    ap.add_argument("--form", default="f64", choices=["f64", "f64ir", "f32ir", "mixedir"])
     ap.add_argument("--problems", type=int, default=512)
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
     ap.add_argument("--steps", type=int, default=0)
@@ -121,8 +121,8 @@ def composite(args):
     if args.form == "f64":
         fn = lambda: solver.solve(work)  # noqa: E731
     else:
-        fn = lambda: solver.solve_ir(work, rel_tol=1e-11, max_refine=10,  # noqa: E731
-                                     inner="f32" if args.form == "f32ir" else "f64")
+        inner = {"f64ir": "f64", "f32ir": "f32", "mixedir": "mixed"}[args.form]
+        fn = lambda: solver.solve_ir(work, rel_tol=1e-11, max_refine=10, inner=inner)  # noqa: E731
     ms = _time(fn, refill, args.launches)
     print(f"composite cross 5x{args.n}^2 {args.form}: " + ("launched once" if ms is None else f"{ms:.3f} ms"))
 
