@@ -92,6 +92,23 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The slowest rank's time (every rank must call this, in the same order)."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(steps: int, world: int, ms: float) -> float:
+    """Whole-job solves/s of `world` independent replicas, each doing `steps` solves in `ms` (the max over
+    ranks)."""
+    return steps * world / (ms / 1e3)
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -379,12 +396,8 @@ def main():
         launches = lib.fp_launch_count() - launches0
         barrier()
         clk = clocks.stop()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return {"ms": ms, "value": args.steps * world / (ms / 1e3), "launches": int(launches), "clocks": clk,
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+        return {"ms": ms, "value": replica_value(args.steps, world, ms), "launches": int(launches), "clocks": clk,
                 "infos": infos[-args.steps:], "solution": [w.clone() for w in work]}
 
     forms_run = ("f64", "f64ir", "f32ir", "mixedir")
@@ -427,11 +440,7 @@ def main():
             solver.solve_ir(host_np, rel_tol=IR_REL_TOL, max_refine=10, inner=INNER[head])
         if it > 0:
             e2e_times.append(time.perf_counter() - t0)
-    e2e_t = sum(e2e_times)
-    if dist is not None:
-        t = torch.tensor([e2e_t], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_t = max_over_ranks(sum(e2e_times), dist, dev)
     field_bytes = sum(int(p.numel()) * 8 for p in pristine)
     e2e = {"value": args.steps * world / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": field_bytes,
            "d2h_bytes_per_step": field_bytes, "form": head}
