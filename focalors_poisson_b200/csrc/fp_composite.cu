@@ -8,6 +8,7 @@
 // one rectangle solve of the node plus the children's dense Schur matrices. The orthogonalisation is
 // the reference's modified Gram-Schmidt, the small Hessenberg least-squares problem (Givens rotations,
 // back substitution) runs on the host in FP64.
+#include "fp_batch.h"
 #include "fp_composite.h"
 #include "fp_ops.cuh"
 
@@ -622,6 +623,65 @@ bool Composite::refine_with_inverse(int d, double* f, cudaStream_t s, GmresInfo*
     return false;
 }
 
+// Schur matrix of an internal child c whose own children are all leaves: the subtree (c and its leaves,
+// c's face toward d Adjacented) is a depth-1 tree, which the spectral batched solver covers when its
+// boundary types allow. K copies of the subtree are solved at once, copy q carrying the unit impulse at
+// interface cell i0 + q; the responses on c's interface row are the matrix's columns. Returns false (and
+// builds nothing) when the subtree is outside the spectral solver's scope.
+bool Composite::schur_by_spectral(Link& L, cudaStream_t s)
+{
+    const int c = L.child;
+    std::vector<int> map = {c};
+    for (auto& k : tree_.children[c])
+    {
+        if (!node_[k.second].kids.empty()) return false;
+        map.push_back(k.second);
+    }
+    BatchProblemDesc desc;
+    for (int g : map) desc.doms.push_back(dom_[g]);  // Adjacented faces already marked, c's parent face included
+    for (size_t q = 1; q < map.size(); ++q) desc.conns.push_back({0, tree_.children[c][q - 1].first, (int)q});
+    long long sub_cells = 0;
+    for (int g : map) sub_cells += dom_[g].cells();
+    const long long K = std::max(1LL, std::min<long long>(L.cn, (4LL << 30) / (sub_cells * 8 * 4)));
+    std::unique_ptr<BatchBase> b;
+    try
+    {
+        b = make_batch(std::vector<BatchProblemDesc>((size_t)K, desc), 0);
+    }
+    catch (const Error& e)
+    {
+        if (e.code != 3) throw;
+        return false;
+    }
+    b->autotune(s);
+    const Domain& C    = dom_[c];
+    const int     face = L.loc ^ 1;  // c's face toward its parent
+    std::vector<DevBuf> bufs(map.size());
+    for (size_t q = 0; q < map.size(); ++q) bufs[q].alloc((size_t)K * dom_[map[q]].cells() * sizeof(double));
+    std::vector<double*> ptrs;
+    for (long long k = 0; k < K; ++k)
+        for (size_t q = 0; q < map.size(); ++q) ptrs.push_back(bufs[q].as<double>() + k * dom_[map[q]].cells());
+    for (int i0 = 0; i0 < L.cn; i0 += (int)K)
+    {
+        const int cnt = (int)std::min<long long>(K, L.cn - i0);
+        for (size_t q = 0; q < map.size(); ++q)
+            FPB_CUDA(cudaMemsetAsync(bufs[q].get(), 0, bufs[q].bytes(), s));
+        k_impulses<double><<<grid_for(cnt, 128), 128, 0, s>>>(bufs[0].as<double>(), C.nx, C.ny, face, i0, cnt);
+        FPB_CHECK_LAUNCH();
+        b->solve(ptrs.data(), nullptr, 0, s);
+        k_impulse_extract<double><<<grid_for((long long)cnt * L.cn, 256), 256, 0, s>>>(
+            bufs[0].as<double>(), C.nx, C.ny, face, L.S.as<double>(), L.cn, i0, cnt);
+        FPB_CHECK_LAUNCH();
+    }
+    // the batched solve scales its right-hand side by hx^2 (the reference's assembly); the Schur matrix is
+    // the response to the unscaled impulse
+    k_scale<<<grid_for((long long)L.cn * L.cn, 256), 256, 0, s>>>(L.S.as<double>(), 1.0 / (C.hx * C.hx),
+                                                                   (long long)L.cn * L.cn);
+    FPB_CHECK_LAUNCH();
+    FPB_CUDA(cudaStreamSynchronize(s));
+    return true;
+}
+
 void Composite::build_schur()
 {
     cudaStream_t s = 0;
@@ -635,6 +695,7 @@ void Composite::build_schur()
                 const long long cells = C.cells();
                 L.S.alloc((size_t)L.cn * L.cn * sizeof(double));
                 const bool leaf = node_[c].kids.empty();
+                if (!leaf && mode_ != GMRES_FULLFIELD && schur_by_spectral(L, s)) continue;
                 long long  nb   = leaf ? std::max(1LL, std::min<long long>(L.cn, (512LL << 20) / (cells * 8))) : 1;
                 DevBuf     work((size_t)nb * cells * sizeof(double));
                 for (int i0 = 0; i0 < L.cn; i0 += (int)nb)

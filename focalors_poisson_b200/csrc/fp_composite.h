@@ -95,6 +95,7 @@ private:
     };
 
     void build_schur();
+    bool schur_by_spectral(Link& L, cudaStream_t s);
     void ensure_built();
     bool built_ = false;
     void assemble(double* const* fields, const double* const* ghosts, cudaStream_t s);

@@ -142,6 +142,19 @@ def tree9(n: int, h: float | None = None) -> Geometry:
                     ["C", "W", "E", "S", "N", "NW", "NE", "SW", "SE"])
 
 
+def tree9_large(n: int = 4096) -> Geometry:
+    """The large composite workload: the 9-subdomain tree of tree9 (n x n cells each, h = 1/n), arms W and E
+    periodic in y, Neumann on the x faces of the W / E arm tips and of the four corners' outer x faces,
+    Dirichlet on every other outer face. (No y-face Neumann: a quarter-wave y-transform of 4096 rows does
+    not fit one CTA's shared memory in FP64.)"""
+    g = tree9(n)
+    g.bc[3][YNEG] = DIRICHLET
+    g.bc[4][YPOS] = DIRICHLET
+    for c, face in ((5, XNEG), (6, XPOS), (7, XNEG), (8, XPOS)):
+        g.bc[c][face] = NEUMANN
+    return g
+
+
 def gaussian_bumps_rhs(g: Geometry, seed: int, n_bumps: int = 32) -> list:
     """Sum of seeded Gaussian bumps over the geometry's bounding box: centres uniform, widths U(0.01,0.05)
     times the box size, amplitudes N(0,1)."""
