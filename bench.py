@@ -325,6 +325,65 @@ def batched_section(args, dev, rank):
 
 
 # ------------------------------------------------------------------------------------------------
+# Large composite: 9 subdomains of 4096^2 in a depth-2 tree, periodic arms (--large; setup ~2.5 min)
+# ------------------------------------------------------------------------------------------------
+def large_section(args, dev):
+    """Forward solves (FP64, FP32 + FP64 refinement) and the adjoint solve of the 9 x 4096^2 tree with
+    periodic W / E arms; each step refills the RHS from a resident copy. Setup (Schur matrices, interface
+    inverses) is timed separately."""
+    import torch
+
+    from focalors_poisson_b200 import capi
+    from focalors_poisson_b200 import workloads as W
+
+    g = W.tree9_large(4096)
+    pristine = W.gaussian_bumps_rhs(g, SEED, device=dev)
+    work = [torch.empty_like(p) for p in pristine]
+    out = {"workload": "tree of 9 x 4096^2 (centre, 4 arms, 4 corners on the y-arms), W / E arms periodic in y, "
+                       "Neumann arm-tip and corner x faces, Dirichlet elsewhere, sum of 32 Gaussian bumps "
+                       f"(seed {SEED}); GMRES(20, 1e-12, 100)", "cells": sum(int(p.numel()) for p in pristine)}
+    t0 = time.perf_counter()
+    c = capi.Composite(g, 20, 1e-12, 100)
+    for w, p in zip(work, pristine):
+        w.copy_(p)
+    c.solve(work)  # builds the Schur matrices and interface inverses on first use
+    torch.cuda.synchronize()
+    out["setup_s"] = time.perf_counter() - t0
+
+    def timed(fn):
+        for _ in range(2):
+            for w, p in zip(work, pristine):
+                w.copy_(p)
+            info = fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 3
+        e0.record()
+        for _ in range(reps):
+            for w, p in zip(work, pristine):
+                w.copy_(p)
+            info = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, info
+
+    ms, info = timed(lambda: c.solve(work))
+    u64 = [w.clone() for w in work]
+    out["f64"] = {"solves_per_s": 1e3 / ms, "ms": ms, "rel_residual": c.residual(u64, pristine),
+                  "gmres_iterations": info["iterations"]}
+    ms, info = timed(lambda: c.solve_ir(work, rel_tol=1e-11, max_refine=10))
+    num = sum(float(((a - b) ** 2).sum()) for a, b in zip(work, u64))
+    den = sum(float((b ** 2).sum()) for b in work)
+    out["f32ir"] = {"solves_per_s": 1e3 / ms, "ms": ms, "rel_residual": c.residual(work, pristine),
+                    "refinements": info["refinements"], "rel_l2_vs_f64": (num / den) ** 0.5}
+    ms, info = timed(lambda: c.adjoint(work))
+    out["adjoint_f64"] = {"solves_per_s": 1e3 / ms, "ms": ms}
+    del c, work, pristine, u64
+    torch.cuda.empty_cache()
+    return out
+
+
+# ------------------------------------------------------------------------------------------------
 # GPU arm
 # ------------------------------------------------------------------------------------------------
 def main():
@@ -335,6 +394,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-uneven section")
+    ap.add_argument("--large", action="store_true", help="add the 9 x 4096^2 tree section (setup ~2.5 min)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -496,6 +556,8 @@ def main():
         del solver, pristine, work
         torch.cuda.empty_cache()
         line["batched_uneven"] = batched_section(args, dev, rank)
+    if args.large and world == 1:
+        line["large_tree"] = large_section(args, dev)
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

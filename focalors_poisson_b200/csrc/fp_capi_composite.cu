@@ -204,8 +204,17 @@ int fp_composite_adjoint_f64(fp_composite* c, double* const* fields, int flags, 
     GmresInfo gi;
     int       rc = guarded([&] {
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        with_device_fields(c, fields, nullptr, flags, s,
-                           [&](double* const* f, const double* const*) { c->c->solve_adjoint(f, s, &gi); });
+        with_device_fields(c, fields, nullptr, flags, s, [&](double* const* f, const double* const*) {
+            if (c->sp64)  // H A^-1 g = H * (spectral solve of H^-1 g, which scales by H again)
+            {
+                c->c->require_nonsingular();
+                c->c->scale_fields(f, false, s);
+                c->sp64->solve(f, nullptr, 0, s);
+                c->c->scale_fields(f, true, s);
+            }
+            else
+                c->c->solve_adjoint(f, s, &gi);
+        });
         if ((flags & FP_CHECK_CONVERGENCE) && !gi.converged)
             throw Error(FP_ERR_NOT_CONVERGED, "GMRES stopped at max_iter above tol (residual " +
                                                   std::to_string(gi.residual) + ")");
@@ -224,7 +233,21 @@ int fp_composite_adjoint_f32ir(fp_composite* c, double* const* fields, int flags
         if (!(rel_tol > 0) || max_refine < 1) throw Error(FP_ERR_INVALID, "rel_tol must be > 0 and max_refine >= 1");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         with_device_fields(c, fields, nullptr, flags, s, [&](double* const* f, const double* const*) {
-            steps = c->c->solve_adjoint_ir(f, s, rel_tol, max_refine, &change, &gi, (flags & FP_IR_INNER_F64) == 0);
+            const bool f32 = (flags & FP_IR_INNER_F64) == 0;
+            if (c->sp64)
+            {
+                c->c->require_nonsingular();
+                if (f32 && !c->sp32)
+                {
+                    c->sp32 = make_batch({c->desc}, 1);
+                    c->sp32->autotune(s);
+                }
+                c->c->scale_fields(f, false, s);
+                steps = (f32 ? c->sp32 : c->sp64)->refine(f, nullptr, rel_tol, max_refine, s, &change);
+                c->c->scale_fields(f, true, s);
+            }
+            else
+                steps = c->c->solve_adjoint_ir(f, s, rel_tol, max_refine, &change, &gi, f32);
         });
         if ((flags & FP_CHECK_CONVERGENCE) && steps >= max_refine && !(change <= rel_tol))
             throw Error(FP_ERR_NOT_CONVERGED, "iterative refinement stopped at max_refine (relative change " +

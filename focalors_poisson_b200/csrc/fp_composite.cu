@@ -865,12 +865,34 @@ void Composite::scale_by_h2(double* const* fields, cudaStream_t s)
     }
 }
 
+// The elimination's GMRES tolerance is absolute and sized for the hx^2-scaled right-hand sides of a forward
+// solve, so the unscaled input is brought to that scale first (c = hx^2 of the root) and the result back.
 void Composite::solve_adjoint(double* const* fields, cudaStream_t s, GmresInfo* info)
 {
     require_nonsingular();
-    mixed_ = false;
+    mixed_         = false;
+    const double c = dom_[tree_.root].hx * dom_[tree_.root].hx;
+    for (size_t d = 0; d < dom_.size(); ++d)
+    {
+        k_scale<<<grid_for(dom_[d].cells(), 256), 256, 0, s>>>(fields[d], c, dom_[d].cells());
+        FPB_CHECK_LAUNCH();
+    }
     eliminate(fields, s, info);
-    scale_by_h2(fields, s);
+    for (size_t d = 0; d < dom_.size(); ++d)
+    {
+        k_scale<<<grid_for(dom_[d].cells(), 256), 256, 0, s>>>(fields[d], dom_[d].hx * dom_[d].hx / c, dom_[d].cells());
+        FPB_CHECK_LAUNCH();
+    }
+}
+
+void Composite::scale_fields(double* const* fields, bool by_h2, cudaStream_t s)
+{
+    for (size_t d = 0; d < dom_.size(); ++d)
+    {
+        const double h2 = dom_[d].hx * dom_[d].hx;
+        k_scale<<<grid_for(dom_[d].cells(), 256), 256, 0, s>>>(fields[d], by_h2 ? h2 : 1.0 / h2, dom_[d].cells());
+        FPB_CHECK_LAUNCH();
+    }
 }
 
 int Composite::solve_adjoint_ir(double* const* fields, cudaStream_t s, double rel_tol, int max_refine,

@@ -71,6 +71,9 @@ public:
     // The same by iterative refinement (FP32 or FP64 inner solves, FP64 residual), as solve_ir.
     int solve_adjoint_ir(double* const* fields, cudaStream_t s, double rel_tol, int max_refine, double* rel_change,
                          GmresInfo* info, bool inner_fp32 = true);
+    // fields *= hx^2 (by_h2) or /= hx^2, per domain
+    void scale_fields(double* const* fields, bool by_h2, cudaStream_t s);
+    void require_nonsingular() const;
     // |fs - A u| / |fs| over all cells, fs = the assembled, hx^2-scaled right-hand side of (rhs, ghosts).
     // rhs is not modified (a copy is assembled).
     double residual_norm(const double* const* u, const double* const* rhs, const double* const* ghosts, cudaStream_t s);
@@ -105,7 +108,6 @@ private:
     void ensure_ir_workspace();
     int  refine(double* const* fields, cudaStream_t s, double rel_tol, int max_refine, double* rel_change,
                 GmresInfo* info, bool inner_fp32);  // fields: assembled, scaled RHS in, solution out
-    void require_nonsingular() const;
     void scale_by_h2(double* const* fields, cudaStream_t s);
     void build_interface_inverse(int d);
     bool refine_with_inverse(int d, double* f, cudaStream_t s, GmresInfo* info);

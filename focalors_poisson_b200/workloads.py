@@ -155,7 +155,7 @@ def tree9_large(n: int = 4096) -> Geometry:
     return g
 
 
-def gaussian_bumps_rhs(g: Geometry, seed: int, n_bumps: int = 32) -> list:
+def gaussian_bumps_rhs(g: Geometry, seed: int, n_bumps: int = 32, device=None) -> list:
     """Sum of seeded Gaussian bumps over the geometry's bounding box: centres uniform, widths U(0.01,0.05)
     times the box size, amplitudes N(0,1)."""
     rng = np.random.default_rng(seed)
@@ -168,6 +168,20 @@ def gaussian_bumps_rhs(g: Geometry, seed: int, n_bumps: int = 32) -> list:
     cy = rng.uniform(y0, y1, n_bumps)
     w = rng.uniform(0.01, 0.05, n_bumps) * size
     amp = rng.standard_normal(n_bumps)
+    if device is not None:  # the same sum evaluated on a torch device (large fields)
+        import torch
+
+        out = []
+        for i in range(g.n_domains):
+            xs = torch.tensor(g.offsets[i][0] + (np.arange(g.nx[i]) + 0.5) * g.hx[i], device=device)
+            ys = torch.tensor(g.offsets[i][1] + (np.arange(g.ny[i]) + 0.5) * g.hy[i], device=device)
+            f = torch.zeros(g.nx[i], g.ny[i], dtype=torch.float64, device=device)
+            for k in range(n_bumps):
+                ex = torch.exp(-((xs - cx[k]) ** 2) / (2.0 * w[k] ** 2))
+                ey = torch.exp(-((ys - cy[k]) ** 2) / (2.0 * w[k] ** 2))
+                f += amp[k] * torch.outer(ex, ey)
+            out.append(f)
+        return out
     out = []
     for i in range(g.n_domains):
         X, Y = g.centres(i)
