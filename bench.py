@@ -35,6 +35,9 @@ N_CELLS = 2048
 GMRES = (20, 1e-14, 100)
 SEED = 2024
 IR_REL_TOL = 1e-11
+# DRAM bytes of one k_transform<double, DD> launch on 2048 x 2048 (ncu capture summarised in
+# profiles/k_transform_DD_2048x2048_f64.md): the input is read once, the output stays in L2
+DD_TRAFFIC_BYTES = 33.769472e6 + 6.144e3
 INNER = {"f64ir": "f64", "f32ir": "f32", "mixedir": "mixed"}
 
 
@@ -525,7 +528,9 @@ def main():
     achieved = bytes_launch / t_kernel / 1e9
     roofline = {"kernel": "k_transform<double, DD> (2048x2048 rows, in place)", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": f"{peak_kind} hbm_gbs", "traffic": None,
+                "peak_source": f"{peak_kind} hbm_gbs", "traffic": DD_TRAFFIC_BYTES,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                                  "(profiles/k_transform_DD_2048x2048_f64.md)",
                 "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": t_kernel * 1e3}
 
     forms = {}
