@@ -93,6 +93,8 @@ template <typename T> struct ChaseTabDev
     const T* cends;
     const T* dsep;
     int      end_neu;  // x+ face Neumann: last separator diagonal d + 1 (x- Neumann is in the type-0 tables)
+    const T* scp;      // separator Thomas factors c_p [p][j] (rows not last)
+    const T* sid;      // 1 / den_p [p][j]
 };
 
 template <typename T> struct ChaseSeg
@@ -186,8 +188,8 @@ __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __rest
     ze[ny] = y[Li - 1];
 }
 
-// Separator system per subdomain and wavenumber (see k_chase_reduced): loop-invariant table entries
-// hoisted, the per-chunk loads issued ahead of the recurrence.
+// Separator system per subdomain and wavenumber (see k_chase_reduced): tabulated Thomas factors for every
+// row but the last, right-hand sides (with modifiers) loaded ahead of the recurrence.
 template <typename T>
 __global__ void k_b_chase_reduced(const ChaseSeg<T>* __restrict__ segs, const long long* __restrict__ prefix,
                                   int nseg, const ChaseTabDev<T>* __restrict__ tabs)
@@ -203,19 +205,15 @@ __global__ void k_b_chase_reduced(const ChaseSeg<T>* __restrict__ segs, const lo
     const int            nrow = sg->nrow, ncol = sg->ncol;
     ModCtx<T>            mc;
     mod_init(sg, ncol, j, mc);
-    const T d    = tb.dsep[j];
-    const T e0_3 = tb.cends[(0 * 4 + 3) * (long long)ny + j];
-    const T e1_0 = tb.cends[(1 * 4 + 0) * (long long)ny + j], e1_1 = tb.cends[(1 * 4 + 1) * (long long)ny + j];
-    const T e1_2 = tb.cends[(1 * 4 + 2) * (long long)ny + j], e1_3 = tb.cends[(1 * 4 + 3) * (long long)ny + j];
-    const T* ze  = sg->zend + j;
-    T*       cw  = sg->work + j;
-    T*       bs  = sg->bsep + j;
-    const T* in  = sg->in;
-    T*       out = sg->out;
-    T        yprev = 0, cprev = 0;
+    const T  e1_1 = tb.cends[(1 * 4 + 1) * (long long)ny + j];
+    const T* ze   = sg->zend + j;
+    T*       bs   = sg->bsep + j;
+    const T* in   = sg->in;
+    T*       out  = sg->out;
+    T        yprev = 0;
     for (int p0 = 0; p0 < P; p0 += kAhead)
     {
-        T rhs_v[kAhead];
+        T rhs_v[kAhead], id_v[kAhead];
 #pragma unroll
         for (int q = 0; q < kAhead; ++q)
         {
@@ -226,6 +224,7 @@ __global__ void k_b_chase_reduced(const ChaseSeg<T>* __restrict__ segs, const lo
                 T r = mod_rhs(sg, nrow, ncol, mc, isep, j, in[(long long)isep * ny + j]) - ze[(long long)(2 * p + 1) * ny];
                 if (p < P - 1) r -= ze[(long long)(2 * (p + 1)) * ny];
                 rhs_v[q] = r;
+                id_v[q]  = p < P - 1 ? tb.sid[(long long)p * ny + j] : (T)0;
             }
         }
 #pragma unroll
@@ -233,26 +232,43 @@ __global__ void k_b_chase_reduced(const ChaseSeg<T>* __restrict__ segs, const lo
         {
             const int p = p0 + q;
             if (p >= P) break;
-            const bool last  = p == P - 1;
-            const T    lower = p > 0 ? -e1_1 : (T)0;
-            T          diag  = (last && tb.end_neu ? d + (T)1 : d) - (p == 0 ? e0_3 : e1_3);
-            if (!last) diag -= e1_0;
-            const T den = diag - lower * cprev;
-            const T up  = last ? (T)0 : -e1_2;
-            const T cp  = up / den;
-            yprev       = (rhs_v[q] - lower * yprev) / den;
-            cw[(long long)p * ny] = cp;
+            const T lower = p > 0 ? -e1_1 : (T)0;
+            T       inv   = id_v[q];
+            if (p == P - 1)  // last row: no next chunk, x+ Neumann end
+            {
+                const T diag = (tb.end_neu ? tb.dsep[j] + (T)1 : tb.dsep[j]) -
+                               (p == 0 ? tb.cends[(0 * 4 + 3) * (long long)ny + j] : tb.cends[(1 * 4 + 3) * (long long)ny + j]);
+                inv = (T)1 / (diag - lower * (p > 0 ? tb.scp[(long long)(p - 1) * ny + j] : (T)0));
+            }
+            yprev                 = (rhs_v[q] - lower * yprev) * inv;
             bs[(long long)p * ny] = yprev;
-            cprev                 = cp;
         }
     }
+    // back substitution, its loads issued ahead in groups as well
     T x = bs[(long long)(P - 1) * ny];
     out[(long long)(nx - 1) * ny + j] = x;
-    for (int p = P - 2; p >= 0; --p)
+    for (int p1 = P - 2; p1 >= 0; p1 -= kAhead)
     {
-        x                                                  = bs[(long long)p * ny] - cw[(long long)p * ny] * x;
-        bs[(long long)p * ny]                              = x;
-        out[(long long)(p * kChunk + kChunk - 1) * ny + j] = x;
+        T yv[kAhead], cv[kAhead];
+#pragma unroll
+        for (int q = 0; q < kAhead; ++q)
+        {
+            const int p = p1 - q;
+            if (p >= 0)
+            {
+                yv[q] = bs[(long long)p * ny];
+                cv[q] = tb.scp[(long long)p * ny + j];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kAhead; ++q)
+        {
+            const int p = p1 - q;
+            if (p < 0) break;
+            x                     = yv[q] - cv[q] * x;
+            bs[(long long)p * ny] = x;  // the correction pass reads the separator solution
+            out[(long long)(p * kChunk + kChunk - 1) * ny + j] = x;
+        }
     }
 }
 
@@ -1067,6 +1083,19 @@ template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDe
         }
         prob_.push_back(std::move(pr));
     }
+    // separator-factor rows each shared table needs: the largest P of the subdomains using it
+    std::map<std::pair<int, double>, int> rows_needed;
+    auto table_key = [](const Dom& D) {
+        int bcd[4];
+        for (int f = 0; f < 4; ++f) bcd[f] = D.d.bc[f] == BC_ADJACENTED ? BC_DIRICHLET : D.d.bc[f];
+        const int sig = bcd[0] + 4 * bcd[1] + 16 * bcd[2] + 64 * bcd[3];
+        return std::make_pair(D.d.ny * 256 + sig, D.d.hx * D.d.hx / D.d.hy / D.d.hy);
+    };
+    for (auto& D : dom_)
+    {
+        int& r = rows_needed[table_key(D)];
+        r      = std::max(r, D.d.nx / kChunk);
+    }
     for (auto& D : dom_)
     {
         D.plan = plans_.get(D.kind, D.d.ny);
@@ -1079,7 +1108,7 @@ template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDe
         auto         it  = tab_index_.find(key);
         if (it == tab_index_.end())
         {
-            tabs_.emplace_back(new DevRect<TS>(2 * kChunk, D.d.ny, D.d.hx, D.d.hy, bcd));
+            tabs_.emplace_back(new DevRect<TS>(2 * kChunk, D.d.ny, D.d.hx, D.d.hy, bcd, rows_needed[key]));
             it = tab_index_.emplace(key, (int)tabs_.size() - 1).first;
         }
         D.tab = it->second;
@@ -1088,7 +1117,8 @@ template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDe
     std::vector<ChaseTabDev<TS>> tv;
     for (auto& t : tabs_)
         tv.push_back({t->cc.template as<TS>(), t->cg.template as<TS>(), t->chh.template as<TS>(),
-                      t->cends.template as<TS>(), t->dsep.template as<TS>(), t->end_neumann ? 1 : 0});
+                      t->cends.template as<TS>(), t->dsep.template as<TS>(), t->end_neumann ? 1 : 0,
+                      t->sep_cp.template as<TS>(), t->sep_iden.template as<TS>()});
     tabs_dev_ = upload(tv);
     W_.alloc((size_t)cells_ * sizeof(TS));
     X_.alloc((size_t)cells_ * sizeof(TS));

@@ -164,12 +164,15 @@ __global__ void __launch_bounds__(256) k_chase_local(T* __restrict__ f, int nx, 
 }
 
 // Separator system per (field, wavenumber). ends: [type][4][j] = g_first, g_last, h_first, h_last.
-// The table entries are loop-invariant (chunk type 1 for every chunk after the first) and the per-chunk
-// loads do not depend on the recurrence, so they are issued ahead of it in groups of kAhead.
+// Its matrix depends on the wavenumber only, so the Thomas factors of every row but the last are tabulated
+// (scp: c_p, sid: 1 / den_p; see separator_factors); per solve the recurrence is y_p = (rhs_p - lower y_{p-1})
+// sid_p and x_p = y_p - c_p x_{p+1}, its loads issued ahead in groups of kAhead. The last row (which
+// depends on P and the x+ Neumann end) is formed here from c_{P-2}.
 template <typename T>
 __global__ void k_chase_reduced(T* __restrict__ f, int nx, int ny, long long batch, const T* __restrict__ ends,
                                 const T* __restrict__ dsep, int end_neumann, const T* __restrict__ zend,
-                                T* __restrict__ bsep, T* __restrict__ work, int skip_last)
+                                T* __restrict__ bsep, const T* __restrict__ scp, const T* __restrict__ sid,
+                                int skip_last)
 {
     constexpr int   kAhead = 8;
     const long long t      = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -178,18 +181,14 @@ __global__ void k_chase_reduced(T* __restrict__ f, int nx, int ny, long long bat
     if (skip_last && j == ny - 1) return;
     const long long b = t / ny;
     const int       P = nx / kChunk;
-    const T         d = dsep[j];
-    const T  e0_3 = ends[(0 * 4 + 3) * (long long)ny + j];
-    const T  e1_0 = ends[(1 * 4 + 0) * (long long)ny + j], e1_1 = ends[(1 * 4 + 1) * (long long)ny + j];
-    const T  e1_2 = ends[(1 * 4 + 2) * (long long)ny + j], e1_3 = ends[(1 * 4 + 3) * (long long)ny + j];
-    const T* ze = zend + b * (long long)P * 2 * ny + j;
-    T*       cw = work + b * (long long)P * ny + j;  // Thomas factors of the separator system
-    T*       bs = bsep + b * (long long)P * ny + j;  // right-hand sides, then the solution B_p
-    T*       fb = f + b * (long long)nx * ny + j;
-    T        yprev = 0, cprev = 0;
+    const T  e1_1 = ends[(1 * 4 + 1) * (long long)ny + j];
+    const T* ze   = zend + b * (long long)P * 2 * ny + j;
+    T*       bs   = bsep + b * (long long)P * ny + j;  // forward values y_p, then the solution B_p
+    T*       fb   = f + b * (long long)nx * ny + j;
+    T        yprev = 0;
     for (int p0 = 0; p0 < P; p0 += kAhead)
     {
-        T rhs_v[kAhead];
+        T rhs_v[kAhead], id_v[kAhead];
 #pragma unroll
         for (int q = 0; q < kAhead; ++q)
         {
@@ -199,6 +198,7 @@ __global__ void k_chase_reduced(T* __restrict__ f, int nx, int ny, long long bat
                 T r = fb[(long long)(p * kChunk + kChunk - 1) * ny] - ze[(long long)(2 * p + 1) * ny];
                 if (p < P - 1) r -= ze[(long long)(2 * (p + 1)) * ny];
                 rhs_v[q] = r;
+                id_v[q]  = p < P - 1 ? sid[(long long)p * ny + j] : (T)0;
             }
         }
 #pragma unroll
@@ -206,26 +206,43 @@ __global__ void k_chase_reduced(T* __restrict__ f, int nx, int ny, long long bat
         {
             const int p = p0 + q;
             if (p >= P) break;
-            const bool last  = p == P - 1;
-            const T    lower = p > 0 ? -e1_1 : (T)0;
-            T          diag  = (last && end_neumann ? d + (T)1 : d) - (p == 0 ? e0_3 : e1_3);
-            if (!last) diag -= e1_0;
-            const T den = diag - lower * cprev;
-            const T up  = last ? (T)0 : -e1_2;
-            const T cp  = up / den;
-            yprev       = (rhs_v[q] - lower * yprev) / den;
-            cw[(long long)p * ny] = cp;
+            const T lower = p > 0 ? -e1_1 : (T)0;
+            T       inv   = id_v[q];
+            if (p == P - 1)  // last row: no next chunk, x+ Neumann end
+            {
+                const T diag = (end_neumann ? dsep[j] + (T)1 : dsep[j]) -
+                               (p == 0 ? ends[(0 * 4 + 3) * (long long)ny + j] : ends[(1 * 4 + 3) * (long long)ny + j]);
+                inv = (T)1 / (diag - lower * (p > 0 ? scp[(long long)(p - 1) * ny + j] : (T)0));
+            }
+            yprev                 = (rhs_v[q] - lower * yprev) * inv;
             bs[(long long)p * ny] = yprev;
-            cprev                 = cp;
         }
     }
+    // back substitution, its loads issued ahead in groups as well
     T x = bs[(long long)(P - 1) * ny];
     fb[(long long)(nx - 1) * ny] = x;
-    for (int p = P - 2; p >= 0; --p)
+    for (int p1 = P - 2; p1 >= 0; p1 -= kAhead)
     {
-        x                                            = bs[(long long)p * ny] - cw[(long long)p * ny] * x;
-        bs[(long long)p * ny]                        = x;
-        fb[(long long)(p * kChunk + kChunk - 1) * ny] = x;
+        T yv[kAhead], cv[kAhead];
+#pragma unroll
+        for (int q = 0; q < kAhead; ++q)
+        {
+            const int p = p1 - q;
+            if (p >= 0)
+            {
+                yv[q] = bs[(long long)p * ny];
+                cv[q] = scp[(long long)p * ny + j];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kAhead; ++q)
+        {
+            const int p = p1 - q;
+            if (p < 0) break;
+            x                     = yv[q] - cv[q] * x;
+            bs[(long long)p * ny] = x;  // the correction pass reads the separator solution
+            fb[(long long)(p * kChunk + kChunk - 1) * ny] = x;
+        }
     }
 }
 

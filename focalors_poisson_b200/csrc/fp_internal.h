@@ -162,9 +162,12 @@ template <typename T> struct DevRect
     bool                             chunked    = false;  // partition chase (nx a multiple of kChunk)
     bool                             end_neumann = false;
     DevBuf                           cc, cg, chh, cends, dsep;  // partition chase tables
+    DevBuf                           sep_cp, sep_iden;          // separator-system Thomas factors [p][j]
+    int                              sep_pmax = 0;              // rows of those tables
     mutable DevBuf                   scratch;                   // partition chase scratch (per batch)
 
-    DevRect(int nx, int ny, double hx, double hy, const int* bc);
+    // sep_rows: separator-factor rows to tabulate (default nx / 32; larger for tables shared by a batch)
+    DevRect(int nx, int ny, double hx, double hy, const int* bc, int sep_rows = 0);
     // In-place solve of `batch` back-to-back fields.
     void solve(T* f, long long batch, cudaStream_t s) const;
     // FP64 plans only: the same solve with FP32 transforms (FP64 rows in and out, FP64 chase); the

@@ -218,7 +218,32 @@ void partition_tables(int ny, const std::vector<double>& d, bool start_neu, std:
 }
 }  // namespace
 
-template <typename T> DevRect<T>::DevRect(int nx_, int ny_, double hx_, double hy_, const int* bc_)
+// Thomas factors of the separator system of the partition chase (fp_chase.cuh), which depend on the
+// wavenumber only: for rows p < pmax taken as not last, cp[p] = up / den_p and iden[p] = 1 / den_p with
+// den_p = diag_p - lower_p cp[p-1]; the last row of a given P is formed in the kernel from cp[P-2].
+void separator_factors(int ny, int pmax, const std::vector<double>& d, const std::vector<double>& ends,
+                       std::vector<double>& cp, std::vector<double>& iden)
+{
+    cp.assign((size_t)pmax * ny, 0.0);
+    iden.assign((size_t)pmax * ny, 0.0);
+    auto e = [&](int typ, int k, int j) { return ends[((size_t)typ * 4 + k) * ny + j]; };
+    for (int j = 0; j < ny; ++j)
+    {
+        double cprev = 0;
+        for (int p = 0; p < pmax; ++p)
+        {
+            const double lower = p > 0 ? -e(1, 1, j) : 0.0;
+            const double diag  = d[j] - (p == 0 ? e(0, 3, j) : e(1, 3, j)) - e(1, 0, j);
+            const double den   = diag - lower * cprev;
+            const double c     = -e(1, 2, j) / den;
+            cp[(size_t)p * ny + j]   = c;
+            iden[(size_t)p * ny + j] = 1.0 / den;
+            cprev                    = c;
+        }
+    }
+}
+
+template <typename T> DevRect<T>::DevRect(int nx_, int ny_, double hx_, double hy_, const int* bc_, int sep_rows)
     : nx(nx_), ny(ny_), hx(hx_), hy(hy_)
 {
     for (int f = 0; f < 4; ++f) bc[f] = bc_[f];
@@ -247,6 +272,11 @@ template <typename T> DevRect<T>::DevRect(int nx_, int ny_, double hx_, double h
         chh   = upload(convert<T>(ph));
         cends = upload(convert<T>(pe));
         dsep  = upload(convert<T>(d));
+        sep_pmax = std::max(sep_rows, nx / kChunk);
+        std::vector<double> scp, sid;
+        separator_factors(ny, sep_pmax, d, pe, scp, sid);
+        sep_cp   = upload(convert<T>(scp));
+        sep_iden = upload(convert<T>(sid));
     }
     if (periodic_x)
     {
@@ -285,7 +315,8 @@ template <typename T> void DevRect<T>::chase(T* f, long long batch, T* scr, cuda
     FPB_CHECK_LAUNCH();
     const long long nr = batch * ny;
     k_chase_reduced<T><<<(unsigned)((nr + 127) / 128), 128, 0, s>>>(f, nx, ny, batch, cends.as<T>(), dsep.as<T>(),
-                                                                   end_neumann ? 1 : 0, zend, bsep, work, skip);
+                                                                   end_neumann ? 1 : 0, zend, bsep,
+                                                                   sep_cp.as<T>(), sep_iden.as<T>(), skip);
     FPB_CHECK_LAUNCH();
     k_chase_correct<T><<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(f, nx, ny, batch, cg.as<T>(), chh.as<T>(), bsep,
                                                                    skip);
