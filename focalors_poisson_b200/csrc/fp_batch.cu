@@ -652,7 +652,8 @@ __global__ void k_myy(const BIface F, const double* H /* 2x2 blocks per m: H[(Y*
 // ---------------------------------------------------------------------------------------------
 // Elementwise over many subdomains
 // ---------------------------------------------------------------------------------------------
-constexpr int kAsmCells = 1024;  // cells per block of k_b_assemble
+constexpr int kAsmCells  = 1024;  // cells per block of k_b_assemble
+constexpr int kElemCells = 1024;  // cells per block of the residual, add-with-norms and copy kernels
 
 struct AsmSeg
 {
@@ -696,14 +697,16 @@ __global__ void __launch_bounds__(256) k_b_residual(const ResSeg* __restrict__ s
     __shared__ double sh[32];
     const int     s  = seg_of(prefix, nseg, blockIdx.x);
     const ResSeg* sg = segs + s;
-    const int     t  = (int)(blockIdx.x - prefix[s]) * blockDim.x + threadIdx.x;
+    const int     t0 = (int)(blockIdx.x - prefix[s]) * kElemCells;
+    const int     t1 = min(sg->a.nx * sg->a.ny, t0 + kElemCells);
     double        rr = 0, ff = 0;
-    if (t < sg->a.nx * sg->a.ny)
+    for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x)
     {
-        const double v = sg->fs[t] - composite_lap(sg->u, t, sg->a);
+        const double fs = sg->fs[t];
+        const double v  = fs - composite_lap(sg->u, t, sg->a);
         if (sg->r) sg->r[t] = v;
-        rr = v * v;
-        ff = sg->fs[t] * sg->fs[t];
+        rr += v * v;
+        ff += fs * fs;
     }
     if (sg->partial)
     {
@@ -733,15 +736,16 @@ __global__ void __launch_bounds__(256) k_b_add_norms(const AddSeg* __restrict__ 
     __shared__ double sh[32];
     const int     s  = seg_of(prefix, nseg, blockIdx.x);
     const AddSeg* sg = segs + s;
-    const long long t = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
+    const long long t0 = (blockIdx.x - prefix[s]) * (long long)kElemCells;
+    const long long t1 = t0 + kElemCells < sg->n ? t0 + kElemCells : sg->n;
     double        cc = 0, uu = 0;
-    if (t < sg->n)
+    for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x)
     {
         const double c = sg->c[t];
         const double u = first ? c : sg->u[t] + c;
         sg->u[t]       = u;
-        cc             = c * c;
-        uu             = u * u;
+        cc += c * c;
+        uu += u * u;
     }
     const double a = block_sum(cc, sh);
     __syncthreads();
@@ -761,10 +765,11 @@ struct CopySeg
 };
 __global__ void k_b_copy(const CopySeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg)
 {
-    const int     s  = seg_of(prefix, nseg, blockIdx.x);
-    const CopySeg sg = segs[s];
-    const long long t = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
-    if (t < sg.n) sg.dst[t] = sg.src[t];
+    const int      s  = seg_of(prefix, nseg, blockIdx.x);
+    const CopySeg* sg = segs + s;
+    const long long t0 = (blockIdx.x - prefix[s]) * (long long)kElemCells;
+    const long long t1 = t0 + kElemCells < sg->n ? t0 + kElemCells : sg->n;
+    for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) sg->dst[t] = sg->src[t];
 }
 
 }  // namespace fpb
@@ -1701,12 +1706,12 @@ void BatchImpl<TS>::set_user_lists(double* const* fields, const double* const* g
         std::vector<AddSeg>    ad;
         std::vector<long long> acn;
         long long              nb = 0;
-        for (size_t g = 0; g < dom_.size(); ++g) nb += (dom_[g].d.cells() + 255) / 256;
+        for (size_t g = 0; g < dom_.size(); ++g) nb += (dom_[g].d.cells() + kElemCells - 1) / kElemCells;
         addp_.alloc((size_t)2 * nb * 8);
         long long b0 = 0;
         for (size_t g = 0; g < dom_.size(); ++g)
         {
-            const long long blocks = (dom_[g].d.cells() + 255) / 256;
+            const long long blocks = (dom_[g].d.cells() + kElemCells - 1) / kElemCells;
             ad.push_back({u_.as<double>() + dom_[g].off, r_.as<double>() + dom_[g].off, dom_[g].d.cells(),
                           addp_.as<double>() + b0, addp_.as<double>() + nb + b0});
             acn.push_back(blocks);
@@ -1716,7 +1721,7 @@ void BatchImpl<TS>::set_user_lists(double* const* fields, const double* const* g
         std::vector<ResSeg>    rs;
         std::vector<long long> rc;
         for (size_t g = 0; g < dom_.size(); ++g) rs.push_back(res_seg(g, r_.as<double>(), fs_.as<double>(), nullptr));
-        for (auto& q : rs) rc.push_back((q.a.nx * (long long)q.a.ny + 255) / 256);
+        for (auto& q : rs) rc.push_back((q.a.nx * (long long)q.a.ny + kElemCells - 1) / kElemCells);
         res_.set(rs, rc);
     }
     std::vector<AsmSeg>    as;
@@ -1744,7 +1749,7 @@ void BatchImpl<TS>::set_user_lists(double* const* fields, const double* const* g
         di[g].in   = f[g];
         dout[g].out = f[g];
         cp.push_back({f[g], ir ? u_.as<double>() + dom_[g].off : nullptr, D.cells()});
-        cc.push_back((D.cells() + 255) / 256);
+        cc.push_back((D.cells() + kElemCells - 1) / kElemCells);
     }
     asm_user_.set(as, ac);
     dst_user_in_.set(di, dst_kinds_, plans_);
@@ -1963,7 +1968,7 @@ void BatchImpl<TS>::residuals(const double* const* u, const double* const* rhs, 
             q.a.ghost[k] = ghosts ? ghosts[4 * g + k] : nullptr;
         }
         as.push_back(q);
-        ac.push_back((D.cells() + 255) / 256);
+        ac.push_back((D.cells() + kElemCells - 1) / kElemCells);
         bo[g + 1] = bo[g] + ac.back();
     }
     std::vector<long long> acb;
