@@ -59,3 +59,32 @@ def test_library_exports_interface():
     for s in ("ConcatPoissonSolver2D5solve", "ConcatPoissonSolver2D13set_parameter", "PoissonSolver2D5solve",
               "Geometry2D7connect", "Variable2D16set_center_field"):
         assert s in syms, s
+
+
+REFERENCE = "/root/reference"
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE) or not os.path.exists(
+    os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "libfpref.so")),
+    reason="needs the reference sources and the oracle library built from them")
+def test_host_data_model_matches_reference(tmp_path):
+    """Geometry2D / Variable2D host bookkeeping (sizes propagated by connect, axis offsets, tree root,
+    boundary-type overrides, set_value at cell centres, set_buffer at ghost cells) prints identically
+    through the reference's own sources and through the drop-in layer."""
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = os.path.join(root, "tests", "cases", "variable_case.cpp")
+    ours = build.compile_driver(src, str(tmp_path / "ours"))
+    refexe = str(tmp_path / "ref")
+    lib = os.path.join(root, "oracle", "_ref")
+    cmd = ["g++", "-std=c++17", "-O2", "-fopenmp", "-w", "-I" + os.path.join(root, "oracle", "shim"), "-I" + REFERENCE,
+           "-include", os.path.join(REFERENCE, "base", "pch.h"), src, "-o", refexe, "-L" + lib, "-lfpref",
+           "-Wl,-rpath," + lib]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    a = subprocess.run([ours], capture_output=True, text=True, timeout=60)
+    b = subprocess.run([refexe], capture_output=True, text=True, timeout=60)
+    assert a.returncode == 0 and b.returncode == 0, (a.stdout[-500:], b.stdout[-500:])
+    assert a.stdout == b.stdout
+
