@@ -10,7 +10,7 @@
 //
 // A smooth length L is transformed by loading the input digit-reversed (a per-plan index table) and
 // running the DIT stages. A length with a prime factor above 7 goes through Bluestein's chirp-z
-// identity on a smooth length M >= 2L-1:  X_k = c_k * sum_n (x_n c_n) conj(c_{k-n}),
+// identity on a smooth length M >= 2L-2:  X_k = c_k * sum_n (x_n c_n) conj(c_{k-n}),
 // c_n = exp(-i pi n^2 / L): DIF of (x c), pointwise product with the (digit-reversed, 1/M-scaled)
 // transform of the chirp kernel, conjugate, DIT, conjugate, times c_k.
 //
@@ -41,6 +41,15 @@ struct FftDesc
     int      nst;
     FftStage st[kFftMaxStages];
 };
+
+// Shared-memory slot of FFT element i: one spare slot after every 8 elements. The butterflies of a
+// power-of-two stage touch elements at strides 1, 8, 64, ... (times the radix); unpadded, 8 threads of a
+// quarter warp (16-byte double2) or 16 of a half warp (8-byte float2) then hit one bank group, and the
+// stages of 4096- and 8192-point FFTs ran at an eighth of shared-memory bandwidth. With the spare slot
+// element i lands in bank group (i + i/8) mod 8 (mod 16 for float2), distinct across those threads.
+__host__ __device__ __forceinline__ int fft_slot(int i) { return i + (i >> 3); }
+// Slots an FFT buffer of executed length M occupies.
+__host__ __device__ __forceinline__ int fft_buf_elems(int M) { return M + ((M + 7) >> 3); }
 
 template <typename T2> struct FftTables
 {
@@ -163,10 +172,10 @@ __device__ __forceinline__ void stage_radix(T2* buf, const FftStage st, int nbf,
     {
         const int blk = t / st.S;
         const int b   = t - blk * st.S;
-        T2*       p   = buf + blk * st.B + b;
+        const int base = blk * st.B + b;
         T2        x[R];
 #pragma unroll
-        for (int q = 0; q < R; ++q) x[q] = p[q * st.S];
+        for (int q = 0; q < R; ++q) x[q] = buf[fft_slot(base + q * st.S)];
         const bool rot = b != 0;
         T2         w1  = rot ? __ldg(tw + st.tw_off + b) : mk<T2>(1, 0);
         if (DIT && rot)
@@ -191,7 +200,7 @@ __device__ __forceinline__ void stage_radix(T2* buf, const FftStage st, int nbf,
             }
         }
 #pragma unroll
-        for (int q = 0; q < R; ++q) p[q * st.S] = x[q];
+        for (int q = 0; q < R; ++q) buf[fft_slot(base + q * st.S)] = x[q];
     }
 }
 
@@ -226,7 +235,7 @@ __device__ void fft_stages(T2* buf, const FftDesc& d, const T2* __restrict__ tw,
 // Slot in buf where input element n (n < M) must be stored before fft_execute.
 template <typename T2> __device__ __forceinline__ int fft_in_slot(const FftDesc& d, const FftTables<T2>& t, int n)
 {
-    return d.blue ? n : __ldg(t.perm + n);
+    return fft_slot(d.blue ? n : __ldg(t.perm + n));
 }
 // Scale applied to input n before storing (Bluestein pre-chirp); zero past L.
 template <typename T2> __device__ __forceinline__ T2 fft_in_value(const FftDesc& d, const FftTables<T2>& t, int n, T2 z)
@@ -247,7 +256,11 @@ template <typename T2> __device__ void fft_execute(T2* buf, const FftDesc& d, co
         return;
     }
     fft_stages<false>(buf, d, t.tw, t.stages);
-    for (int k = threadIdx.x; k < d.M; k += blockDim.x) buf[k] = cconj(cmul(buf[k], __ldg(t.bhat + k)));
+    for (int k = threadIdx.x; k < d.M; k += blockDim.x)
+    {
+        const int sl = fft_slot(k);
+        buf[sl]      = cconj(cmul(buf[sl], __ldg(t.bhat + k)));
+    }
     __syncthreads();
     fft_stages<true>(buf, d, t.tw, t.stages);
 }
@@ -255,8 +268,8 @@ template <typename T2> __device__ void fft_execute(T2* buf, const FftDesc& d, co
 // Spectrum value X_k, 0 <= k < L, after fft_execute.
 template <typename T2> __device__ __forceinline__ T2 fft_out(const T2* buf, const FftDesc& d, const FftTables<T2>& t, int k)
 {
-    if (!d.blue) return buf[k];
-    return cmul(cconj(buf[k]), __ldg(t.chirp + k));
+    if (!d.blue) return buf[fft_slot(k)];
+    return cmul(cconj(buf[fft_slot(k)]), __ldg(t.chirp + k));
 }
 
 }  // namespace fpb

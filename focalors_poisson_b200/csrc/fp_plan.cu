@@ -150,10 +150,13 @@ HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit)
     }
     else
     {
-        // Smallest-cost 7-smooth M >= 2L-1.
+        // Smallest-cost 7-smooth M >= 2L-2. The chirp kernel is even (b_{-k} = b_k), so the one slot
+        // that lags L-1 and -(L-1) share when M = 2L-2 receives the same value from both and the cyclic
+        // convolution still equals the linear one on outputs 0..L-1. For L = 2^k + 1 (DST-I of a
+        // power-of-two row) and L = 2^(k+1) + 1 (the quarter-wave families) M is then a power of two.
         int    best = -1;
         double best_cost = 1e300;
-        for (int M = 2 * L - 1; M <= 3 * L; ++M)
+        for (int M = 2 * L - 2; M <= 3 * L; ++M)
         {
             std::vector<int> r = radices(M);
             if (r.empty()) continue;
@@ -180,9 +183,9 @@ HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit)
         h.bhat.resize(best);
         for (int p = 0; p < best; ++p) h.bhat[p] = b[idx[p]] / (long double)best;
     }
-    if ((size_t)h.d.M * elem_bytes > smem_limit)
+    if ((size_t)fft_buf_elems(h.d.M) * elem_bytes > smem_limit)
         throw std::runtime_error("transform length " + std::to_string(L) + " needs " +
-                                 std::to_string((size_t)h.d.M * elem_bytes) +
+                                 std::to_string((size_t)fft_buf_elems(h.d.M) * elem_bytes) +
                                  " bytes of shared memory, more than this build supports");
     return h;
 }

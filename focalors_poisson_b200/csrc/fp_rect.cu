@@ -91,8 +91,9 @@ template <typename T> DevTransform<T>::DevTransform(int kind_, int n_) : kind(ki
     s1      = (T)kt.s1;
     s2      = (T)kt.s2;
     threads = std::min(512, std::max(64, ((fd.M / 16 + 31) / 32) * 32));
-    const int K_scan = (n + 1) / 2;  // DD prefix-sum arrays: 2K values, in the Bluestein tail when it fits
-    smem = (size_t)fd.M * sizeof(T2) + ((kind == K_DD && fd.M - fd.L < K_scan) ? (size_t)2 * K_scan * sizeof(T) : 0);
+    const int K_scan = (n + 1) / 2;  // DD prefix-sum arrays: 2K values, in the buffer's tail when it fits
+    const int E      = fft_buf_elems(fd.M);
+    smem = (size_t)E * sizeof(T2) + ((kind == K_DD && E - fft_slot(fd.L) < K_scan) ? (size_t)2 * K_scan * sizeof(T) : 0);
     if (smem > max_dynamic_smem()) throw Error(3, "transform of length " + std::to_string(n) + " needs more shared memory than a CTA has");
 }
 

@@ -235,8 +235,9 @@ __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN*
     {
         // DD: X_{2k} = -Im Y_k (k >= 1), X_{2k+1} = Re Y_0 / 2 + sum_{q=1..k} Re Y_q; out_m = s1 X_{m+1}
         const int K  = (n + 1) / 2;  // odd outputs X_1, X_3, ...
-        // scan arrays: the unused tail [L, M) of a Bluestein buffer when it is long enough, else past M
-        T*        ca = reinterpret_cast<T*>(buf + ((a.fd.M - L >= K) ? L : a.fd.M));
+        // scan arrays: the slots past element L-1 when the buffer has K of them, else past the buffer
+        const int lo = fft_slot(L), hi = fft_buf_elems(a.fd.M);
+        T*        ca = reinterpret_cast<T*>(buf + ((hi - lo >= K) ? lo : hi));
         T*        cb = ca + K;
         for (int k = threadIdx.x; k <= n / 2; k += blockDim.x)
         {
