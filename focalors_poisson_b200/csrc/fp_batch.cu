@@ -51,7 +51,8 @@ struct DstSeg
 };
 
 // One work item = the rows one FFT carries (two for the pairing families) of one segment.
-// ACC: out (FP64) += result instead of out = result.
+// ACC: out (FP64) += result instead of out = result. plans: two argument sets per plan (forward, inverse).
+// DD and DN run their inverse with INV = 0 and the forward arguments (they are their own transposes).
 template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC>
 __global__ void __launch_bounds__(512) k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix,
                                                  int nseg, long long nitems, const XformArgs<T>* __restrict__ plans)
@@ -65,7 +66,7 @@ __global__ void __launch_bounds__(512) k_b_xform(const DstSeg* __restrict__ segs
     {
         const int           s  = seg_of(prefix, nseg, it);
         const DstSeg&       sg = segs[s];
-        const XformArgs<T>& P  = plans[sg.plan];
+        const XformArgs<T>& P  = plans[2 * sg.plan + INV];
         const int           n  = P.n;
         const long long     r0 = kPair ? 2 * (it - prefix[s]) : (it - prefix[s]);
         const bool          has_b = kPair && r0 + 1 < sg.rows;
@@ -827,23 +828,14 @@ template <typename T> struct PlanSet  // transform plans by (family, row length)
         smem = std::max(smem, tr.back()->smem);
         return index[key] = (int)tr.size() - 1;
     }
+    // Device arguments, two per plan: [2 p] forward, [2 p + 1] inverse.
     void finish()
     {
         std::vector<XformArgs<T>> v;
         for (auto& t : tr)
         {
-            typedef typename Cplx<T>::type T2;
-            XformArgs<T> x{};
-            x.n  = t->n;
-            x.fd = t->fd;
-            x.ft = FftTables<T2>{t->tw.template as<T2>(), t->chirp.template as<T2>(), t->bhat.template as<T2>(),
-                                 t->perm.template as<int>(), t->stages.template as<int4>()};
-            x.ta = t->ta.template as<T>();
-            x.tb = t->tb.template as<T>();
-            x.tc = t->tc.template as<T2>();
-            x.s1 = t->s1;
-            x.s2 = t->s2;
-            v.push_back(x);
+            v.push_back(t->args(false));
+            v.push_back(t->args(true));
         }
         dev = upload(v);
     }

@@ -10,9 +10,12 @@
 //
 // A smooth length L is transformed by loading the input digit-reversed (a per-plan index table) and
 // running the DIT stages. A length with a prime factor above 7 goes through Bluestein's chirp-z
-// identity on a smooth length M >= 2L-2:  X_k = c_k * sum_n (x_n c_n) conj(c_{k-n}),
-// c_n = exp(-i pi n^2 / L): DIF of (x c), pointwise product with the (digit-reversed, 1/M-scaled)
-// transform of the chirp kernel, conjugate, DIT, conjugate, times c_k.
+// identity X_k = c_k * sum_n (x_n c_n) conj(c_{k-n}), c_n = exp(-i pi n^2 / L), restricted to a window:
+// inputs n in [in0, in0+nin) (the others are zero) and outputs k in [out0, out0+nout) (the others are
+// not needed). Then only the kernel lags -(nin-1) .. nout-1 occur and a cyclic convolution of smooth
+// length M >= nin + nout - 1 is exact (2L-2 for the full window, whose two extreme lags share a value).
+// Steps: DIF of (x c) placed from slot 0, pointwise product with the (digit-reversed, 1/M-scaled)
+// transform of the kernel, conjugate, DIT, conjugate, times c_k; output k sits in slot k - out0.
 //
 // All twiddles, chirps and permutations are precomputed on the host in long double and read
 // through the read-only cache.
@@ -38,6 +41,8 @@ struct FftDesc
     int      L;     // logical transform length
     int      M;     // executed length (L, or the Bluestein length)
     int      blue;  // 1: Bluestein
+    int      in0, nin;    // Bluestein window: nonzero inputs [in0, in0+nin)
+    int      out0, nout;  // and outputs kept [out0, out0+nout); (0, L, 0, L) for a direct transform
     int      nst;
     FftStage st[kFftMaxStages];
 };
@@ -232,23 +237,31 @@ __device__ void fft_stages(T2* buf, const FftDesc& d, const T2* __restrict__ tw,
     }
 }
 
-// Slot in buf where input element n (n < M) must be stored before fft_execute.
-template <typename T2> __device__ __forceinline__ int fft_in_slot(const FftDesc& d, const FftTables<T2>& t, int n)
+// Slot in buf of buffer position i (i < M) before fft_execute: digit-reversed for a direct transform,
+// i itself for Bluestein. Position i carries input element i + in0.
+template <typename T2> __device__ __forceinline__ int fft_in_slot(const FftDesc& d, const FftTables<T2>& t, int i)
 {
-    return fft_slot(d.blue ? n : __ldg(t.perm + n));
+    return fft_slot(d.blue ? i : __ldg(t.perm + i));
 }
-// Scale applied to input n before storing (Bluestein pre-chirp); zero past L.
-template <typename T2> __device__ __forceinline__ T2 fft_in_value(const FftDesc& d, const FftTables<T2>& t, int n, T2 z)
+// Value stored at position i for input element e = i + in0 with value z: z itself (direct), z c_e
+// (Bluestein, inside the window) or zero.
+template <typename T2> __device__ __forceinline__ T2 fft_in_value(const FftDesc& d, const FftTables<T2>& t, int i, T2 z)
 {
     if (!d.blue) return z;
-    if (n >= d.L) return mk<T2>(0, 0);
-    return cmul(z, __ldg(t.chirp + n));
+    if (i >= d.nin) return mk<T2>(0, 0);
+    return cmul(z, __ldg(t.chirp + i + d.in0));
 }
 
-// In-place transform; on return buf holds the natural-order spectrum (direct) or its Bluestein
-// intermediate, read back through fft_out.
+// Elements one thread carries through a pass of an element-wise phase (pre-processing, Bluestein
+// products, post-processing): the pass issues the global and table loads of all of them before it stores
+// any, so it waits for one memory latency per kFftBatch elements rather than one per element.
+constexpr int kFftBatch = 4;
+
+// In-place transform; on return buf holds the natural-order spectrum X_k for k in the output window
+// (all k < L for a direct transform), read with fft_out. Ends with a barrier.
 template <typename T2> __device__ void fft_execute(T2* buf, const FftDesc& d, const FftTables<T2>& t)
 {
+    constexpr int U = kFftBatch;
     __syncthreads();
     if (!d.blue)
     {
@@ -256,20 +269,59 @@ template <typename T2> __device__ void fft_execute(T2* buf, const FftDesc& d, co
         return;
     }
     fft_stages<false>(buf, d, t.tw, t.stages);
-    for (int k = threadIdx.x; k < d.M; k += blockDim.x)
+    for (int k0 = threadIdx.x; k0 < d.M; k0 += U * blockDim.x)
     {
-        const int sl = fft_slot(k);
-        buf[sl]      = cconj(cmul(buf[sl], __ldg(t.bhat + k)));
+        T2 b[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int k = k0 + u * (int)blockDim.x;
+            b[u]        = (k < d.M) ? __ldg(t.bhat + k) : mk<T2>(0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int k = k0 + u * (int)blockDim.x;
+            if (k < d.M)
+            {
+                const int sl = fft_slot(k);
+                buf[sl]      = cconj(cmul(buf[sl], b[u]));
+            }
+        }
     }
     __syncthreads();
     fft_stages<true>(buf, d, t.tw, t.stages);
+    // post-chirp: X_{out0+k} = conj(buf_k) c_{out0+k}
+    for (int k0 = threadIdx.x; k0 < d.nout; k0 += U * blockDim.x)
+    {
+        T2 c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int k = k0 + u * (int)blockDim.x;
+            c[u]        = (k < d.nout) ? __ldg(t.chirp + d.out0 + k) : mk<T2>(0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int k = k0 + u * (int)blockDim.x;
+            if (k < d.nout)
+            {
+                const int sl = fft_slot(k);
+                buf[sl]      = cmul(cconj(buf[sl]), c[u]);
+            }
+        }
+    }
+    __syncthreads();
 }
 
-// Spectrum value X_k, 0 <= k < L, after fft_execute.
-template <typename T2> __device__ __forceinline__ T2 fft_out(const T2* buf, const FftDesc& d, const FftTables<T2>& t, int k)
+// Spectrum value X_k after fft_execute, k in the output window.
+template <typename T2> __device__ __forceinline__ T2 fft_out(const T2* buf, const FftDesc& d, int k)
 {
-    if (!d.blue) return buf[fft_slot(k)];
-    return cmul(cconj(buf[fft_slot(k)]), __ldg(t.chirp + k));
+    return buf[fft_slot(k - d.out0)];
 }
+
+// L - k for 0 < k <= L, and 0 for k = 0: the index of X_{-k}.
+__device__ __forceinline__ int fft_mirror(int k, int L) { return k == 0 ? 0 : L - k; }
 
 }  // namespace fpb

@@ -135,13 +135,15 @@ template <typename T> struct DevTransform
 {
     typedef typename Cplx<T>::type T2;
     int     kind = 0, n = 0;
-    FftDesc fd{};
-    DevBuf  tw, chirp, bhat, perm, stages, ta, tb, tc;
+    FftDesc fd{}, fd_inv{};  // forward / inverse windows of one plan
+    DevBuf  tw, chirp, bhat, bhat_inv, perm, stages, ta, tb, tc;
     T       s1 = 0, s2 = 0;
     int     threads = 128;
     size_t  smem    = 0;
 
     DevTransform(int kind, int n);
+    // Everything but the rows for one direction.
+    XformArgs<T> args(bool inverse) const;
     // rows = fields * nx contiguous rows of length n; in and out may alias.
     void run(const T* in, T* out, long long rows, bool inverse, cudaStream_t s) const { run_io<T>(in, out, rows, inverse, s); }
     // Same with rows of another element type (FP64 rows through an FP32 transform).

@@ -134,7 +134,57 @@ int fft_length(int kind, int n)
     }
 }
 
+FftWindow fft_window(int kind, int n, bool inverse)
+{
+    if (kind == K_ND && inverse) return FftWindow{1, 2 * n, 1, n};  // herm_input 1..2n; outputs X_{j+1}
+    if (kind == K_ND || kind == K_DN) return FftWindow{1, n, 1, 2 * n};  // inputs 1..n; X_k, X_{L-k}, k <= n
+    const int L = fft_length(kind, n);
+    return FftWindow{0, L, 0, L};
+}
+
+namespace
+{
+// Shortest cyclic convolution that is exact for window w of a length-L chirp-z transform.
+int window_span(int L, const FftWindow& w)
+{
+    if (w.in0 == w.out0 && w.nin == L && w.nout == L) return 2 * L - 2;  // the full window: even kernel
+    return w.nin + w.nout - 1;
+}
+
+// FFT_M of the kernel conj(c_{delta + j}), lags j = -(nin-1) .. nout-1 placed at j mod M, delta =
+// out0 - in0; digit-reversed and scaled by 1/M.
+std::vector<cld> bluestein_kernel(int L, int M, const FftWindow& w, const FftDesc& d)
+{
+    std::vector<cld> b(M, cld(0, 0));
+    const long long  delta = (long long)w.out0 - w.in0;
+    for (long long j = -(long long)(w.nin - 1); j <= (long long)w.nout - 1; ++j)
+    {
+        long long e = delta + j;  // chirp index; c_e = exp(-i pi e^2 / L) depends on e^2 mod 2L
+        long long q = ((e % (2LL * L)) * (e % (2LL * L))) % (2LL * L);
+        b[(size_t)(((j % M) + M) % M)] = std::conj(root_of_unity(q, 2LL * L));
+    }
+    host_dft(b);
+    std::vector<int> idx = dif_order(d);
+    std::vector<cld> r(M);
+    for (int p = 0; p < M; ++p) r[p] = b[idx[p]] / (long double)M;
+    return r;
+}
+
+void set_window(FftDesc& d, const FftWindow& w)
+{
+    d.in0  = w.in0;
+    d.nin  = w.nin;
+    d.out0 = w.out0;
+    d.nout = w.nout;
+}
+}  // namespace
+
 HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit)
+{
+    return plan_fft(L, elem_bytes, smem_limit, FftWindow{0, L, 0, L}, FftWindow{0, L, 0, L});
+}
+
+HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftWindow iw)
 {
     HostFft h;
     h.d.L = L;
@@ -143,20 +193,23 @@ HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit)
     {
         h.d.M    = L;
         h.d.blue = 0;
+        set_window(h.d, FftWindow{0, L, 0, L});
         build_stages(h.d, rad, h.tw);
         std::vector<int> idx = dif_order(h.d);
         h.perm.assign(L, 0);
         for (int p = 0; p < L; ++p) h.perm[idx[p]] = p;
+        h.d_inv = h.d;
     }
     else
     {
-        // Smallest-cost 7-smooth M >= 2L-2. The chirp kernel is even (b_{-k} = b_k), so the one slot
-        // that lags L-1 and -(L-1) share when M = 2L-2 receives the same value from both and the cyclic
-        // convolution still equals the linear one on outputs 0..L-1. For L = 2^k + 1 (DST-I of a
-        // power-of-two row) and L = 2^(k+1) + 1 (the quarter-wave families) M is then a power of two.
-        int    best = -1;
-        double best_cost = 1e300;
-        for (int M = 2 * L - 2; M <= 3 * L; ++M)
+        for (const FftWindow& w : {fw, iw})
+            if (w.in0 < 0 || w.nin < 1 || w.in0 + w.nin > L || w.out0 < 0 || w.nout < 1 || w.out0 + w.nout > L)
+                throw std::runtime_error("FFT plan: window outside the transform");
+        // Smallest-cost 7-smooth M covering both windows' convolutions.
+        const int need = std::max(window_span(L, fw), window_span(L, iw));
+        int       best = -1;
+        double    best_cost = 1e300;
+        for (int M = need; M <= need + need / 2; ++M)
         {
             std::vector<int> r = radices(M);
             if (r.empty()) continue;
@@ -173,15 +226,14 @@ HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit)
         h.d.M    = best;
         h.d.blue = 1;
         build_stages(h.d, radices(best), h.tw);
+        h.d_inv = h.d;
+        set_window(h.d, fw);
+        set_window(h.d_inv, iw);
         h.chirp.resize(L);
         for (int n = 0; n < L; ++n) h.chirp[n] = root_of_unity(((long long)n * n) % (2LL * L), 2LL * L);
-        std::vector<cld> b(best, cld(0, 0));
-        for (int n = 0; n < L; ++n) b[n] = std::conj(h.chirp[n]);
-        for (int n = 1; n < L; ++n) b[best - n] = std::conj(h.chirp[n]);
-        host_dft(b);
-        std::vector<int> idx = dif_order(h.d);
-        h.bhat.resize(best);
-        for (int p = 0; p < best; ++p) h.bhat[p] = b[idx[p]] / (long double)best;
+        h.bhat = bluestein_kernel(L, best, fw, h.d);
+        if (fw.in0 != iw.in0 || fw.nin != iw.nin || fw.out0 != iw.out0 || fw.nout != iw.nout)
+            h.bhat_inv = bluestein_kernel(L, best, iw, h.d);
     }
     if ((size_t)fft_buf_elems(h.d.M) * elem_bytes > smem_limit)
         throw std::runtime_error("transform length " + std::to_string(L) + " needs " +

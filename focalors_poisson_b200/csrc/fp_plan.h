@@ -46,17 +46,30 @@ int kind_of(int bc_neg, int bc_pos);  // -1 if unsupported
 // Length of the complex FFT each family's device transform runs (fp_transform.cuh).
 int fft_length(int kind, int n);
 
+// Inputs a transform reads and outputs it keeps, for Bluestein's windowed convolution (fp_fft.cuh).
+struct FftWindow
+{
+    int in0, nin, out0, nout;
+};
+// Window of a family's complex FFT in one direction: the quarter-wave families read elements 1..n and
+// keep 1..2n (ND inverse: reads 1..2n, keeps 1..n); the others use the whole length.
+FftWindow fft_window(int kind, int n, bool inverse);
+
 struct HostFft
 {
-    FftDesc                               d{};
+    FftDesc                               d{};      // forward window
+    FftDesc                               d_inv{};  // inverse window (same M, stages and tables)
     std::vector<std::complex<long double>> tw;
     std::vector<std::complex<long double>> chirp;
-    std::vector<std::complex<long double>> bhat;  // digit-reversed, scaled by 1/M
+    std::vector<std::complex<long double>> bhat;      // digit-reversed, scaled by 1/M
+    std::vector<std::complex<long double>> bhat_inv;  // kernel of the inverse window, if it differs
     std::vector<int>                       perm;
 };
 // Plans a length-L complex DFT whose single buffer must fit in smem_limit bytes for complex
-// elements of elem_bytes. Throws std::runtime_error if it cannot.
+// elements of elem_bytes, with the forward and inverse windows fw and iw (used when L needs
+// Bluestein). Throws std::runtime_error if it cannot.
 HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit);
+HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftWindow iw);
 
 // Per-family tables computed with the reference's own double expressions so that the device
 // transform reproduces the reference's values, not merely the exact transform.

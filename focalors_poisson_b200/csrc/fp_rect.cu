@@ -61,18 +61,20 @@ template <typename T> DevTransform<T>::DevTransform(int kind_, int n_) : kind(ki
     HostFft   h;
     try
     {
-        h = plan_fft(L, sizeof(T2), max_dynamic_smem());
+        h = plan_fft(L, sizeof(T2), max_dynamic_smem(), fft_window(kind, n, false), fft_window(kind, n, true));
     }
     catch (const std::runtime_error& e)
     {
         throw Error(3, e.what());
     }
-    fd = h.d;
-    tw = upload(convert_c<T2>(h.tw));
+    fd     = h.d;
+    fd_inv = h.d_inv;
+    tw     = upload(convert_c<T2>(h.tw));
     if (fd.blue)
     {
         chirp = upload(convert_c<T2>(h.chirp));
         bhat  = upload(convert_c<T2>(h.bhat));
+        if (!h.bhat_inv.empty()) bhat_inv = upload(convert_c<T2>(h.bhat_inv));
     }
     else
     {
@@ -97,22 +99,31 @@ template <typename T> DevTransform<T>::DevTransform(int kind_, int n_) : kind(ki
     if (smem > max_dynamic_smem()) throw Error(3, "transform of length " + std::to_string(n) + " needs more shared memory than a CTA has");
 }
 
+template <typename T> XformArgs<T> DevTransform<T>::args(bool inverse) const
+{
+    XformArgs<T> a{};
+    const bool   inv_tab = inverse && bhat_inv.bytes() > 0;
+    a.n  = n;
+    a.fd = inverse ? fd_inv : fd;
+    a.ft = FftTables<T2>{tw.as<T2>(), chirp.as<T2>(), (inv_tab ? bhat_inv : bhat).template as<T2>(), perm.as<int>(),
+                         stages.as<int4>()};
+    a.tc = tc.as<T2>();
+    a.ta = ta.as<T>();
+    a.tb = tb.as<T>();
+    a.s1 = s1;
+    a.s2 = s2;
+    return a;
+}
+
 template <typename T>
 template <typename TIO>
 void DevTransform<T>::run_io(const TIO* in, TIO* out, long long rows, bool inverse, cudaStream_t s) const
 {
     TransformArgs<T, TIO> a;
+    static_cast<XformArgs<T>&>(a) = args(inverse);
     a.in    = in;
     a.out   = out;
     a.rows  = rows;
-    a.n     = n;
-    a.fd    = fd;
-    a.ft    = FftTables<T2>{tw.as<T2>(), chirp.as<T2>(), bhat.as<T2>(), perm.as<int>(), stages.as<int4>()};
-    a.tc    = tc.as<T2>();
-    a.ta    = ta.as<T>();
-    a.tb    = tb.as<T>();
-    a.s1    = s1;
-    a.s2    = s2;
     const int inv = inverse ? 1 : 0;
 #define FPB_CASE(K)                                                                                        \
     case K:                                                                                                \

@@ -191,42 +191,192 @@ template <typename T> __device__ void block_scan2(T* xa, T* xb, int K)
     __syncthreads();
 }
 
+// Table values the output slot j of a family reads (NN forward: its post-twiddle; ND forward and PP
+// forward: the reference's cos / sin pair), loaded in a batch before the slot's spectrum values.
+template <typename T, int KIND, int INV>
+__device__ __forceinline__ typename Cplx<T>::type out_table(const XformArgs<T>& a, int j)
+{
+    typedef typename Cplx<T>::type T2;
+    const int n = a.n;
+    if (KIND == 1 && !INV) return a.tc[(j < n - 1) ? n - 1 - j : 0];
+    if ((KIND == 2 && !INV) || (KIND == 4 && !INV)) return mk<T2>(__ldg(a.ta + j), __ldg(a.tb + j));
+    return mk<T2>(0, 0);
+}
+
+// Output values (row a, row b) of slot j for every family except DD, from the spectrum X in buf.
+// tv: out_table(j); la: PP forward's f(i, ny-1).
+template <typename T, int KIND, int INV>
+__device__ __forceinline__ typename Cplx<T>::type out_value(const XformArgs<T>& a, const typename Cplx<T>::type* buf,
+                                                          int j, typename Cplx<T>::type tv, T la)
+{
+    typedef typename Cplx<T>::type T2;
+    const int n    = a.n;
+    const int L    = a.fd.L;
+    const T   half = (T)0.5;
+    if (KIND == 1 && !INV)
+    {
+        // reference slot j holds mode m = n-1-j negated and scaled, the mean (m = 0) in slot n-1
+        const int m  = (j < n - 1) ? n - 1 - j : 0;
+        const T2  Zk = fft_out(buf, a.fd, m);
+        const T2  Zm = fft_out(buf, a.fd, fft_mirror(m, L));
+        const T2  w  = tv;  // (cos, -sin)(pi m / 2n)
+        const T Ur = half * (Zk.x + Zm.x), Ui = half * (Zk.y - Zm.y);
+        const T Vr = half * (Zk.y + Zm.y), Vi = -half * (Zk.x - Zm.x);
+        const T Ca = w.x * Ur - w.y * Ui, Cb = w.x * Vr - w.y * Vi;  // Re(w V)
+        const T sc = (j < n - 1) ? -a.s1 : a.s2;
+        return mk<T2>(sc * Ca, sc * Cb);
+    }
+    else if (KIND == 1 && INV)
+    {
+        const int m = (j & 1) ? n - 1 - (j - 1) / 2 : j / 2;
+        return fft_out(buf, a.fd, m);
+    }
+    else if (KIND == 2 && INV)
+    {
+        const T2 Z = fft_out(buf, a.fd, j + 1);
+        const T  s = alt_neg_even<T>(j) * a.s1;
+        return mk<T2>(s * Z.x, s * Z.y);
+    }
+    else if (KIND == 2 || KIND == 3)
+    {
+        const int k  = j + 1;
+        const T2  Xk = fft_out(buf, a.fd, k);
+        const T2  Xm = fft_out(buf, a.fd, fft_mirror(k, L));
+        const T   Ur = half * (Xk.x + Xm.x), Ui = half * (Xk.y - Xm.y);
+        const T   Vr = half * (Xk.y + Xm.y), Vi = -half * (Xk.x - Xm.x);
+        if (KIND == 2)
+        {
+            const T c = tv.x, s = tv.y;
+            return mk<T2>(s * Ur - c * Ui, s * Vr - c * Vi);
+        }
+        return mk<T2>(alt_pos_even<T>(j) * Ui, alt_pos_even<T>(j) * Vi);
+    }
+    else if (KIND == 4 && !INV)
+    {
+        const int h  = n / 2;
+        T         ts = 0;
+        if (j > 0)
+        {
+            const int ks = (j & 1) ? (h - (j - 1) / 2 - 1) : (h - j / 2);
+            const T2  Sk = fft_out(buf, a.fd, ks);
+            const T2  Sm = fft_out(buf, a.fd, fft_mirror(ks, L));
+            ts           = -(half * (Sk.y - Sm.y));
+        }
+        const int kc = (j & 1) ? (j + 1) / 2 : j / 2;
+        const T2  Ck = fft_out(buf, a.fd, kc);
+        const T2  Cm = fft_out(buf, a.fd, fft_mirror(kc, L));
+        const T   tc = la - half * (Ck.y + Cm.y);
+        return mk<T2>(a.s1 * (tv.x * ts + tv.y * tc), (T)0);
+    }
+    else  // PP inverse
+    {
+        const int h  = n / 2;
+        T         fc = 0, fs = 0;
+        if (j < h)
+        {
+            const T2 Xk = fft_out(buf, a.fd, j + 1);
+            const T2 Xm = fft_out(buf, a.fd, fft_mirror(j + 1, L));
+            fc          = alt_neg_even<T>(j) * (half * (Xk.y - Xm.y));
+            fs          = half * (Xk.y + Xm.y);
+        }
+        else if (j <= n - 2)
+        {
+            const int m  = n - 2 - j;
+            const T2  Yk = fft_out(buf, a.fd, m + 1);
+            const T2  Ym = fft_out(buf, a.fd, fft_mirror(m + 1, L));
+            fc           = -(alt_neg_even<T>(m) * (half * (Yk.y - Ym.y)));
+            fs           = half * (Yk.y + Ym.y);
+        }
+        else
+        {
+            fs = fft_out(buf, a.fd, 0).y;  // Re V_0 = Im Z_0
+        }
+        return mk<T2>(a.s1 * (fc + fs), (T)0);
+    }
+}
+
+// Writes U output pairs v[u] to oa[idx[u]] (and ob[idx[u]] when ob), skipping idx < 0. ACC adds them
+// to the values already there in FP64; those reads are issued together before the first store.
+template <int U, bool ACC, typename TOUT, typename T2>
+__device__ __forceinline__ void put_batch(TOUT* oa, TOUT* ob, const int* idx, const T2* v)
+{
+    double pa[U], pb[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+    {
+        pa[u] = 0;
+        pb[u] = 0;
+        if (ACC && idx[u] >= 0)
+        {
+            pa[u] = (double)oa[idx[u]];
+            if (ob) pb[u] = (double)ob[idx[u]];
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+    {
+        if (idx[u] < 0) continue;
+        if (ACC)
+        {
+            oa[idx[u]] = (TOUT)(pa[u] + (double)v[u].x);
+            if (ob) ob[idx[u]] = (TOUT)(pb[u] + (double)v[u].y);
+        }
+        else
+        {
+            oa[idx[u]] = (TOUT)v[u].x;
+            if (ob) ob[idx[u]] = (TOUT)v[u].y;
+        }
+    }
+}
+
 // One work item: rows fa (and fb, when has_b and the family pairs rows) of length a.n transformed into
 // oa (ob). buf: the item's shared-memory FFT buffer; rowsc: two scratch values. ACC: out += result
 // (FP64 accumulation of a correction) instead of out = result. Ends with the CTA synchronised.
+// Every element-wise pass handles kFftBatch elements per thread at a time, loads first.
 template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC>
 __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN* fa, const TIN* fb, TOUT* oa, TOUT* ob,
                                                bool has_b, typename Cplx<T>::type* buf, T* rowsc)
 {
     typedef typename Cplx<T>::type T2;
     constexpr bool kHerm = INV && (KIND == 1 || KIND == 2);  // real-output families
+    constexpr int  U     = kFftBatch;
     const int      n     = a.n;
     const int      L     = a.fd.L;
-    auto put = [&](TOUT* o, int idx, T v) {
-        if (ACC) o[idx] = (TOUT)((double)o[idx] + (double)v);
-        else o[idx] = (TOUT)v;
-    };
+    const int      M     = a.fd.M;
+    const int      nt    = (int)blockDim.x;
 
     if (KIND == 4 && !INV && threadIdx.x == 0) rowsc[0] = (T)fa[n - 1];  // PP forward: f(i, ny-1)
 
-    for (int i = threadIdx.x; i < a.fd.M; i += blockDim.x)
+    for (int i0 = threadIdx.x; i0 < M; i0 += U * nt)
     {
-        T2 z = mk<T2>(0, 0);
-        if (i < L)
+        T2  v[U];
+        int sl[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
         {
-            if (KIND == 4) z = pp_input<T, INV>(a, fa, i);
-            else if (kHerm)
+            const int i = i0 + u * nt;  // buffer position; input element i + in0
+            T2        z = mk<T2>(0, 0);
+            if (i < a.fd.nin)
             {
-                const T2 ha = herm_input<T, KIND>(a, fa, i);
-                const T2 hb = has_b ? herm_input<T, KIND>(a, fb, i) : mk<T2>(0, 0);
-                z           = mk<T2>(ha.x - hb.y, ha.y + hb.x);  // h_a + i h_b
+                const int e = i + a.fd.in0;
+                if (KIND == 4) z = pp_input<T, INV>(a, fa, e);
+                else if (kHerm)
+                {
+                    const T2 ha = herm_input<T, KIND>(a, fa, e);
+                    const T2 hb = has_b ? herm_input<T, KIND>(a, fb, e) : mk<T2>(0, 0);
+                    z           = mk<T2>(ha.x - hb.y, ha.y + hb.x);  // h_a + i h_b
+                }
+                else
+                {
+                    z = mk<T2>(real_input<T, KIND, INV>(a, fa, e), has_b ? real_input<T, KIND, INV>(a, fb, e) : (T)0);
+                }
             }
-            else
-            {
-                z = mk<T2>(real_input<T, KIND, INV>(a, fa, i), has_b ? real_input<T, KIND, INV>(a, fb, i) : (T)0);
-            }
+            sl[u] = (i < M) ? fft_in_slot(a.fd, a.ft, i) : -1;
+            v[u]  = (i < M) ? fft_in_value(a.fd, a.ft, i, z) : z;
         }
-        buf[fft_in_slot(a.fd, a.ft, i)] = fft_in_value(a.fd, a.ft, i, z);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (sl[u] >= 0) buf[sl[u]] = v[u];
     }
     fft_execute(buf, a.fd, a.ft);
 
@@ -236,135 +386,75 @@ __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN*
         // DD: X_{2k} = -Im Y_k (k >= 1), X_{2k+1} = Re Y_0 / 2 + sum_{q=1..k} Re Y_q; out_m = s1 X_{m+1}
         const int K  = (n + 1) / 2;  // odd outputs X_1, X_3, ...
         // scan arrays: the slots past element L-1 when the buffer has K of them, else past the buffer
-        const int lo = fft_slot(L), hi = fft_buf_elems(a.fd.M);
+        const int lo = fft_slot(L), hi = fft_buf_elems(M);
         T*        ca = reinterpret_cast<T*>(buf + ((hi - lo >= K) ? lo : hi));
         T*        cb = ca + K;
-        for (int k = threadIdx.x; k <= n / 2; k += blockDim.x)
+        for (int k0 = threadIdx.x; k0 <= n / 2; k0 += U * nt)
         {
-            const T2 Zk = fft_out(buf, a.fd, a.ft, k % L);
-            const T2 Zm = fft_out(buf, a.fd, a.ft, (L - k) % L);
-            if (k < K)
+            int idx[U];
+            T2  v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
             {
-                const T sc = (k == 0) ? (T)0.5 : (T)1;
-                ca[k]      = sc * (half * (Zk.x + Zm.x));  // Re Y^a_k
-                cb[k]      = sc * (half * (Zk.y + Zm.y));  // Re Y^b_k
+                const int k = k0 + u * nt;
+                idx[u]      = -1;
+                v[u]        = mk<T2>(0, 0);
+                if (k > n / 2) continue;
+                const T2 Zk = fft_out(buf, a.fd, k);
+                const T2 Zm = fft_out(buf, a.fd, fft_mirror(k, L));
+                if (k < K)
+                {
+                    const T sc = (k == 0) ? (T)0.5 : (T)1;
+                    ca[k]      = sc * (half * (Zk.x + Zm.x));  // Re Y^a_k
+                    cb[k]      = sc * (half * (Zk.y + Zm.y));  // Re Y^b_k
+                }
+                if (k >= 1 && 2 * k <= n)
+                {
+                    idx[u] = 2 * k - 1;
+                    v[u]   = mk<T2>(a.s1 * (-(half * (Zk.y - Zm.y))), a.s1 * (half * (Zk.x - Zm.x)));  // -Im Y^a_k, -Im Y^b_k
+                }
             }
-            if (k >= 1 && 2 * k <= n)
-            {
-                put(oa, 2 * k - 1, a.s1 * (-(half * (Zk.y - Zm.y))));  // -Im Y^a_k
-                if (ob) put(ob, 2 * k - 1, a.s1 * (half * (Zk.x - Zm.x)));  // -Im Y^b_k
-            }
+            put_batch<U, ACC>(oa, ob, idx, v);
         }
         __syncthreads();
         block_scan2(ca, cb, K);
-        for (int k = threadIdx.x; k < K; k += blockDim.x)
+        for (int k0 = threadIdx.x; k0 < K; k0 += U * nt)
         {
-            put(oa, 2 * k, a.s1 * ca[k]);
-            if (ob) put(ob, 2 * k, a.s1 * cb[k]);
+            int idx[U];
+            T2  v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+            {
+                const int k = k0 + u * nt;
+                idx[u]      = (k < K) ? 2 * k : -1;
+                v[u]        = (k < K) ? mk<T2>(a.s1 * ca[k], a.s1 * cb[k]) : mk<T2>(0, 0);
+            }
+            put_batch<U, ACC>(oa, ob, idx, v);
         }
         __syncthreads();
         return;
     }
 
-    for (int j = threadIdx.x; j < n; j += blockDim.x)
+    const T la = (KIND == 4 && !INV) ? rowsc[0] : (T)0;
+    for (int j0 = threadIdx.x; j0 < n; j0 += U * nt)
     {
-        if (KIND == 1 && !INV)
+        T2 tv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
         {
-            // reference slot j holds mode m = n-1-j negated and scaled, the mean (m = 0) in slot n-1
-            const int m  = (j < n - 1) ? n - 1 - j : 0;
-            const T2  Zk = fft_out(buf, a.fd, a.ft, m);
-            const T2  Zm = fft_out(buf, a.fd, a.ft, (L - m) % L);
-            const T2  w  = a.tc[m];  // (cos, -sin)(pi m / 2n)
-            const T Ur = half * (Zk.x + Zm.x), Ui = half * (Zk.y - Zm.y);
-            const T Vr = half * (Zk.y + Zm.y), Vi = -half * (Zk.x - Zm.x);
-            const T Ca = w.x * Ur - w.y * Ui, Cb = w.x * Vr - w.y * Vi;  // Re(w V)
-            if (j < n - 1)
-            {
-                put(oa, j, -a.s1 * Ca);
-                if (ob) put(ob, j, -a.s1 * Cb);
-            }
-            else
-            {
-                put(oa, j, a.s2 * Ca);
-                if (ob) put(ob, j, a.s2 * Cb);
-            }
+            const int j = j0 + u * nt;
+            tv[u]       = (j < n) ? out_table<T, KIND, INV>(a, j) : mk<T2>(0, 0);
         }
-        else if (KIND == 1 && INV)
+        int idx[U];
+        T2  v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
         {
-            const int  m = (j & 1) ? n - 1 - (j - 1) / 2 : j / 2;
-            const T2   Z = fft_out(buf, a.fd, a.ft, m);
-            put(oa, j, Z.x);
-            if (ob) put(ob, j, Z.y);
+            const int j = j0 + u * nt;
+            idx[u]      = (j < n) ? j : -1;
+            v[u]        = (j < n) ? out_value<T, KIND, INV>(a, buf, j, tv[u], la) : mk<T2>(0, 0);
         }
-        else if (KIND == 2 && INV)
-        {
-            const T2 Z = fft_out(buf, a.fd, a.ft, j + 1);
-            const T  s = alt_neg_even<T>(j) * a.s1;
-            put(oa, j, s * Z.x);
-            if (ob) put(ob, j, s * Z.y);
-        }
-        else if (KIND == 2 || KIND == 3)
-        {
-            const int k  = j + 1;
-            const T2  Xk = fft_out(buf, a.fd, a.ft, k % L);
-            const T2  Xm = fft_out(buf, a.fd, a.ft, (L - k) % L);
-            const T   Ur = half * (Xk.x + Xm.x), Ui = half * (Xk.y - Xm.y);
-            const T   Vr = half * (Xk.y + Xm.y), Vi = -half * (Xk.x - Xm.x);
-            if (KIND == 2)
-            {
-                const T c = __ldg(a.ta + j), s = __ldg(a.tb + j);
-                put(oa, j, s * Ur - c * Ui);
-                if (ob) put(ob, j, s * Vr - c * Vi);
-            }
-            else
-            {
-                put(oa, j, alt_pos_even<T>(j) * Ui);
-                if (ob) put(ob, j, alt_pos_even<T>(j) * Vi);
-            }
-        }
-        else if (KIND == 4 && !INV)
-        {
-            const int h  = n / 2;
-            const T   la = rowsc[0];
-            T         ts = 0;
-            if (j > 0)
-            {
-                const int ks = (j & 1) ? (h - (j - 1) / 2 - 1) : (h - j / 2);
-                const T2  Sk = fft_out(buf, a.fd, a.ft, ks);
-                const T2  Sm = fft_out(buf, a.fd, a.ft, (L - ks) % L);
-                ts           = -(half * (Sk.y - Sm.y));
-            }
-            const int kc = (j & 1) ? (j + 1) / 2 : j / 2;
-            const T2  Ck = fft_out(buf, a.fd, a.ft, kc);
-            const T2  Cm = fft_out(buf, a.fd, a.ft, (L - kc) % L);
-            const T   tc = la - half * (Ck.y + Cm.y);
-            put(oa, j, a.s1 * (__ldg(a.ta + j) * ts + __ldg(a.tb + j) * tc));
-        }
-        else if (KIND == 4)
-        {
-            const int h  = n / 2;
-            T         fc = 0, fs = 0;
-            if (j < h)
-            {
-                const T2 Xk = fft_out(buf, a.fd, a.ft, j + 1);
-                const T2 Xm = fft_out(buf, a.fd, a.ft, (L - j - 1) % L);
-                fc          = alt_neg_even<T>(j) * (half * (Xk.y - Xm.y));
-                fs          = half * (Xk.y + Xm.y);
-            }
-            else if (j <= n - 2)
-            {
-                const int m  = n - 2 - j;
-                const T2  Yk = fft_out(buf, a.fd, a.ft, m + 1);
-                const T2  Ym = fft_out(buf, a.fd, a.ft, (L - m - 1) % L);
-                fc           = -(alt_neg_even<T>(m) * (half * (Yk.y - Ym.y)));
-                fs           = half * (Yk.y + Ym.y);
-            }
-            else
-            {
-                fs = fft_out(buf, a.fd, a.ft, 0).y;  // Re V_0 = Im Z_0
-            }
-            put(oa, j, a.s1 * (fc + fs));
-        }
+        put_batch<U, ACC>(oa, ob, idx, v);
     }
     __syncthreads();
 }

@@ -33,7 +33,7 @@ def test_transforms_golden_f64_host_and_device():
 
 
 @pytest.mark.parametrize("kind", list(PAIRS))
-@pytest.mark.parametrize("ny", [6, 64, 130, 256, 1000, 2048])
+@pytest.mark.parametrize("ny", [6, 64, 130, 256, 1000, 2048, 3000, 4096])
 def test_transforms_large_vs_oracle(kind, ny):
     rng = np.random.default_rng(ny)
     f = rng.standard_normal((5, ny))
