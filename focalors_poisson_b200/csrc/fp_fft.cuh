@@ -170,17 +170,20 @@ template <int R, typename T2> __device__ __forceinline__ void dft(T2* x)
 
 // Leg q of butterfly b is rotated by w^q, w = exp(-2 pi i b / B): one table load per butterfly, the
 // powers by repeated multiplication (w^2 = w w, w^3 = w^2 w, ...; at most 7 products, a few ulp).
-template <int R, bool DIT, typename T2>
-__device__ __forceinline__ void stage_radix(T2* buf, const FftStage st, int nbf, const T2* __restrict__ tw)
+// ld(k) supplies element k, sto(k, v) takes the result for element k: shared memory for an ordinary
+// stage, the input pre-processing or the output post-processing for the fused first / last stages.
+template <int R, bool DIT, typename T2, typename LD, typename ST>
+__device__ __forceinline__ void stage_radix_io(const FftStage st, int nbf, const T2* __restrict__ tw, const LD& ld,
+                                               const ST& sto)
 {
     for (int t = threadIdx.x; t < nbf; t += blockDim.x)
     {
-        const int blk = t / st.S;
-        const int b   = t - blk * st.S;
+        const int blk  = t / st.S;
+        const int b    = t - blk * st.S;
         const int base = blk * st.B + b;
         T2        x[R];
 #pragma unroll
-        for (int q = 0; q < R; ++q) x[q] = buf[fft_slot(base + q * st.S)];
+        for (int q = 0; q < R; ++q) x[q] = ld(base + q * st.S);
         const bool rot = b != 0;
         T2         w1  = rot ? __ldg(tw + st.tw_off + b) : mk<T2>(1, 0);
         if (DIT && rot)
@@ -205,113 +208,143 @@ __device__ __forceinline__ void stage_radix(T2* buf, const FftStage st, int nbf,
             }
         }
 #pragma unroll
-        for (int q = 0; q < R; ++q) buf[fft_slot(base + q * st.S)] = x[q];
+        for (int q = 0; q < R; ++q) sto(base + q * st.S, x[q]);
     }
 }
 
-// Runs all stages (DIF order or DIT order) on buf. Ends with a barrier.
-template <bool DIT, typename T2>
-__device__ void fft_stages(T2* buf, const FftDesc& d, const T2* __restrict__ tw, const int4* __restrict__ stages)
+template <typename T2> struct SmemLd
 {
-    const int nst = d.nst, M = d.M;
-    for (int s0 = 0; s0 < nst; ++s0)
+    const T2* buf;
+    __device__ __forceinline__ T2 operator()(int k) const { return buf[fft_slot(k)]; }
+};
+template <typename T2> struct SmemSt
+{
+    T2* buf;
+    __device__ __forceinline__ void operator()(int k, T2 v) const { buf[fft_slot(k)] = v; }
+};
+
+__device__ __forceinline__ FftStage fft_stage(const int4* __restrict__ stages, int s)
+{
+    const int4 q = __ldg(stages + s);
+    FftStage   st;
+    st.R      = q.x;
+    st.S      = q.y;
+    st.B      = q.z;
+    st.tw_off = q.w;
+    return st;
+}
+
+template <bool DIT, typename T2, typename LD, typename ST>
+__device__ __forceinline__ void stage_io(const FftStage st, int M, const T2* __restrict__ tw, const LD& ld, const ST& sto)
+{
+    const int nbf = M / st.R;
+    switch (st.R)
     {
-        const int  s = DIT ? nst - 1 - s0 : s0;
-        const int4 q = __ldg(stages + s);
-        FftStage   st;
-        st.R          = q.x;
-        st.S          = q.y;
-        st.B          = q.z;
-        st.tw_off     = q.w;
-        const int nbf = M / st.R;
-        switch (st.R)
-        {
-            case 2: stage_radix<2, DIT>(buf, st, nbf, tw); break;
-            case 3: stage_radix<3, DIT>(buf, st, nbf, tw); break;
-            case 4: stage_radix<4, DIT>(buf, st, nbf, tw); break;
-            case 5: stage_radix<5, DIT>(buf, st, nbf, tw); break;
-            case 7: stage_radix<7, DIT>(buf, st, nbf, tw); break;
-            default: stage_radix<8, DIT>(buf, st, nbf, tw); break;
-        }
+        case 2: stage_radix_io<2, DIT>(st, nbf, tw, ld, sto); break;
+        case 3: stage_radix_io<3, DIT>(st, nbf, tw, ld, sto); break;
+        case 4: stage_radix_io<4, DIT>(st, nbf, tw, ld, sto); break;
+        case 5: stage_radix_io<5, DIT>(st, nbf, tw, ld, sto); break;
+        case 7: stage_radix_io<7, DIT>(st, nbf, tw, ld, sto); break;
+        default: stage_radix_io<8, DIT>(st, nbf, tw, ld, sto); break;
+    }
+}
+
+// Runs stages [s0, s1) in place on buf, in DIF order (s0 first) or DIT order (s1 - 1 first), with a
+// barrier after each.
+template <bool DIT, typename T2>
+__device__ void fft_stages(T2* buf, const FftDesc& d, const T2* __restrict__ tw, const int4* __restrict__ stages, int s0,
+                           int s1)
+{
+    const SmemLd<T2> ld{buf};
+    const SmemSt<T2> sto{buf};
+    for (int i = s0; i < s1; ++i)
+    {
+        const int s = DIT ? s1 - 1 - (i - s0) : i;
+        stage_io<DIT>(fft_stage(stages, s), d.M, tw, ld, sto);
         __syncthreads();
     }
 }
 
-// Slot in buf of buffer position i (i < M) before fft_execute: digit-reversed for a direct transform,
-// i itself for Bluestein. Position i carries input element i + in0.
+// The last DIF stage, the product with the kernel transform and the first DIT stage in one pass: both
+// stages have span 1 (no twiddles) and act on the same R consecutive elements, so the group stays in
+// registers between them. Ends with a barrier.
+template <int R, typename T2> __device__ __forceinline__ void stage_kernel_product_r(T2* buf, int M, const T2* __restrict__ bhat)
+{
+    for (int blk = threadIdx.x; blk < M / R; blk += blockDim.x)
+    {
+        T2 h[R], x[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) h[q] = __ldg(bhat + blk * R + q);
+#pragma unroll
+        for (int q = 0; q < R; ++q) x[q] = buf[fft_slot(blk * R + q)];
+        dft<R>(x);
+#pragma unroll
+        for (int q = 0; q < R; ++q) x[q] = cconj(cmul(x[q], h[q]));
+        dft<R>(x);
+#pragma unroll
+        for (int q = 0; q < R; ++q) buf[fft_slot(blk * R + q)] = x[q];
+    }
+    __syncthreads();
+}
+template <typename T2> __device__ __forceinline__ void stage_kernel_product(T2* buf, int M, int R, const T2* __restrict__ bhat)
+{
+    switch (R)
+    {
+        case 2: stage_kernel_product_r<2>(buf, M, bhat); break;
+        case 3: stage_kernel_product_r<3>(buf, M, bhat); break;
+        case 4: stage_kernel_product_r<4>(buf, M, bhat); break;
+        case 5: stage_kernel_product_r<5>(buf, M, bhat); break;
+        case 7: stage_kernel_product_r<7>(buf, M, bhat); break;
+        default: stage_kernel_product_r<8>(buf, M, bhat); break;
+    }
+}
+
+// Slot in buf of input element i (i < L) of a direct transform before fft_execute: digit-reversed.
 template <typename T2> __device__ __forceinline__ int fft_in_slot(const FftDesc& d, const FftTables<T2>& t, int i)
 {
-    return fft_slot(d.blue ? i : __ldg(t.perm + i));
-}
-// Value stored at position i for input element e = i + in0 with value z: z itself (direct), z c_e
-// (Bluestein, inside the window) or zero.
-template <typename T2> __device__ __forceinline__ T2 fft_in_value(const FftDesc& d, const FftTables<T2>& t, int i, T2 z)
-{
-    if (!d.blue) return z;
-    if (i >= d.nin) return mk<T2>(0, 0);
-    return cmul(z, __ldg(t.chirp + i + d.in0));
+    return fft_slot(__ldg(t.perm + i));
 }
 
-// Elements one thread carries through a pass of an element-wise phase (pre-processing, Bluestein
-// products, post-processing): the pass issues the global and table loads of all of them before it stores
-// any, so it waits for one memory latency per kFftBatch elements rather than one per element.
+// Elements one thread carries through a pass of an element-wise phase (pre- and post-processing): the
+// pass issues the global and table loads of all of them before it stores any, so it waits for one
+// memory latency per kFftBatch elements rather than one per element.
 constexpr int kFftBatch = 4;
 
-// In-place transform; on return buf holds the natural-order spectrum X_k for k in the output window
-// (all k < L for a direct transform), read with fft_out. Ends with a barrier.
+// Direct transform of the digit-reversed sequence in buf; on return buf holds the natural-order
+// spectrum X_k, k < L (read with fft_out). Ends with a barrier.
 template <typename T2> __device__ void fft_execute(T2* buf, const FftDesc& d, const FftTables<T2>& t)
 {
-    constexpr int U = kFftBatch;
     __syncthreads();
-    if (!d.blue)
+    fft_stages<true>(buf, d, t.tw, t.stages, 0, d.nst);
+}
+
+// Output store of the last Bluestein stage: X_{out0+k} = conj(y_k) c_{out0+k} for k in the window.
+template <typename T2> struct PostChirpSt
+{
+    T2*                   buf;
+    const T2* __restrict__ chirp;
+    int                   out0, nout;
+    __device__ __forceinline__ void operator()(int k, T2 v) const
     {
-        fft_stages<true>(buf, d, t.tw, t.stages);
-        return;
+        if (k < nout) buf[fft_slot(k)] = cmul(cconj(v), __ldg(chirp + out0 + k));
     }
-    fft_stages<false>(buf, d, t.tw, t.stages);
-    for (int k0 = threadIdx.x; k0 < d.M; k0 += U * blockDim.x)
-    {
-        T2 b[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-        {
-            const int k = k0 + u * (int)blockDim.x;
-            b[u]        = (k < d.M) ? __ldg(t.bhat + k) : mk<T2>(0, 0);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-        {
-            const int k = k0 + u * (int)blockDim.x;
-            if (k < d.M)
-            {
-                const int sl = fft_slot(k);
-                buf[sl]      = cconj(cmul(buf[sl], b[u]));
-            }
-        }
-    }
+};
+
+// Bluestein transform (d.blue, d.nst >= 2) of the input supplied by ld0: ld0(i) is the pre-chirped value
+// of buffer position i (input element i + in0 times c_{i+in0}, zero outside the window). The input
+// pre-processing runs inside the first DIF stage, the kernel product between the last DIF and first DIT
+// stages, and the post-chirp inside the last DIT stage. On return buf holds X_k for k in the output
+// window (fft_out). Starts and ends with a barrier.
+template <typename T2, typename LD> __device__ void fft_execute_bluestein(T2* buf, const FftDesc& d, const FftTables<T2>& t, const LD& ld0)
+{
+    const int nst = d.nst;
     __syncthreads();
-    fft_stages<true>(buf, d, t.tw, t.stages);
-    // post-chirp: X_{out0+k} = conj(buf_k) c_{out0+k}
-    for (int k0 = threadIdx.x; k0 < d.nout; k0 += U * blockDim.x)
-    {
-        T2 c[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-        {
-            const int k = k0 + u * (int)blockDim.x;
-            c[u]        = (k < d.nout) ? __ldg(t.chirp + d.out0 + k) : mk<T2>(0, 0);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-        {
-            const int k = k0 + u * (int)blockDim.x;
-            if (k < d.nout)
-            {
-                const int sl = fft_slot(k);
-                buf[sl]      = cmul(cconj(buf[sl]), c[u]);
-            }
-        }
-    }
+    stage_io<false>(fft_stage(t.stages, 0), d.M, t.tw, ld0, SmemSt<T2>{buf});
+    __syncthreads();
+    fft_stages<false>(buf, d, t.tw, t.stages, 1, nst - 1);
+    stage_kernel_product(buf, d.M, fft_stage(t.stages, nst - 1).R, t.bhat);
+    fft_stages<true>(buf, d, t.tw, t.stages, 1, nst - 1);
+    stage_io<true>(fft_stage(t.stages, 0), d.M, t.tw, SmemLd<T2>{buf}, PostChirpSt<T2>{buf, t.chirp, d.out0, d.nout});
     __syncthreads();
 }
 

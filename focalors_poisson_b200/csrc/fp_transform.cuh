@@ -347,38 +347,45 @@ __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN*
 
     if (KIND == 4 && !INV && threadIdx.x == 0) rowsc[0] = (T)fa[n - 1];  // PP forward: f(i, ny-1)
 
-    for (int i0 = threadIdx.x; i0 < M; i0 += U * nt)
-    {
-        T2  v[U];
-        int sl[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
+    // FFT input (before any pre-chirp) of element e < L
+    auto zval = [&](int e) -> T2 {
+        if (KIND == 4) return pp_input<T, INV>(a, fa, e);
+        if (kHerm)
         {
-            const int i = i0 + u * nt;  // buffer position; input element i + in0
-            T2        z = mk<T2>(0, 0);
-            if (i < a.fd.nin)
-            {
-                const int e = i + a.fd.in0;
-                if (KIND == 4) z = pp_input<T, INV>(a, fa, e);
-                else if (kHerm)
-                {
-                    const T2 ha = herm_input<T, KIND>(a, fa, e);
-                    const T2 hb = has_b ? herm_input<T, KIND>(a, fb, e) : mk<T2>(0, 0);
-                    z           = mk<T2>(ha.x - hb.y, ha.y + hb.x);  // h_a + i h_b
-                }
-                else
-                {
-                    z = mk<T2>(real_input<T, KIND, INV>(a, fa, e), has_b ? real_input<T, KIND, INV>(a, fb, e) : (T)0);
-                }
-            }
-            sl[u] = (i < M) ? fft_in_slot(a.fd, a.ft, i) : -1;
-            v[u]  = (i < M) ? fft_in_value(a.fd, a.ft, i, z) : z;
+            const T2 ha = herm_input<T, KIND>(a, fa, e);
+            const T2 hb = has_b ? herm_input<T, KIND>(a, fb, e) : mk<T2>(0, 0);
+            return mk<T2>(ha.x - hb.y, ha.y + hb.x);  // h_a + i h_b
         }
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-            if (sl[u] >= 0) buf[sl[u]] = v[u];
+        return mk<T2>(real_input<T, KIND, INV>(a, fa, e), has_b ? real_input<T, KIND, INV>(a, fb, e) : (T)0);
+    };
+    if (a.fd.blue)
+    {
+        auto ld0 = [&](int i) -> T2 {
+            if (i >= a.fd.nin) return mk<T2>(0, 0);
+            const int e = i + a.fd.in0;
+            return cmul(zval(e), __ldg(a.ft.chirp + e));
+        };
+        fft_execute_bluestein(buf, a.fd, a.ft, ld0);
     }
-    fft_execute(buf, a.fd, a.ft);
+    else
+    {
+        for (int i0 = threadIdx.x; i0 < M; i0 += U * nt)
+        {
+            T2  v[U];
+            int sl[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+            {
+                const int i = i0 + u * nt;
+                sl[u]       = (i < M) ? fft_in_slot(a.fd, a.ft, i) : -1;
+                v[u]        = (i < M) ? zval(i) : mk<T2>(0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (sl[u] >= 0) buf[sl[u]] = v[u];
+        }
+        fft_execute(buf, a.fd, a.ft);
+    }
 
     const T half = (T)0.5;
     if (KIND == 0)
