@@ -189,86 +189,118 @@ __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __rest
     ze[ny] = y[Li - 1];
 }
 
-// Separator system per subdomain and wavenumber (see k_chase_reduced): tabulated Thomas factors for every
-// row but the last, right-hand sides (with modifiers) loaded ahead of the recurrence.
+// Separator system per subdomain and wavenumber (the system of k_chase_reduced, tabulated Thomas factors
+// for every row but the last). Per wavenumber j the forward elimination y_p = (rhs_p - lower y_{p-1}) inv_p
+// and the back substitution x_p = y_p - scp_p x_{p+1} (p = 0..P-1, one separator per chunk) are affine
+// recurrences along p. A CTA takes 32 wavenumbers (lane = j, so every access is coalesced along j) and
+// splits the separators into kRedWarps contiguous ranges, one per warp: each warp composes the maps of its
+// range, the CTA combines the compositions of the ranges before (after) it through shared memory, and the
+// warp walks its range from that incoming value. The dependent chain per thread is P / kRedWarps maps per
+// sweep instead of P memory round trips; the maps are the sequential ones, composed in another order.
+constexpr int kRedWarps = 8;
+
 template <typename T>
-__global__ void k_b_chase_reduced(const ChaseSeg<T>* __restrict__ segs, const long long* __restrict__ prefix,
-                                  int nseg, const ChaseTabDev<T>* __restrict__ tabs)
+__global__ void __launch_bounds__(32 * kRedWarps) k_b_chase_reduced(const ChaseSeg<T>* __restrict__ segs,
+                                                                    const long long* __restrict__ prefix, int nseg,
+                                                                    const ChaseTabDev<T>* __restrict__ tabs)
 {
     constexpr int      kAhead = 8;
-    const int          s  = seg_of(prefix, nseg, blockIdx.x);
-    const ChaseSeg<T>* sg = segs + s;
-    const long long    t  = (blockIdx.x - prefix[s]) * (long long)blockDim.x + threadIdx.x;
-    const int          ny = sg->ny, nx = sg->nx, P = nx / kChunk;
-    if (t >= ny) return;
-    const int            j    = (int)t;
+    __shared__ T       sa[kRedWarps][32], sb[kRedWarps][32];
+    const int          s    = seg_of(prefix, nseg, blockIdx.x);
+    const ChaseSeg<T>* sg   = segs + s;
+    const int          ny   = sg->ny, nx = sg->nx, P = nx / kChunk;
+    const int          lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int          j0   = (int)(blockIdx.x - prefix[s]) * 32 + lane;
+    const bool         act  = j0 < ny;
+    const int          j    = act ? j0 : 0;  // idle lanes compute on column 0 and store nothing
+    const int          per  = (P + kRedWarps - 1) / kRedWarps;
+    const int          pb = min(P, w * per), pe = min(P, pb + per);
     const ChaseTabDev<T> tb   = tabs[sg->tab];
     const int            nrow = sg->nrow, ncol = sg->ncol;
     ModCtx<T>            mc;
     mod_init(sg, ncol, j, mc);
     const T  e1_1 = tb.cends[(1 * 4 + 1) * (long long)ny + j];
     const T* ze   = sg->zend + j;
-    T*       bs   = sg->bsep + j;
     const T* in   = sg->in;
-    T*       out  = sg->out;
-    T        yprev = 0;
-    for (int p0 = 0; p0 < P; p0 += kAhead)
+    T*       bs   = sg->bsep + j;  // y_p, then x_p (the correction pass reads x)
+    T*       wk   = sg->work + j;  // A_p of y_p = A_p y_{p-1} + B_p
+
+    // forward maps of the range: A_p = -lower inv_p, B_p = rhs_p inv_p (B kept in bs), composed in (ca, cb)
+    T ca = 1, cb = 0;
+    for (int p0 = pb; p0 < pe; p0 += kAhead)
     {
-        T rhs_v[kAhead], id_v[kAhead];
+        T rhs_v[kAhead], inv_v[kAhead];
 #pragma unroll
         for (int q = 0; q < kAhead; ++q)
         {
             const int p = p0 + q;
-            if (p < P)
+            if (p >= pe) break;
+            const int isep = p * kChunk + kChunk - 1;
+            T r = mod_rhs(sg, nrow, ncol, mc, isep, j, in[(long long)isep * ny + j]) - ze[(long long)(2 * p + 1) * ny];
+            if (p < P - 1) r -= ze[(long long)(2 * (p + 1)) * ny];
+            rhs_v[q] = r;
+            if (p < P - 1) inv_v[q] = tb.sid[(long long)p * ny + j];
+            else  // last row: no next chunk, x+ Neumann end
             {
-                const int isep = p * kChunk + kChunk - 1;
-                T r = mod_rhs(sg, nrow, ncol, mc, isep, j, in[(long long)isep * ny + j]) - ze[(long long)(2 * p + 1) * ny];
-                if (p < P - 1) r -= ze[(long long)(2 * (p + 1)) * ny];
-                rhs_v[q] = r;
-                id_v[q]  = p < P - 1 ? tb.sid[(long long)p * ny + j] : (T)0;
+                const T lower = p > 0 ? -e1_1 : (T)0;
+                const T diag  = (tb.end_neu ? tb.dsep[j] + (T)1 : tb.dsep[j]) -
+                               (p == 0 ? tb.cends[(0 * 4 + 3) * (long long)ny + j] : tb.cends[(1 * 4 + 3) * (long long)ny + j]);
+                inv_v[q] = (T)1 / (diag - lower * (p > 0 ? tb.scp[(long long)(p - 1) * ny + j] : (T)0));
             }
         }
 #pragma unroll
         for (int q = 0; q < kAhead; ++q)
         {
             const int p = p0 + q;
-            if (p >= P) break;
-            const T lower = p > 0 ? -e1_1 : (T)0;
-            T       inv   = id_v[q];
-            if (p == P - 1)  // last row: no next chunk, x+ Neumann end
+            if (p >= pe) break;
+            const T A = p > 0 ? e1_1 * inv_v[q] : (T)0;  // -lower inv
+            const T B = rhs_v[q] * inv_v[q];
+            if (act)
             {
-                const T diag = (tb.end_neu ? tb.dsep[j] + (T)1 : tb.dsep[j]) -
-                               (p == 0 ? tb.cends[(0 * 4 + 3) * (long long)ny + j] : tb.cends[(1 * 4 + 3) * (long long)ny + j]);
-                inv = (T)1 / (diag - lower * (p > 0 ? tb.scp[(long long)(p - 1) * ny + j] : (T)0));
+                wk[(long long)p * ny] = A;
+                bs[(long long)p * ny] = B;
             }
-            yprev                 = (rhs_v[q] - lower * yprev) * inv;
-            bs[(long long)p * ny] = yprev;
+            cb = A * cb + B;
+            ca = A * ca;
         }
     }
-    // back substitution, its loads issued ahead in groups as well
-    T x = bs[(long long)(P - 1) * ny];
-    out[(long long)(nx - 1) * ny + j] = x;
-    for (int p1 = P - 2; p1 >= 0; p1 -= kAhead)
+    sa[w][lane] = ca;
+    sb[w][lane] = cb;
+    __syncthreads();
+    T y = 0;  // y_{pb-1}
+    for (int v = 0; v < w; ++v) y = sa[v][lane] * y + sb[v][lane];
+    for (int p = pb; p < pe; ++p)
     {
-        T yv[kAhead], cv[kAhead];
-#pragma unroll
-        for (int q = 0; q < kAhead; ++q)
+        const T A = act ? wk[(long long)p * ny] : (T)0, B = act ? bs[(long long)p * ny] : (T)0;
+        y         = A * y + B;
+        if (act) bs[(long long)p * ny] = y;
+    }
+    __syncthreads();  // every warp has read the forward compositions
+
+    // back substitution maps x_p = -c_p x_{p+1} + y_p (c_{P-1} = 0), composed from the top of the range down
+    ca = 1;
+    cb = 0;
+    for (int p = pe - 1; p >= pb; --p)
+    {
+        const T c  = p < P - 1 ? tb.scp[(long long)p * ny + j] : (T)0;
+        const T yp = act ? bs[(long long)p * ny] : (T)0;
+        cb         = -c * cb + yp;
+        ca         = -c * ca;
+    }
+    sa[w][lane] = ca;
+    sb[w][lane] = cb;
+    __syncthreads();
+    T x = 0;  // x_{pe}
+    for (int v = kRedWarps - 1; v > w; --v) x = sa[v][lane] * x + sb[v][lane];
+    for (int p = pe - 1; p >= pb; --p)
+    {
+        const T c  = p < P - 1 ? tb.scp[(long long)p * ny + j] : (T)0;
+        const T yp = act ? bs[(long long)p * ny] : (T)0;
+        x          = yp - c * x;
+        if (act)
         {
-            const int p = p1 - q;
-            if (p >= 0)
-            {
-                yv[q] = bs[(long long)p * ny];
-                cv[q] = tb.scp[(long long)p * ny + j];
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kAhead; ++q)
-        {
-            const int p = p1 - q;
-            if (p < 0) break;
-            x                     = yv[q] - cv[q] * x;
-            bs[(long long)p * ny] = x;  // the correction pass reads the separator solution
-            out[(long long)(p * kChunk + kChunk - 1) * ny + j] = x;
+            bs[(long long)p * ny] = x;
+            sg->out[(long long)(p * kChunk + kChunk - 1) * ny + j] = x;
         }
     }
 }
@@ -1572,7 +1604,7 @@ template <typename TS> void BatchImpl<TS>::build_chase_lists()
         for (auto& c : v)
         {
             a.push_back(((long long)(c.nx / kChunk) * c.ny + bt - 1) / bt);
-            b.push_back((c.ny + 127) / 128);
+            b.push_back((c.ny + 31) / 32);
         }
         lc.set(v, a);
         red.set(v, b);
@@ -1588,7 +1620,7 @@ template <typename TS> void BatchImpl<TS>::chase_run(const Segments& lc, const S
     const ChaseTabDev<TS>* tabs = tabs_dev_.as<ChaseTabDev<TS>>();
     k_b_chase_local<TS><<<(unsigned)lc.total, tm_.chase_threads, 0, s>>>(lc.as<ChaseSeg<TS>>(), lc.pre(), lc.n, tabs);
     FPB_CHECK_LAUNCH();
-    k_b_chase_reduced<TS><<<(unsigned)red.total, 128, 0, s>>>(red.as<ChaseSeg<TS>>(), red.pre(), red.n, tabs);
+    k_b_chase_reduced<TS><<<(unsigned)red.total, 32 * kRedWarps, 0, s>>>(red.as<ChaseSeg<TS>>(), red.pre(), red.n, tabs);
     FPB_CHECK_LAUNCH();
     k_b_chase_correct<TS><<<(unsigned)lc.total, tm_.chase_threads, 0, s>>>(lc.as<ChaseSeg<TS>>(), lc.pre(), lc.n, tabs);
     FPB_CHECK_LAUNCH();
