@@ -197,7 +197,6 @@ __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __rest
 // range, the CTA combines the compositions of the ranges before (after) it through shared memory, and the
 // warp walks its range from that incoming value. The dependent chain per thread is P / kRedWarps maps per
 // sweep instead of P memory round trips; the maps are the sequential ones, composed in another order.
-constexpr int kRedWarps = 8;
 
 template <typename T>
 __global__ void __launch_bounds__(32 * kRedWarps) k_b_chase_reduced(const ChaseSeg<T>* __restrict__ segs,

@@ -165,82 +165,113 @@ __global__ void __launch_bounds__(256) k_chase_local(T* __restrict__ f, int nx, 
 
 // Separator system per (field, wavenumber). ends: [type][4][j] = g_first, g_last, h_first, h_last.
 // Its matrix depends on the wavenumber only, so the Thomas factors of every row but the last are tabulated
-// (scp: c_p, sid: 1 / den_p; see separator_factors); per solve the recurrence is y_p = (rhs_p - lower y_{p-1})
-// sid_p and x_p = y_p - c_p x_{p+1}, its loads issued ahead in groups of kAhead. The last row (which
-// depends on P and the x+ Neumann end) is formed here from c_{P-2}.
+// (scp: c_p, sid: 1 / den_p; see separator_factors); the last row (which depends on P and the x+ Neumann
+// end) is formed here from c_{P-2}. Per solve the forward elimination y_p = (rhs_p - lower y_{p-1}) sid_p
+// and the back substitution x_p = y_p - c_p x_{p+1} are affine recurrences along p, evaluated as a blocked
+// scan: a CTA takes 32 wavenumbers of one field (lane = j, every access coalesced along j) and splits the
+// separators into kRedWarps contiguous ranges, one per warp; each warp composes the maps of its range, the
+// CTA combines the compositions of the ranges before (after) it through shared memory, and the warp walks
+// its range from that incoming value. work: P values per (field, wavenumber), the forward map slopes.
+constexpr int kRedWarps = 8;
+
 template <typename T>
-__global__ void k_chase_reduced(T* __restrict__ f, int nx, int ny, long long batch, const T* __restrict__ ends,
-                                const T* __restrict__ dsep, int end_neumann, const T* __restrict__ zend,
-                                T* __restrict__ bsep, const T* __restrict__ scp, const T* __restrict__ sid,
-                                int skip_last)
+__global__ void __launch_bounds__(32 * kRedWarps) k_chase_reduced(T* __restrict__ f, int nx, int ny, long long batch,
+                                                                  const T* __restrict__ ends, const T* __restrict__ dsep,
+                                                                  int end_neumann, const T* __restrict__ zend,
+                                                                  T* __restrict__ bsep, T* __restrict__ work,
+                                                                  const T* __restrict__ scp, const T* __restrict__ sid,
+                                                                  int skip_last)
 {
     constexpr int   kAhead = 8;
-    const long long t      = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= batch * ny) return;
-    const int j = (int)(t % ny);
-    if (skip_last && j == ny - 1) return;
-    const long long b = t / ny;
-    const int       P = nx / kChunk;
-    const T  e1_1 = ends[(1 * 4 + 1) * (long long)ny + j];
-    const T* ze   = zend + b * (long long)P * 2 * ny + j;
-    T*       bs   = bsep + b * (long long)P * ny + j;  // forward values y_p, then the solution B_p
-    T*       fb   = f + b * (long long)nx * ny + j;
-    T        yprev = 0;
-    for (int p0 = 0; p0 < P; p0 += kAhead)
+    __shared__ T    sa[kRedWarps][32], sb[kRedWarps][32];
+    const int       tiles = (ny + 31) / 32;
+    const long long b     = blockIdx.x / tiles;
+    if (b >= batch) return;  // uniform over the CTA
+    const int  lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int  j0   = (int)(blockIdx.x % tiles) * 32 + lane;
+    const bool act  = j0 < ny && !(skip_last && j0 == ny - 1);
+    const int  j    = j0 < ny ? j0 : 0;  // idle lanes compute on column 0 and store nothing
+    const int  P    = nx / kChunk;
+    const int  per  = (P + kRedWarps - 1) / kRedWarps;
+    const int  pb = min(P, w * per), pe = min(P, pb + per);
+    const T    e1_1 = ends[(1 * 4 + 1) * (long long)ny + j];
+    const T*   ze   = zend + b * (long long)P * 2 * ny + j;
+    T*         bs   = bsep + b * (long long)P * ny + j;  // B_p, then y_p, then the solution x_p
+    T*         wk   = work + b * (long long)P * ny + j;  // A_p of y_p = A_p y_{p-1} + B_p
+    T*         fb   = f + b * (long long)nx * ny + j;
+
+    T ca = 1, cb = 0;
+    for (int p0 = pb; p0 < pe; p0 += kAhead)
     {
-        T rhs_v[kAhead], id_v[kAhead];
+        T rhs_v[kAhead], inv_v[kAhead];
 #pragma unroll
         for (int q = 0; q < kAhead; ++q)
         {
             const int p = p0 + q;
-            if (p < P)
+            if (p >= pe) break;
+            T r = fb[(long long)(p * kChunk + kChunk - 1) * ny] - ze[(long long)(2 * p + 1) * ny];
+            if (p < P - 1) r -= ze[(long long)(2 * (p + 1)) * ny];
+            rhs_v[q] = r;
+            if (p < P - 1) inv_v[q] = sid[(long long)p * ny + j];
+            else  // last row: no next chunk, x+ Neumann end
             {
-                T r = fb[(long long)(p * kChunk + kChunk - 1) * ny] - ze[(long long)(2 * p + 1) * ny];
-                if (p < P - 1) r -= ze[(long long)(2 * (p + 1)) * ny];
-                rhs_v[q] = r;
-                id_v[q]  = p < P - 1 ? sid[(long long)p * ny + j] : (T)0;
+                const T lower = p > 0 ? -e1_1 : (T)0;
+                const T diag  = (end_neumann ? dsep[j] + (T)1 : dsep[j]) -
+                               (p == 0 ? ends[(0 * 4 + 3) * (long long)ny + j] : ends[(1 * 4 + 3) * (long long)ny + j]);
+                inv_v[q] = (T)1 / (diag - lower * (p > 0 ? scp[(long long)(p - 1) * ny + j] : (T)0));
             }
         }
 #pragma unroll
         for (int q = 0; q < kAhead; ++q)
         {
             const int p = p0 + q;
-            if (p >= P) break;
-            const T lower = p > 0 ? -e1_1 : (T)0;
-            T       inv   = id_v[q];
-            if (p == P - 1)  // last row: no next chunk, x+ Neumann end
+            if (p >= pe) break;
+            const T A = p > 0 ? e1_1 * inv_v[q] : (T)0;  // -lower inv
+            const T B = rhs_v[q] * inv_v[q];
+            if (act)
             {
-                const T diag = (end_neumann ? dsep[j] + (T)1 : dsep[j]) -
-                               (p == 0 ? ends[(0 * 4 + 3) * (long long)ny + j] : ends[(1 * 4 + 3) * (long long)ny + j]);
-                inv = (T)1 / (diag - lower * (p > 0 ? scp[(long long)(p - 1) * ny + j] : (T)0));
+                wk[(long long)p * ny] = A;
+                bs[(long long)p * ny] = B;
             }
-            yprev                 = (rhs_v[q] - lower * yprev) * inv;
-            bs[(long long)p * ny] = yprev;
+            cb = A * cb + B;
+            ca = A * ca;
         }
     }
-    // back substitution, its loads issued ahead in groups as well
-    T x = bs[(long long)(P - 1) * ny];
-    fb[(long long)(nx - 1) * ny] = x;
-    for (int p1 = P - 2; p1 >= 0; p1 -= kAhead)
+    sa[w][lane] = ca;
+    sb[w][lane] = cb;
+    __syncthreads();
+    T y = 0;  // y_{pb-1}
+    for (int v = 0; v < w; ++v) y = sa[v][lane] * y + sb[v][lane];
+    for (int p = pb; p < pe; ++p)
     {
-        T yv[kAhead], cv[kAhead];
-#pragma unroll
-        for (int q = 0; q < kAhead; ++q)
+        const T A = act ? wk[(long long)p * ny] : (T)0, B = act ? bs[(long long)p * ny] : (T)0;
+        y         = A * y + B;
+        if (act) bs[(long long)p * ny] = y;
+    }
+    __syncthreads();  // every warp has read the forward compositions
+
+    ca = 1;
+    cb = 0;
+    for (int p = pe - 1; p >= pb; --p)  // x_p = -c_p x_{p+1} + y_p, c_{P-1} = 0
+    {
+        const T c  = p < P - 1 ? scp[(long long)p * ny + j] : (T)0;
+        const T yp = act ? bs[(long long)p * ny] : (T)0;
+        cb         = -c * cb + yp;
+        ca         = -c * ca;
+    }
+    sa[w][lane] = ca;
+    sb[w][lane] = cb;
+    __syncthreads();
+    T x = 0;  // x_{pe}
+    for (int v = kRedWarps - 1; v > w; --v) x = sa[v][lane] * x + sb[v][lane];
+    for (int p = pe - 1; p >= pb; --p)
+    {
+        const T c  = p < P - 1 ? scp[(long long)p * ny + j] : (T)0;
+        const T yp = act ? bs[(long long)p * ny] : (T)0;
+        x          = yp - c * x;
+        if (act)
         {
-            const int p = p1 - q;
-            if (p >= 0)
-            {
-                yv[q] = bs[(long long)p * ny];
-                cv[q] = scp[(long long)p * ny + j];
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kAhead; ++q)
-        {
-            const int p = p1 - q;
-            if (p < 0) break;
-            x                     = yv[q] - cv[q] * x;
-            bs[(long long)p * ny] = x;  // the correction pass reads the separator solution
+            bs[(long long)p * ny]                          = x;  // the correction pass reads it
             fb[(long long)(p * kChunk + kChunk - 1) * ny] = x;
         }
     }

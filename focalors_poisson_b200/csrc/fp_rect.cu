@@ -325,10 +325,10 @@ template <typename T> void DevRect<T>::chase(T* f, long long batch, T* scr, cuda
     const long long nl   = batch * P * ny;
     k_chase_local<T><<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(f, nx, ny, batch, cc.as<T>(), zend, skip);
     FPB_CHECK_LAUNCH();
-    const long long nr = batch * ny;
-    k_chase_reduced<T><<<(unsigned)((nr + 127) / 128), 128, 0, s>>>(f, nx, ny, batch, cends.as<T>(), dsep.as<T>(),
-                                                                   end_neumann ? 1 : 0, zend, bsep,
-                                                                   sep_cp.as<T>(), sep_iden.as<T>(), skip);
+    const long long nr = batch * ((ny + 31) / 32);  // CTAs: 32 wavenumbers of one field each
+    k_chase_reduced<T><<<(unsigned)nr, 32 * kRedWarps, 0, s>>>(f, nx, ny, batch, cends.as<T>(), dsep.as<T>(),
+                                                               end_neumann ? 1 : 0, zend, bsep, work,
+                                                               sep_cp.as<T>(), sep_iden.as<T>(), skip);
     FPB_CHECK_LAUNCH();
     k_chase_correct<T><<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(f, nx, ny, batch, cg.as<T>(), chh.as<T>(), bsep,
                                                                    skip);
