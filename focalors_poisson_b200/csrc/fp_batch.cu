@@ -413,7 +413,7 @@ struct BIface
 
 // Dense products of the interface solve run as 32-row tiles x column chunks, 8 warps per tile splitting
 // the chunk's columns; partial sums are added in a fixed order by the finishing kernel (reproducible).
-constexpr int kIfTile = 32, kIfWarps = 8, kIfChunkYY = 1024, kIfChunkYX = 512;
+constexpr int kIfTile = 32, kIfWarps = 8, kIfChunkYY = 1024, kIfChunkYX = 128;
 
 __device__ __forceinline__ double chi_edge(int n, int m, int i) { return dst_basis(n, m, i); }
 
@@ -526,14 +526,21 @@ __global__ void __launch_bounds__(256) k_if_yx_part(const BIface* __restrict__ P
     const int     tile = b / F.yx_chunks, chunk = b - tile * F.yx_chunks;
     const int     lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int     k    = tile * kIfTile + lane;
-    const int     m1   = min(F.nx, (chunk + 1) * kIfChunkYX);
-    double        acc[4] = {0, 0, 0, 0};
-    if (k < F.ny)
+    const int     nx = F.nx, ny = F.ny, nxe = F.nxe, nye = F.nye;
+    const int     m1   = min(nx, (chunk + 1) * kIfChunkYX);
+    const double* Kp   = F.K;
+    const double* wxy  = F.wxy;
+    double        acc[4] = {0, 0, 0, 0};  // [e*2+Y], static indices so they stay in registers
+    if (k < ny)
+#pragma unroll 4
         for (int m = chunk * kIfChunkYX + warp; m < m1; m += kIfWarps)
         {
-            const double Kmk = F.K[(long long)m * F.ny + k];
-            for (int e = 0; e < F.nxe; ++e)
-                for (int Y = 0; Y < F.nye; ++Y) acc[e * 2 + Y] += Kmk * F.wxy[(e * 2 + Y) * F.nx + m];
+            const double Kmk = Kp[(long long)m * ny + k];
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+#pragma unroll
+                for (int Y = 0; Y < 2; ++Y)
+                    if (e < nxe && Y < nye) acc[e * 2 + Y] += Kmk * wxy[(e * 2 + Y) * nx + m];
         }
     for (int i = 0; i < 4; ++i) red[warp][i][lane] = acc[i];
     __syncthreads();
