@@ -53,8 +53,11 @@ struct DstSeg
 // One work item = the rows one FFT carries (two for the pairing families) of one segment.
 // ACC: out (FP64) += result instead of out = result. plans: two argument sets per plan (forward, inverse).
 // DD and DN run their inverse with INV = 0 and the forward arguments (they are their own transposes).
+// Register cap: the arguments are read through a global pointer here (not from the parameter bank as in
+// k_transform), and uncapped the FP64 instances take 104-110 registers, which allows only 2 CTAs of 256
+// threads per SM; at 80 (16 bytes of spill) three fit, as many as their shared memory allows.
 template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC>
-__global__ void __launch_bounds__(512) k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix,
+__global__ void __maxnreg__(sizeof(T) == 8 ? 80 : 64) k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix,
                                                  int nseg, long long nitems, const XformArgs<T>* __restrict__ plans)
 {
     typedef typename Cplx<T>::type T2;
