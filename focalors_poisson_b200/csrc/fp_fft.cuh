@@ -168,8 +168,33 @@ template <int R, typename T2> __device__ __forceinline__ void dft(T2* x)
     else dft8(x);
 }
 
+// x[q] *= w^q for q = 1..R-1: odd powers w^(2j+1) = w^(2j-1) w^2 and even powers w^(2j) = w^(2j-2) w^2 as two
+// interleaved chains, depth R/2 instead of R-2, three powers live (a few ulp either way).
+template <int R, typename T2> __device__ __forceinline__ void rotate_legs(T2* x, T2 w1)
+{
+    x[1] = cmul(x[1], w1);
+    if (R == 2) return;
+    const T2 w2 = cmul(w1, w1);
+    T2       wo = w1, we = w2;
+    x[2]        = cmul(x[2], w2);
+#pragma unroll
+    for (int q = 3; q < R; ++q)
+    {
+        if (q & 1)
+        {
+            wo   = cmul(wo, w2);
+            x[q] = cmul(x[q], wo);
+        }
+        else
+        {
+            we   = cmul(we, w2);
+            x[q] = cmul(x[q], we);
+        }
+    }
+}
+
 // Leg q of butterfly b is rotated by w^q, w = exp(-2 pi i b / B): one table load per butterfly, the
-// powers by repeated multiplication (w^2 = w w, w^3 = w^2 w, ...; at most 7 products, a few ulp).
+// powers from it by rotate_legs.
 // ld(k) supplies element k, sto(k, v) takes the result for element k: shared memory for an ordinary
 // stage, the input pre-processing or the output post-processing for the fused first / last stages.
 template <int R, bool DIT, typename T2, typename LD, typename ST>
@@ -186,27 +211,9 @@ __device__ __forceinline__ void stage_radix_io(const FftStage st, int nbf, const
         for (int q = 0; q < R; ++q) x[q] = ld(base + q * st.S);
         const bool rot = b != 0;
         T2         w1  = rot ? __ldg(tw + st.tw_off + b) : mk<T2>(1, 0);
-        if (DIT && rot)
-        {
-            T2 wq = w1;
-#pragma unroll
-            for (int q = 1; q < R; ++q)
-            {
-                x[q] = cmul(x[q], wq);
-                wq   = cmul(wq, w1);
-            }
-        }
+        if (DIT && rot) rotate_legs<R>(x, w1);
         dft<R>(x);
-        if (!DIT && rot)
-        {
-            T2 wq = w1;
-#pragma unroll
-            for (int q = 1; q < R; ++q)
-            {
-                x[q] = cmul(x[q], wq);
-                wq   = cmul(wq, w1);
-            }
-        }
+        if (!DIT && rot) rotate_legs<R>(x, w1);
 #pragma unroll
         for (int q = 0; q < R; ++q) sto(base + q * st.S, x[q]);
     }

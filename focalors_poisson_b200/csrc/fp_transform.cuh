@@ -466,8 +466,9 @@ __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN*
     __syncthreads();
 }
 
+// Register cap (FP64 80): three CTAs of 256 threads per SM, as many as a 4096-point FP64 buffer allows.
 template <typename T, int KIND, int INV, typename TIO = T>
-__global__ void __launch_bounds__(512) k_transform(const TransformArgs<T, TIO> a)
+__global__ void __maxnreg__(sizeof(T) == 8 ? 80 : 64) k_transform(const TransformArgs<T, TIO> a)
 {
     typedef typename Cplx<T>::type T2;
     extern __shared__ __align__(16) unsigned char fp_smem_raw[];
