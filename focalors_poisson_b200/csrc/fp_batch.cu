@@ -1932,6 +1932,10 @@ int BatchImpl<TS>::refine(double* const* fields, const double* const* ghosts, do
     std::vector<double> hp((size_t)2 * nb);
     double              change = 1.0;
     int                 steps  = 0;
+    // With more than one step allowed, the first solution goes straight into u: its "correction" is the
+    // whole solution (change 1), so the add-and-norms pass would only copy it. With one step the pass
+    // stays, for its check of the solution's values.
+    const bool direct_first = max_refine > 1;
     while (steps < max_refine)
     {
         if (steps == 0 && first)
@@ -1941,12 +1945,22 @@ int BatchImpl<TS>::refine(double* const* fields, const double* const* ghosts, do
             for (size_t g = 0; g < dom_.size(); ++g)
             {
                 fi[g] = fs_.as<double>() + dom_[g].off;
-                ro[g] = r_.as<double>() + dom_[g].off;
+                ro[g] = (direct_first ? u_ : r_).as<double>() + dom_[g].off;
             }
-            first->solve_assembled(fi.data(), ro.data(), s);  // r <- first solution
+            first->solve_assembled(fi.data(), ro.data(), s);  // u (or r) <- first solution
         }
+        else if (steps == 0)
+            inner(dst_fs_, direct_first ? dst_out_u_ : dst_out_r_, false, s);
         else
-            inner(steps == 0 ? dst_fs_ : dst_r_, dst_out_r_, false, s);  // r <- correction
+            inner(dst_r_, dst_out_r_, false, s);  // r <- correction
+        if (steps == 0 && direct_first)
+        {
+            ++steps;
+            change = 1.0;
+            k_b_residual<<<(unsigned)res_.total, 256, 0, s>>>(res_.as<ResSeg>(), res_.pre(), res_.n);
+            FPB_CHECK_LAUNCH();
+            continue;
+        }
         k_b_add_norms<<<(unsigned)addn_.total, 256, 0, s>>>(addn_.as<AddSeg>(), addn_.pre(), addn_.n, steps == 0);
         FPB_CHECK_LAUNCH();
         ++steps;
