@@ -695,7 +695,7 @@ __global__ void k_myy(const BIface F, const double* H /* 2x2 blocks per m: H[(Y*
 // Elementwise over many subdomains
 // ---------------------------------------------------------------------------------------------
 constexpr int kAsmCells  = 1024;  // cells per block of k_b_assemble
-constexpr int kElemCells = 1024;  // cells per block of the residual, add-with-norms and copy kernels
+constexpr int kElemCells = 1024;  // cells per block of the residual and add-with-norms kernels
 
 struct AsmSeg
 {
@@ -799,20 +799,6 @@ __global__ void __launch_bounds__(256) k_b_add_norms(const AddSeg* __restrict__ 
     }
 }
 
-struct CopySeg
-{
-    double*       dst;
-    const double* src;
-    long long     n;
-};
-__global__ void k_b_copy(const CopySeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg)
-{
-    const int      s  = seg_of(prefix, nseg, blockIdx.x);
-    const CopySeg* sg = segs + s;
-    const long long t0 = (blockIdx.x - prefix[s]) * (long long)kElemCells;
-    const long long t1 = t0 + kElemCells < sg->n ? t0 + kElemCells : sg->n;
-    for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) sg->dst[t] = sg->src[t];
-}
 
 }  // namespace fpb
 
@@ -1029,7 +1015,7 @@ private:
     std::map<std::pair<int, double>, int>     tab_index_;
     std::vector<std::unique_ptr<DevRect<TS>>> tabs_;
     DevBuf                                    tabs_dev_;
-    DevBuf                                    W_, X_, fs_, u_, r_, chs_;  // work, chase out, IR, chase scratch
+    DevBuf                                    W_, X_, fs_, r_, chs_;  // work, chase out, IR, chase scratch
     DevBuf                                    edge_;  // bY, gYp, sYp, yYp per y-edge (nx each), per problem
     std::vector<ChaseSeg<TS>>                 chase1_leaf_, chase1_root_, chase2_all_;
     Segments                                  l1_lc_, l1_red_, r1_lc_, r1_red_, a2_lc_, a2_red_;
@@ -1040,7 +1026,7 @@ private:
     std::vector<DstSeg>                       dst_W_in_rec_, dst_X_out_rec_;
     std::vector<int>                          dst_kinds_;
     XList                                     dst_fs_, dst_r_, dst_out_u_, dst_out_r_, dst_user_in_, dst_user_out_;
-    Segments                                  res_, asm_user_, copy_out_;
+    Segments                                  res_, asm_user_;
     Segments                                  addn_;  // u += r with norms (adaptive refinement)
     DevBuf                                    addp_;
     std::map<std::tuple<int, int, int>, DevBuf> basis_;  // y-basis column tables (family, n, column)
@@ -1720,48 +1706,50 @@ void BatchImpl<TS>::set_user_lists(double* const* fields, const double* const* g
     if (ir && !fs_.get())
     {
         fs_.alloc((size_t)cells_ * 8);
-        u_.alloc((size_t)cells_ * 8);
         r_.alloc((size_t)cells_ * 8);
         // IR lists between internal buffers
-        std::vector<DstSeg> a = dst_W_in_rec_, b = dst_W_in_rec_, c = dst_X_out_rec_;
+        std::vector<DstSeg> a = dst_W_in_rec_, b = dst_W_in_rec_;
         for (size_t g = 0; g < dom_.size(); ++g)
         {
-            a[g].in  = fs_.as<double>() + dom_[g].off;
-            b[g].in  = r_.as<double>() + dom_[g].off;
-            c[g].out = u_.as<double>() + dom_[g].off;
+            a[g].in = fs_.as<double>() + dom_[g].off;
+            b[g].in = r_.as<double>() + dom_[g].off;
         }
         dst_fs_.set(a, dst_kinds_, plans_);
         dst_r_.set(b, dst_kinds_, plans_);
-        dst_out_u_.set(c, dst_kinds_, plans_);
         std::vector<DstSeg> d = dst_X_out_rec_;
         for (size_t g = 0; g < dom_.size(); ++g) d[g].out = r_.as<double>() + dom_[g].off;
         dst_out_r_.set(d, dst_kinds_, plans_);
-        std::vector<AddSeg>    ad;
-        std::vector<long long> acn;
-        long long              nb = 0;
+        long long nb = 0;
         for (size_t g = 0; g < dom_.size(); ++g) nb += (dom_[g].d.cells() + kElemCells - 1) / kElemCells;
         addp_.alloc((size_t)2 * nb * 8);
-        long long b0 = 0;
-        for (size_t g = 0; g < dom_.size(); ++g)
+    }
+    if (ir)  // the iterate u lives in the caller's fields (their right-hand sides are in fs once assembled)
+    {
+        std::vector<DstSeg> c = dst_X_out_rec_;
+        for (int g = 0; g < nd; ++g) c[g].out = f[g];
+        dst_out_u_.set(c, dst_kinds_, plans_);
+        const long long        nb = (long long)(addp_.bytes() / 16);
+        std::vector<AddSeg>    ad;
+        std::vector<long long> acn;
+        long long              b0 = 0;
+        for (int g = 0; g < nd; ++g)
         {
             const long long blocks = (dom_[g].d.cells() + kElemCells - 1) / kElemCells;
-            ad.push_back({u_.as<double>() + dom_[g].off, r_.as<double>() + dom_[g].off, dom_[g].d.cells(),
-                          addp_.as<double>() + b0, addp_.as<double>() + nb + b0});
+            ad.push_back({f[g], r_.as<double>() + dom_[g].off, dom_[g].d.cells(), addp_.as<double>() + b0,
+                          addp_.as<double>() + nb + b0});
             acn.push_back(blocks);
             b0 += blocks;
         }
         addn_.set(ad, acn);
         std::vector<ResSeg>    rs;
         std::vector<long long> rc;
-        for (size_t g = 0; g < dom_.size(); ++g) rs.push_back(res_seg(g, r_.as<double>(), fs_.as<double>(), nullptr));
+        for (int g = 0; g < nd; ++g) rs.push_back(res_seg(g, r_.as<double>(), fs_.as<double>(), f.data()));
         for (auto& q : rs) rc.push_back((q.a.nx * (long long)q.a.ny + kElemCells - 1) / kElemCells);
         res_.set(rs, rc);
     }
     std::vector<AsmSeg>    as;
     std::vector<long long> ac;
     std::vector<DstSeg>    di = dst_W_in_rec_, dout = dst_X_out_rec_;
-    std::vector<CopySeg>   cp;
-    std::vector<long long> cc;
     for (int g = 0; g < nd; ++g)
     {
         const Domain& D = dom_[g].d;
@@ -1781,20 +1769,17 @@ void BatchImpl<TS>::set_user_lists(double* const* fields, const double* const* g
         ac.push_back((D.cells() + kAsmCells - 1) / kAsmCells);
         di[g].in   = f[g];
         dout[g].out = f[g];
-        cp.push_back({f[g], ir ? u_.as<double>() + dom_[g].off : nullptr, D.cells()});
-        cc.push_back((D.cells() + kElemCells - 1) / kElemCells);
     }
     asm_user_.set(as, ac);
     dst_user_in_.set(di, dst_kinds_, plans_);
     dst_user_out_.set(dout, dst_kinds_, plans_);
-    if (ir) copy_out_.set(cp, cc);
 }
 
 template <typename TS> ResSeg BatchImpl<TS>::res_seg(size_t g, double* r, const double* fs, const double* const* u_user)
 {
     const Domain& D = dom_[g].d;
     ResSeg        q{};
-    auto          U = [&](size_t h) -> const double* { return u_user ? u_user[h] : u_.as<double>() + dom_[h].off; };
+    auto          U = [&](size_t h) -> const double* { return u_user[h]; };
     q.r    = r ? r + dom_[g].off : nullptr;
     q.fs   = fs + dom_[g].off;
     q.u    = U(g);
@@ -1845,8 +1830,6 @@ template <typename TS> void BatchImpl<TS>::run(int steps, cudaStream_t s)
         FPB_CHECK_LAUNCH();
         inner(dst_r_, dst_out_u_, true, s);
     }
-    k_b_copy<<<(unsigned)copy_out_.total, 256, 0, s>>>(copy_out_.as<CopySeg>(), copy_out_.pre(), copy_out_.n);
-    FPB_CHECK_LAUNCH();
 }
 
 template <typename TS>
@@ -1945,7 +1928,7 @@ int BatchImpl<TS>::refine(double* const* fields, const double* const* ghosts, do
             for (size_t g = 0; g < dom_.size(); ++g)
             {
                 fi[g] = fs_.as<double>() + dom_[g].off;
-                ro[g] = (direct_first ? u_ : r_).as<double>() + dom_[g].off;
+                ro[g] = direct_first ? user_ptrs_[g] : r_.as<double>() + dom_[g].off;
             }
             first->solve_assembled(fi.data(), ro.data(), s);  // u (or r) <- first solution
         }
@@ -1984,8 +1967,6 @@ int BatchImpl<TS>::refine(double* const* fields, const double* const* ghosts, do
             FPB_CHECK_LAUNCH();
         }
     }
-    k_b_copy<<<(unsigned)copy_out_.total, 256, 0, s>>>(copy_out_.as<CopySeg>(), copy_out_.pre(), copy_out_.n);
-    FPB_CHECK_LAUNCH();
     if (rel_change) *rel_change = change;
     return steps;
 }
