@@ -143,7 +143,9 @@ int fp_composite_solve_f64(fp_composite* c, double* const* fields, const double*
  * the observed contraction predicts the error left after the last correction is below rel_tol) or
  * max_refine steps (FP_ERR_NOT_CONVERGED with FP_CHECK_CONVERGENCE if the target was missed).
  * With FP_IR_INNER_F64 the inner solves are the FP64 ones (refinement then only removes the single
- * FP64 solve's round-off, about eps * cond(A)). */
+ * FP64 solve's round-off, about eps * cond(A)). Device-resident fields hold the iterate while the
+ * refinement runs (their right-hand sides are kept in an assembled copy), so after an error they hold
+ * neither the right-hand side nor a finished solution. */
 #define FP_IR_INNER_F64 32
 /* With FP32 inner solves: make the first inner solve the FP64 one (its answer already carries only FP64
  * round-off, eps * cond(A)), so that one or two FP32 corrections finish the refinement. Spectral path only;
