@@ -220,7 +220,17 @@ __global__ void __launch_bounds__(32 * kRedWarps) k_b_chase_reduced(const ChaseS
     const ChaseTabDev<T> tb   = tabs[sg->tab];
     const int            nrow = sg->nrow, ncol = sg->ncol;
     ModCtx<T>            mc;
-    mod_init(sg, ncol, j, mc);
+    if (ncol > 0)  // column-term weights of the CTA's 32 wavenumbers: computed once (warp 0), shared
+    {
+        __shared__ double spsi[kMaxMods][32];
+        if (w == 0)
+        {
+            mod_init(sg, ncol, j, mc);
+            for (int c = 0; c < ncol; ++c) spsi[c][lane] = mc.psi[c];
+        }
+        __syncthreads();
+        for (int c = 0; c < ncol; ++c) mc.psi[c] = spsi[c][lane];
+    }
     const T  e1_1 = tb.cends[(1 * 4 + 1) * (long long)ny + j];
     const T* ze   = sg->zend + j;
     const T* in   = sg->in;
