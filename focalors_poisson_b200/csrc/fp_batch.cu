@@ -488,9 +488,12 @@ __global__ void __launch_bounds__(256) k_if_yy_part(const BIface* __restrict__ P
     const int     n    = F.nye * F.nx;
     const int     q    = tile * kIfTile + lane;
     const int     c1   = min(n, (chunk + 1) * kIfChunkYY);
+    const double* rinv = F.rinv;
+    const double* rhs  = F.rhsY;
     double        acc  = 0;
     if (q < n)
-        for (int c = chunk * kIfChunkYY + warp; c < c1; c += kIfWarps) acc += F.rinv[(long long)c * n + q] * F.rhsY[c];
+#pragma unroll 4
+        for (int c = chunk * kIfChunkYY + warp; c < c1; c += kIfWarps) acc += rinv[(long long)c * n + q] * rhs[c];
     red[warp][lane] = acc;
     __syncthreads();
     if (warp == 0 && q < n)

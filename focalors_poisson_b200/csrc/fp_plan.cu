@@ -250,8 +250,8 @@ KindTables kind_tables(int kind, int n)
     {
         case K_DD:  // poisson_fft2d.cpp:22; folding weights of the length-(n+1) DST-I
             t.s1 = std::sqrt(2.0 / (1. + n));
-            t.c.resize(n + 1);
-            for (int j = 0; j <= n; ++j) t.c[j] = cld(std::sin(kPi * (long double)j / (long double)(n + 1)), 0.0L);
+            t.a.resize(n + 1);
+            for (int j = 0; j <= n; ++j) t.a[j] = (double)std::sin(kPi * (long double)j / (long double)(n + 1));
             break;
         case K_NN:                                             // poisson_fft2d.cpp:81-90
             t.s1 = std::sqrt(2.0 / n);

@@ -76,10 +76,10 @@ HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftW
 struct KindTables
 {
     std::vector<double> a, b;  // NN: cos/sin(pi (j+1) / n / 2); ND: cos/sin(2 n pi (j+1) / (2n+1));
-                               // PP: cos/sin(pi (2j+1) / 4)
+                               // PP: cos/sin(pi (2j+1) / 4); DD: a = sin(pi j/(n+1)), j <= n (b empty)
     double s1 = 0, s2 = 0;     // DD: sqrt(2/(1+n)); NN: sqrt(2/n), sqrt(1/n); ND/DN: sqrt(4/(2n+1));
                                // PP: sqrt(2/n)
-    std::vector<std::complex<long double>> c;  // DD: sin(pi j/(n+1)), j <= n; NN: exp(-i pi m / 2n), m < n
+    std::vector<std::complex<long double>> c;  // NN: exp(-i pi m / 2n), m < n
 };
 KindTables kind_tables(int kind, int n);
 

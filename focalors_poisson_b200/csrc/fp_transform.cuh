@@ -35,9 +35,9 @@ template <typename T> struct XformArgs
     int           n;  // row length (ny)
     FftDesc       fd;
     FftTables<T2> ft;
-    const T*      ta;  // family table a (ND: cos, PP: cos)
+    const T*      ta;  // family table a (ND: cos, PP: cos, DD: sin(pi j/(N+1)) folding weights)
     const T*      tb;  // family table b (ND: sin, PP: sin)
-    const T2*     tc;  // DD: (sin(pi j/(N+1)), 0); NN: exp(-i pi m / 2N)
+    const T2*     tc;  // NN: exp(-i pi m / 2N)
     T             s1, s2;
 };
 
@@ -65,7 +65,7 @@ __device__ __forceinline__ T real_input(const TA& a, const TIO* f, int i)
     {
         if (i == 0) return (T)0;
         const T xj = (T)f[i - 1], xm = (T)f[n - i];  // x_j, x_{L-j}
-        return a.tc[i].x * (xj + xm) + (T)0.5 * (xj - xm);
+        return __ldg(a.ta + i) * (xj + xm) + (T)0.5 * (xj - xm);
     }
     if (KIND == 1)  // NN forward: Makhoul reordering
         return (T)((2 * i < n) ? f[2 * i] : f[2 * n - 1 - 2 * i]);
