@@ -1,11 +1,10 @@
 // fp_rect_solve_f64_noalloc: the rectangle solve for callers that must not allocate device memory at
-// solve time, e.g. code inside a CUDA stream capture (cudaMalloc/cudaFree are not capturable and would
-// break the capture), or code whose device memory is owned by another allocator (a framework's caching
-// allocator, a fixed memory budget) where a library cudaMalloc would either fail or synchronise the
-// device behind that allocator's back.
+// solve time: code whose device memory is owned by another allocator (a framework's caching allocator,
+// a fixed memory budget), where a library cudaMalloc would either fail or synchronise the device behind
+// that allocator's back.
 //
 // The partition chase of fp_rect_solve_f64 keeps per-call scratch (chunk end values, the separator
-// solution and its Thomas factors: 4 * batch * (nx/32) * ny doubles) in a buffer the plan grows with
+// solution and the slopes of the separator scan: 4 * batch * (nx/32) * ny doubles) in a buffer the plan grows with
 // cudaMalloc. This variant takes that scratch from one file-scope device array instead, so it calls no
 // allocator at all. Limits and sharing rules are stated next to the array below.
 #include "../../include/fp_capi.h"

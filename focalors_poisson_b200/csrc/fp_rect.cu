@@ -303,7 +303,7 @@ template <typename T> long long DevRect<T>::chase_scratch_elems(long long batch)
 {
     if (!chunked) return 0;
     const long long P = nx / kChunk;
-    return batch * P * ny * 4;  // chunk end values (2), separator solution (1), separator factors (1)
+    return batch * P * ny * 4;  // chunk end values (2), separator solution (1), separator scan slopes (1)
 }
 
 template <typename T> void DevRect<T>::chase(T* f, long long batch, T* scr, cudaStream_t s) const

@@ -71,10 +71,10 @@ int fp_rect_solve_f64(fp_rect* r, double* f, long long batch, int flags, void* s
 int fp_rect_solve_f32(fp_rect* r, float* f, long long batch, int flags, void* stream);
 int fp_rect_destroy(fp_rect* r);
 
-/* fp_rect_solve_f64 for callers that cannot allocate device memory when they solve: code running
- * inside a CUDA stream capture (allocation calls are not capturable) or under another allocator's
- * memory budget. No counterpart in the reference (its solve is host-only). Same result as
- * fp_rect_solve_f64 with FP_DEVICE: `f` is device memory, the work is queued on `stream`, nothing is
+/* fp_rect_solve_f64 for callers that cannot allocate device memory when they solve: code whose device
+ * memory belongs to another allocator (a framework's caching allocator, a fixed memory budget), where a
+ * library cudaMalloc would fail or synchronise the device behind that allocator. No counterpart in the
+ * reference (its solve is host-only). Same result as fp_rect_solve_f64 with FP_DEVICE: `f` is device memory, the work is queued on `stream`, nothing is
  * allocated or freed. Its scratch is one fixed device array of 2^21 doubles (16 MiB) that every GPU
  * loading the library holds until exit; solves needing more (4 * batch * (nx/32) * ny doubles when nx
  * is a multiple of 32, none otherwise) are rejected with FP_ERR_UNSUPPORTED. The first call on a

@@ -1,5 +1,5 @@
 """fp_rect_solve_f64_noalloc: the rectangle solve for callers that cannot allocate device memory when
-they solve (inside a CUDA stream capture, or under another allocator's budget). Its scratch is one fixed
+they solve (their device memory belongs to another allocator or a fixed budget). Its scratch is one fixed
 device array shared by every call; this checks it against the allocating entry point, fp_rect_solve_f64,
 on two calls in a row (the array keeps the previous call's contents), and that oversize solves are
 refused. Kept in a file pytest collects last."""
