@@ -98,3 +98,29 @@ def test_bluestein_tables_replay_dft(driver, kind, n):
     if kind == K_ND:
         assert len(p["i"]) == M  # the inverse window has its own kernel table
         assert (p["inv"]["in0"], p["inv"]["nin"], p["inv"]["out0"], p["inv"]["nout"]) == (1, 2 * n, 1, n)
+
+
+@pytest.mark.parametrize("kind", [K_DD, K_ND, K_DN])
+def test_bluestein_tables_batch_sizes(driver, kind):
+    """Row lengths of the batched workload (multiples of 32 in 64..1024): every Bluestein plan replays the DFT
+    on both windows, and its length is the cheapest smooth one at or above what the window needs."""
+    rng = np.random.default_rng(kind)
+    checked = 0
+    for n in range(64, 1025, 96):
+        p = plan(driver, kind, n)
+        f = p["fwd"]
+        if not f["blue"]:
+            continue
+        L, M = f["L"], f["M"]
+        full = f["nin"] == L and f["nout"] == L
+        need = 2 * L - 2 if full else max(f["nin"] + f["nout"], p["inv"]["nin"] + p["inv"]["nout"]) - 1
+        assert need <= M <= need + need // 2, (kind, n, M)
+        for tag, bhat in (("fwd", p["b"]), ("inv", p["i"] if len(p["i"]) else p["b"])):
+            w = p[tag]
+            z = np.zeros(L, complex)
+            z[w["in0"]: w["in0"] + w["nin"]] = rng.standard_normal(w["nin"]) + 1j * rng.standard_normal(w["nin"])
+            ref = np.fft.fft(z)[w["out0"]: w["out0"] + w["nout"]]
+            got = replay(p, w, bhat, z)
+            assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), (kind, n, tag)
+        checked += 1
+    assert checked >= 5
