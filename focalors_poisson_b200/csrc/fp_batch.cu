@@ -368,7 +368,20 @@ __global__ void k_b_colvals(const ColReq<T>* __restrict__ reqs, const long long*
     const int       i = (int)(w - prefix[q]);
     const T*        row = R.X + (long long)i * R.ny;
     double          acc = 0;
-    for (int k = lane; k < R.ny; k += 32) acc += (R.tab ? R.tab[k] : dst_basis(R.ny, k, R.j)) * (double)row[k];
+    constexpr int   U   = 8;  // elements per lane loaded ahead of the (in-order) accumulation
+    for (int k0 = lane; k0 < R.ny; k0 += 32 * U)
+    {
+        double xv[U], bv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int k = k0 + 32 * u;
+            xv[u]       = k < R.ny ? (double)row[k] : 0.0;
+            bv[u]       = k < R.ny ? (R.tab ? R.tab[k] : dst_basis(R.ny, k, R.j)) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc += bv[u] * xv[u];
+    }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if (lane == 0) R.out[i] = R.coef * acc;
 }
@@ -1424,10 +1437,21 @@ template <typename TS> void BatchImpl<TS>::build_spectral()
 // Null for DD, whose basis dst_basis() evaluates directly.
 template <typename TS> const double* BatchImpl<TS>::basis_col(int kind, int n, int j)
 {
-    if (kind == K_DD) return nullptr;
     auto key = std::make_tuple(kind, n, j);
     auto it  = basis_.find(key);
     if (it != basis_.end()) return it->second.template as<double>();
+    if (kind == K_DD)  // the DST-I basis in closed form, as dst_basis (sin in long double)
+    {
+        const long double   pi = 3.141592653589793238462643383279502884L;
+        const double        sc = std::sqrt(2.0 / (n + 1));
+        std::vector<double> e(n);
+        for (int k = 0; k < n; ++k)
+        {
+            const long long q = (long long)(k + 1) * (j + 1) % (2LL * (n + 1));
+            e[k]              = sc * (double)std::sin(pi * (long double)q / (long double)(n + 1));
+        }
+        return (basis_[key] = upload(e)).template as<double>();
+    }
     DevTransform<double> tr(kind, n);
     std::vector<double>  e(n, 0.0);
     e[j]      = 1.0;
@@ -1503,7 +1527,7 @@ template <typename TS> void BatchImpl<TS>::build_static_lists()
             const int  jl = L.leaf_face == YNEG ? 0 : L.d.ny - 1;
             l1.push_back(base_seg(g, W + L.off, X + L.off));
             lc.push_back({X + L.off, L.d.nx, L.d.ny, jl, ev(p, Y, 0), -1.0, basis_col(L.kind, L.d.ny, jl)});
-            rc.push_back({X + ro, F.nx, F.ny, F.jy[Y], ev(p, Y, 1), 1.0, nullptr});
+            rc.push_back({X + ro, F.nx, F.ny, F.jy[Y], ev(p, Y, 1), 1.0, basis_col(K_DD, F.ny, F.jy[Y])});
             eg.push_back({ev(p, Y, 1), F.gY + Y * F.nx, 1, eplans_.get(K_DD, F.nx)});
             eo.push_back({F.sY + Y * F.nx, ev(p, Y, 2), 1, eplans_.get(K_DD, F.nx)});
             eo.push_back({F.yY + Y * F.nx, ev(p, Y, 3), 1, eplans_.get(K_DD, F.nx)});
