@@ -270,12 +270,19 @@ Variable2D::~Variable2D()
 {
     for (auto& kv : buffer_map)
         for (auto& kv2 : kv.second) delete[] kv2.second;
+    for (auto& kv : boundary_value_map)
+        for (auto& kv2 : kv.second) delete[] kv2.second;
 }
 void Variable2D::set_geometry(Geometry2D& g)
 {
     geometry = &g;
     for (auto& [d, adj] : g.adjacency)
         for (auto& kv : adj) boundary_type_map[d][kv.first] = PDEBoundaryType::Adjacented;
+    for (auto* d : g.domains)  // corner node values start at zero for every domain (variable2d.cpp:38-44)
+    {
+        xneg_ypos_corner_map[d] = 0.0;
+        xpos_yneg_corner_map[d] = 0.0;
+    }
 }
 void Variable2D::check_geometry(Domain2DUniform* s)
 {
@@ -283,18 +290,37 @@ void Variable2D::check_geometry(Domain2DUniform* s)
     if (s->parent != geometry) throw std::runtime_error("Domain not found in geometry");
     if (s->nx <= 0 || s->ny <= 0) throw std::runtime_error("Domain mesh size invalid");
 }
-void Variable2D::set_center_field(Domain2DUniform* s, field2& f)
+// Field of (nx + extra) x (ny + extra) values and four zeroed ghost buffers of the matching lengths
+// (reference variable2d.cpp:64-150: extra = 1 for node-centred corner fields, 0 otherwise).
+void Variable2D::attach_field(Domain2DUniform* s, field2& f, int extra, VariablePositionType pos)
 {
     check_geometry(s);
-    f.init(s->nx, s->ny, name + "_" + s->name);
+    f.init(s->nx + extra, s->ny + extra, name + "_" + s->name);
     field_map[s] = &f;
     for (LocationType loc : kBoundaryLocations2D)
     {
-        const int n = (loc == LocationType::XNegative || loc == LocationType::XPositive) ? s->ny : s->nx;
+        const bool xface = loc == LocationType::XNegative || loc == LocationType::XPositive;
+        const int  n     = (xface ? s->ny : s->nx) + extra;
         delete[] buffer_map[s][loc];
         buffer_map[s][loc] = new double[(size_t)n]();
     }
-    position_type = VariablePositionType::Center;
+    position_type = pos;
+}
+void Variable2D::set_center_field(Domain2DUniform* s, field2& f) { attach_field(s, f, 0, VariablePositionType::Center); }
+void Variable2D::set_inner_field(Domain2DUniform* s, field2& f) { attach_field(s, f, 0, VariablePositionType::Center); }
+void Variable2D::set_x_edge_field(Domain2DUniform* s, field2& f) { attach_field(s, f, 0, VariablePositionType::XFace); }
+void Variable2D::set_y_edge_field(Domain2DUniform* s, field2& f) { attach_field(s, f, 0, VariablePositionType::YFace); }
+void Variable2D::set_corner_field(Domain2DUniform* s, field2& f) { attach_field(s, f, 1, VariablePositionType::Corner); }
+
+// Offset of value (i, j) from the domain's corner, in cells, for the variable's position
+// (variable2d.cpp:231-254): cell centres (0.5, 0.5), x faces (0, 0.5), y faces (0.5, 0), nodes (0, 0).
+void Variable2D::position_shift(double& sx, double& sy) const
+{
+    sx = 0.5;
+    sy = 0.5;
+    if (position_type == VariablePositionType::XFace) sx = 0.0;
+    else if (position_type == VariablePositionType::YFace) sy = 0.0;
+    else if (position_type == VariablePositionType::Corner) sx = sy = 0.0;
 }
 void Variable2D::set_boundary_type(Domain2DUniform* s, LocationType loc, PDEBoundaryType type)
 {
@@ -324,30 +350,111 @@ void Variable2D::set_boundary_type(PDEBoundaryType type)
         for (LocationType loc : kBoundaryLocations2D)
             if (!boundary_type_map[d].count(loc)) set_boundary_type(d, loc, type);
 }
+// Constant boundary value on one face (variable2d.cpp:202-224); the x- face value also sets the
+// (x-, y+) corner, the y- face value the (x+, y-) corner.
+void Variable2D::set_boundary_value(Domain2DUniform* s, LocationType loc, double in_value)
+{
+    check_geometry(s);
+    has_boundary_value_map[s][loc] = true;
+    const bool xface = loc == LocationType::XNegative || loc == LocationType::XPositive;
+    const int  n     = xface ? s->ny : s->nx;
+    double*&   v     = boundary_value_map[s][loc];
+    delete[] v;
+    v = new double[(size_t)n];
+    for (int k = 0; k < n; ++k) v[k] = in_value;
+    if (loc == LocationType::XNegative) xneg_ypos_corner_map[s] = in_value;
+    if (loc == LocationType::YNegative) xpos_yneg_corner_map[s] = in_value;
+}
+// Boundary value from f evaluated on the face itself (variable2d.cpp:226-316): the coordinate normal
+// to the face is the face's, the tangential one follows the variable's position; node fields have one
+// value more along the face.
+void Variable2D::set_boundary_value(Domain2DUniform* s, LocationType loc, std::function<double(double, double)> f)
+{
+    check_geometry(s);
+    has_boundary_value_map[s][loc] = true;
+    double sx, sy;
+    position_shift(sx, sy);
+    const bool xface = loc == LocationType::XNegative || loc == LocationType::XPositive;
+    const int  extra = position_type == VariablePositionType::Corner ? 1 : 0;
+    const int  n     = (xface ? s->ny : s->nx) + extra;
+    double*&   v     = boundary_value_map[s][loc];
+    delete[] v;
+    v = new double[(size_t)n];
+    for (int k = 0; k < n; ++k)
+    {
+        double gx, gy;
+        if (xface)
+        {
+            const int i = loc == LocationType::XNegative ? 0 : s->nx;
+            gx          = s->get_offset_x() + i * s->get_hx();
+            gy          = s->get_offset_y() + (sy + k) * s->get_hy();
+        }
+        else
+        {
+            const int j = loc == LocationType::YNegative ? 0 : s->ny;
+            gx          = s->get_offset_x() + (sx + k) * s->get_hx();
+            gy          = s->get_offset_y() + j * s->get_hy();
+        }
+        v[k] = f(gx, gy);
+    }
+}
+// Every non-Adjacented face with a boundary type and no boundary value yet (variable2d.cpp:318-343).
+void Variable2D::set_boundary(std::function<double(double, double)> f)
+{
+    if (geometry == nullptr) throw std::runtime_error("Variable2D has no geometry set");
+    for (auto& kv : field_map)
+    {
+        Domain2DUniform* d = kv.first;
+        for (LocationType loc : kBoundaryLocations2D)
+        {
+            auto it = boundary_type_map[d].find(loc);
+            if (it == boundary_type_map[d].end() || it->second == PDEBoundaryType::Adjacented ||
+                it->second == PDEBoundaryType::Null)
+                continue;
+            auto hv = has_boundary_value_map[d].find(loc);
+            if (hv != has_boundary_value_map[d].end() && hv->second) continue;
+            set_boundary_value(d, loc, f);
+        }
+    }
+}
+// Ghost buffer of one face: f at the ghost positions one cell outside the face (variable2d.cpp:345-416).
 void Variable2D::set_buffer_value(Domain2DUniform* s, LocationType loc, std::function<double(double, double)> f)
 {
     check_geometry(s);
+    double sx, sy;
+    position_shift(sx, sy);
     const bool xface = loc == LocationType::XNegative || loc == LocationType::XPositive;
-    const int  n     = xface ? s->ny : s->nx;
+    const int  extra = position_type == VariablePositionType::Corner ? 1 : 0;
+    const int  n     = (xface ? s->ny : s->nx) + extra;
     double*&   buf   = buffer_map[s][loc];
     if (!buf) buf = new double[(size_t)n]();
     for (int k = 0; k < n; ++k)
     {
-        double gx, gy;  // ghost cell centre, one cell outside the face (variable2d.cpp:386-416)
+        double gx, gy;
         if (xface)
         {
             const int i = (loc == LocationType::XNegative) ? -1 : s->nx;
-            gx          = s->get_offset_x() + (0.5 + i) * s->get_hx();
-            gy          = s->get_offset_y() + (0.5 + k) * s->get_hy();
+            gx          = s->get_offset_x() + (sx + i) * s->get_hx();
+            gy          = s->get_offset_y() + (sy + k) * s->get_hy();
         }
         else
         {
             const int j = (loc == LocationType::YNegative) ? -1 : s->ny;
-            gx          = s->get_offset_x() + (0.5 + k) * s->get_hx();
-            gy          = s->get_offset_y() + (0.5 + j) * s->get_hy();
+            gx          = s->get_offset_x() + (sx + k) * s->get_hx();
+            gy          = s->get_offset_y() + (sy + j) * s->get_hy();
         }
         buf[k] = f(gx, gy);
     }
+}
+// Corner node values of staggered fields (variable2d.cpp:418-436): x faces keep the (x+, y-) node
+// half a cell below the domain, y faces the (x-, y+) node half a cell left of it.
+void Variable2D::set_corner(Domain2DUniform* s, std::function<double(double, double)> f)
+{
+    check_geometry(s);
+    if (position_type == VariablePositionType::XFace)
+        xpos_yneg_corner_map[s] = f(s->get_offset_x() + s->nx * s->hx, s->get_offset_y() - 0.5 * s->hy);
+    else if (position_type == VariablePositionType::YFace)
+        xneg_ypos_corner_map[s] = f(s->get_offset_x() - 0.5 * s->hx, s->get_offset_y() + s->ny * s->hy);
 }
 void Variable2D::set_buffer(std::function<double(double, double)> f)
 {
@@ -362,12 +469,18 @@ void Variable2D::set_buffer(std::function<double(double, double)> f)
             set_buffer_value(kv.first, loc, f);
         }
 }
+void Variable2D::set_corner(std::function<double(double, double)> f)
+{
+    for (auto& kv : field_map) set_corner(kv.first, f);
+}
 void Variable2D::set_value(std::function<double(double, double)> func)
 {
+    double sx, sy;
+    position_shift(sx, sy);
     for (auto& [s, f] : field_map)
         for (int i = 0; i < f->get_nx(); ++i)
             for (int j = 0; j < f->get_ny(); ++j)
-                (*f)(i, j) = func(s->get_offset_x() + (0.5 + i) * s->get_hx(), s->get_offset_y() + (0.5 + j) * s->get_hy());
+                (*f)(i, j) = func(s->get_offset_x() + (sx + i) * s->get_hx(), s->get_offset_y() + (sy + j) * s->get_hy());
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -428,6 +541,9 @@ void ConcatPoissonSolver2D::construct()
     {
         Domain2DUniform* s = order[d];
         if (!variable->field_map.count(s)) throw std::runtime_error("ConcatPoissonSolver2D: domain " + s->name + " has no field");
+        if (variable->field_map[s]->get_nx() != s->nx || variable->field_map[s]->get_ny() != s->ny)
+            throw std::runtime_error("ConcatPoissonSolver2D: field of domain " + s->name +
+                                     " is not nx x ny (node-centred corner fields are not solved)");
         nx[d] = s->nx;
         ny[d] = s->ny;
         hx[d] = s->hx;

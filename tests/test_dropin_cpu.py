@@ -9,6 +9,7 @@ import pytest
 import dropin_cases as DC
 from golden_io import COMPOSITE_CASES, load
 from focalors_poisson_b200 import build
+from oracle import refpath
 
 
 @pytest.fixture(scope="module")
@@ -61,10 +62,10 @@ def test_library_exports_interface():
         assert s in syms, s
 
 
-REFERENCE = "/root/reference"
+REFERENCE = refpath.reference_dir()
 
 
-@pytest.mark.skipif(not os.path.isdir(REFERENCE) or not os.path.exists(
+@pytest.mark.skipif(not refpath.available() or not os.path.exists(
     os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "libfpref.so")),
     reason="needs the reference sources and the oracle library built from them")
 def test_host_data_model_matches_reference(tmp_path):
