@@ -931,13 +931,7 @@ struct XList
 
 template <typename T, int K, int I, typename TIN, typename TOUT, bool ACC> void prep_x()
 {
-    static bool attr = false;
-    if (!attr)
-    {
-        FPB_CUDA(cudaFuncSetAttribute(k_b_xform<T, K, I, TIN, TOUT, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)max_dynamic_smem()));
-        attr = true;
-    }
+    allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC>);
 }
 
 template <typename T, int K, int I, typename TIN, typename TOUT, bool ACC>

@@ -182,7 +182,11 @@ template <typename T> struct DevRect
     void chase(T* f, long long batch, T* scratch, cudaStream_t s) const;
 };
 
+constexpr int kMaxDevices = 128;
+// Opt-in dynamic shared memory per CTA on the current device (cached per device).
 size_t max_dynamic_smem();
+// Sets func's MaxDynamicSharedMemorySize to max_dynamic_smem() on the current device, once per device.
+void allow_max_dynamic_smem(const void* func);
 
 }  // namespace fpb
 

@@ -26,10 +26,10 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoallocScratchDoubles
 double* scratch_address()
 {
     static std::mutex mu;
-    static double*    addr[128] = {};
-    int               dev       = 0;
+    static double*    addr[fpb::kMaxDevices] = {};
+    int               dev                    = 0;
     FPB_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 128) throw fpb::Error(FP_ERR_UNSUPPORTED, "device index out of range");
+    if (dev < 0 || dev >= fpb::kMaxDevices) throw fpb::Error(FP_ERR_UNSUPPORTED, "device index out of range");
     std::lock_guard<std::mutex> lk(mu);
     if (!addr[dev])
     {

@@ -4,21 +4,43 @@
 
 #include <algorithm>
 #include <mutex>
+#include <set>
 #include <type_traits>
 
 namespace fpb
 {
 
+// Largest dynamic shared memory a CTA may opt into on the current device, less room for static arrays.
+// Cached per device: a process may drive several GPUs.
 size_t max_dynamic_smem()
 {
-    static size_t v = [] {
-        int dev = 0, optin = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess) return (size_t)48 * 1024;
+    static std::mutex mu;
+    static size_t     cache[kMaxDevices] = {};
+    int               dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return (size_t)48 * 1024;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!cache[dev])
+    {
+        int optin = 0;
         if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
             return (size_t)48 * 1024;
-        return (size_t)optin - 1024;  // room for the kernel's static shared arrays
-    }();
-    return v;
+        cache[dev] = (size_t)optin - 1024;  // room for the kernel's static shared arrays
+    }
+    return cache[dev];
+}
+
+// Function attributes are per device: the opt-in to max_dynamic_smem() is made once per (device, kernel).
+void allow_max_dynamic_smem(const void* func)
+{
+    static std::mutex                             mu;
+    static std::set<std::pair<int, const void*>> done;
+    int                                           dev = 0;
+    FPB_CUDA(cudaGetDevice(&dev));
+    const size_t smem = max_dynamic_smem();
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({dev, func})) return;
+    FPB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    done.insert({dev, func});
 }
 
 namespace
@@ -41,11 +63,7 @@ template <typename T2> std::vector<T2> convert_c(const std::vector<std::complex<
 template <typename T, int K, int I, typename TIO>
 void launch_k(const TransformArgs<T, TIO>& a, long long rows, int threads, size_t smem, cudaStream_t s)
 {
-    static std::once_flag once;
-    std::call_once(once, [] {
-        cudaFuncSetAttribute(k_transform<T, K, I, TIO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)max_dynamic_smem());
-    });
+    allow_max_dynamic_smem((const void*)k_transform<T, K, I, TIO>);
     const long long grid = FamilyTraits<K, I>::kPairRows ? (rows + 1) / 2 : rows;
     if (grid <= 0) return;
     k_transform<T, K, I, TIO><<<(unsigned)grid, threads, smem, s>>>(a);
