@@ -56,20 +56,31 @@ struct DstSeg
 // Register cap: the arguments are read through a global pointer here (not from the parameter bank as in
 // k_transform), and uncapped the FP64 instances take 104-110 registers, which allows only 2 CTAs of 256
 // threads per SM; at 80 (16 bytes of spill) three fit, as many as their shared memory allows.
-template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC>
-__global__ void __maxnreg__(sizeof(T) == 8 ? 80 : 64) k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix,
+// ENG 1 (register engine): every segment of the launch has a plan of the same length M (M/16 threads per
+// CTA); the CTA copies a plan's tables into shared memory when its items move to another plan.
+template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG>
+__global__ void __maxnreg__((xform_maxnreg<ENG, T>())) k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix,
                                                  int nseg, long long nitems, const XformArgs<T>* __restrict__ plans)
 {
     typedef typename Cplx<T>::type T2;
     extern __shared__ __align__(16) unsigned char fp_smem_raw[];
     T2*            buf = reinterpret_cast<T2*>(fp_smem_raw);
     __shared__ T   rowsc[2];
-    constexpr bool kPair = FamilyTraits<KIND, INV>::kPairRows;
+    constexpr bool kPair  = FamilyTraits<KIND, INV>::kPairRows;
+    int            loaded = -1;
     for (long long it = blockIdx.x; it < nitems; it += gridDim.x)
     {
         const int           s  = seg_of(prefix, nseg, it);
         const DstSeg&       sg = segs[s];
         const XformArgs<T>& P  = plans[2 * sg.plan + INV];
+        if constexpr (ENG == 1)
+        {
+            if (sg.plan != loaded)
+            {
+                reg_tables_to_smem(P, buf);
+                loaded = sg.plan;
+            }
+        }
         const int           n  = P.n;
         const long long     r0 = kPair ? 2 * (it - prefix[s]) : (it - prefix[s]);
         const bool          has_b = kPair && r0 + 1 < sg.rows;
@@ -77,7 +88,7 @@ __global__ void __maxnreg__(sizeof(T) == 8 ? 80 : 64) k_b_xform(const DstSeg* __
         const TIN*          fb    = has_b ? fa + n : fa;
         TOUT*               oa    = static_cast<TOUT*>(sg.out) + r0 * n;
         TOUT*               ob    = has_b ? oa + n : nullptr;
-        transform_rows<T, KIND, INV, TIN, TOUT, ACC>(P, fa, fb, oa, ob, has_b, buf, rowsc);
+        transform_rows<T, KIND, INV, TIN, TOUT, ACC, ENG>(P, fa, fb, oa, ob, has_b, buf, rowsc);
     }
 }
 
@@ -86,19 +97,24 @@ __global__ void __maxnreg__(sizeof(T) == 8 ? 80 : 64) k_b_xform(const DstSeg* __
 // modifiers: rhs(i, k) = in(i, k) + sum_rows [i == row] c v[k] + sum_cols c s[i] psi_k(j)
 // (a row term is a spectral vector on one row; a column term is a physical column of values at
 // column j, whose y-DST is s[i] psi_k(j)).
+// Rows are stored in T (FP64, or FP32 in the reduced-precision inner solves); the elimination itself,
+// its tables and its scratch are FP64 for both. The lowest wavenumbers' tridiagonal systems are nearly
+// singular (diagonal -2 - O(h^2), condition ~ nx^2): eliminated in FP32 they lose about 2 of FP32's 7
+// digits (rel. error ~1e-2 at nx = 2048), in FP64 the FP32-rounded input is solved to ~1e-12, so an
+// FP32-storage inner solve keeps FP32 accuracy (~1e-7) and refinement needs fewer steps.
 // ---------------------------------------------------------------------------------------------
 constexpr int kMaxMods = 4;
 
-template <typename T> struct ChaseTabDev
+struct ChaseTabDev
 {
-    const T* cc;
-    const T* cg;
-    const T* chh;
-    const T* cends;
-    const T* dsep;
-    int      end_neu;  // x+ face Neumann: last separator diagonal d + 1 (x- Neumann is in the type-0 tables)
-    const T* scp;      // separator Thomas factors c_p [p][j] (rows not last)
-    const T* sid;      // 1 / den_p [p][j]
+    const double* cc;
+    const double* cg;
+    const double* chh;
+    const double* cends;
+    const double* dsep;
+    int           end_neu;  // x+ face Neumann: last separator diagonal d + 1 (x- Neumann is in the type-0 tables)
+    const double* scp;      // separator Thomas factors c_p [p][j] (rows not last)
+    const double* sid;      // 1 / den_p [p][j]
 };
 
 template <typename T> struct ChaseSeg
@@ -106,9 +122,9 @@ template <typename T> struct ChaseSeg
     const T* in;
     T*       out;
     int      nx, ny, tab;
-    T*       zend;  // scratch: 2 P ny
-    T*       bsep;  // P ny
-    T*       work;  // P ny
+    double*  zend;  // scratch: 2 P ny
+    double*  bsep;  // P ny
+    double*  work;  // P ny
     int      nrow, ncol;
     int      row_i[kMaxMods];
     const double* row_v[kMaxMods];
@@ -131,15 +147,13 @@ __device__ __forceinline__ void mod_init(const ChaseSeg<T>* __restrict__ sg, int
         m.psi[c] = sg->col_c[c] * (sg->col_tab[c] ? sg->col_tab[c][k] : dst_basis(sg->ny, k, sg->col_j[c]));
 }
 template <typename T>
-__device__ __forceinline__ T mod_rhs(const ChaseSeg<T>* __restrict__ sg, int nrow, int ncol, const ModCtx<T>& m, int i,
-                                     int k, T raw)
+__device__ __forceinline__ double mod_rhs(const ChaseSeg<T>* __restrict__ sg, int nrow, int ncol, const ModCtx<T>& m,
+                                          int i, int k, double v)
 {
-    if (nrow == 0 && ncol == 0) return raw;
-    double v = (double)raw;
     for (int r = 0; r < nrow; ++r)
         if (sg->row_i[r] == i) v += sg->row_c[r] * sg->row_v[r][k];
     for (int c = 0; c < ncol; ++c) v += m.psi[c] * sg->col_s[c][i];
-    return (T)v;
+    return v;
 }
 
 // blocks of segment s: prefix (in blocks); per segment P*ny threads (local / correct) or ny (reduced)
@@ -149,7 +163,7 @@ __device__ __forceinline__ T mod_rhs(const ChaseSeg<T>* __restrict__ sg, int nro
 template <typename T>
 __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __restrict__ segs,
                                                        const long long* __restrict__ prefix, int nseg,
-                                                       const ChaseTabDev<T>* __restrict__ tabs)
+                                                       const ChaseTabDev* __restrict__ tabs)
 {
     constexpr int      Li = kChunk - 1;
     const int          s  = seg_of(prefix, nseg, blockIdx.x);
@@ -157,26 +171,26 @@ __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __rest
     const int          ny = sg->ny, P = sg->nx / kChunk;
     const int          t  = (int)(blockIdx.x - prefix[s]) * blockDim.x + threadIdx.x;
     if (t >= P * ny) return;
-    const int j = t % ny, p = t / ny;
-    const int typ = p == 0 ? 0 : 1;
-    const T*  col = sg->in + (long long)p * kChunk * ny + j;
-    T*        out = sg->out + (long long)p * kChunk * ny + j;
-    const T*  c   = tabs[sg->tab].cc + (long long)typ * Li * ny + j;
-    T         y[Li];
+    const int     j   = t % ny, p = t / ny;
+    const int     typ = p == 0 ? 0 : 1;
+    const T*      col = sg->in + (long long)p * kChunk * ny + j;
+    T*            out = sg->out + (long long)p * kChunk * ny + j;
+    const double* c   = tabs[sg->tab].cc + (long long)typ * Li * ny + j;
+    double        y[Li];
 #pragma unroll
-    for (int r = 0; r < Li; ++r) y[r] = col[(long long)r * ny];
+    for (int r = 0; r < Li; ++r) y[r] = (double)col[(long long)r * ny];
     const int ncol = sg->ncol;
     for (int q = 0; q < ncol; ++q)
     {
         const double  ps = sg->col_c[q] * (sg->col_tab[q] ? sg->col_tab[q][j] : dst_basis(ny, j, sg->col_j[q]));
         const double* sv = sg->col_s[q] + p * kChunk;
 #pragma unroll
-        for (int r = 0; r < Li; ++r) y[r] = (T)((double)y[r] + ps * sv[r]);
+        for (int r = 0; r < Li; ++r) y[r] += ps * sv[r];
     }
     if (p == 0)
         for (int q = 0; q < sg->nrow; ++q)
-            if (sg->row_i[q] == 0) y[0] = (T)((double)y[0] + sg->row_c[q] * sg->row_v[q][j]);
-    T prev = 0;
+            if (sg->row_i[q] == 0) y[0] += sg->row_c[q] * sg->row_v[q][j];
+    double prev = 0;
 #pragma unroll
     for (int r = 0; r < Li; ++r)
     {
@@ -186,10 +200,10 @@ __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __rest
 #pragma unroll
     for (int r = Li - 2; r >= 0; --r) y[r] = y[r] - __ldg(c + (long long)r * ny) * y[r + 1];
 #pragma unroll
-    for (int r = 0; r < Li; ++r) out[(long long)r * ny] = y[r];
-    T* ze  = sg->zend + (long long)(p * 2) * ny + j;
-    ze[0]  = y[0];
-    ze[ny] = y[Li - 1];
+    for (int r = 0; r < Li; ++r) out[(long long)r * ny] = (T)y[r];
+    double* ze = sg->zend + (long long)(p * 2) * ny + j;
+    ze[0]      = y[0];
+    ze[ny]     = y[Li - 1];
 }
 
 // Separator system per subdomain and wavenumber (the system of k_chase_reduced, tabulated Thomas factors
@@ -204,10 +218,10 @@ __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __rest
 template <typename T>
 __global__ void __launch_bounds__(32 * kRedWarps) k_b_chase_reduced(const ChaseSeg<T>* __restrict__ segs,
                                                                     const long long* __restrict__ prefix, int nseg,
-                                                                    const ChaseTabDev<T>* __restrict__ tabs)
+                                                                    const ChaseTabDev* __restrict__ tabs)
 {
     constexpr int      kAhead = 8;
-    __shared__ T       sa[kRedWarps][32], sb[kRedWarps][32];
+    __shared__ double  sa[kRedWarps][32], sb[kRedWarps][32];
     const int          s    = seg_of(prefix, nseg, blockIdx.x);
     const ChaseSeg<T>* sg   = segs + s;
     const int          ny   = sg->ny, nx = sg->nx, P = nx / kChunk;
@@ -217,7 +231,7 @@ __global__ void __launch_bounds__(32 * kRedWarps) k_b_chase_reduced(const ChaseS
     const int          j    = act ? j0 : 0;  // idle lanes compute on column 0 and store nothing
     const int          per  = (P + kRedWarps - 1) / kRedWarps;
     const int          pb = min(P, w * per), pe = min(P, pb + per);
-    const ChaseTabDev<T> tb   = tabs[sg->tab];
+    const ChaseTabDev tb   = tabs[sg->tab];
     const int            nrow = sg->nrow, ncol = sg->ncol;
     ModCtx<T>            mc;
     if (ncol > 0)  // column-term weights of the CTA's 32 wavenumbers: computed once (warp 0), shared
@@ -231,33 +245,35 @@ __global__ void __launch_bounds__(32 * kRedWarps) k_b_chase_reduced(const ChaseS
         __syncthreads();
         for (int c = 0; c < ncol; ++c) mc.psi[c] = spsi[c][lane];
     }
-    const T  e1_1 = tb.cends[(1 * 4 + 1) * (long long)ny + j];
-    const T* ze   = sg->zend + j;
-    const T* in   = sg->in;
-    T*       bs   = sg->bsep + j;  // y_p, then x_p (the correction pass reads x)
-    T*       wk   = sg->work + j;  // A_p of y_p = A_p y_{p-1} + B_p
+    const double  e1_1 = tb.cends[(1 * 4 + 1) * (long long)ny + j];
+    const double* ze   = sg->zend + j;
+    const T*      in   = sg->in;
+    double*       bs   = sg->bsep + j;  // y_p, then x_p (the correction pass reads x)
+    double*       wk   = sg->work + j;  // A_p of y_p = A_p y_{p-1} + B_p
 
     // forward maps of the range: A_p = -lower inv_p, B_p = rhs_p inv_p (B kept in bs), composed in (ca, cb)
-    T ca = 1, cb = 0;
+    double ca = 1, cb = 0;
     for (int p0 = pb; p0 < pe; p0 += kAhead)
     {
-        T rhs_v[kAhead], inv_v[kAhead];
+        double rhs_v[kAhead], inv_v[kAhead];
 #pragma unroll
         for (int q = 0; q < kAhead; ++q)
         {
             const int p = p0 + q;
             if (p >= pe) break;
             const int isep = p * kChunk + kChunk - 1;
-            T r = mod_rhs(sg, nrow, ncol, mc, isep, j, in[(long long)isep * ny + j]) - ze[(long long)(2 * p + 1) * ny];
+            double r = mod_rhs(sg, nrow, ncol, mc, isep, j, (double)in[(long long)isep * ny + j]) -
+                       ze[(long long)(2 * p + 1) * ny];
             if (p < P - 1) r -= ze[(long long)(2 * (p + 1)) * ny];
             rhs_v[q] = r;
             if (p < P - 1) inv_v[q] = tb.sid[(long long)p * ny + j];
             else  // last row: no next chunk, x+ Neumann end
             {
-                const T lower = p > 0 ? -e1_1 : (T)0;
-                const T diag  = (tb.end_neu ? tb.dsep[j] + (T)1 : tb.dsep[j]) -
-                               (p == 0 ? tb.cends[(0 * 4 + 3) * (long long)ny + j] : tb.cends[(1 * 4 + 3) * (long long)ny + j]);
-                inv_v[q] = (T)1 / (diag - lower * (p > 0 ? tb.scp[(long long)(p - 1) * ny + j] : (T)0));
+                const double lower = p > 0 ? -e1_1 : 0.0;
+                const double diag  = (tb.end_neu ? tb.dsep[j] + 1.0 : tb.dsep[j]) -
+                                    (p == 0 ? tb.cends[(0 * 4 + 3) * (long long)ny + j]
+                                            : tb.cends[(1 * 4 + 3) * (long long)ny + j]);
+                inv_v[q] = 1.0 / (diag - lower * (p > 0 ? tb.scp[(long long)(p - 1) * ny + j] : 0.0));
             }
         }
 #pragma unroll
@@ -265,8 +281,8 @@ __global__ void __launch_bounds__(32 * kRedWarps) k_b_chase_reduced(const ChaseS
         {
             const int p = p0 + q;
             if (p >= pe) break;
-            const T A = p > 0 ? e1_1 * inv_v[q] : (T)0;  // -lower inv
-            const T B = rhs_v[q] * inv_v[q];
+            const double A = p > 0 ? e1_1 * inv_v[q] : 0.0;  // -lower inv
+            const double B = rhs_v[q] * inv_v[q];
             if (act)
             {
                 wk[(long long)p * ny] = A;
@@ -279,11 +295,11 @@ __global__ void __launch_bounds__(32 * kRedWarps) k_b_chase_reduced(const ChaseS
     sa[w][lane] = ca;
     sb[w][lane] = cb;
     __syncthreads();
-    T y = 0;  // y_{pb-1}
+    double y = 0;  // y_{pb-1}
     for (int v = 0; v < w; ++v) y = sa[v][lane] * y + sb[v][lane];
     for (int p = pb; p < pe; ++p)
     {
-        const T A = act ? wk[(long long)p * ny] : (T)0, B = act ? bs[(long long)p * ny] : (T)0;
+        const double A = act ? wk[(long long)p * ny] : 0.0, B = act ? bs[(long long)p * ny] : 0.0;
         y         = A * y + B;
         if (act) bs[(long long)p * ny] = y;
     }
@@ -294,25 +310,25 @@ __global__ void __launch_bounds__(32 * kRedWarps) k_b_chase_reduced(const ChaseS
     cb = 0;
     for (int p = pe - 1; p >= pb; --p)
     {
-        const T c  = p < P - 1 ? tb.scp[(long long)p * ny + j] : (T)0;
-        const T yp = act ? bs[(long long)p * ny] : (T)0;
-        cb         = -c * cb + yp;
+        const double c  = p < P - 1 ? tb.scp[(long long)p * ny + j] : 0.0;
+        const double yp = act ? bs[(long long)p * ny] : 0.0;
+        cb              = -c * cb + yp;
         ca         = -c * ca;
     }
     sa[w][lane] = ca;
     sb[w][lane] = cb;
     __syncthreads();
-    T x = 0;  // x_{pe}
+    double x = 0;  // x_{pe}
     for (int v = kRedWarps - 1; v > w; --v) x = sa[v][lane] * x + sb[v][lane];
     for (int p = pe - 1; p >= pb; --p)
     {
-        const T c  = p < P - 1 ? tb.scp[(long long)p * ny + j] : (T)0;
-        const T yp = act ? bs[(long long)p * ny] : (T)0;
-        x          = yp - c * x;
+        const double c  = p < P - 1 ? tb.scp[(long long)p * ny + j] : 0.0;
+        const double yp = act ? bs[(long long)p * ny] : 0.0;
+        x               = yp - c * x;
         if (act)
         {
             bs[(long long)p * ny] = x;
-            sg->out[(long long)(p * kChunk + kChunk - 1) * ny + j] = x;
+            sg->out[(long long)(p * kChunk + kChunk - 1) * ny + j] = (T)x;
         }
     }
 }
@@ -320,7 +336,7 @@ __global__ void __launch_bounds__(32 * kRedWarps) k_b_chase_reduced(const ChaseS
 template <typename T>
 __global__ void __launch_bounds__(256) k_b_chase_correct(const ChaseSeg<T>* __restrict__ segs,
                                                          const long long* __restrict__ prefix, int nseg,
-                                                         const ChaseTabDev<T>* __restrict__ tabs)
+                                                         const ChaseTabDev* __restrict__ tabs)
 {
     constexpr int      Li = kChunk - 1;
     const int          s  = seg_of(prefix, nseg, blockIdx.x);
@@ -330,18 +346,18 @@ __global__ void __launch_bounds__(256) k_b_chase_correct(const ChaseSeg<T>* __re
     if (t >= P * ny) return;
     const int            j   = t % ny, p = t / ny;
     const int            typ = p == 0 ? 0 : 1;
-    const ChaseTabDev<T> tb  = tabs[sg->tab];
-    const T*             bs  = sg->bsep + j;
-    const T              bl  = p > 0 ? bs[(long long)(p - 1) * ny] : (T)0;
-    const T              br  = bs[(long long)p * ny];
-    T*                   col = sg->out + (long long)p * kChunk * ny + j;
-    const T*             g   = tb.cg + (long long)typ * Li * ny + j;
-    const T*             h   = tb.chh + (long long)typ * Li * ny + j;
+    const ChaseTabDev tb  = tabs[sg->tab];
+    const double*     bs  = sg->bsep + j;
+    const double      bl  = p > 0 ? bs[(long long)(p - 1) * ny] : 0.0;
+    const double      br  = bs[(long long)p * ny];
+    T*                col = sg->out + (long long)p * kChunk * ny + j;
+    const double*     g   = tb.cg + (long long)typ * Li * ny + j;
+    const double*     h   = tb.chh + (long long)typ * Li * ny + j;
 #pragma unroll 8
     for (int r = 0; r < Li; ++r)
     {
         const long long o = (long long)r * ny;
-        col[o]            = col[o] - bl * __ldg(g + o) - br * __ldg(h + o);
+        col[o]            = (T)((double)col[o] - bl * __ldg(g + o) - br * __ldg(h + o));
     }
 }
 
@@ -771,7 +787,7 @@ __global__ void __launch_bounds__(256) k_b_residual(const ResSeg* __restrict__ s
     for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x)
     {
         const double fs = sg->fs[t];
-        const double v  = fs - composite_lap(sg->u, t, sg->a);
+        const double v  = composite_residual_at(sg->u, fs, t, sg->a);
         if (sg->r) sg->r[t] = v;
         rr += v * v;
         ff += fs * fs;
@@ -871,13 +887,14 @@ template <typename T> struct PlanSet  // transform plans by (family, row length)
     std::map<std::pair<int, int>, int>            index;
     std::vector<std::unique_ptr<DevTransform<T>>> tr;
     DevBuf                                        dev;
-    size_t                                        smem = 0;
+    size_t                                        smem       = 0;
+    bool                                          stage_only = false;  // plans on the stage engine only
     int get(int kind, int n)
     {
         auto key = std::make_pair(kind, n);
         auto it  = index.find(key);
         if (it != index.end()) return it->second;
-        tr.emplace_back(new DevTransform<T>(kind, n));
+        tr.emplace_back(new DevTransform<T>(kind, n, !stage_only));
         smem = std::max(smem, tr.back()->smem);
         return index[key] = (int)tr.size() - 1;
     }
@@ -894,13 +911,15 @@ template <typename T> struct PlanSet  // transform plans by (family, row length)
     }
 };
 
-// A transform work list split by family: one launch per family present, each sized for the shared memory
-// of its own largest plan.
+// A transform work list split by family and engine: one launch per family for its stage-engine plans (the
+// autotuned CTA shape, shared memory of the largest plan) and one per (family, length M) for its
+// register-engine plans (M/16 threads per CTA).
 struct XList
 {
     struct Part
     {
         int      kind = 0;
+        int      eng = 0, threads = 0;  // register engine: threads per CTA (stage engine: autotuned)
         size_t   smem = 0;
         Segments seg;
     };
@@ -910,37 +929,61 @@ struct XList
         parts.clear();
         for (int k : {K_DD, K_ND, K_DN})
         {
-            std::vector<DstSeg>    r;
-            std::vector<long long> c;
-            size_t                 sm = 0;
+            std::map<int, std::vector<size_t>> groups;  // -1: stage engine, else M of the register engine
             for (size_t i = 0; i < recs.size(); ++i)
                 if (kinds[i] == k)
+                {
+                    const FftDesc& d = ps.tr[recs[i].plan]->fd;
+                    groups[d.eng == 1 ? d.M : -1].push_back(i);
+                }
+            for (auto& g : groups)
+            {
+                std::vector<DstSeg>    r;
+                std::vector<long long> c;
+                size_t                 sm = 0;
+                for (size_t i : g.second)
                 {
                     r.push_back(recs[i]);
                     c.push_back((recs[i].rows + 1) / 2);
                     sm = std::max(sm, ps.tr[recs[i].plan]->smem);
                 }
-            if (r.empty()) continue;
-            parts.emplace_back();
-            parts.back().kind = k;
-            parts.back().smem = sm;
-            parts.back().seg.set(r, c);
+                parts.emplace_back();
+                parts.back().kind    = k;
+                parts.back().eng     = g.first > 0 ? 1 : 0;
+                parts.back().threads = g.first > 0 ? g.first / 16 : 0;
+                parts.back().smem    = sm;
+                parts.back().seg.set(r, c);
+            }
         }
     }
 };
 
 template <typename T, int K, int I, typename TIN, typename TOUT, bool ACC> void prep_x()
 {
-    allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC>);
+    allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 0>);
+    allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 1>);
 }
 
+// Stage engine: the autotuned CTA shape (threads, CTAs per SM); register engine: `threads` per CTA and as
+// many CTAs as are resident at once, each looping over items.
 template <typename T, int K, int I, typename TIN, typename TOUT, bool ACC>
-void launch_x1(const Segments& sg, const PlanSet<T>& ps, const BatchTiming& tm, cudaStream_t s, size_t smem = 0)
+void launch_x1(const Segments& sg, const PlanSet<T>& ps, const BatchTiming& tm, cudaStream_t s, size_t smem = 0,
+               int eng = 0, int threads = 0)
 {
     if (sg.total == 0) return;
     prep_x<T, K, I, TIN, TOUT, ACC>();
+    const size_t sm = smem ? smem : ps.smem;
+    if (eng == 1)
+    {
+        const void*     fn   = (const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 1>;
+        const long long grid = std::min<long long>(sg.total, resident_ctas(fn, threads, sm));
+        k_b_xform<T, K, I, TIN, TOUT, ACC, 1><<<(unsigned)grid, threads, sm, s>>>(
+            sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, ps.dev.template as<XformArgs<T>>());
+        FPB_CHECK_LAUNCH();
+        return;
+    }
     const long long grid = std::min<long long>(sg.total, (long long)sm_count() * tm.dst_blocks_per_sm);
-    k_b_xform<T, K, I, TIN, TOUT, ACC><<<(unsigned)grid, tm.dst_threads, smem ? smem : ps.smem, s>>>(
+    k_b_xform<T, K, I, TIN, TOUT, ACC, 0><<<(unsigned)grid, tm.dst_threads, sm, s>>>(
         sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, ps.dev.template as<XformArgs<T>>());
     FPB_CHECK_LAUNCH();
 }
@@ -951,13 +994,14 @@ void launch_x(const XList& L, bool inverse, const PlanSet<T>& ps, const BatchTim
 {
     for (auto& part : L.parts)
     {
+        const int e = part.eng, th = part.threads;
         switch (part.kind)
         {
-            case K_DD: launch_x1<T, K_DD, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem); break;
-            case K_DN: launch_x1<T, K_DN, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem); break;
+            case K_DD: launch_x1<T, K_DD, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th); break;
+            case K_DN: launch_x1<T, K_DN, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th); break;
             default:
-                if (inverse) launch_x1<T, K_ND, 1, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem);
-                else launch_x1<T, K_ND, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem);
+                if (inverse) launch_x1<T, K_ND, 1, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th);
+                else launch_x1<T, K_ND, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th);
         }
     }
 }
@@ -1033,7 +1077,7 @@ private:
     PlanSet<TS>                               plans_;
     PlanSet<double>                           eplans_;  // FP64 DSTs of edge vectors (length nx of roots)
     std::map<std::pair<int, double>, int>     tab_index_;
-    std::vector<std::unique_ptr<DevRect<TS>>> tabs_;
+    std::vector<std::unique_ptr<DevRect<double>>> tabs_;  // chase tables (FP64 in both storage precisions)
     DevBuf                                    tabs_dev_;
     DevBuf                                    W_, X_, fs_, r_, chs_;  // work, chase out, IR, chase scratch
     DevBuf                                    edge_;  // bY, gYp, sYp, yYp per y-edge (nx each), per problem
@@ -1063,6 +1107,7 @@ private:
 
 template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDesc>& probs)
 {
+    eplans_.stage_only = true;  // one launch covers edge rows of every length (one CTA shape)
     if (probs.empty()) throw Error(1, "empty batch");
     for (size_t p = 0; p < probs.size(); ++p)
     {
@@ -1152,23 +1197,22 @@ template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDe
         auto         it  = tab_index_.find(key);
         if (it == tab_index_.end())
         {
-            tabs_.emplace_back(new DevRect<TS>(2 * kChunk, D.d.ny, D.d.hx, D.d.hy, bcd, rows_needed[key]));
+            tabs_.emplace_back(new DevRect<double>(2 * kChunk, D.d.ny, D.d.hx, D.d.hy, bcd, rows_needed[key], false));
             it = tab_index_.emplace(key, (int)tabs_.size() - 1).first;
         }
         D.tab = it->second;
     }
     plans_.finish();
-    std::vector<ChaseTabDev<TS>> tv;
+    std::vector<ChaseTabDev> tv;
     for (auto& t : tabs_)
-        tv.push_back({t->cc.template as<TS>(), t->cg.template as<TS>(), t->chh.template as<TS>(),
-                      t->cends.template as<TS>(), t->dsep.template as<TS>(), t->end_neumann ? 1 : 0,
-                      t->sep_cp.template as<TS>(), t->sep_iden.template as<TS>()});
+        tv.push_back({t->cc.as<double>(), t->cg.as<double>(), t->chh.as<double>(), t->cends.as<double>(),
+                      t->dsep.as<double>(), t->end_neumann ? 1 : 0, t->sep_cp.as<double>(), t->sep_iden.as<double>()});
     tabs_dev_ = upload(tv);
     W_.alloc((size_t)cells_ * sizeof(TS));
     X_.alloc((size_t)cells_ * sizeof(TS));
     long long sep = 0;
     for (auto& D : dom_) sep += (long long)(D.d.nx / kChunk) * D.d.ny * 4;
-    chs_.alloc((size_t)sep * sizeof(TS));
+    chs_.alloc((size_t)sep * sizeof(double));
     build_spectral();
     build_static_lists();
     prep_x_all<TS, double, TS, false>();
@@ -1482,7 +1526,7 @@ template <typename TS> void BatchImpl<TS>::build_static_lists()
         c.nx   = D.d.nx;
         c.ny   = D.d.ny;
         c.tab  = D.tab;
-        c.zend = chs_.as<TS>() + soff[g];
+        c.zend = chs_.as<double>() + soff[g];
         c.bsep = c.zend + 2 * P * D.d.ny;
         c.work = c.bsep + P * D.d.ny;
         return c;
@@ -1643,7 +1687,7 @@ template <typename TS> void BatchImpl<TS>::build_chase_lists()
 template <typename TS> void BatchImpl<TS>::chase_run(const Segments& lc, const Segments& red, cudaStream_t s)
 {
     if (lc.n == 0) return;
-    const ChaseTabDev<TS>* tabs = tabs_dev_.as<ChaseTabDev<TS>>();
+    const ChaseTabDev* tabs = tabs_dev_.as<ChaseTabDev>();
     k_b_chase_local<TS><<<(unsigned)lc.total, tm_.chase_threads, 0, s>>>(lc.as<ChaseSeg<TS>>(), lc.pre(), lc.n, tabs);
     FPB_CHECK_LAUNCH();
     k_b_chase_reduced<TS><<<(unsigned)red.total, 32 * kRedWarps, 0, s>>>(red.as<ChaseSeg<TS>>(), red.pre(), red.n, tabs);
@@ -2094,7 +2138,7 @@ template <typename TS> void BatchImpl<TS>::autotune(cudaStream_t s)
     for (int th : {128, 192, 256, 384, 512})
     {
         int occ = 0;
-        FPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_xform<TS, K_DD, 0, TS, TS, false>, th,
+        FPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_xform<TS, K_DD, 0, TS, TS, false, 0>, th,
                                                                plans_.smem));
         // persistent grids of 1, 2, 4, the occupancy limit CTAs per SM, or one CTA per work item (1 << 20)
         for (int bps : {1, 2, 4, occ, 1 << 20})

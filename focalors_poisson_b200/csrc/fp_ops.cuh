@@ -354,13 +354,43 @@ struct ResidualArgs
 // (Dirichlet), mirrored (Neumann), wrapped (periodic); an Adjacented face contributes the neighbour's
 // adjacent cell with coefficient 1 -- the operator ConcatPoissonSolver2D::solve inverts
 // (pe/concat/concat_solver2d.cpp:101-157, interface terms from bond_add with coefficient -1).
-__device__ __forceinline__ double composite_lap(const double* __restrict__ u, long long t, const ResidualArgs& a)
+//
+// The residual is computed in double-FP64 ("double-double") arithmetic and rounded once. For a smooth
+// solution the stencil's terms are ~cond(A) times larger than their sum, and a plain FP64 sum carries an
+// error of eps * |terms|: the computed residual of the exact solution would then be ~eps * cond(A)
+// relative (1e-8 at h = 1/4096), and iterative refinement on it cannot get below that. Here every sum is
+// exact to second order (TwoSum; products by r2 through an FMA remainder), so the residual is accurate to
+// ~eps relative to itself and refinement converges to the solution's own FP64 rounding.
+// The _rn intrinsics are never contracted into FMAs, which would break the error-free transformations.
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e)
+{
+    s              = __dadd_rn(a, b);
+    const double v = __dsub_rn(s, a);
+    e              = __dadd_rn(__dsub_rn(a, __dsub_rn(s, v)), __dsub_rn(b, v));
+}
+__device__ __forceinline__ void dd_acc(double& hi, double& lo, double x)
+{
+    double s, e;
+    two_sum(hi, x, s, e);
+    hi = s;
+    lo += e;
+}
+__device__ __forceinline__ void dd_acc_prod(double& hi, double& lo, double a, double b)
+{
+    const double p = __dmul_rn(a, b);
+    dd_acc(hi, lo, p);
+    lo += fma(a, b, -p);
+}
+
+// fs_t - (A u)_t, compensated as above.
+__device__ __forceinline__ double composite_residual_at(const double* __restrict__ u, double fs, long long t,
+                                                        const ResidualArgs& a)
 {
     const int    i = (int)t / a.ny, j = (int)t - i * a.ny;  // a subdomain holds fewer than 2^31 cells
     const int    nx = a.nx, ny = a.ny;
     const double c  = u[t];
-    double       xm, xp, ym, yp, ycoef_m = a.r2, ycoef_p = a.r2;
-    auto ghost = [&](int face, int k, double own, double wrap, double& coef) -> double {
+    double       wym = a.r2, wyp = a.r2;  // y neighbours' weights: 1 across an Adjacented face
+    auto ghost = [&](int face, int k, double own, double wrap, double& w) -> double {
         switch (a.bc[face])
         {
             case 0: return 0.0;
@@ -368,27 +398,31 @@ __device__ __forceinline__ double composite_lap(const double* __restrict__ u, lo
             case 2: return wrap;
             default:
             {
-                coef = 1.0;
+                w = 1.0;
                 return a.nb[face][edge_index(face ^ 1, a.nbnx[face], a.nbny[face], k)];
             }
         }
     };
-    double dummy = 1.0;
-    xm = (i > 0) ? u[t - ny] : ghost(0, j, c, u[(long long)(nx - 1) * ny + j], dummy);
-    xp = (i < nx - 1) ? u[t + ny] : ghost(1, j, c, u[j], dummy);
-    ym = (j > 0) ? u[t - 1] : ghost(2, i, c, u[(long long)i * ny + ny - 1], ycoef_m);
-    yp = (j < ny - 1) ? u[t + 1] : ghost(3, i, c, u[(long long)i * ny], ycoef_p);
-    const double lap = xm + xp - 2.0 * c + a.r2 * ((j < ny - 1 || a.bc[3] != 3 ? yp : 0.0) +
-                                                   (j > 0 || a.bc[2] != 3 ? ym : 0.0) - 2.0 * c) +
-                       ((j == ny - 1 && a.bc[3] == 3) ? ycoef_p * yp : 0.0) +
-                       ((j == 0 && a.bc[2] == 3) ? ycoef_m * ym : 0.0);
-    return lap;
+    double       wx = 1.0;
+    const double xm = (i > 0) ? u[t - ny] : ghost(0, j, c, u[(long long)(nx - 1) * ny + j], wx);
+    const double xp = (i < nx - 1) ? u[t + ny] : ghost(1, j, c, u[j], wx);
+    const double ym = (j > 0) ? u[t - 1] : ghost(2, i, c, u[(long long)i * ny + ny - 1], wym);
+    const double yp = (j < ny - 1) ? u[t + 1] : ghost(3, i, c, u[(long long)i * ny], wyp);
+    double       hi = xm, lo = 0.0;
+    dd_acc(hi, lo, xp);
+    dd_acc(hi, lo, -2.0 * c);
+    dd_acc_prod(hi, lo, wym, ym);
+    dd_acc_prod(hi, lo, wyp, yp);
+    dd_acc_prod(hi, lo, a.r2, -2.0 * c);
+    double s, e;
+    two_sum(fs, -hi, s, e);
+    return s + (e - lo);
 }
 static __global__ void k_composite_residual(double* __restrict__ r, const double* __restrict__ fs,
-                                     const double* __restrict__ u, const ResidualArgs a)
+                                            const double* __restrict__ u, const ResidualArgs a)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)a.nx * a.ny) return;
-    r[t] = fs[t] - composite_lap(u, t, a);
+    r[t] = composite_residual_at(u, fs[t], t, a);
 }
 }  // namespace fpb
