@@ -43,6 +43,9 @@ struct FftDesc
     int      blue;  // 1: Bluestein
     int      in0, nin;    // Bluestein window: nonzero inputs [in0, in0+nin)
     int      out0, nout;  // and outputs kept [out0, out0+nout); (0, L, 0, L) for a direct transform
+    int      eng;   // 0: the stage engine of this file; 1: the register engine (fp_fft16.cuh, M a power of 2)
+    int      pad;   // shared-memory layout: element i in slot i + (i >> pad) (3 here, 4 for the register engine)
+    int      lgM;   // log2 M (register engine)
     int      nst;
     FftStage st[kFftMaxStages];
 };
@@ -355,10 +358,13 @@ template <typename T2, typename LD> __device__ void fft_execute_bluestein(T2* bu
     __syncthreads();
 }
 
-// Spectrum value X_k after fft_execute, k in the output window.
+// Slot of element i in the layout of plan d (either engine).
+__host__ __device__ __forceinline__ int fft_slot_d(const FftDesc& d, int i) { return i + (i >> d.pad); }
+
+// Spectrum value X_k after the transform, k in the output window (either engine).
 template <typename T2> __device__ __forceinline__ T2 fft_out(const T2* buf, const FftDesc& d, int k)
 {
-    return buf[fft_slot(k - d.out0)];
+    return buf[fft_slot_d(d, k - d.out0)];
 }
 
 // L - k for 0 < k <= L, and 0 for k = 0: the index of X_{-k}.

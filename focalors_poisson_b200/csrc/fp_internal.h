@@ -141,7 +141,9 @@ template <typename T> struct DevTransform
     int     threads = 128;
     size_t  smem    = 0;
 
-    DevTransform(int kind, int n);
+    // allow_register false: keep the plan on the stage engine (callers that launch plans of several
+    // lengths with one CTA shape).
+    DevTransform(int kind, int n, bool allow_register = true);
     // Everything but the rows for one direction.
     XformArgs<T> args(bool inverse) const;
     // rows = fields * nx contiguous rows of length n; in and out may alias.
@@ -169,7 +171,8 @@ template <typename T> struct DevRect
     mutable DevBuf                   scratch;                   // partition chase scratch (per batch)
 
     // sep_rows: separator-factor rows to tabulate (default nx / 32; larger for tables shared by a batch)
-    DevRect(int nx, int ny, double hx, double hy, const int* bc, int sep_rows = 0);
+    // with_transform false: chase tables only (no transform plan; tr stays null).
+    DevRect(int nx, int ny, double hx, double hy, const int* bc, int sep_rows = 0, bool with_transform = true);
     // In-place solve of `batch` back-to-back fields.
     void solve(T* f, long long batch, cudaStream_t s) const;
     // FP64 plans only: the same solve with FP32 transforms (FP64 rows in and out, FP64 chase); the
@@ -186,7 +189,10 @@ constexpr int kMaxDevices = 128;
 // Opt-in dynamic shared memory per CTA on the current device (cached per device).
 size_t max_dynamic_smem();
 // Sets func's MaxDynamicSharedMemorySize to max_dynamic_smem() on the current device, once per device.
+// Kernels must have been given that attribute before resident_ctas is asked about them.
 void allow_max_dynamic_smem(const void* func);
+// CTAs of `threads` threads and `smem` bytes of dynamic shared memory resident on the whole current device.
+long long resident_ctas(const void* func, int threads, size_t smem);
 
 }  // namespace fpb
 

@@ -4,7 +4,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <stdexcept>
+#include <string>
 
 namespace fpb
 {
@@ -184,10 +186,90 @@ HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit)
     return plan_fft(L, elem_bytes, smem_limit, FftWindow{0, L, 0, L}, FftWindow{0, L, 0, L});
 }
 
-HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftWindow iw)
+namespace
+{
+// FP_FFT_ENGINE=stage keeps every plan on the stage engine (for comparisons); unset or anything else lets
+// the planner pick the register engine where it applies.
+bool register_engine_allowed()
+{
+    const char* e = std::getenv("FP_FFT_ENGINE");
+    return !(e && std::string(e) == "stage");
+}
+
+// Natural-order FFT_M of the windowed Bluestein kernel (see bluestein_kernel), scaled by 1/M.
+std::vector<cld> bluestein_kernel_natural(int L, int M, const FftWindow& w)
+{
+    std::vector<cld> b(M, cld(0, 0));
+    const long long  delta = (long long)w.out0 - w.in0;
+    for (long long j = -(long long)(w.nin - 1); j <= (long long)w.nout - 1; ++j)
+    {
+        long long e = delta + j;
+        long long q = ((e % (2LL * L)) * (e % (2LL * L))) % (2LL * L);
+        b[(size_t)(((j % M) + M) % M)] = std::conj(root_of_unity(q, 2LL * L));
+    }
+    host_dft(b);
+    for (auto& x : b) x /= (long double)M;
+    return b;
+}
+
+// Register-engine plan (fp_fft16.cuh): L a power of two >= kRegMinM (direct), or an L that is not 7-smooth
+// (Bluestein) with a power-of-two convolution length. False when neither applies or the buffer and
+// tables exceed smem_limit; the stage engine then takes the length.
+bool plan_register(int L, size_t elem_bytes, size_t smem_limit, const FftWindow& fw, const FftWindow& iw, HostFft& h)
+{
+    const bool pow2  = L >= kRegMinM && (L & (L - 1)) == 0;
+    const int  max_M = elem_bytes >= 16 ? 8192 : 16384;  // FP64: 512 threads x 128 registers; FP32: 1024 x 64
+    int        M     = L;
+    if (!pow2)
+    {
+        if (!radices(L).empty()) return false;  // smooth: the stage engine runs it without Bluestein
+        const int need = std::max(window_span(L, fw), window_span(L, iw));
+        M              = kRegMinM;
+        while (M < need) M *= 2;
+    }
+    if (M > max_M) return false;
+    const size_t elems = (size_t)reg_buf_elems(M) + M / 16 + (pow2 ? 0 : reg_chirp_entries(L));
+    if (elems * elem_bytes > smem_limit) return false;
+    h.d      = FftDesc{};
+    h.d.L    = L;
+    h.d.M    = M;
+    h.d.blue = pow2 ? 0 : 1;
+    h.d.eng  = 1;
+    h.d.pad  = kRegPad;
+    int lg   = 0;
+    while ((1 << lg) < M) ++lg;
+    h.d.lgM = lg;
+    h.d.nst = 0;
+    h.tw.resize(M / 16);
+    for (int m = 0; m < M / 16; ++m) h.tw[m] = root_of_unity(m, M);
+    h.d_inv = h.d;
+    if (pow2)
+    {
+        set_window(h.d, FftWindow{0, L, 0, L});
+        set_window(h.d_inv, FftWindow{0, L, 0, L});
+        return true;
+    }
+    set_window(h.d, fw);
+    set_window(h.d_inv, iw);
+    // chirp tables: exp(-i pi b / L) for b < 64, then exp(-i pi 64 a / L) for 64 a < 2L
+    h.chirp.resize(reg_chirp_entries(L));
+    for (int b = 0; b < kChirpLo; ++b) h.chirp[b] = root_of_unity(b, 2LL * L);
+    for (int a = 0; kChirpLo + a < (int)h.chirp.size(); ++a)
+        h.chirp[kChirpLo + a] = root_of_unity((long long)kChirpLo * a, 2LL * L);
+    h.bhat = bluestein_kernel_natural(L, M, fw);
+    if (fw.in0 != iw.in0 || fw.nin != iw.nin || fw.out0 != iw.out0 || fw.nout != iw.nout)
+        h.bhat_inv = bluestein_kernel_natural(L, M, iw);
+    return true;
+}
+}  // namespace
+
+HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftWindow iw, bool allow_register)
 {
     HostFft h;
-    h.d.L = L;
+    if (allow_register && register_engine_allowed() && plan_register(L, elem_bytes, smem_limit, fw, iw, h)) return h;
+    h.d.L   = L;
+    h.d.eng = 0;
+    h.d.pad = 3;
     std::vector<int> rad = radices(L);
     if (!rad.empty() || L == 1)
     {

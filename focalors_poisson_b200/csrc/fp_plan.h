@@ -3,6 +3,7 @@
 #pragma once
 
 #include "fp_fft.cuh"
+#include "fp_fft16.cuh"
 
 #include <complex>
 #include <string>
@@ -59,17 +60,22 @@ struct HostFft
 {
     FftDesc                               d{};      // forward window
     FftDesc                               d_inv{};  // inverse window (same M, stages and tables)
-    std::vector<std::complex<long double>> tw;
-    std::vector<std::complex<long double>> chirp;
-    std::vector<std::complex<long double>> bhat;      // digit-reversed, scaled by 1/M
+    std::vector<std::complex<long double>> tw;     // stage engine: stage twiddles; register engine:
+                                                   // exp(-2 pi i m / M), m < M/16
+    std::vector<std::complex<long double>> chirp;  // stage engine: c_n, n < L; register engine: the two
+                                                   // chirp tables (fp_fft16.cuh reg_chirp)
+    std::vector<std::complex<long double>> bhat;      // scaled by 1/M; digit-reversed for the stage engine,
+                                                      // natural order for the register engine
     std::vector<std::complex<long double>> bhat_inv;  // kernel of the inverse window, if it differs
     std::vector<int>                       perm;
 };
 // Plans a length-L complex DFT whose single buffer must fit in smem_limit bytes for complex
 // elements of elem_bytes, with the forward and inverse windows fw and iw (used when L needs
-// Bluestein). Throws std::runtime_error if it cannot.
+// Bluestein): on the register engine (fp_fft16.cuh) when L is a power of two >= 512 or needs Bluestein
+// and a power-of-two convolution length fits (and allow_register), else on the stage engine
+// (fp_fft.cuh). Throws std::runtime_error if it cannot.
 HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit);
-HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftWindow iw);
+HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftWindow iw, bool allow_register = true);
 
 // Per-family tables computed with the reference's own double expressions so that the device
 // transform reproduces the reference's values, not merely the exact transform.

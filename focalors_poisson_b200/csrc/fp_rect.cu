@@ -3,8 +3,10 @@
 #include "fp_internal.h"
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <set>
+#include <tuple>
 #include <type_traits>
 
 namespace fpb
@@ -27,6 +29,26 @@ size_t max_dynamic_smem()
         cache[dev] = (size_t)optin - 1024;  // room for the kernel's static shared arrays
     }
     return cache[dev];
+}
+
+// CTAs of `threads` threads and `smem` dynamic shared memory that fit on the current device at once
+// (SMs x resident CTAs per SM), cached per (device, kernel, shape).
+long long resident_ctas(const void* func, int threads, size_t smem)
+{
+    static std::mutex                                                     mu;
+    static std::map<std::tuple<int, const void*, int, size_t>, long long> cache;
+    int                                                                   dev = 0;
+    FPB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    auto                        key = std::make_tuple(dev, func, threads, smem);
+    auto                        it  = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int per_sm = 0, sms = 0;
+    FPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem));
+    FPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long long v = (long long)std::max(1, per_sm) * std::max(1, sms);
+    cache[key]        = v;
+    return v;
 }
 
 // Function attributes are per device: the opt-in to max_dynamic_smem() is made once per (device, kernel).
@@ -60,18 +82,22 @@ template <typename T2> std::vector<T2> convert_c(const std::vector<std::complex<
     return r;
 }
 
-template <typename T, int K, int I, typename TIO>
+// One CTA per item on the stage engine; on the register engine as many CTAs as fit on the GPU at once,
+// each looping over items (its tables are loaded once per CTA).
+template <typename T, int K, int I, typename TIO, int ENG>
 void launch_k(const TransformArgs<T, TIO>& a, long long rows, int threads, size_t smem, cudaStream_t s)
 {
-    allow_max_dynamic_smem((const void*)k_transform<T, K, I, TIO>);
-    const long long grid = FamilyTraits<K, I>::kPairRows ? (rows + 1) / 2 : rows;
-    if (grid <= 0) return;
-    k_transform<T, K, I, TIO><<<(unsigned)grid, threads, smem, s>>>(a);
+    const void* fn = (const void*)k_transform<T, K, I, TIO, ENG>;
+    allow_max_dynamic_smem(fn);
+    const long long items = FamilyTraits<K, I>::kPairRows ? (rows + 1) / 2 : rows;
+    if (items <= 0) return;
+    const long long grid = ENG == 1 ? std::min<long long>(items, resident_ctas(fn, threads, smem)) : items;
+    k_transform<T, K, I, TIO, ENG><<<(unsigned)grid, threads, smem, s>>>(a);
     FPB_CHECK_LAUNCH();
 }
 }  // namespace
 
-template <typename T> DevTransform<T>::DevTransform(int kind_, int n_) : kind(kind_), n(n_)
+template <typename T> DevTransform<T>::DevTransform(int kind_, int n_, bool allow_register) : kind(kind_), n(n_)
 {
     if (n < 2) throw Error(1, "row length must be at least 2");
     if (kind == K_PP && (n % 2)) throw Error(1, "periodic transform needs an even length");
@@ -79,7 +105,8 @@ template <typename T> DevTransform<T>::DevTransform(int kind_, int n_) : kind(ki
     HostFft   h;
     try
     {
-        h = plan_fft(L, sizeof(T2), max_dynamic_smem(), fft_window(kind, n, false), fft_window(kind, n, true));
+        h = plan_fft(L, sizeof(T2), max_dynamic_smem(), fft_window(kind, n, false), fft_window(kind, n, true),
+                     allow_register);
     }
     catch (const std::runtime_error& e)
     {
@@ -110,10 +137,21 @@ template <typename T> DevTransform<T>::DevTransform(int kind_, int n_) : kind(ki
     if (!kt.c.empty()) tc = upload(convert_c<T2>(kt.c));
     s1      = (T)kt.s1;
     s2      = (T)kt.s2;
-    threads = std::min(512, std::max(64, ((fd.M / 16 + 31) / 32) * 32));
     const int K_scan = (n + 1) / 2;  // DD prefix-sum arrays: 2K values, in the buffer's tail when it fits
-    const int E      = fft_buf_elems(fd.M);
-    smem = (size_t)E * sizeof(T2) + ((kind == K_DD && E - fft_slot(fd.L) < K_scan) ? (size_t)2 * K_scan * sizeof(T) : 0);
+    int       E, tail;                // shared-memory elements; free slots past element L-1 of the buffer
+    if (fd.eng == 1)
+    {
+        threads = fd.M / 16;
+        E       = reg_smem_elems(fd);
+        tail    = reg_buf_elems(fd.M) - reg_slot(fd.L);
+    }
+    else
+    {
+        threads = std::min(512, std::max(64, ((fd.M / 16 + 31) / 32) * 32));
+        E       = fft_buf_elems(fd.M);
+        tail    = E - fft_slot(fd.L);
+    }
+    smem = (size_t)E * sizeof(T2) + ((kind == K_DD && tail < K_scan) ? (size_t)2 * K_scan * sizeof(T) : 0);
     if (smem > max_dynamic_smem()) throw Error(3, "transform of length " + std::to_string(n) + " needs more shared memory than a CTA has");
 }
 
@@ -145,8 +183,13 @@ void DevTransform<T>::run_io(const TIO* in, TIO* out, long long rows, bool inver
     const int inv = inverse ? 1 : 0;
 #define FPB_CASE(K)                                                                                        \
     case K:                                                                                                \
-        if (inv) launch_k<T, K, 1, TIO>(a, rows, threads, smem, s);                                         \
-        else launch_k<T, K, 0, TIO>(a, rows, threads, smem, s);                                             \
+        if (fd.eng == 1)                                                                                   \
+        {                                                                                                  \
+            if (inv) launch_k<T, K, 1, TIO, 1>(a, rows, threads, smem, s);                                  \
+            else launch_k<T, K, 0, TIO, 1>(a, rows, threads, smem, s);                                      \
+        }                                                                                                  \
+        else if (inv) launch_k<T, K, 1, TIO, 0>(a, rows, threads, smem, s);                                 \
+        else launch_k<T, K, 0, TIO, 0>(a, rows, threads, smem, s);                                          \
         break;
     switch (kind)
     {
@@ -273,7 +316,8 @@ void separator_factors(int ny, int pmax, const std::vector<double>& d, const std
     }
 }
 
-template <typename T> DevRect<T>::DevRect(int nx_, int ny_, double hx_, double hy_, const int* bc_, int sep_rows)
+template <typename T>
+DevRect<T>::DevRect(int nx_, int ny_, double hx_, double hy_, const int* bc_, int sep_rows, bool with_transform)
     : nx(nx_), ny(ny_), hx(hx_), hy(hy_)
 {
     for (int f = 0; f < 4; ++f) bc[f] = bc_[f];
@@ -284,7 +328,7 @@ template <typename T> DevRect<T>::DevRect(int nx_, int ny_, double hx_, double h
     const bool xp = bc[XNEG] == BC_PERIODIC && bc[XPOS] == BC_PERIODIC;
     if (!xp && (bc[XNEG] == BC_PERIODIC || bc[XPOS] == BC_PERIODIC || bc[XNEG] == BC_NULL || bc[XPOS] == BC_NULL))
         throw Error(1, "unsupported x boundary pair");
-    tr.reset(new DevTransform<T>(kind, ny));
+    if (with_transform) tr.reset(new DevTransform<T>(kind, ny));
     periodic_x = xp;
     singular   = !(dir_like(bc[0]) || dir_like(bc[1]) || dir_like(bc[2]) || dir_like(bc[3]));
     std::vector<double> d = x_diag(ny, hx, hy, bc[YNEG], bc[YPOS]);

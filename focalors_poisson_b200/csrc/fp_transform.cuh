@@ -22,6 +22,7 @@
 #pragma once
 
 #include "fp_fft.cuh"
+#include "fp_fft16.cuh"
 
 namespace fpb
 {
@@ -329,11 +330,29 @@ __device__ __forceinline__ void put_batch(TOUT* oa, TOUT* ob, const int* idx, co
     }
 }
 
+// Shared memory of a register-engine plan: the exchange buffer, then the rotation table (M/16 entries),
+// then the chirp tables (Bluestein plans); in elements of the complex type.
+__host__ __device__ __forceinline__ int reg_tables_off(const FftDesc& d) { return reg_buf_elems(d.M); }
+__host__ __device__ __forceinline__ int reg_smem_elems(const FftDesc& d)
+{
+    return reg_buf_elems(d.M) + (d.M >> 4) + (d.blue ? reg_chirp_entries(d.L) : 0);
+}
+// Register-engine kernels copy the plan's tables into shared memory once per CTA and plan.
+template <typename T>
+__device__ __forceinline__ void reg_tables_to_smem(const XformArgs<T>& a, typename Cplx<T>::type* buf)
+{
+    typedef typename Cplx<T>::type T2;
+    T2* stw = buf + reg_tables_off(a.fd);
+    reg_load_tables(a.fd, a.ft, stw, stw + (a.fd.M >> 4));
+}
+
 // One work item: rows fa (and fb, when has_b and the family pairs rows) of length a.n transformed into
 // oa (ob). buf: the item's shared-memory FFT buffer; rowsc: two scratch values. ACC: out += result
-// (FP64 accumulation of a correction) instead of out = result. Ends with the CTA synchronised.
-// Every element-wise pass handles kFftBatch elements per thread at a time, loads first.
-template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC>
+// (FP64 accumulation of a correction) instead of out = result. ENG: the plan's FFT engine (0 stage
+// engine, 1 register engine, whose tables the kernel has already put in shared memory after the buffer).
+// Ends with the CTA synchronised. Every element-wise pass handles kFftBatch elements per thread at a
+// time, loads first.
+template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG = 0>
 __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN* fa, const TIN* fb, TOUT* oa, TOUT* ob,
                                                bool has_b, typename Cplx<T>::type* buf, T* rowsc)
 {
@@ -358,7 +377,12 @@ __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN*
         }
         return mk<T2>(real_input<T, KIND, INV>(a, fa, e), has_b ? real_input<T, KIND, INV>(a, fb, e) : (T)0);
     };
-    if (a.fd.blue)
+    if constexpr (ENG == 1)
+    {
+        const T2* stw = buf + reg_tables_off(a.fd);
+        reg_transform(buf, a.fd, a.ft, stw, stw + (M >> 4), zval);
+    }
+    else if (a.fd.blue)
     {
         auto ld0 = [&](int i) -> T2 {
             if (i >= a.fd.nin) return mk<T2>(0, 0);
@@ -392,8 +416,9 @@ __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN*
     {
         // DD: X_{2k} = -Im Y_k (k >= 1), X_{2k+1} = Re Y_0 / 2 + sum_{q=1..k} Re Y_q; out_m = s1 X_{m+1}
         const int K  = (n + 1) / 2;  // odd outputs X_1, X_3, ...
-        // scan arrays: the slots past element L-1 when the buffer has K of them, else past the buffer
-        const int lo = fft_slot(L), hi = fft_buf_elems(M);
+        // scan arrays: the slots past element L-1 when the buffer has K of them, else past the buffer (and
+        // the register engine's tables)
+        const int lo = fft_slot_d(a.fd, L), hi = ENG == 1 ? reg_smem_elems(a.fd) : fft_buf_elems(M);
         T*        ca = reinterpret_cast<T*>(buf + ((hi - lo >= K) ? lo : hi));
         T*        cb = ca + K;
         for (int k0 = threadIdx.x; k0 <= n / 2; k0 += U * nt)
@@ -466,25 +491,40 @@ __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN*
     __syncthreads();
 }
 
-// Register cap (FP64 80): three CTAs of 256 threads per SM, as many as a 4096-point FP64 buffer allows.
-template <typename T, int KIND, int INV, typename TIO = T>
-__global__ void __maxnreg__(sizeof(T) == 8 ? 80 : 64) k_transform(const TransformArgs<T, TIO> a)
+// Register caps. Stage engine: FP64 80, so that three CTAs of 256 threads fit per SM, as many as a
+// 4096-point FP64 buffer allows. Register engine (16 complex values per thread, M/16 threads per CTA):
+// FP64 128 (plans up to M = 8192, 512 threads, 64 K registers), FP32 64 (plans up to M = 16384, 1024
+// threads).
+template <int ENG, typename T> constexpr int xform_maxnreg()
+{
+    return ENG == 1 ? (sizeof(T) == 8 ? 128 : 64) : (sizeof(T) == 8 ? 80 : 64);
+}
+
+// Each CTA takes items (row pairs) blockIdx.x, blockIdx.x + gridDim.x, ... and, on the register engine,
+// loads the plan's tables into shared memory once.
+template <typename T, int KIND, int INV, typename TIO = T, int ENG = 0>
+__global__ void __maxnreg__((xform_maxnreg<ENG, T>())) k_transform(const TransformArgs<T, TIO> a)
 {
     typedef typename Cplx<T>::type T2;
     extern __shared__ __align__(16) unsigned char fp_smem_raw[];
     T2*          buf = reinterpret_cast<T2*>(fp_smem_raw);
     __shared__ T rowsc[2];
 
-    constexpr bool  kPair = FamilyTraits<KIND, INV>::kPairRows;
-    const int       n     = a.n;
-    const long long r0    = kPair ? 2LL * blockIdx.x : (long long)blockIdx.x;
-    if (r0 >= a.rows) return;
-    const bool has_b = kPair && r0 + 1 < a.rows;
-    const TIO* fa    = a.in + r0 * n;
-    const TIO* fb    = has_b ? fa + n : fa;
-    TIO*       oa    = a.out + r0 * n;
-    TIO*       ob    = has_b ? oa + n : nullptr;
-    transform_rows<T, KIND, INV, TIO, TIO, false>(a, fa, fb, oa, ob, has_b, buf, rowsc);
+    constexpr bool  kPair  = FamilyTraits<KIND, INV>::kPairRows;
+    const int       n      = a.n;
+    const long long nitems = kPair ? (a.rows + 1) / 2 : a.rows;
+    if ((long long)blockIdx.x >= nitems) return;
+    if constexpr (ENG == 1) reg_tables_to_smem(a, buf);
+    for (long long it = blockIdx.x; it < nitems; it += gridDim.x)
+    {
+        const long long r0    = kPair ? 2LL * it : it;
+        const bool      has_b = kPair && r0 + 1 < a.rows;
+        const TIO*      fa    = a.in + r0 * n;
+        const TIO*      fb    = has_b ? fa + n : fa;
+        TIO*            oa    = a.out + r0 * n;
+        TIO*            ob    = has_b ? oa + n : nullptr;
+        transform_rows<T, KIND, INV, TIO, TIO, false, ENG>(a, fa, fb, oa, ob, has_b, buf, rowsc);
+    }
 }
 
 }  // namespace fpb

@@ -27,18 +27,18 @@ def driver(tmp_path_factory):
     return out
 
 
-def plan(driver, kind, n):
-    txt = subprocess.run([driver, str(kind), str(n)], check=True, capture_output=True, text=True).stdout
-    p = {"c": [], "b": [], "i": []}
+def plan(driver, kind, n, engine="stage"):
+    txt = subprocess.run([driver, str(kind), str(n), engine], check=True, capture_output=True, text=True).stdout
+    p = {"c": [], "b": [], "i": [], "t": []}
     for line in txt.splitlines():
         f = line.split()
         if f[0] in ("fwd", "inv"):
-            p[f[0]] = dict(zip(("L", "M", "blue", "in0", "nin", "out0", "nout"), map(int, f[1:])))
+            p[f[0]] = dict(zip(("L", "M", "blue", "in0", "nin", "out0", "nout", "eng", "lgM"), map(int, f[1:])))
         elif f[0] == "radices":
             p["radices"] = [int(x) for x in f[1:]]
         else:
             p[f[0]].append(complex(float(f[1]), float(f[2])))
-    for k in ("c", "b", "i"):
+    for k in ("c", "b", "i", "t"):
         p[k] = np.array(p[k])
     return p
 
@@ -124,3 +124,84 @@ def test_bluestein_tables_batch_sizes(driver, kind):
             assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), (kind, n, tag)
         checked += 1
     assert checked >= 5
+
+
+# ---------------------------------------------------------------------------------------------------
+# Register engine (csrc/fp_fft16.cuh): Stockham passes on 16 registers per thread, replayed in numpy with
+# the plan's own tables
+# ---------------------------------------------------------------------------------------------------
+def reg_fft(x, tw):
+    """The register engine's forward FFT of x (length M = 2^m >= 512) with its pass order (a radix
+    2^(m mod 4) pass first, then radix-16 passes), the column layout of thread t (elements t + T q), the
+    exchange destinations (j / Ns) Ns R + j mod Ns + r Ns and the rotation base tw[(j mod Ns) M / (16 Ns)]."""
+    M = len(x)
+    T = M // 16
+    m = M.bit_length() - 1
+    radices = ([2 ** (m % 4)] if m % 4 else []) + [16] * (m // 4)
+    col = x.reshape(16, T).T.copy()  # col[t, q] = x[t + T q]
+    Ns = 1
+    for R in radices:
+        B = 16 // R
+        dest = np.zeros(M, complex)
+        last = Ns * R == M
+        for t in range(T):
+            for b in range(B):
+                j = t + b * T
+                q = b + np.arange(R) * B
+                legs = col[t, q]
+                k = j % Ns
+                if Ns > 1 and k:
+                    legs = legs * tw[k * (M // (16 * Ns))] ** np.arange(R)
+                out = np.fft.fft(legs)
+                if last:
+                    col[t, q] = out
+                else:
+                    dest[(j // Ns) * Ns * R + k + np.arange(R) * Ns] = out
+        if not last:
+            col = dest.reshape(16, T).T.copy()
+        Ns *= R
+    return col.T.reshape(M)
+
+
+def reg_chirp(c, L, e):
+    """c_e from the two chirp tables: exp(-i pi m / L), m = e^2 mod 2L = 64 a + b."""
+    m = (np.asarray(e, dtype=np.int64) ** 2) % (2 * L)
+    return c[64 + (m >> 6)] * c[m & 63]
+
+
+@pytest.mark.parametrize("kind,n", [(K_DD, 2048), (K_DD, 1000), (K_DD, 512), (K_ND, 2048), (K_DN, 1000),
+                                    (K_DD, 4096), (K_NN, 2048)])
+def test_register_engine_plans_replay_dft(driver, kind, n):
+    """Register-engine plans: the power-of-two length (direct when L is a power of two, else the smallest one
+    covering the window's convolution), the rotation table and the two-level chirp tables; the engine's
+    passes replayed on them give the DFT (Bluestein: pre-chirp, forward FFT, kernel product in natural
+    order, conjugate, forward FFT, conjugate, post-chirp)."""
+    p = plan(driver, kind, n, "register")
+    f = p["fwd"]
+    L, M = f["L"], f["M"]
+    assert f["eng"] == 1 and M == 2 ** f["lgM"] and M >= 512
+    assert np.allclose(p["t"], np.exp(-2j * np.pi * np.arange(M // 16) / M), atol=1e-18)
+    rng = np.random.default_rng(n + 10 * kind)
+    if not f["blue"]:
+        assert M == L
+        z = rng.standard_normal(L) + 1j * rng.standard_normal(L)
+        got = reg_fft(z, p["t"])
+        ref = np.fft.fft(z)
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+        return
+    full = f["nin"] == L and f["nout"] == L
+    need = 2 * L - 2 if full else max(f["nin"] + f["nout"], p["inv"]["nin"] + p["inv"]["nout"]) - 1
+    assert need <= M < 2 * need
+    assert len(p["c"]) == 64 + (2 * L + 63) // 64
+    for tag, bhat in (("fwd", p["b"]), ("inv", p["i"] if len(p["i"]) else p["b"])):
+        w = p[tag]
+        z = np.zeros(L, complex)
+        z[w["in0"]: w["in0"] + w["nin"]] = rng.standard_normal(w["nin"]) + 1j * rng.standard_normal(w["nin"])
+        a = np.zeros(M, complex)
+        e = np.arange(w["nin"]) + w["in0"]
+        a[: w["nin"]] = z[e] * reg_chirp(p["c"], L, e)
+        y = np.conj(reg_fft(np.conj(reg_fft(a, p["t"]) * bhat), p["t"]))
+        k = np.arange(w["nout"]) + w["out0"]
+        got = y[: w["nout"]] * reg_chirp(p["c"], L, k)
+        ref = np.fft.fft(z)[k]
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), (kind, n, tag)
