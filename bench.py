@@ -113,6 +113,24 @@ def replica_value(steps: int, world: int, ms: float) -> float:
     return steps * world / (ms / 1e3)
 
 
+def partition_problems(cells, world: int):
+    """Split independent problems over `world` ranks, balanced by cells: the largest problems first, each onto
+    the rank with the fewest cells so far (ties to the lower rank). Deterministic, so every rank computes the
+    same split without communicating. Returns one sorted list of problem indices per rank."""
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for p in sorted(range(len(cells)), key=lambda i: (-cells[i], i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(p)
+        load[r] += cells[p]
+    return [sorted(x) for x in parts]
+
+
+def sharded_value(problems: int, ms_max: float) -> float:
+    """Whole-job solves/s of one batch of `problems` split over the ranks, the slowest rank taking ms_max."""
+    return problems / (ms_max / 1e3)
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -208,25 +226,34 @@ BATCH_PROBLEMS = 512
 BATCH_FORMS = (("f64", 0), ("f32", 3))  # (storage precision, refinement steps)
 
 
-def batched_section(args, dev, rank):
+def batched_section(args, dev, rank, world=1, dist=None):
     """solves/s of the batched workload in its FP64-direct and FP32+refinement forms (each step: refill the
-    512 right-hand sides from a resident copy, then one replay of the captured graph), their accuracy
-    against the FP64 solve refined twice, the plain per-problem FP64 path on a sample, and the reference
-    CPU build on a sample."""
+    right-hand sides from a resident copy, then one replay of the captured graph), their accuracy against
+    the FP64 solve refined twice, the plain per-problem FP64 path on a sample, and the reference CPU build
+    on a sample. With several ranks the 512 problems are split between them (partition_problems), one
+    batch and one captured graph per GPU; no data crosses between GPUs, and the job's time is the slowest
+    rank's."""
     import torch
 
     from focalors_poisson_b200 import capi
     from focalors_poisson_b200 import workloads as W
 
-    probs, rhs = W.batched_uneven(BATCH_PROBLEMS, SEED)
+    all_probs, all_rhs = W.batched_uneven(BATCH_PROBLEMS, SEED)
+    mine = partition_problems([g.cells() for g in all_probs], world)[rank]
+    probs, rhs = [all_probs[p] for p in mine], [all_rhs[p] for p in mine]
     flat = [x for r in rhs for x in r]
     cells = sum(int(x.size) for x in flat)
     pristine = [torch.tensor(x, device=dev) for x in flat]
     work = [torch.empty_like(p) for p in pristine]
     starts = np.cumsum([0] + [len(g.nx) for g in probs])
     out = {"workload": f"{BATCH_PROBLEMS} L/T problems (3-4 subdomains, sides uniform in 64..1024 step 32, "
-                       f"seed {SEED}), Dirichlet outer faces, N(0,1) RHS", "cells": cells,
+                       f"seed {SEED}), Dirichlet outer faces, N(0,1) RHS",
+           "cells": sum(g.cells() for g in all_probs),
            "l2_policy": "inputs larger than L2 (4.4 GB of FP64 fields re-filled each step)", "forms": {}}
+    if world > 1:
+        out["sharding"] = {"ranks": world, "split": "problems balanced by cells, one batch and one graph per GPU, "
+                                                    "no collective on the data path",
+                           "problems_rank0": len(mine), "cells_rank0": cells}
 
     def refill():
         for w, p in zip(work, pristine):
@@ -240,7 +267,8 @@ def batched_section(args, dev, rank):
     exact = [w.clone() for w in work]
     del ref
     lib = capi.lib()
-    csample = list(range(0, BATCH_PROBLEMS, 128))  # problems the reference also solves (CPU leg below)
+    # problems the reference also solves (CPU leg below, rank 0): every 128th of this rank's share
+    csample = list(range(0, len(probs), 128))
     sample_out = {}
     for prec, steps in BATCH_FORMS:
         t0 = time.perf_counter()
@@ -259,10 +287,10 @@ def batched_section(args, dev, rank):
             b.solve(work, steps=steps, graph=True)
         e1.record()
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
         launches = (lib.fp_launch_count() - l0) / args.steps
         perr = []
-        for p in range(BATCH_PROBLEMS):
+        for p in range(len(probs)):
             rng_ = range(starts[p], starts[p + 1])
             num = sum(float(((work[d] - exact[d]) ** 2).sum()) for d in rng_)
             den = sum(float((exact[d] ** 2).sum()) for d in rng_)
@@ -272,8 +300,9 @@ def batched_section(args, dev, rank):
         key = f"{prec}" + (f"+ir{steps}" if steps else "")
         sample_out[key] = {p: [work[d].cpu().numpy() for d in range(starts[p], starts[p + 1])] for p in csample}
         out["forms"][key] = {
-            "solves_per_s": BATCH_PROBLEMS / (ms / 1e3), "ms_per_batch": ms, "setup_s": setup,
-            "max_rel_l2_vs_refined": max(perr), "max_rel_residual": float(res.max()),
+            "solves_per_s": sharded_value(BATCH_PROBLEMS, ms), "ms_per_batch": ms, "setup_s": setup,
+            "max_rel_l2_vs_refined": max_over_ranks(max(perr), dist, dev),
+            "max_rel_residual": max_over_ranks(float(res.max()), dist, dev),
             "gpu_launches_per_batch": launches, "graph_kernels": info["graph_kernels"],
             "launch_shape": {k: info[k] for k in ("dst_threads", "dst_blocks_per_sm", "chase_threads")}}
         del b
@@ -282,7 +311,7 @@ def batched_section(args, dev, rank):
     out["headline_form"] = max(ok, key=lambda k: ok[k]["solves_per_s"]) if ok else None
     # plain FP64 GPU path: the single-problem C-ABI Schur GMRES solve (FP_NO_SPECTRAL), one problem after
     # another, on every 32nd problem (setup excluded)
-    sample = list(range(0, BATCH_PROBLEMS, 32))
+    sample = list(range(0, len(probs), 32))
     tot = 0.0
     for p in sample:
         solver = capi.Composite(probs[p], 20, 1e-12, 100, spectral=False)
@@ -708,10 +737,10 @@ def main():
                 "solve_seconds": ref["seconds"], "refine_seconds": ref["refine_seconds"]}
         for form in forms_run:
             res[form].pop("host", None)
-    if not args.no_batched and world == 1:
+    if not args.no_batched:
         del solver, pristine, work
         torch.cuda.empty_cache()
-        line["batched_uneven"] = batched_section(args, dev, rank)
+        line["batched_uneven"] = batched_section(args, dev, rank, world, dist)
     if args.large and world == 1:
         line["large_tree"] = large_section(args, dev)
     if rank == 0:

@@ -239,10 +239,11 @@ def lt_problem(seed: int, sides=SIDES) -> Geometry:
                     names)
 
 
-def batched_uneven(count: int = 512, seed: int = 2024):
+def batched_uneven(count: int = 512, seed: int = 2024, rhs: bool = True):
     """The batched-uneven workload: `count` independent L/T problems (problem p uses seed + p) and their
-    seeded N(0,1) right-hand sides (seed + p + 1000003)."""
+    seeded N(0,1) right-hand sides (seed + p + 1000003; None with rhs=False)."""
     geos = [lt_problem(seed + p) for p in range(count)]
-    rhs = [gaussian_rhs(g, seed + p + 1000003, zero_mean=False) for p, g in enumerate(geos)]
-    return geos, rhs
+    if not rhs:
+        return geos, None
+    return geos, [gaussian_rhs(g, seed + p + 1000003, zero_mean=False) for p, g in enumerate(geos)]
 

@@ -81,3 +81,32 @@ def test_schur_gmres_path_matches_reference(case):
     assert info["converged"], info
     assert RS.rel_l2(got, ref["refined"]) <= 1e-10
     assert RS.rel_l2(got, ref["plain"]) <= max(1e-10, 3.0 * ref["rel_correction"])
+
+
+@pytest.fixture(scope="module")
+def tree_case():
+    """The 9-subdomain tree of the large composite workload (centre, 4 arms, 4 corners on the N / S arms,
+    W / E arms periodic in y, Neumann tip faces) at 128^2 per subdomain with its 32-bump right-hand side.
+    Its depth-2 tree makes the reference build the Schur matrices of the internal arms itself, one subtree
+    solve per interface cell (about a minute on 16 host threads at this size)."""
+    assert R.available(), "oracle/_ref/libfpref.so (the reference's own sources, built by build()) is missing"
+    g = W.tree9_large(128)
+    rhs = W.gaussian_bumps_rhs(g, 5)
+    return g, rhs, RS.reference_answer(g, rhs, 20, 1e-12, 100)
+
+
+@pytest.mark.parametrize("form", ["f64", "f32ir"])
+def test_large_tree_matches_reference(tree_case, form):
+    """Root Schur GMRES with the internal children's Schur matrices from batched spectral subtree solves
+    (FP64), and FP32-transform inner solves in FP64 refinement, against the reference's refined answer."""
+    g, rhs, ref = tree_case
+    solver = capi.Composite(g, 20, 1e-14, 200)
+    if form == "f64":
+        got, info = _gpu(solver, rhs, lambda s, t: s.solve(t))
+        bound = 1e-10
+    else:
+        got, info = _gpu(solver, rhs, lambda s, t: s.solve_ir(t, rel_tol=1e-13, max_refine=10))
+        bound = 1e-12
+    err = RS.rel_l2(got, ref["refined"])
+    assert err <= bound, (form, err, info)
+    assert RS.rel_l2(got, ref["plain"]) <= max(bound, 3.0 * ref["rel_correction"])
