@@ -28,6 +28,7 @@ SIGNATURES = {
     "fp_transform_f32": ([_i, _i, _i, _i, _i, _vp, _vp, _i, _vp], _i),
     "fp_rect_create": ([_i, _i, _d, _d, _vp, _i, _vp], _i),
     "fp_rect_solve_f64": ([_vp, _vp, _ll, _i, _vp], _i),
+    "fp_rect_chase_f64": ([_vp, _vp, _ll, _i, _vp], _i),
     "fp_rect_solve_f32": ([_vp, _vp, _ll, _i, _vp], _i),
     "fp_rect_destroy": ([_vp], _i),
     "fp_rect_solve_f64_noalloc": ([_vp, _vp, _ll, _vp], _i),
@@ -151,6 +152,17 @@ class Rect:
         p, flags, stream, keep = _args(f, want)
         fn = lib().fp_rect_solve_f32 if want == np.float32 else lib().fp_rect_solve_f64
         check(fn(self.h, p, batch, flags, stream))
+        if not _is_torch(f) and keep is not f:
+            f[...] = keep
+        return f
+
+    def chase(self, f):
+        """The chasing step alone (ChasingMethod2D::chasing) on fields already in transformed space; FP64."""
+        if self.precision != FP_F64 or f.shape[-2:] != (self.nx, self.ny):
+            raise ValueError("chase needs an FP64 solver and fields of its shape")
+        batch = int(np.prod(f.shape[:-2])) if len(f.shape) > 2 else 1
+        p, flags, stream, keep = _args(f, np.float64)
+        check(lib().fp_rect_chase_f64(self.h, p, batch, flags, stream))
         if not _is_torch(f) and keep is not f:
             f[...] = keep
         return f

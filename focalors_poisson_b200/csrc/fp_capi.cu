@@ -86,8 +86,9 @@ using namespace fpb;
 
 namespace fpb
 {
+// The whole solve, or with chase_only the chasing step alone (the field is in transformed space).
 template <typename T, typename R>
-void rect_solve(fp_rect* r, R* plan, T* f, long long batch, int flags, void* stream)
+void rect_solve(fp_rect* r, R* plan, T* f, long long batch, int flags, void* stream, bool chase_only = false)
 {
     if (!plan) throw Error(FP_ERR_INVALID, "solver was created with the other precision");
     if (!f) throw Error(FP_ERR_INVALID, "null field pointer");
@@ -95,14 +96,16 @@ void rect_solve(fp_rect* r, R* plan, T* f, long long batch, int flags, void* str
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (flags & FP_DEVICE)
     {
-        plan->solve(f, batch, s);
+        if (chase_only) plan->chase_alone(f, batch, s);
+        else plan->solve(f, batch, s);
         if (flags & FP_SYNC) FPB_CUDA(cudaStreamSynchronize(s));
         return;
     }
     const size_t bytes = (size_t)batch * plan->nx * plan->ny * sizeof(T);
     r->staging.ensure(bytes);
     FPB_CUDA(cudaMemcpyAsync(r->staging.get(), f, bytes, cudaMemcpyHostToDevice, s));
-    plan->solve(r->staging.as<T>(), batch, s);
+    if (chase_only) plan->chase_alone(r->staging.as<T>(), batch, s);
+    else plan->solve(r->staging.as<T>(), batch, s);
     FPB_CUDA(cudaMemcpyAsync(f, r->staging.get(), bytes, cudaMemcpyDeviceToHost, s));
     FPB_CUDA(cudaStreamSynchronize(s));
 }
@@ -155,6 +158,14 @@ int fp_rect_solve_f32(fp_rect* r, float* f, long long batch, int flags, void* st
     return guarded([&] {
         if (!r) throw Error(FP_ERR_INVALID, "null solver");
         rect_solve<float>(r, r->r32.get(), f, batch, flags, stream);
+    });
+}
+
+int fp_rect_chase_f64(fp_rect* r, double* f, long long batch, int flags, void* stream)
+{
+    return guarded([&] {
+        if (!r) throw Error(FP_ERR_INVALID, "null solver");
+        rect_solve<double>(r, r->r64.get(), f, batch, flags, stream, true);
     });
 }
 

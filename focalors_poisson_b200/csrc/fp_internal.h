@@ -183,6 +183,8 @@ template <typename T> struct DevRect
     long long chase_scratch_elems(long long batch) const;
     // The chase alone, with caller-provided scratch of chase_scratch_elems(batch) elements.
     void chase(T* f, long long batch, T* scratch, cudaStream_t s) const;
+    // The chase alone on fields already in transformed space, scratch from the plan.
+    void chase_alone(T* f, long long batch, cudaStream_t s) const;
 };
 
 constexpr int kMaxDevices = 128;

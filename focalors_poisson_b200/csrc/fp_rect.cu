@@ -425,6 +425,14 @@ template <typename T> void DevRect<T>::solve(T* f, long long batch, cudaStream_t
     tr->run(f, f, batch * nx, true, s);
 }
 
+template <typename T> void DevRect<T>::chase_alone(T* f, long long batch, cudaStream_t s) const
+{
+    if (batch <= 0) return;
+    const long long need = chase_scratch_elems(batch);
+    if (need) scratch.ensure((size_t)need * sizeof(T));
+    chase(f, batch, scratch.as<T>(), s);
+}
+
 template struct DevTransform<double>;
 template struct DevTransform<float>;
 template void DevTransform<float>::run_io<double>(const double*, double*, long long, bool, cudaStream_t) const;

@@ -69,6 +69,11 @@ typedef struct fp_rect fp_rect;
 int fp_rect_create(int nx, int ny, double hx, double hy, const int* bc, int precision, fp_rect** out);
 int fp_rect_solve_f64(fp_rect* r, double* f, long long batch, int flags, void* stream);
 int fp_rect_solve_f32(fp_rect* r, float* f, long long batch, int flags, void* stream);
+/* The chasing step of PoissonSolver2D::solve alone (ChasingMethod2D::chasing, reference
+ * pe/poisson/chasing_method2d.cpp:3-89): every wavenumber's tridiagonal system along x solved in place on
+ * fields that are already in the y-transformed space, FP_F64 solvers. Same pointer and stream semantics as
+ * fp_rect_solve_f64. */
+int fp_rect_chase_f64(fp_rect* r, double* f, long long batch, int flags, void* stream);
 int fp_rect_destroy(fp_rect* r);
 
 /* fp_rect_solve_f64 for callers that cannot allocate device memory when they solve: code whose device

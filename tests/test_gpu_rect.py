@@ -85,3 +85,20 @@ def test_rect_batched_device_vs_oracle(shape):
         t32 = torch.tensor(f, device="cuda", dtype=torch.float32)
         capi.Rect(nx, ny, hx, hy, bc, precision=capi.FP_F32).solve(t32)
         assert rel_max(t32.double().cpu().numpy(), ref) <= 5e-3, (bc, "f32")
+
+
+@pytest.mark.parametrize("nx,ny,bc", [(128, 96, (0, 1, 1, 0)), (50, 64, (1, 1, 0, 0)), (64, 40, (2, 2, 1, 1))])
+def test_chase_entry_composes_the_solve(nx, ny, bc):
+    """fp_rect_chase_f64 is the solve's middle step: forward transform, chase, inverse transform through three
+    separate C-ABI calls equal one fp_rect_solve_f64."""
+    torch = torch_cuda()
+    rect = capi.Rect(nx, ny, 1.0 / nx, 1.0 / ny, bc)
+    f = torch.randn(2, nx, ny, dtype=torch.float64, device="cuda")
+    want = f.clone()
+    rect.solve(want)
+    got = f.clone()
+    capi.transform(bc[2], bc[3], got, out=got)
+    rect.chase(got)
+    capi.transform(bc[2], bc[3], got, inverse=True, out=got)
+    torch.cuda.synchronize()
+    assert rel_max(got.cpu().numpy(), want.cpu().numpy()) <= 1e-13
