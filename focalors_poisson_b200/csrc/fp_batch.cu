@@ -115,6 +115,7 @@ struct ChaseTabDev
     int           end_neu;  // x+ face Neumann: last separator diagonal d + 1 (x- Neumann is in the type-0 tables)
     const double* scp;      // separator Thomas factors c_p [p][j] (rows not last)
     const double* sid;      // 1 / den_p [p][j]
+    const double* cc_back;  // a copy of cc read by the back substitution (see k_b_chase_local)
 };
 
 template <typename T> struct ChaseSeg
@@ -160,8 +161,11 @@ __device__ __forceinline__ double mod_rhs(const ChaseSeg<T>* __restrict__ sg, in
 // Interior rows of the chunks. Modifiers: a row term can only fall on interior row 0 of chunk 0 (row
 // nx-1 is the last separator, handled by k_b_chase_reduced); column terms add s_c[i] psi_c(j) to every
 // row, applied as one pass per term over the thread's 31 rows.
+// The back substitution reads its factors from a second copy of the table: from the same addresses the
+// compiler keeps all 31 forward-sweep factors live in registers until the backward sweep (158 registers,
+// 3 CTAs of 128 threads per SM); from a distinct array it loads them again, and two CTAs of 256 threads fit.
 template <typename T>
-__global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __restrict__ segs,
+__global__ void __launch_bounds__(256, 2) k_b_chase_local(const ChaseSeg<T>* __restrict__ segs,
                                                        const long long* __restrict__ prefix, int nseg,
                                                        const ChaseTabDev* __restrict__ tabs)
 {
@@ -176,6 +180,7 @@ __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __rest
     const T*      col = sg->in + (long long)p * kChunk * ny + j;
     T*            out = sg->out + (long long)p * kChunk * ny + j;
     const double* c   = tabs[sg->tab].cc + (long long)typ * Li * ny + j;
+    const double* cb  = tabs[sg->tab].cc_back + (long long)typ * Li * ny + j;
     double        y[Li];
 #pragma unroll
     for (int r = 0; r < Li; ++r) y[r] = (double)col[(long long)r * ny];
@@ -198,7 +203,7 @@ __global__ void __launch_bounds__(256) k_b_chase_local(const ChaseSeg<T>* __rest
         y[r] = prev;
     }
 #pragma unroll
-    for (int r = Li - 2; r >= 0; --r) y[r] = y[r] - __ldg(c + (long long)r * ny) * y[r + 1];
+    for (int r = Li - 2; r >= 0; --r) y[r] = y[r] - __ldg(cb + (long long)r * ny) * y[r + 1];
 #pragma unroll
     for (int r = 0; r < Li; ++r) out[(long long)r * ny] = (T)y[r];
     double* ze = sg->zend + (long long)(p * 2) * ny + j;
@@ -1078,6 +1083,7 @@ private:
     PlanSet<double>                           eplans_;  // FP64 DSTs of edge vectors (length nx of roots)
     std::map<std::pair<int, double>, int>     tab_index_;
     std::vector<std::unique_ptr<DevRect<double>>> tabs_;  // chase tables (FP64 in both storage precisions)
+    std::vector<DevBuf>                           tab_back_;  // the back substitution's copy of each cc
     DevBuf                                    tabs_dev_;
     DevBuf                                    W_, X_, fs_, r_, chs_;  // work, chase out, IR, chase scratch
     DevBuf                                    edge_;  // bY, gYp, sYp, yYp per y-edge (nx each), per problem
@@ -1205,8 +1211,13 @@ template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDe
     plans_.finish();
     std::vector<ChaseTabDev> tv;
     for (auto& t : tabs_)
+    {
+        tab_back_.emplace_back(t->cc.bytes());
+        FPB_CUDA(cudaMemcpy(tab_back_.back().get(), t->cc.get(), t->cc.bytes(), cudaMemcpyDeviceToDevice));
         tv.push_back({t->cc.as<double>(), t->cg.as<double>(), t->chh.as<double>(), t->cends.as<double>(),
-                      t->dsep.as<double>(), t->end_neumann ? 1 : 0, t->sep_cp.as<double>(), t->sep_iden.as<double>()});
+                      t->dsep.as<double>(), t->end_neumann ? 1 : 0, t->sep_cp.as<double>(), t->sep_iden.as<double>(),
+                      tab_back_.back().as<double>()});
+    }
     tabs_dev_ = upload(tv);
     W_.alloc((size_t)cells_ * sizeof(TS));
     X_.alloc((size_t)cells_ * sizeof(TS));

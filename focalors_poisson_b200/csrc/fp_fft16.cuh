@@ -19,9 +19,8 @@
 // forward FFT ends with the spectrum in registers, the product with the kernel transform (natural order,
 // read from global memory in the column layout, coalesced) and the conjugation happen in registers, and
 // the second FFT starts from them: the kernel product costs no shared-memory sweep at all. The chirp
-// c_e = exp(-i pi e^2 / L) is the product of two entries of small shared-memory tables (exp(-i pi m / L)
-// split as m = 64 a + b), and the pass rotations come from one shared-memory table of exp(-2 pi i m / M),
-// m < M/16; all three tables are copied from global memory once per CTA.
+// c_e = exp(-i pi e^2 / L), e < L, and the pass rotations exp(-2 pi i m / M), m < M/16, are tables that
+// each CTA copies from global memory into shared memory once.
 //
 // Shared memory: element i lives in slot i + i/16 (the radix-16 destinations j*16 + r of the first pass
 // then fall in distinct bank groups across a quarter warp for 16-byte elements and a half warp for
@@ -36,13 +35,11 @@ namespace fpb
 constexpr int kRegE    = 16;   // elements per thread
 constexpr int kRegPad  = 4;    // slot(i) = i + (i >> kRegPad)
 constexpr int kRegMinM = 512;  // at least one warp per FFT
-constexpr int kChirpLo = 64;   // chirp table split: exp(-i pi m / L), m = 64 a + b
 
 __host__ __device__ __forceinline__ int reg_slot(int i) { return i + (i >> kRegPad); }
 __host__ __device__ __forceinline__ int reg_buf_elems(int M) { return M + (M >> kRegPad); }
-// Entries of the chirp tables for length L: kChirpLo values exp(-i pi b / L), then the values
-// exp(-i pi 64 a / L) for 64 a < 2L.
-__host__ __device__ __forceinline__ int reg_chirp_entries(int L) { return kChirpLo + (2 * L + kChirpLo - 1) / kChirpLo; }
+// Entries of the chirp table for length L: c_e, e < L.
+__host__ __device__ __forceinline__ int reg_chirp_entries(int L) { return L; }
 
 // v * exp(-2 pi i m / 16) for a compile-time m in 0..15.
 template <int m, typename T2> __device__ __forceinline__ T2 w16mul(T2 v)
@@ -178,14 +175,10 @@ __device__ __forceinline__ void reg_fft(T2 (&v)[kRegE], T2* buf, int M, int lgM,
     }
 }
 
-// c_e = exp(-i pi e^2 / L) from the two chirp tables in shared memory (0 <= e < L).
-template <typename T2> __device__ __forceinline__ T2 reg_chirp(const T2* __restrict__ ch, int e, int L)
-{
-    const int m = (int)(((long long)e * e) % (2LL * L));
-    return cmul(ch[kChirpLo + (m >> 6)], ch[m & (kChirpLo - 1)]);
-}
+// c_e = exp(-i pi e^2 / L) from the chirp table in shared memory (0 <= e < L).
+template <typename T2> __device__ __forceinline__ T2 reg_chirp(const T2* __restrict__ ch, int e, int) { return ch[e]; }
 
-// Copies the rotation table (M/16 entries) and, for Bluestein plans, the chirp tables into shared memory.
+// Copies the rotation table (M/16 entries) and, for Bluestein plans, the chirp table into shared memory.
 // Ends with a barrier.
 template <typename T2>
 __device__ __forceinline__ void reg_load_tables(const FftDesc& d, const FftTables<T2>& ft, T2* stw, T2* sch)

@@ -196,6 +196,28 @@ bool register_engine_allowed()
     return !(e && std::string(e) == "stage");
 }
 
+// The stage engine's Bluestein length for a convolution of at least `need` points: the 7-smooth length in
+// [need, 1.5 need] with the smallest estimated cost (-1 if none).
+int stage_bluestein_length(int need)
+{
+    int    best      = -1;
+    double best_cost = 1e300;
+    for (int M = need; M <= need + need / 2; ++M)
+    {
+        std::vector<int> r = radices(M);
+        if (r.empty()) continue;
+        double c = 0;
+        for (int x : r) c += stage_cost(x);
+        c *= M;
+        if (c < best_cost)
+        {
+            best_cost = c;
+            best      = M;
+        }
+    }
+    return best;
+}
+
 // Natural-order FFT_M of the windowed Bluestein kernel (see bluestein_kernel), scaled by 1/M.
 std::vector<cld> bluestein_kernel_natural(int L, int M, const FftWindow& w)
 {
@@ -226,6 +248,10 @@ bool plan_register(int L, size_t elem_bytes, size_t smem_limit, const FftWindow&
         const int need = std::max(window_span(L, fw), window_span(L, iw));
         M              = kRegMinM;
         while (M < need) M *= 2;
+        // a power of two longer than the stage engine's own choice (ND / DN windows need 3n - 1: 6144 against
+        // 8192 at n = 2048) costs more than the register engine saves
+        const int stage_M = stage_bluestein_length(need);
+        if (stage_M > 0 && M > stage_M) return false;
     }
     if (M > max_M) return false;
     const size_t elems = (size_t)reg_buf_elems(M) + M / 16 + (pow2 ? 0 : reg_chirp_entries(L));
@@ -251,11 +277,8 @@ bool plan_register(int L, size_t elem_bytes, size_t smem_limit, const FftWindow&
     }
     set_window(h.d, fw);
     set_window(h.d_inv, iw);
-    // chirp tables: exp(-i pi b / L) for b < 64, then exp(-i pi 64 a / L) for 64 a < 2L
-    h.chirp.resize(reg_chirp_entries(L));
-    for (int b = 0; b < kChirpLo; ++b) h.chirp[b] = root_of_unity(b, 2LL * L);
-    for (int a = 0; kChirpLo + a < (int)h.chirp.size(); ++a)
-        h.chirp[kChirpLo + a] = root_of_unity((long long)kChirpLo * a, 2LL * L);
+    h.chirp.resize(L);  // c_e = exp(-i pi e^2 / L)
+    for (int e = 0; e < L; ++e) h.chirp[e] = root_of_unity(((long long)e * e) % (2LL * L), 2LL * L);
     h.bhat = bluestein_kernel_natural(L, M, fw);
     if (fw.in0 != iw.in0 || fw.nin != iw.nin || fw.out0 != iw.out0 || fw.nout != iw.nout)
         h.bhat_inv = bluestein_kernel_natural(L, M, iw);
@@ -289,21 +312,7 @@ HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftW
                 throw std::runtime_error("FFT plan: window outside the transform");
         // Smallest-cost 7-smooth M covering both windows' convolutions.
         const int need = std::max(window_span(L, fw), window_span(L, iw));
-        int       best = -1;
-        double    best_cost = 1e300;
-        for (int M = need; M <= need + need / 2; ++M)
-        {
-            std::vector<int> r = radices(M);
-            if (r.empty()) continue;
-            double c = 0;
-            for (int x : r) c += stage_cost(x);
-            c *= M;
-            if (c < best_cost)
-            {
-                best_cost = c;
-                best      = M;
-            }
-        }
+        const int best = stage_bluestein_length(need);
         if (best < 0) throw std::runtime_error("FFT plan: no Bluestein length");
         h.d.M    = best;
         h.d.blue = 1;

@@ -62,8 +62,7 @@ struct HostFft
     FftDesc                               d_inv{};  // inverse window (same M, stages and tables)
     std::vector<std::complex<long double>> tw;     // stage engine: stage twiddles; register engine:
                                                    // exp(-2 pi i m / M), m < M/16
-    std::vector<std::complex<long double>> chirp;  // stage engine: c_n, n < L; register engine: the two
-                                                   // chirp tables (fp_fft16.cuh reg_chirp)
+    std::vector<std::complex<long double>> chirp;  // Bluestein: c_n = exp(-i pi n^2 / L), n < L
     std::vector<std::complex<long double>> bhat;      // scaled by 1/M; digit-reversed for the stage engine,
                                                       // natural order for the register engine
     std::vector<std::complex<long double>> bhat_inv;  // kernel of the inverse window, if it differs

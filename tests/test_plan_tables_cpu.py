@@ -164,16 +164,15 @@ def reg_fft(x, tw):
 
 
 def reg_chirp(c, L, e):
-    """c_e from the two chirp tables: exp(-i pi m / L), m = e^2 mod 2L = 64 a + b."""
-    m = (np.asarray(e, dtype=np.int64) ** 2) % (2 * L)
-    return c[64 + (m >> 6)] * c[m & 63]
+    """c_e = exp(-i pi e^2 / L) from the plan's chirp table."""
+    return c[np.asarray(e)]
 
 
-@pytest.mark.parametrize("kind,n", [(K_DD, 2048), (K_DD, 1000), (K_DD, 512), (K_ND, 2048), (K_DN, 1000),
+@pytest.mark.parametrize("kind,n", [(K_DD, 2048), (K_DD, 1024), (K_DD, 512), (K_ND, 1365), (K_DN, 682),
                                     (K_DD, 4096), (K_NN, 2048)])
 def test_register_engine_plans_replay_dft(driver, kind, n):
     """Register-engine plans: the power-of-two length (direct when L is a power of two, else the smallest one
-    covering the window's convolution), the rotation table and the two-level chirp tables; the engine's
+    covering the window's convolution), the rotation table and the chirp table; the engine's
     passes replayed on them give the DFT (Bluestein: pre-chirp, forward FFT, kernel product in natural
     order, conjugate, forward FFT, conjugate, post-chirp)."""
     p = plan(driver, kind, n, "register")
@@ -192,7 +191,8 @@ def test_register_engine_plans_replay_dft(driver, kind, n):
     full = f["nin"] == L and f["nout"] == L
     need = 2 * L - 2 if full else max(f["nin"] + f["nout"], p["inv"]["nin"] + p["inv"]["nout"]) - 1
     assert need <= M < 2 * need
-    assert len(p["c"]) == 64 + (2 * L + 63) // 64
+    assert len(p["c"]) == L
+    assert np.allclose(p["c"], np.exp(-1j * np.pi * ((np.arange(L) ** 2) % (2 * L)) / L), atol=1e-15)
     for tag, bhat in (("fwd", p["b"]), ("inv", p["i"] if len(p["i"]) else p["b"])):
         w = p[tag]
         z = np.zeros(L, complex)
@@ -205,3 +205,13 @@ def test_register_engine_plans_replay_dft(driver, kind, n):
         got = y[: w["nout"]] * reg_chirp(p["c"], L, k)
         ref = np.fft.fft(z)[k]
         assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), (kind, n, tag)
+
+
+@pytest.mark.parametrize("kind,n,eng,M", [(K_DD, 2048, 1, 4096), (K_ND, 2048, 0, 6144), (K_DN, 2048, 0, 6144),
+                                         (K_DD, 1000, 1, 2048), (K_NN, 2048, 1, 2048), (K_NN, 1000, 0, 1000)])
+def test_engine_choice(driver, kind, n, eng, M):
+    """The planner puts a length on the register engine when it is a power of two >= 512, or needs Bluestein
+    and the power-of-two convolution length is no longer than the one the stage engine would pick; otherwise
+    the stage engine runs it (ND / DN at 2048: 6144 against 8192)."""
+    f = plan(driver, kind, n, "register")["fwd"]
+    assert (f["eng"], f["M"]) == (eng, M)
