@@ -29,6 +29,8 @@ SIGNATURES = {
     "fp_rect_create": ([_i, _i, _d, _d, _vp, _i, _vp], _i),
     "fp_rect_solve_f64": ([_vp, _vp, _ll, _i, _vp], _i),
     "fp_rect_chase_f64": ([_vp, _vp, _ll, _i, _vp], _i),
+    "fp_field_fill": ([_vp, _i, _i, _d, _d, _d, _d, _i, _vp, _i, _i, _vp], _i),
+    "fp_buffer_fill": ([_vp, _i, _i, _i, _d, _d, _d, _d, _i, _vp, _i, _vp], _i),
     "fp_rect_solve_f32": ([_vp, _vp, _ll, _i, _vp], _i),
     "fp_rect_destroy": ([_vp], _i),
     "fp_rect_solve_f64_noalloc": ([_vp, _vp, _ll, _vp], _i),
@@ -380,3 +382,51 @@ class Batch:
             _lib.fp_batch_destroy(self.h)
             self.h = None
 
+
+
+# ---------------------------------------------------------------------------------------------------------
+# Device-side field set-up (fp_field_fill / fp_buffer_fill)
+# ---------------------------------------------------------------------------------------------------------
+FACTOR_ONE, FACTOR_SIN, FACTOR_COS, FACTOR_GAUSS, FACTOR_QUADRATIC = range(5)
+POS_CENTER, POS_XFACE, POS_YFACE, POS_CORNER = range(4)
+
+
+class Term(ctypes.Structure):
+    """a * X(x) * Y(y), factors FACTOR_* with parameters px, py (include/fp_capi.h fp_term)."""
+    _fields_ = [("a", ctypes.c_double), ("kind_x", ctypes.c_int), ("kind_y", ctypes.c_int),
+                ("px", ctypes.c_double * 3), ("py", ctypes.c_double * 3)]
+
+
+def term(a, kx=FACTOR_ONE, px=(0.0, 0.0, 0.0), ky=FACTOR_ONE, py=(0.0, 0.0, 0.0)):
+    px = tuple(px) + (0.0,) * (3 - len(px))
+    py = tuple(py) + (0.0,) * (3 - len(py))
+    return Term(float(a), int(kx), int(ky), (ctypes.c_double * 3)(*px), (ctypes.c_double * 3)(*py))
+
+
+def _terms(terms):
+    arr = (Term * max(1, len(terms)))(*terms)
+    return arr, len(terms)
+
+
+def field_fill(f, hx, hy, ox, oy, terms, position=POS_CENTER, accumulate=False):
+    """Variable2D::set_value on the device: f (an (nx, ny) CUDA float64 tensor) = the sum of `terms` at the
+    value positions of a domain with offset (ox, oy) and steps hx, hy."""
+    import torch
+
+    nx, ny = f.shape
+    arr, n = _terms(terms)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    check(lib().fp_field_fill(ctypes.c_void_p(f.data_ptr()), nx, ny, float(hx), float(hy), float(ox), float(oy),
+                              int(position), arr, n, int(bool(accumulate)), s))
+    return f
+
+
+def buffer_fill(buf, face, nx, ny, hx, hy, ox, oy, terms, position=POS_CENTER):
+    """Variable2D::set_buffer_value on the device: the ghost values of `face` into the CUDA tensor buf."""
+    import torch
+
+    arr, n = _terms(terms)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    check(lib().fp_buffer_fill(ctypes.c_void_p(buf.data_ptr()), int(face), nx, ny, float(hx), float(hy), float(ox),
+                               float(oy), int(position), arr, n, s))
+    return buf

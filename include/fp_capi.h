@@ -210,6 +210,46 @@ int fp_batch_residuals(fp_batch* b, const double* const* u, const double* const*
 int fp_batch_info(const fp_batch* b, int* n_problems, int* n_domains, int* launch_shape, long long* graph_kernels);
 int fp_batch_destroy(fp_batch* b);
 
+/* ---------------------------------------------------------------------------------------------------
+ * Device-side field set-up: Variable2D::set_value and Variable2D::set_buffer_value (reference
+ * base/domain/variable2d.cpp:345-416, 467-511) for analytic functions, evaluated on the device so that a
+ * right-hand side or ghost buffer need not be filled on the host and copied. The function is a sum of up to
+ * 48 separable terms  a * X(x) * Y(y), each factor one of
+ *   FP_FACTOR_ONE        1
+ *   FP_FACTOR_SIN        sin(p0 t + p1)
+ *   FP_FACTOR_COS        cos(p0 t + p1)
+ *   FP_FACTOR_GAUSS      exp(-((t - p0) / p1)^2)
+ *   FP_FACTOR_QUADRATIC  p0 + p1 t + p2 t^2
+ * Positions follow the reference's variable positions: value (i, j) sits at (ox + (i + sx) hx,
+ * oy + (j + sy) hy) with (sx, sy) = (0.5, 0.5) for FP_POS_CENTER, (0, 0.5) XFACE, (0.5, 0) YFACE, (0, 0)
+ * CORNER. Pointers are device memory; the work is queued on `stream` (NULL = legacy default stream).
+ * ------------------------------------------------------------------------------------------------- */
+#define FP_FACTOR_ONE 0
+#define FP_FACTOR_SIN 1
+#define FP_FACTOR_COS 2
+#define FP_FACTOR_GAUSS 3
+#define FP_FACTOR_QUADRATIC 4
+#define FP_POS_CENTER 0
+#define FP_POS_XFACE 1
+#define FP_POS_YFACE 2
+#define FP_POS_CORNER 3
+
+typedef struct fp_term
+{
+    double a;               /* coefficient */
+    int    kind_x, kind_y;  /* FP_FACTOR_* of the x and y factors */
+    double px[3], py[3];    /* their parameters */
+} fp_term;
+
+/* f (nx x ny, row-major) = (or += with accumulate) the sum of the terms at the value positions: the
+ * values Variable2D::set_value(func) stores for domain offset (ox, oy) and steps hx, hy. */
+int fp_field_fill(double* f, int nx, int ny, double hx, double hy, double ox, double oy, int position,
+                  const fp_term* terms, int nterms, int accumulate, void* stream);
+/* The ghost buffer of `face` (LocationType order; ny values for x faces, nx for y faces, one more for
+ * FP_POS_CORNER): the sum of the terms one cell outside the face, as Variable2D::set_buffer_value. */
+int fp_buffer_fill(double* buf, int face, int nx, int ny, double hx, double hy, double ox, double oy, int position,
+                   const fp_term* terms, int nterms, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
