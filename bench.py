@@ -3,17 +3,18 @@
 Workload (the largest cross configuration that fits one GPU): a cross of 5 subdomains of 2048 x 2048 cells
 (centre + 4 arms), h = 1/2048, Neumann arm tips, Dirichlet elsewhere, seeded zero-mean Gaussian RHS,
 GMRES(m=20, tol=1e-14, maxIter=100) on the interface unknowns. One step = one full composite solve
-(inputs re-filled from a resident copy first, since a solve consumes its right-hand side). Three forms are
+(inputs re-filled from a resident copy first, since a solve consumes its right-hand side). Four forms are
 timed (FP64, FP64 + refinement, FP32 + FP64 refinement, FP64 solve + FP32 corrections); the headline is the
-fastest whose
-answer is within 1e-10 relative L2 of the refined solution. A second section (`batched_uneven`) times the
-512-problem batched workload the same way (N = 1 only; --no-batched skips it).
+fastest whose answer is within 1e-10 relative L2 of the refined solution. Every form's answer is also
+compared with the reference's own answer to the same workload (the CPU leg, which times it). Further
+sections: the 512-problem batched workload (`batched_uneven`; split between the ranks when N > 1;
+--no-batched skips it) and the 9 x 4096^2 tree (`large_tree`, N = 1; --no-large skips it).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
     python bench.py --probe transform|rect|composite|batch ...   (one kernel family or solve; see PROBE_USAGE)
 
-N > 1 runs N independent replicas (the path does not shard), one process per GPU under torchrun.
-Prints one JSON line on rank 0.
+N > 1 runs N independent replicas of the cross, one process per GPU under torchrun. Prints one JSON line on
+rank 0.
 """
 from __future__ import annotations
 
@@ -370,7 +371,7 @@ def batched_section(args, dev, rank, world=1, dist=None):
 
 
 # ------------------------------------------------------------------------------------------------
-# Large composite: 9 subdomains of 4096^2 in a depth-2 tree, periodic arms (--large; setup ~2.5 min)
+# Large composite: 9 subdomains of 4096^2 in a depth-2 tree, periodic arms (--no-large skips; setup ~2 min)
 # ------------------------------------------------------------------------------------------------
 def large_section(args, dev):
     """Forward solves (FP64, FP32 + FP64 refinement) and the adjoint solve of the 9 x 4096^2 tree with
@@ -550,7 +551,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-uneven section")
-    ap.add_argument("--large", action="store_true", help="add the 9 x 4096^2 tree section (setup ~2.5 min)")
+    ap.add_argument("--no-large", action="store_true", help="skip the 9 x 4096^2 tree section (setup ~2 min)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -664,8 +665,25 @@ def main():
             e2e_times.append(time.perf_counter() - t0)
     e2e_t = max_over_ranks(sum(e2e_times), dist, dev)
     field_bytes = sum(int(p.numel()) * 8 for p in pristine)
+    # the host link alone: the same bytes copied host -> device and back from the pinned buffers, timed
+    # with events (the bound e2e could reach if the copies and the solve overlapped perfectly is
+    # 1 / max(copies, solve); a call that copies, solves, copies back is bounded by 1 / (copies + solve))
+    c0, c1, c2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    for _ in range(2):
+        c0.record(stream)
+        for w, h in zip(work, host):
+            w.copy_(h, non_blocking=True)
+        c1.record(stream)
+        for w, h in zip(work, host):
+            h.copy_(w, non_blocking=True)
+        c2.record(stream)
+        torch.cuda.synchronize()
+    h2d_ms, d2h_ms = c0.elapsed_time(c1), c1.elapsed_time(c2)
     e2e = {"value": args.steps * world / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": field_bytes,
-           "d2h_bytes_per_step": field_bytes, "form": head}
+           "d2h_bytes_per_step": field_bytes, "form": head,
+           "host_link": {"h2d_ms": h2d_ms, "d2h_ms": d2h_ms, "h2d_gbs": field_bytes / h2d_ms / 1e6,
+                         "d2h_gbs": field_bytes / d2h_ms / 1e6,
+                         "serial_bound_solves_per_s": 1e3 / (h2d_ms + d2h_ms + r["ms"] / args.steps)}}
     ms, value, launches, clk, infos = r["ms"], r["value"], r["launches"], r["clocks"], r["infos"]
     t_max = ms
 
@@ -691,6 +709,26 @@ def main():
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
                                   "(profiles/k_transform_DD_2048x2048_f64.md)",
                 "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": t_kernel * 1e3}
+    # the chase (the solve's other kernel family): the x-direction tridiagonal solves of one 2048^2 FP64
+    # subdomain, fp_rect_chase_f64 (local chunk sweeps, separator scan, correction), 2*N*8 bytes algorithmic
+    rect = capi.Rect(N_CELLS, N_CELLS, 1.0 / N_CELLS, 1.0 / N_CELLS, (0, 0, 0, 0))
+    for _ in range(3):
+        rect.chase(x)
+    torch.cuda.synchronize()
+    k0.record(stream)
+    for _ in range(reps):
+        rect.chase(x)
+    k1.record(stream)
+    torch.cuda.synchronize()
+    t_chase = k0.elapsed_time(k1) / reps / 1e3
+    ach_chase = bytes_launch / t_chase / 1e9
+    roofline_chase = {"kernel": "k_chase_local + k_chase_reduced + k_chase_correct (2048x2048, FP64, one chase)",
+                      "bound": "hbm", "achieved": ach_chase, "peak": peak, "unit": "GB/s", "frac": ach_chase / peak,
+                      "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": bytes_launch,
+                      "avg_launch_ms": t_chase * 1e3,
+                      "traffic_note": "the chase reads and writes the field twice (chunk sweeps, then the "
+                                      "correction): 4*N*8 bytes of DRAM traffic for 2*N*8 algorithmic"}
+    del rect, x
 
     forms = {}
     for form, rr in res.items():
@@ -713,6 +751,7 @@ def main():
                            "f32ir": "FP32 transforms + FP64 iterative refinement",
                            "mixedir": "FP64 solve, then FP32-storage corrections in FP64 iterative refinement"}[head],
         "forms": forms, "clocks": clk, "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
+        "roofline_chase": roofline_chase,
         "setup": {"seconds": setup_s, "what": "capi.Composite creation for this workload (plans, chase tables, "
                                                "closed-form interface operators and the reduced-system inverse of "
                                                "the spectral path; the Schur GMRES path builds lazily), wall clock"},
@@ -741,7 +780,7 @@ def main():
         del solver, pristine, work
         torch.cuda.empty_cache()
         line["batched_uneven"] = batched_section(args, dev, rank, world, dist)
-    if args.large and world == 1:
+    if not args.no_large and world == 1:
         line["large_tree"] = large_section(args, dev)
     if rank == 0:
         print(json.dumps(line))
