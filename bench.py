@@ -703,7 +703,7 @@ def main():
     bytes_launch = 2 * N_CELLS * N_CELLS * 8
     peak, peak_kind = measured_peaks()
     achieved = bytes_launch / t_kernel / 1e9
-    roofline = {"kernel": "k_transform<double, DD> (2048x2048 rows, in place)", "bound": "hbm",
+    roofline = {"kernel": "k_b_xform<double, DD, 0, double, double, ACC=false> (one run of 2048 rows of 2048, in place; the instantiation the FP64 solve launches)", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} hbm_gbs", "traffic": DD_TRAFFIC_BYTES,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "

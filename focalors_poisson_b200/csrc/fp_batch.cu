@@ -18,78 +18,12 @@ namespace fpb
 // Device side
 // =============================================================================================
 
-// Largest s with prefix[s] <= x (prefix ascending, prefix[0] = 0).
-__device__ __forceinline__ int seg_of(const long long* __restrict__ prefix, int n, long long x)
-{
-    int lo = 0, hi = n - 1;
-    while (lo < hi)
-    {
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(prefix + mid) <= x) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
 // sqrt(2/(n+1)) sin(pi (k+1)(j+1)/(n+1)): DST-I basis vector k at point j (the reference's DD transform,
 // pe/poisson/poisson_fft2d.cpp:19-57, is this orthonormal matrix).
 __device__ __forceinline__ double dst_basis(int n, int k, int j)
 {
     const long long q = (long long)(k + 1) * (j + 1) % (2LL * (n + 1));
     return sqrt(2.0 / (n + 1)) * sinpi((double)q / (double)(n + 1));
-}
-
-// ---------------------------------------------------------------------------------------------
-// y-transforms of rows of many lengths in one persistent launch (one family and direction per launch;
-// the per-row work is transform_rows of fp_transform.cuh)
-// ---------------------------------------------------------------------------------------------
-struct DstSeg
-{
-    const void* in;
-    void*       out;
-    int         rows, plan;
-};
-
-// One work item = the rows one FFT carries (two for the pairing families) of one segment.
-// ACC: out (FP64) += result instead of out = result. plans: two argument sets per plan (forward, inverse).
-// DD and DN run their inverse with INV = 0 and the forward arguments (they are their own transposes).
-// Register cap: the arguments are read through a global pointer here (not from the parameter bank as in
-// k_transform), and uncapped the FP64 instances take 104-110 registers, which allows only 2 CTAs of 256
-// threads per SM; at 80 (16 bytes of spill) three fit, as many as their shared memory allows.
-// ENG 1 (register engine): every segment of the launch has a plan of the same length M (M/16 threads per
-// CTA); the CTA copies a plan's tables into shared memory when its items move to another plan.
-template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG>
-__global__ void __maxnreg__((xform_maxnreg<ENG, T>())) k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix,
-                                                 int nseg, long long nitems, const XformArgs<T>* __restrict__ plans)
-{
-    typedef typename Cplx<T>::type T2;
-    extern __shared__ __align__(16) unsigned char fp_smem_raw[];
-    T2*            buf = reinterpret_cast<T2*>(fp_smem_raw);
-    __shared__ T   rowsc[2];
-    constexpr bool kPair  = FamilyTraits<KIND, INV>::kPairRows;
-    int            loaded = -1;
-    for (long long it = blockIdx.x; it < nitems; it += gridDim.x)
-    {
-        const int           s  = seg_of(prefix, nseg, it);
-        const DstSeg&       sg = segs[s];
-        const XformArgs<T>& P  = plans[2 * sg.plan + INV];
-        if constexpr (ENG == 1)
-        {
-            if (sg.plan != loaded)
-            {
-                reg_tables_to_smem(P, buf);
-                loaded = sg.plan;
-            }
-        }
-        const int           n  = P.n;
-        const long long     r0 = kPair ? 2 * (it - prefix[s]) : (it - prefix[s]);
-        const bool          has_b = kPair && r0 + 1 < sg.rows;
-        const TIN*          fa    = static_cast<const TIN*>(sg.in) + r0 * n;
-        const TIN*          fb    = has_b ? fa + n : fa;
-        TOUT*               oa    = static_cast<TOUT*>(sg.out) + r0 * n;
-        TOUT*               ob    = has_b ? oa + n : nullptr;
-        transform_rows<T, KIND, INV, TIN, TOUT, ACC, ENG>(P, fa, fb, oa, ob, has_b, buf, rowsc);
-    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -983,13 +917,13 @@ void launch_x1(const Segments& sg, const PlanSet<T>& ps, const BatchTiming& tm, 
         const void*     fn   = (const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 1>;
         const long long grid = std::min<long long>(sg.total, resident_ctas(fn, threads, sm));
         k_b_xform<T, K, I, TIN, TOUT, ACC, 1><<<(unsigned)grid, threads, sm, s>>>(
-            sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, ps.dev.template as<XformArgs<T>>());
+            sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, ps.dev.template as<XformArgs<T>>(), DstSeg{});
         FPB_CHECK_LAUNCH();
         return;
     }
     const long long grid = std::min<long long>(sg.total, (long long)sm_count() * tm.dst_blocks_per_sm);
     k_b_xform<T, K, I, TIN, TOUT, ACC, 0><<<(unsigned)grid, tm.dst_threads, sm, s>>>(
-        sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, ps.dev.template as<XformArgs<T>>());
+        sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, ps.dev.template as<XformArgs<T>>(), DstSeg{});
     FPB_CHECK_LAUNCH();
 }
 

@@ -3,6 +3,7 @@
 #include "fp_internal.h"
 
 #include <algorithm>
+#include <climits>
 #include <map>
 #include <mutex>
 #include <set>
@@ -82,17 +83,17 @@ template <typename T2> std::vector<T2> convert_c(const std::vector<std::complex<
     return r;
 }
 
-// One CTA per item on the stage engine; on the register engine as many CTAs as fit on the GPU at once,
-// each looping over items (its tables are loaded once per CTA).
+// One run of rows through k_b_xform: one CTA per item on the stage engine; on the register engine as many
+// CTAs as fit on the GPU at once, each looping over items (its tables are loaded once per CTA).
 template <typename T, int K, int I, typename TIO, int ENG>
-void launch_k(const TransformArgs<T, TIO>& a, long long rows, int threads, size_t smem, cudaStream_t s)
+void launch_k(const DstSeg& one, const XformArgs<T>* dargs, long long rows, int threads, size_t smem, cudaStream_t s)
 {
-    const void* fn = (const void*)k_transform<T, K, I, TIO, ENG>;
+    const void* fn = (const void*)k_b_xform<T, K, I, TIO, TIO, false, ENG>;
     allow_max_dynamic_smem(fn);
     const long long items = FamilyTraits<K, I>::kPairRows ? (rows + 1) / 2 : rows;
     if (items <= 0) return;
     const long long grid = ENG == 1 ? std::min<long long>(items, resident_ctas(fn, threads, smem)) : items;
-    k_transform<T, K, I, TIO, ENG><<<(unsigned)grid, threads, smem, s>>>(a);
+    k_b_xform<T, K, I, TIO, TIO, false, ENG><<<(unsigned)grid, threads, smem, s>>>(nullptr, nullptr, 1, items, dargs, one);
     FPB_CHECK_LAUNCH();
 }
 }  // namespace
@@ -152,6 +153,8 @@ template <typename T> DevTransform<T>::DevTransform(int kind_, int n_, bool allo
         tail    = E - fft_slot(fd.L);
     }
     smem = (size_t)E * sizeof(T2) + ((kind == K_DD && tail < K_scan) ? (size_t)2 * K_scan * sizeof(T) : 0);
+    std::vector<XformArgs<T>> both = {args(false), args(true)};
+    dargs                          = upload(both);
     if (smem > max_dynamic_smem()) throw Error(3, "transform of length " + std::to_string(n) + " needs more shared memory than a CTA has");
 }
 
@@ -175,21 +178,19 @@ template <typename T>
 template <typename TIO>
 void DevTransform<T>::run_io(const TIO* in, TIO* out, long long rows, bool inverse, cudaStream_t s) const
 {
-    TransformArgs<T, TIO> a;
-    static_cast<XformArgs<T>&>(a) = args(inverse);
-    a.in    = in;
-    a.out   = out;
-    a.rows  = rows;
-    const int inv = inverse ? 1 : 0;
+    if (rows > (long long)INT_MAX) throw Error(3, "more than 2^31 rows in one transform call");
+    const DstSeg        a{in, out, (int)rows, 0};
+    const XformArgs<T>* d   = dargs.as<XformArgs<T>>();
+    const int           inv = inverse ? 1 : 0;
 #define FPB_CASE(K)                                                                                        \
     case K:                                                                                                \
         if (fd.eng == 1)                                                                                   \
         {                                                                                                  \
-            if (inv) launch_k<T, K, 1, TIO, 1>(a, rows, threads, smem, s);                                  \
-            else launch_k<T, K, 0, TIO, 1>(a, rows, threads, smem, s);                                      \
+            if (inv) launch_k<T, K, 1, TIO, 1>(a, d, rows, threads, smem, s);                                  \
+            else launch_k<T, K, 0, TIO, 1>(a, d, rows, threads, smem, s);                                      \
         }                                                                                                  \
-        else if (inv) launch_k<T, K, 1, TIO, 0>(a, rows, threads, smem, s);                                 \
-        else launch_k<T, K, 0, TIO, 0>(a, rows, threads, smem, s);                                          \
+        else if (inv) launch_k<T, K, 1, TIO, 0>(a, d, rows, threads, smem, s);                                 \
+        else launch_k<T, K, 0, TIO, 0>(a, d, rows, threads, smem, s);                                          \
         break;
     switch (kind)
     {

@@ -42,13 +42,6 @@ template <typename T> struct XformArgs
     T             s1, s2;
 };
 
-template <typename T, typename TIO = T> struct TransformArgs : XformArgs<T>
-{
-    const TIO* in;
-    TIO*       out;
-    long long  rows;  // rows in the batch (fields * nx)
-};
-
 template <int KIND, int INV> struct FamilyTraits
 {
     static constexpr bool kPairRows = (KIND != 4);
@@ -500,30 +493,73 @@ template <int ENG, typename T> constexpr int xform_maxnreg()
     return ENG == 1 ? (sizeof(T) == 8 ? 128 : 64) : (sizeof(T) == 8 ? 80 : 64);
 }
 
-// Each CTA takes items (row pairs) blockIdx.x, blockIdx.x + gridDim.x, ... and, on the register engine,
-// loads the plan's tables into shared memory once.
-template <typename T, int KIND, int INV, typename TIO = T, int ENG = 0>
-__global__ void __maxnreg__((xform_maxnreg<ENG, T>())) k_transform(const TransformArgs<T, TIO> a)
+// Largest s with prefix[s] <= x (prefix ascending, prefix[0] = 0).
+__device__ __forceinline__ int seg_of(const long long* __restrict__ prefix, int n, long long x)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// A run of `rows` contiguous rows of one length transformed with plan `plan` (an index into the kernel's
+// argument array: entries 2 plan and 2 plan + 1 are the forward and inverse arguments).
+struct DstSeg
+{
+    const void* in;
+    void*       out;
+    int         rows, plan;
+};
+
+// The y-transform kernel of the library, for a single run of rows (the transform and rectangle entry
+// points: segs == nullptr, the run passed by value in `one`, plans = the plan's two argument sets) and for
+// many runs of rows of several lengths in one persistent launch (the batched and composite solvers: a work
+// list segs / prefix). One family and direction per launch; the per-row work is transform_rows.
+// One work item = the rows one FFT carries (two for the pairing families) of one run; CTA b takes items
+// b, b + gridDim.x, .... ACC: out (FP64) += result instead of out = result. DD and DN are their own
+// transposes (the batched solver runs their inverse with INV = 0 and the forward arguments).
+// The arguments are read through a global pointer; uncapped, the stage engine's FP64 instances take
+// 104-110 registers, which allows only 2 CTAs of 256 threads per SM, and at 80 (16 bytes of spill) three fit,
+// as many as their shared memory allows (see xform_maxnreg).
+// ENG 1 (register engine): every run of one launch has a plan of the same length M (M/16 threads per CTA);
+// the CTA copies a plan's tables into shared memory when its items move to another plan.
+template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG>
+__global__ void __maxnreg__((xform_maxnreg<ENG, T>()))
+    k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg, long long nitems,
+              const XformArgs<T>* __restrict__ plans, const DstSeg one)
 {
     typedef typename Cplx<T>::type T2;
     extern __shared__ __align__(16) unsigned char fp_smem_raw[];
-    T2*          buf = reinterpret_cast<T2*>(fp_smem_raw);
-    __shared__ T rowsc[2];
-
-    constexpr bool  kPair  = FamilyTraits<KIND, INV>::kPairRows;
-    const int       n      = a.n;
-    const long long nitems = kPair ? (a.rows + 1) / 2 : a.rows;
-    if ((long long)blockIdx.x >= nitems) return;
-    if constexpr (ENG == 1) reg_tables_to_smem(a, buf);
+    T2*            buf = reinterpret_cast<T2*>(fp_smem_raw);
+    __shared__ T   rowsc[2];
+    constexpr bool kPair  = FamilyTraits<KIND, INV>::kPairRows;
+    int            loaded = -1;
     for (long long it = blockIdx.x; it < nitems; it += gridDim.x)
     {
-        const long long r0    = kPair ? 2LL * it : it;
-        const bool      has_b = kPair && r0 + 1 < a.rows;
-        const TIO*      fa    = a.in + r0 * n;
-        const TIO*      fb    = has_b ? fa + n : fa;
-        TIO*            oa    = a.out + r0 * n;
-        TIO*            ob    = has_b ? oa + n : nullptr;
-        transform_rows<T, KIND, INV, TIO, TIO, false, ENG>(a, fa, fb, oa, ob, has_b, buf, rowsc);
+        const int           s  = segs ? seg_of(prefix, nseg, it) : 0;
+        const DstSeg        sg = segs ? segs[s] : one;
+        const long long     i0 = segs ? prefix[s] : 0;
+        const XformArgs<T>& P  = plans[2 * sg.plan + INV];
+        if constexpr (ENG == 1)
+        {
+            if (sg.plan != loaded)
+            {
+                reg_tables_to_smem(P, buf);
+                loaded = sg.plan;
+            }
+        }
+        const int       n     = P.n;
+        const long long r0    = kPair ? 2 * (it - i0) : (it - i0);
+        const bool      has_b = kPair && r0 + 1 < sg.rows;
+        const TIN*      fa    = static_cast<const TIN*>(sg.in) + r0 * n;
+        const TIN*      fb    = has_b ? fa + n : fa;
+        TOUT*           oa    = static_cast<TOUT*>(sg.out) + r0 * n;
+        TOUT*           ob    = has_b ? oa + n : nullptr;
+        transform_rows<T, KIND, INV, TIN, TOUT, ACC, ENG>(P, fa, fb, oa, ob, has_b, buf, rowsc);
     }
 }
 
