@@ -32,6 +32,9 @@ SIGNATURES = {
     "fp_field_fill": ([_vp, _i, _i, _d, _d, _d, _d, _i, _vp, _i, _i, _vp], _i),
     "fp_buffer_fill": ([_vp, _i, _i, _i, _d, _d, _d, _d, _i, _vp, _i, _vp], _i),
     "fp_rect_solve_f32": ([_vp, _vp, _ll, _i, _vp], _i),
+    "fp_rect3d_create": ([_i, _i, _i, _d, _d, _d, _vp, _vp], _i),
+    "fp_rect3d_solve_f64": ([_vp, _vp, _ll, _i, _vp], _i),
+    "fp_rect3d_destroy": ([_vp], _i),
     "fp_rect_destroy": ([_vp], _i),
     "fp_rect_solve_f64_noalloc": ([_vp, _vp, _ll, _vp], _i),
     "fp_composite_create": ([_vp, _i, _d, _i, _i, _vp], _i),
@@ -172,6 +175,33 @@ class Rect:
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
             _lib.fp_rect_destroy(self.h)
+            self.h = None
+
+
+class Rect3D:
+    """PoissonSolver3D(nx, ny, nz, hx, hy, hz, bc[6]) on the GPU: solve() works in place on (…, nx, ny, nz)
+    float64 arrays (z contiguous, the reference's field3 layout)."""
+
+    def __init__(self, nx, ny, nz, hx, hy, hz, bc):
+        self.shape = (nx, ny, nz)
+        h = ctypes.c_void_p()
+        bca = (ctypes.c_int * 6)(*[int(b) for b in bc])
+        check(lib().fp_rect3d_create(nx, ny, nz, float(hx), float(hy), float(hz), bca, ctypes.byref(h)))
+        self.h = h
+
+    def solve(self, f):
+        if tuple(f.shape[-3:]) != self.shape:
+            raise ValueError("field shape does not match the solver")
+        batch = int(np.prod(f.shape[:-3])) if len(f.shape) > 3 else 1
+        p, flags, stream, keep = _args(f, np.float64)
+        check(lib().fp_rect3d_solve_f64(self.h, p, batch, flags, stream))
+        if not _is_torch(f) and keep is not f:
+            f[...] = keep
+        return f
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fp_rect3d_destroy(self.h)
             self.h = None
 
 

@@ -18,11 +18,14 @@ namespace fpb
 {
 
 // only_last: one thread per field, handling just the last wavenumber (the singular one), for use next
-// to the chunked kernels below.
+// to the chunked kernels below. With `singular`, the wavenumbers j >= sing_from take the singular
+// recursions: the last one (sing_from = ny - 1) in 2D and in 3D without periodic x; in 3D with periodic x
+// the reference applies the singular periodic formula to every y-mode of the last z-mode
+// (pe/poisson/chasing_method3d.cpp:55-76), sing_from = (nz - 1) ny in the combined mode index.
 template <typename T>
 __global__ void k_chase(T* __restrict__ f, int nx, int ny, long long batch, const T* __restrict__ ctab,
                         const T* __restrict__ z1, const T* __restrict__ z2, int periodic, int singular,
-                        int only_last)
+                        int only_last, int sing_from)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (only_last ? batch : batch * ny)) return;
@@ -31,7 +34,7 @@ __global__ void k_chase(T* __restrict__ f, int nx, int ny, long long batch, cons
     T*              col = f + b * (long long)nx * ny + j;
     const long long s   = ny;
 
-    if (singular && j == ny - 1)
+    if (singular && j >= sing_from)
     {
         if (!periodic)
         {

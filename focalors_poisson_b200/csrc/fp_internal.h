@@ -163,7 +163,8 @@ template <typename T> struct DevRect
     DevBuf                           ctab;  // nx*ny chase coefficients (meaning in fp_chase.cuh)
     DevBuf                           z1, z2;  // periodic-x Sherman-Morrison vectors (nx*ny each)
     bool                             periodic_x = false;
-    bool                             singular   = false;  // no Dirichlet-like face: last wavenumber singular
+    bool                             singular   = false;  // no Dirichlet-like face: wavenumbers >= sing_from
+    int                              sing_from  = 0;      // singular (the last one, ny - 1, except in 3D)
     bool                             chunked    = false;  // partition chase (nx a multiple of kChunk)
     bool                             end_neumann = false;
     DevBuf                           cc, cg, chh, cends, dsep;  // partition chase tables
@@ -174,6 +175,10 @@ template <typename T> struct DevRect
     // sep_rows: separator-factor rows to tabulate (default nx / 32; larger for tables shared by a batch)
     // with_transform false: chase tables only (no transform plan; tr stays null).
     DevRect(int nx, int ny, double hx, double hy, const int* bc, int sep_rows = 0, bool with_transform = true);
+    // Chase tables only, for d.size() systems of length nx with diagonals d (the 3D solver's combined
+    // z / y modes) and the x boundary types; singular systems are those from sing_from on.
+    DevRect(int nx, const std::vector<double>& d, int bc_xneg, int bc_xpos, bool singular, int sing_from);
+    void build_chase_tables(const std::vector<double>& d, int sep_rows);
     // In-place solve of `batch` back-to-back fields.
     void solve(T* f, long long batch, cudaStream_t s) const;
     // FP64 plans only: the same solve with FP32 transforms (FP64 rows in and out, FP64 chase); the

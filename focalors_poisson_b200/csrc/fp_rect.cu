@@ -330,14 +330,38 @@ DevRect<T>::DevRect(int nx_, int ny_, double hx_, double hy_, const int* bc_, in
     if (!xp && (bc[XNEG] == BC_PERIODIC || bc[XPOS] == BC_PERIODIC || bc[XNEG] == BC_NULL || bc[XPOS] == BC_NULL))
         throw Error(1, "unsupported x boundary pair");
     if (with_transform) tr.reset(new DevTransform<T>(kind, ny));
-    periodic_x = xp;
-    singular   = !(dir_like(bc[0]) || dir_like(bc[1]) || dir_like(bc[2]) || dir_like(bc[3]));
-    std::vector<double> d = x_diag(ny, hx, hy, bc[YNEG], bc[YPOS]);
+    singular  = !(dir_like(bc[0]) || dir_like(bc[1]) || dir_like(bc[2]) || dir_like(bc[3]));
+    sing_from = ny - 1;
+    build_chase_tables(x_diag(ny, hx, hy, bc[YNEG], bc[YPOS]), sep_rows);
+}
+
+template <typename T>
+DevRect<T>::DevRect(int nx_, const std::vector<double>& d, int bc_xneg, int bc_xpos, bool singular_, int sing_from_)
+    : nx(nx_), ny((int)d.size())
+{
+    bc[XNEG] = bc_xneg;
+    bc[XPOS] = bc_xpos;
+    bc[YNEG] = bc[YPOS] = BC_DIRICHLET;
+    if (nx < 2 || ny < 1) throw Error(1, "each subdomain needs at least 2 cells per direction");
+    const bool xp = bc_xneg == BC_PERIODIC && bc_xpos == BC_PERIODIC;
+    if (!xp && (bc_xneg == BC_PERIODIC || bc_xpos == BC_PERIODIC || bc_xneg == BC_NULL || bc_xpos == BC_NULL))
+        throw Error(1, "unsupported x boundary pair");
+    singular  = singular_;
+    sing_from = sing_from_;
+    build_chase_tables(d, 0);
+}
+
+// Thomas tables of the nx x ny systems with diagonals d[j] (unit off-diagonals, the x boundary types of bc).
+template <typename T> void DevRect<T>::build_chase_tables(const std::vector<double>& d, int sep_rows)
+{
+    const bool xp = bc[XNEG] == BC_PERIODIC && bc[XPOS] == BC_PERIODIC;
+    periodic_x    = xp;
     std::vector<double> c;
     chase_table(nx, ny, d, !xp && bc[XNEG] == BC_NEUMANN, !xp && bc[XPOS] == BC_NEUMANN, c);
     ctab        = upload(convert<T>(c));
     end_neumann = !xp && bc[XPOS] == BC_NEUMANN;
-    chunked     = !xp && nx % kChunk == 0 && nx >= 2 * kChunk;
+    // the chunked kernels treat only the last wavenumber as singular
+    chunked     = !xp && nx % kChunk == 0 && nx >= 2 * kChunk && (!singular || sing_from == ny - 1);
     if (chunked)
     {
         std::vector<double> pc, pg, ph, pe;
@@ -376,7 +400,7 @@ template <typename T> void DevRect<T>::chase(T* f, long long batch, T* scr, cuda
         const long long nthreads = batch * ny;
         const int       block    = 128;
         k_chase<T><<<(unsigned)((nthreads + block - 1) / block), block, 0, s>>>(
-            f, nx, ny, batch, ctab.as<T>(), z1.as<T>(), z2.as<T>(), periodic_x ? 1 : 0, singular ? 1 : 0, 0);
+            f, nx, ny, batch, ctab.as<T>(), z1.as<T>(), z2.as<T>(), periodic_x ? 1 : 0, singular ? 1 : 0, 0, sing_from);
         FPB_CHECK_LAUNCH();
         return;
     }
@@ -399,7 +423,7 @@ template <typename T> void DevRect<T>::chase(T* f, long long batch, T* scr, cuda
     if (singular)
     {
         k_chase<T><<<(unsigned)((batch + 127) / 128), 128, 0, s>>>(f, nx, ny, batch, ctab.as<T>(), z1.as<T>(),
-                                                                  z2.as<T>(), 0, 1, 1);
+                                                                  z2.as<T>(), 0, 1, 1, ny - 1);
         FPB_CHECK_LAUNCH();
     }
 }

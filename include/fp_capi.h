@@ -88,6 +88,20 @@ int fp_rect_destroy(fp_rect* r);
 int fp_rect_solve_f64_noalloc(fp_rect* r, double* f, long long batch, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * 3D rectangle: PoissonSolver3D(nx, ny, nz, hx, hy, hz, 6 x PDEBoundaryType) and its solve(field3&)
+ * (reference pe/poisson/poisson_solver3d.h:10-37, pe/poisson/poisson_solver3d.cpp:3-123): z-transform,
+ * y-transform, one tridiagonal solve per (z, y) mode pair along x, inverse transforms. Fields are field3
+ * arrays, value(i, j, k) = f[(i*ny + j)*nz + k] (base/field/field3.cpp:378-388); bc[6] in the order x-, x+,
+ * y-, y+, z-, z+. `batch` fields back to back, solved in place; pointer and stream semantics as
+ * fp_rect_solve_f64.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct fp_rect3d fp_rect3d;
+
+int fp_rect3d_create(int nx, int ny, int nz, double hx, double hy, double hz, const int* bc, fp_rect3d** out);
+int fp_rect3d_solve_f64(fp_rect3d* r, double* f, long long batch, int flags, void* stream);
+int fp_rect3d_destroy(fp_rect3d* r);
+
+/* ---------------------------------------------------------------------------------------------
  * Composite geometry: Geometry2D + Variable2D + ConcatPoissonSolver2D (reference
  * base/domain/geometry2d.h:15-59, pe/concat/concat_solver2d.h:18-56): a tree of rectangles coupled
  * through shared faces, solved by block elimination with a Schur-complement GMRES at every internal

@@ -210,11 +210,13 @@ def cal_lambda(n: int, bn: int, bp: int) -> np.ndarray:
     return lam
 
 
-def chase(fh: np.ndarray, x_diag: np.ndarray, no_dirichlet: bool, bx_neg: int, bx_pos: int) -> np.ndarray:
+def chase(fh: np.ndarray, x_diag: np.ndarray, no_dirichlet: bool, bx_neg: int, bx_pos: int,
+          sing_from: int | None = None) -> np.ndarray:
     """ChasingMethod2D::chasing on the transformed field fh (nx, ny): one tridiagonal system of length nx
     per wavenumber k (column), diagonal x_diag[k], unit off-diagonals.
     chasing_method2d.cpp:44-89; chasing_method_base.cpp:24-154 (standard / singular),
-    :178-279 (periodic / periodic singular)."""
+    :178-279 (periodic / periodic singular). Without a Dirichlet face the columns from sing_from on (the
+    last one by default) take the singular recursions (ChasingMethod3D uses a range, see PoissonSolver3D)."""
     fh = np.asarray(fh, dtype=np.float64)
     n, K = fh.shape
     out = np.empty_like(fh)
@@ -222,7 +224,7 @@ def chase(fh: np.ndarray, x_diag: np.ndarray, no_dirichlet: bool, bx_neg: int, b
     periodic = bx_neg == P and bx_pos == P
     sing = np.zeros(K, dtype=bool)
     if no_dirichlet:
-        sing[K - 1] = True  # has_last_vector: the last wavenumber is the singular one
+        sing[(K - 1 if sing_from is None else sing_from):] = True  # has_last_vector: the last wavenumber(s)
     reg = ~sing
 
     def standard(f, dd, start_neu, end_neu):
@@ -253,8 +255,8 @@ def chase(fh: np.ndarray, x_diag: np.ndarray, no_dirichlet: bool, bx_neg: int, b
         g2 = (y[n - 1] / (1.0 + z1[n - 1]) - y[0] / z1[0]) / (z2[n - 1] / (1.0 + z1[n - 1]) - (1.0 + z2[0]) / z1[0])
         g1 = y[0] / z1[0] - g2 * ((1.0 + z2[0]) / z1[0])
         out[:, reg] = y - g1 * z1 - g2 * z2
-        if sing.any():
-            f = fh[:, K - 1]
+        for col in np.nonzero(sing)[0]:
+            f = fh[:, col]
             x = np.zeros(n)
             x[0] = 0.0
             x1 = f[0] / n
@@ -263,17 +265,17 @@ def chase(fh: np.ndarray, x_diag: np.ndarray, no_dirichlet: bool, bx_neg: int, b
             x[1] = x1
             for i in range(2, n):
                 x[i] = f[i - 1] - x[i - 2] + 2.0 * x[i - 1]
-            out[:, K - 1] = x
+            out[:, col] = x
     else:
         out[:, reg] = standard(fh[:, reg], d[reg], bx_neg == N, bx_pos == N)
-        if sing.any():
-            f = fh[:, K - 1]
+        for col in np.nonzero(sing)[0]:
+            f = fh[:, col]
             x = np.zeros(n)
             x[0] = 0.0
             x[1] = 0.0 + f[0]
             for i in range(2, n):
                 x[i] = f[i - 1] - x[i - 2] + 2.0 * x[i - 1]
-            out[:, K - 1] = x
+            out[:, col] = x
     return out
 
 
@@ -294,6 +296,54 @@ class PoissonSolver2D:
         uh = chase(fh, self.x_diag, self.no_dirichlet, self.bc[0], self.bc[1])
         self.calls += 1
         return transform_inverse(self.kind, uh)
+
+
+def cal_lambda3(n: int, bn: int, bp: int) -> np.ndarray:
+    """PoissonSolver3DBase::cal_lambda, pe/poisson/poisson_solver3d_base.cpp:41-74 (begin = 1): the 2D
+    eigenvalues shifted by -2."""
+    lam = np.empty(n)
+    for i in range(1, n + 1):
+        if bn == P and bp == P:
+            lam[i - 1] = -2.0 - 2.0 * math.cos(2.0 * PI / n * math.floor(i / 2.0))
+        elif bn == N and bp == N:
+            lam[i - 1] = -2.0 - 2.0 * math.cos(PI / n * i)
+        elif is_dir_like(bn) and is_dir_like(bp):
+            lam[i - 1] = -2.0 + 2.0 * math.cos(PI / (n + 1) * i)
+        elif (is_dir_like(bn) and bp == N) or (bn == N and is_dir_like(bp)):
+            lam[i - 1] = -2.0 - 2.0 * math.cos(2.0 * PI * i / (2 * n + 1))
+        else:
+            raise ValueError("unsupported boundary pair")
+    return lam
+
+
+class PoissonSolver3D:
+    """PoissonSolver3D (pe/poisson/poisson_solver3d.cpp:49-123) on a field3 f of shape (nx, ny, nz), z
+    contiguous. bc = (x-, x+, y-, y+, z-, z+). z-transform (:98-99), y-transform after a transpose (:101-105),
+    ChasingMethod3D along x over every (z-mode k, y-mode j) pair with x_diag[k][j] = -2 + (hx/hy)^2 lambda_y[j]
+    + (hx/hz)^2 lambda_z[k] (:57-70, chasing_method3d.cpp:3-103), inverse transforms (:113-122). Without a
+    Dirichlet face the singular systems are the last (k, j) pair, or with periodic x every j of the last k
+    (chasing_method3d.cpp:55-90)."""
+
+    def __init__(self, nx, ny, nz, hx, hy, hz, bc):
+        self.shape = (nx, ny, nz)
+        self.bc = tuple(bc)
+        self.ky, self.kz = transform_kind(bc[2], bc[3]), transform_kind(bc[4], bc[5])
+        ly, lz = cal_lambda3(ny, bc[2], bc[3]), cal_lambda3(nz, bc[4], bc[5])
+        self.x_diag = -2.0 + float(hx) * float(hx) / float(hy) / float(hy) * ly[None, :] + \
+            float(hx) * float(hx) / float(hz) / float(hz) * lz[:, None]  # [k][j]
+        self.no_dirichlet = not any(is_dir_like(b) for b in bc)
+        periodic_x = bc[0] == P and bc[1] == P
+        self.sing_from = (nz - 1) * ny if periodic_x else nz * ny - 1
+
+    def solve(self, f: np.ndarray) -> np.ndarray:
+        nx, ny, nz = self.shape
+        a = transform_forward(self.kz, np.asarray(f, dtype=np.float64).reshape(nx * ny, nz)).reshape(nx, ny, nz)
+        b = transform_forward(self.ky, np.ascontiguousarray(a.transpose(0, 2, 1)).reshape(nx * nz, ny))
+        u = chase(b.reshape(nx, nz * ny), self.x_diag.reshape(-1), self.no_dirichlet, self.bc[0], self.bc[1],
+                  self.sing_from)
+        c = transform_inverse(self.ky, u.reshape(nx * nz, ny)).reshape(nx, nz, ny)
+        c = np.ascontiguousarray(c.transpose(0, 2, 1)).reshape(nx * ny, nz)
+        return transform_inverse(self.kz, c).reshape(nx, ny, nz)
 
 
 def bond_add(f: np.ndarray, loc: int, a: float, nb: np.ndarray) -> None:

@@ -10,6 +10,8 @@
 //                         (pe/poisson/poisson_fft2d.cpp:19-465), chosen like
 //                         PoissonSolver2DBase::create_fft (pe/poisson/poisson_solver2d_base.cpp:64-91)
 //   fpref_poisson2d_solve PoissonSolver2D(nx,ny,hx,hy,4 x BC).solve (pe/poisson/poisson_solver2d.cpp:3-90)
+//   fpref_poisson3d_solve PoissonSolver3D(nx,ny,nz,hx,hy,hz,6 x BC).solve
+//                         (pe/poisson/poisson_solver3d.cpp:3-123)
 //   fpref_concat_*        Geometry2D + Variable2D + ConcatPoissonSolver2D
 //                         (pe/concat/concat_solver2d.cpp:19-223), the case-file flow of
 //                         case/validation/2d/concat_solver_reference.cpp:42-115
@@ -28,6 +30,7 @@
 #include "pe/concat/schur_mat2d.h"
 #include "pe/poisson/poisson_fft2d.h"
 #include "pe/poisson/poisson_solver2d.h"
+#include "pe/poisson/poisson_solver3d.h"
 
 #include <algorithm>
 #include <chrono>
@@ -207,6 +210,35 @@ int fpref_poisson2d_solve(int nx, int ny, double hx, double hy, const int* bc, d
         times.push_back(std::chrono::duration<double>(t1 - t0).count());
     }
     copy_out(F, f);
+    if (seconds_per_solve)
+    {
+        std::sort(times.begin(), times.end());
+        *seconds_per_solve = times[times.size() / 2];
+    }
+    return 0;
+}
+
+// PoissonSolver3D on a field3 of nx x ny x nz values, value(i, j, k) = f[(i ny + j) nz + k]
+// (base/field/field3.cpp:378-388); bc in the order x-, x+, y-, y+, z-, z+.
+int fpref_poisson3d_solve(int nx, int ny, int nz, double hx, double hy, double hz, const int* bc, double* f,
+                          int repeats, double* seconds_per_solve)
+{
+    PoissonSolver3D s(nx, ny, nz, hx, hy, hz, bc_of(bc[0]), bc_of(bc[1]), bc_of(bc[2]), bc_of(bc[3]), bc_of(bc[4]),
+                      bc_of(bc[5]));
+    const size_t        n = (size_t)nx * ny * nz;
+    std::vector<double> keep(f, f + n), times;
+    field3              F(nx, ny, nz);
+    if (repeats < 1) repeats = 1;
+    for (int r = 0; r < repeats; ++r)
+    {
+        F.set_size(nx, ny, nz);
+        std::memcpy(F.value, keep.data(), n * sizeof(double));
+        auto t0 = std::chrono::steady_clock::now();
+        s.solve(F);
+        auto t1 = std::chrono::steady_clock::now();
+        times.push_back(std::chrono::duration<double>(t1 - t0).count());
+    }
+    std::memcpy(f, F.value, n * sizeof(double));
     if (seconds_per_solve)
     {
         std::sort(times.begin(), times.end());

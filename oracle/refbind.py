@@ -32,6 +32,9 @@ def lib():
         L.fpref_poisson2d_solve.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, vp, vp,
                                             ctypes.c_int, dp]
         L.fpref_poisson2d_solve.restype = ctypes.c_int
+        L.fpref_poisson3d_solve.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_double, vp, vp, ctypes.c_int, dp]
+        L.fpref_poisson3d_solve.restype = ctypes.c_int
         L.fpref_concat_create.argtypes = [ctypes.c_int, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, vp, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_int, vp]
         L.fpref_concat_create.restype = vp
@@ -67,6 +70,17 @@ def poisson2d_solve(f: np.ndarray, hx: float, hy: float, bc, repeats: int = 1):
     bca = np.asarray(bc, dtype=np.int32)
     t = ctypes.c_double(0.0)
     lib().fpref_poisson2d_solve(f.shape[0], f.shape[1], float(hx), float(hy), _ptr(bca), _ptr(f), repeats,
+                                ctypes.byref(t))
+    return f, t.value
+
+
+def poisson3d_solve(f: np.ndarray, hx: float, hy: float, hz: float, bc, repeats: int = 1):
+    """The reference's PoissonSolver3D(nx, ny, nz, hx, hy, hz, bc[6]).solve on a copy of f (nx, ny, nz)."""
+    f = np.array(f, dtype=np.float64, copy=True, order="C")
+    bca = np.asarray(bc, dtype=np.int32)
+    t = ctypes.c_double(0.0)
+    nx, ny, nz = f.shape
+    lib().fpref_poisson3d_solve(nx, ny, nz, float(hx), float(hy), float(hz), _ptr(bca), _ptr(f), repeats,
                                 ctypes.byref(t))
     return f, t.value
 

@@ -83,6 +83,32 @@ def poisson():
     save("poisson.npz", **out)
 
 
+def poisson3d():
+    """PoissonSolver3D (pe/poisson/poisson_solver3d.cpp:3-123) of the reference's own sources on seeded random
+    fields: every x pair of {DD, NN, PP, DN} with every y and z pair of {DD, NN, DN, ND, PP}, 6 x 6 x 4 cells
+    (nx, ny, nz), unequal spacings, and two cases of 64 cells along x (the partition chase)."""
+    pairs = [(D, D), (N, N), (D, N), (N, D), (P, P)]
+    rng = np.random.default_rng(303)
+    out, combos = {}, []
+    f = rng.standard_normal((6, 6, 4))
+    out["small_in"] = f
+    for bx in [(D, D), (N, N), (P, P), (D, N)]:
+        for by in pairs:
+            for bz in pairs:
+                bc = bx + by + bz
+                out[f"small_{len(combos)}"] = R.poisson3d_solve(f, 0.3, 0.2, 0.25, bc)[0]
+                combos.append(bc)
+    out["combos"] = np.asarray(combos, dtype=np.int32)
+    for tag, (shape, h, bc) in {"a": ((64, 12, 10), (1 / 64, 1 / 12, 1 / 10), (D, N, P, P, D, D)),
+                                 "b": ((64, 10, 8), (0.02, 0.03, 0.05), (N, N, N, N, N, N))}.items():
+        g = rng.standard_normal(shape)
+        out[f"{tag}_in"] = g
+        out[f"{tag}_h"] = np.asarray(h)
+        out[f"{tag}_bc"] = np.asarray(bc, dtype=np.int32)
+        out[f"{tag}_out"] = R.poisson3d_solve(g, *h, bc)[0]
+    save("poisson3d.npz", **out)
+
+
 def composite(name, g: W.Geometry, rhs, m, tol, max_iter, ghosts=None, extra=None):
     lx = [a * h for a, h in zip(g.nx, g.hx)]
     ly = [b * h for b, h in zip(g.ny, g.hy)]
@@ -206,6 +232,7 @@ def mocks():
 if __name__ == "__main__":
     transforms()
     poisson()
+    poisson3d()
     fixture6()
     cross_config1()
     cross_neumann()
