@@ -37,9 +37,9 @@ N_CELLS = 2048
 GMRES = (20, 1e-14, 100)
 SEED = 2024
 IR_REL_TOL = 1e-11
-# DRAM bytes of one k_transform<double, DD> launch on 2048 x 2048 (ncu capture summarised in
-# profiles/k_transform_DD_2048x2048_f64.md): the input is read once, the output stays in L2
-DD_TRAFFIC_BYTES = 33.769472e6 + 6.144e3
+# DRAM bytes of one k_b_xform<double, DD> launch on 2048 x 2048 (ncu capture summarised in
+# profiles/k_b_xform_DD_2048x2048_f64.md): the input is read once, the output stays in L2
+DD_TRAFFIC_BYTES = 33.75232e6 + 0.313856e6
 INNER = {"f64ir": "f64", "f32ir": "f32", "mixedir": "mixed"}
 
 
@@ -227,6 +227,15 @@ BATCH_PROBLEMS = 512
 BATCH_FORMS = (("f64", 0), ("f32", 3))  # (storage precision, refinement steps)
 
 
+def launch_shape(info):
+    """The batched solver's autotuned launch shape. The transform grid is either persistent (a fixed number of
+    CTAs per SM looping over the work items) or one CTA per work item; fp_batch_info reports the latter as
+    1 << 20 CTAs per SM."""
+    bps = info["dst_blocks_per_sm"]
+    grid = "one CTA per work item" if bps >= 1 << 20 else f"persistent, {bps} CTAs per SM"
+    return {"dst_threads": info["dst_threads"], "dst_grid": grid, "chase_threads": info["chase_threads"]}
+
+
 def batched_section(args, dev, rank, world=1, dist=None):
     """solves/s of the batched workload in its FP64-direct and FP32+refinement forms (each step: refill the
     right-hand sides from a resident copy, then one replay of the captured graph), their accuracy against
@@ -305,7 +314,7 @@ def batched_section(args, dev, rank, world=1, dist=None):
             "max_rel_l2_vs_refined": max_over_ranks(max(perr), dist, dev),
             "max_rel_residual": max_over_ranks(float(res.max()), dist, dev),
             "gpu_launches_per_batch": launches, "graph_kernels": info["graph_kernels"],
-            "launch_shape": {k: info[k] for k in ("dst_threads", "dst_blocks_per_sm", "chase_threads")}}
+            "launch_shape": launch_shape(info)}
         del b
         torch.cuda.empty_cache()
     ok = {k: v for k, v in out["forms"].items() if v["max_rel_l2_vs_refined"] <= 1e-10}
@@ -707,7 +716,7 @@ def main():
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} hbm_gbs", "traffic": DD_TRAFFIC_BYTES,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
-                                  "(profiles/k_transform_DD_2048x2048_f64.md)",
+                                  "(profiles/k_b_xform_DD_2048x2048_f64.md)",
                 "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": t_kernel * 1e3}
     # the chase (the solve's other kernel family): the x-direction tridiagonal solves of one 2048^2 FP64
     # subdomain, fp_rect_chase_f64 (local chunk sweeps, separator scan, correction), 2*N*8 bytes algorithmic

@@ -219,8 +219,9 @@ int fp_batch_solve(fp_batch* b, double* const* fields, const double* const* ghos
 /* Per-problem |fs - A u| / |fs| (as fp_composite_residual); rel_residuals: host array of n_problems. */
 int fp_batch_residuals(fp_batch* b, const double* const* u, const double* const* rhs, const double* const* ghosts,
                        void* stream, double* rel_residuals);
-/* Counts, the autotuned launch shape (DST threads per CTA, DST CTAs per SM, chase threads per CTA) and the
- * number of kernels in the captured graph (0 before the first FP_BATCH_GRAPH solve). */
+/* Counts, the autotuned launch shape (DST threads per CTA, DST CTAs per SM of a persistent grid or 1 << 20 for
+ * one CTA per work item, chase threads per CTA) and the number of kernels in the captured graph (0 before the
+ * first FP_BATCH_GRAPH solve). */
 int fp_batch_info(const fp_batch* b, int* n_problems, int* n_domains, int* launch_shape, long long* graph_kernels);
 int fp_batch_destroy(fp_batch* b);
 
