@@ -43,6 +43,8 @@ SIGNATURES = {
     "fp_composite_solve_f32ir": ([_vp, _vp, _vp, _i, _vp, _d, _i, _vp], _i),
     "fp_composite_adjoint_f64": ([_vp, _vp, _i, _vp, _vp], _i),
     "fp_composite_adjoint_f32ir": ([_vp, _vp, _i, _vp, _d, _i, _vp], _i),
+    "fp_composite_solve_async": ([_vp, _vp, _vp, _vp, _i, _d, _i, _vp], _i),
+    "fp_composite_wait": ([_vp, _i, _vp], _i),
     "fp_composite_residual": ([_vp, _vp, _vp, _vp, _vp, _vp], _i),
     "fp_composite_tree": ([_vp, _vp, _vp], _i),
     "fp_composite_destroy": ([_vp], _i),
@@ -54,6 +56,8 @@ SIGNATURES = {
 }
 FP_GMRES_FULLFIELD, FP_CHECK_CONVERGENCE, FP_NO_INTERFACE_INVERSE, FP_IR_INNER_F64 = 4, 8, 16, 32
 FP_BATCH_F32, FP_BATCH_NO_AUTOTUNE, FP_BATCH_GRAPH, FP_NO_SPECTRAL, FP_IR_FIRST_F64 = 64, 128, 256, 512, 1024
+FP_FORM_F64, FP_FORM_F64IR, FP_FORM_F32IR, FP_FORM_MIXEDIR = 0, 1, 2, 3
+FORMS = {"f64": FP_FORM_F64, "f64ir": FP_FORM_F64IR, "f32ir": FP_FORM_F32IR, "mixedir": FP_FORM_MIXEDIR}
 
 
 class Geometry(ctypes.Structure):
@@ -299,6 +303,64 @@ class Composite:
             flags |= FP_IR_FIRST_F64
         check(lib().fp_composite_solve_f32ir(self.h, fp, gp, flags, stream, float(rel_tol), int(max_refine),
                                              ctypes.byref(info)))
+        return self._info(info)
+
+    def _host_pointers(self, arrays, what):
+        if len(arrays) != self.nd:
+            raise ValueError(f"one {what} array per domain expected")
+        ptrs = []
+        for a, shp in zip(arrays, self.shapes):
+            if tuple(a.shape) != shp:
+                raise ValueError(f"{what} shape {tuple(a.shape)} != domain shape {shp}")
+            if _is_torch(a):
+                import torch
+
+                if a.is_cuda or a.dtype != torch.float64 or not a.is_contiguous():
+                    raise TypeError(f"{what} tensors must be contiguous float64 host tensors")
+                ptrs.append(a.data_ptr())
+            else:
+                if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+                    raise TypeError(f"{what} arrays must be contiguous float64 numpy arrays")
+                ptrs.append(a.ctypes.data)
+        return ptrs
+
+    def solve_async(self, rhs, out, ghosts=None, form="mixedir", rel_tol=1e-12, max_refine=10, stream=None):
+        """Queue one solve of a stream of independent problems with host buffers (fp_composite_solve_async):
+        rhs / out are per-domain host arrays (numpy or CPU torch tensors; page-locked memory lets the copies
+        overlap the solves), out may be rhs. Returns at once; wait() finishes every queued call. The arrays are
+        kept alive here until then and must not be touched meanwhile."""
+        if form not in FORMS:
+            raise ValueError(f"form must be one of {sorted(FORMS)}")
+        rp = self._host_pointers(rhs, "rhs")
+        op = self._host_pointers(out, "out")
+        keep = [rhs, out, ghosts]
+        gp = None
+        if ghosts is not None:
+            gl = []
+            for d in range(self.nd):
+                for face in range(4):
+                    gv = None if ghosts[d] is None else ghosts[d][face]
+                    if gv is None:
+                        gl.append(None)
+                        continue
+                    if not (isinstance(gv, np.ndarray) and gv.dtype == np.float64 and gv.flags.c_contiguous):
+                        raise TypeError("ghost buffers must be contiguous float64 numpy arrays")
+                    gl.append(gv.ctypes.data)
+            gp = (ctypes.c_void_p * (4 * self.nd))(*gl)
+        st = None if stream is None else ctypes.c_void_p(int(stream))
+        check(lib().fp_composite_solve_async(self.h, (ctypes.c_void_p * self.nd)(*rp),
+                                             (ctypes.c_void_p * self.nd)(*op), gp, FORMS[form], float(rel_tol),
+                                             int(max_refine), st))
+        self.__dict__.setdefault("_queued", []).append(keep)
+
+    def wait(self, check_convergence=False):
+        """Wait for the solves queued by solve_async; returns the info of the last one."""
+        info = SolveInfo()
+        try:
+            check(lib().fp_composite_wait(self.h, FP_CHECK_CONVERGENCE if check_convergence else 0,
+                                          ctypes.byref(info)))
+        finally:
+            self.__dict__["_queued"] = []
         return self._info(info)
 
     def adjoint(self, fields, check_convergence=False):

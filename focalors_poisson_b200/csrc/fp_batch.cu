@@ -780,6 +780,63 @@ __global__ void __launch_bounds__(256) k_b_add_norms(const AddSeg* __restrict__ 
     }
 }
 
+// State of a refinement run on the device (the refinement graph's loop control).
+struct IrState
+{
+    int    steps;       // inner solves taken
+    int    stop;        // the last check ended the loop
+    int    err;         // non-finite correction or solution norm in this run
+    int    err_sticky;  // the same over every run since the host last cleared it
+    double change;      // last |correction| / |u|
+    double last;        // the change before it
+};
+
+__global__ void k_ir_init(IrState* st)
+{
+    st->steps  = 1;  // the first inner solve wrote the solution itself
+    st->stop   = 0;
+    st->err    = 0;
+    st->change = 1.0;
+    st->last   = 0.0;
+}
+
+// After an add-with-norms pass: reduces its per-block partial sums (nb of |c|^2, then nb of |u|^2), applies the
+// stop rule of the host loop (BatchImpl::refine) and sets the refinement graph's loop condition.
+__global__ void __launch_bounds__(256) k_ir_check(const double* __restrict__ part, long long nb, IrState* st,
+                                                  double rel_tol, int max_refine, cudaGraphConditionalHandle loop)
+{
+    __shared__ double sh[32];
+    double            c = 0, u = 0;
+    for (long long b = threadIdx.x; b < nb; b += blockDim.x)
+    {
+        c += part[b];
+        u += part[nb + b];
+    }
+    const double cn = block_sum(c, sh);
+    __syncthreads();
+    const double un = block_sum(u, sh);
+    if (threadIdx.x != 0) return;
+    const int steps = st->steps + 1;
+    st->steps       = steps;
+    int stop        = steps >= max_refine;
+    if (!isfinite(cn) || !isfinite(un))
+    {
+        st->err        = 1;
+        st->err_sticky = 1;
+        stop           = 1;
+    }
+    else
+    {
+        const double last   = st->change;
+        const double change = un > 0 ? sqrt(cn / un) : 0.0;
+        st->last            = last;
+        st->change          = change;
+        if (change <= rel_tol || (steps >= 2 && last > 0 && change * (change / last) <= rel_tol)) stop = 1;
+    }
+    st->stop = stop;
+    cudaGraphSetConditional(loop, stop ? 0u : 1u);
+}
+
 
 }  // namespace fpb
 
@@ -962,6 +1019,8 @@ public:
     ~BatchImpl() override
     {
         if (graph_) cudaGraphExecDestroy(graph_);
+        if (irgraph_) cudaGraphExecDestroy(irgraph_);
+        if (irhost_) cudaFreeHost(irhost_);
     }
     void solve(double* const* fields, const double* const* ghosts, int steps, cudaStream_t s) override;
     void solve_graph(double* const* fields, const double* const* ghosts, int steps, cudaStream_t s) override;
@@ -974,8 +1033,11 @@ public:
     void          autotune(cudaStream_t s) override;
     long long     graph_kernels() const override { return graph_kernels_; }
     int           refine(double* const* fields, const double* const* ghosts, double rel_tol, int max_refine,
-                         cudaStream_t s, double* rel_change, BatchBase* first) override;
+                         cudaStream_t s, double* rel_change, BatchBase* first, bool defer) override;
+    void          refine_result(int* steps, double* rel_change) override;
     void          solve_assembled(const double* const* in, double* const* out, cudaStream_t s) override;
+    void          prepare_assembled(const double* const* in, double* const* out) override;
+    long long     assembled_generation() const override { return ext_gen_; }
 
 private:
     struct Dom
@@ -1008,6 +1070,10 @@ private:
     void   set_user_lists(double* const* fields, const double* const* ghosts, int steps);
     ResSeg res_seg(size_t g, double* r, const double* fs, const double* const* u_user);
     void   run(int steps, cudaStream_t s);
+    void   drop_graphs();
+    void   build_ir_graph(double rel_tol, int max_refine, BatchBase* first, const double* const* fi,
+                          double* const* fo);
+    int    ir_outcome(double* rel_change, long long runs);
 
     std::vector<DevBuf>                       eig_keep_;  // eigenvalue arrays referenced by BIface
     std::vector<Dom>                          dom_;
@@ -1043,6 +1109,19 @@ private:
     BatchTiming                               tm_;
     cudaGraphExec_t                           graph_         = nullptr;
     long long                                 graph_kernels_ = 0;
+    long long                                 ext_gen_       = 0;  // rebuilds of ext_in_list_ / ext_out_list_
+    // refinement graph (refine with max_refine > 1) and its key
+    cudaGraphExec_t                           irgraph_  = nullptr;
+    const BatchBase*                          irfirst_  = nullptr;
+    int                                       irmax_    = 0;
+    double                                    irtol_    = 0;
+    long long                                 irgen_    = -1;
+    long long                                 ir_pro_   = 0, ir_body_ = 0;  // kernels before / in the loop
+    long long                                 ir_pending_ = 0;              // deferred runs not yet reported
+    DevBuf                                    irst_;                        // IrState
+    IrState*                                  irhost_ = nullptr;            // pinned copy of it after each run
+    int                                       last_steps_  = 0;             // outcome of the last refinement
+    double                                    last_change_ = 0;
 };
 
 template <typename TS> BatchImpl<TS>::BatchImpl(const std::vector<BatchProblemDesc>& probs)
@@ -1713,11 +1792,7 @@ void BatchImpl<TS>::set_user_lists(double* const* fields, const double* const* g
     std::vector<const double*> gh;
     if (ghosts) gh.assign(ghosts, ghosts + 4 * nd);
     if (f == user_ptrs_ && gh == user_ghosts_ && steps == user_steps_) return;
-    if (graph_)
-    {
-        cudaGraphExecDestroy(graph_);
-        graph_ = nullptr;
-    }
+    drop_graphs();
     FPB_CUDA(cudaDeviceSynchronize());  // the lists below may still be read by queued work
     user_ptrs_   = f;
     user_ghosts_ = gh;
@@ -1899,96 +1974,223 @@ template <typename TS> void BatchImpl<TS>::solve_graph(double* const* fields, co
     note_launches(graph_kernels_);
 }
 
-template <typename TS>
-void BatchImpl<TS>::solve_assembled(const double* const* in, double* const* out, cudaStream_t s)
+template <typename TS> void BatchImpl<TS>::prepare_assembled(const double* const* in, double* const* out)
 {
     const int                  nd = (int)dom_.size();
     std::vector<const double*> vi(in, in + nd);
     std::vector<double*>       vo(out, out + nd);
-    if (vi != ext_in_ || vo != ext_out_)
+    if (vi == ext_in_ && vo == ext_out_) return;
+    FPB_CUDA(cudaDeviceSynchronize());  // the lists below may still be read by queued work
+    std::vector<DstSeg> a = dst_W_in_rec_, b = dst_X_out_rec_;
+    for (int g = 0; g < nd; ++g)
     {
-        FPB_CUDA(cudaDeviceSynchronize());  // the lists below may still be read by queued work
-        std::vector<DstSeg> a = dst_W_in_rec_, b = dst_X_out_rec_;
-        for (int g = 0; g < nd; ++g)
-        {
-            a[g].in  = vi[g];
-            b[g].out = vo[g];
-        }
-        ext_in_list_.set(a, dst_kinds_, plans_);
-        ext_out_list_.set(b, dst_kinds_, plans_);
-        ext_in_  = vi;
-        ext_out_ = vo;
+        a[g].in  = vi[g];
+        b[g].out = vo[g];
     }
+    ext_in_list_.set(a, dst_kinds_, plans_);
+    ext_out_list_.set(b, dst_kinds_, plans_);
+    ext_in_  = vi;
+    ext_out_ = vo;
+    ++ext_gen_;
+}
+
+template <typename TS>
+void BatchImpl<TS>::solve_assembled(const double* const* in, double* const* out, cudaStream_t s)
+{
+    prepare_assembled(in, out);
     inner(ext_in_list_, ext_out_list_, false, s);
+}
+
+// The refinement as one graph: assembly, the first solve (written straight into u), then a while node whose
+// body is one correction (residual, inner solve, u += r with norms, k_ir_check, which ends the loop).
+template <typename TS>
+void BatchImpl<TS>::build_ir_graph(double rel_tol, int max_refine, BatchBase* first, const double* const* fi,
+                                   double* const* fo)
+{
+    cudaStream_t cap = nullptr, cb = nullptr;
+    cudaGraph_t  g   = nullptr;
+    FPB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    const long long before = launches_noted();
+    bool            in_cap = false, in_body = false;
+    try
+    {
+        FPB_CUDA(cudaStreamCreateWithFlags(&cb, cudaStreamNonBlocking));
+        FPB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        in_cap = true;
+        k_b_assemble<<<(unsigned)asm_user_.total, 256, 0, cap>>>(asm_user_.as<AsmSeg>(), asm_user_.pre(), asm_user_.n);
+        FPB_CHECK_LAUNCH();
+        if (first) first->solve_assembled(fi, fo, cap);
+        else inner(dst_fs_, dst_out_u_, false, cap);
+        k_ir_init<<<1, 1, 0, cap>>>(irst_.as<IrState>());
+        FPB_CHECK_LAUNCH();
+        ir_pro_ = launches_noted() - before;
+        cudaStreamCaptureStatus  cs;
+        cudaGraph_t              cg    = nullptr;
+        const cudaGraphNode_t*   deps  = nullptr;
+        size_t                   ndeps = 0;
+        FPB_CUDA(cudaStreamGetCaptureInfo(cap, &cs, nullptr, &cg, &deps, &ndeps));
+        cudaGraphConditionalHandle loop;
+        FPB_CUDA(cudaGraphConditionalHandleCreate(&loop, cg, 1u, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np = {};
+        np.type                = cudaGraphNodeTypeConditional;
+        np.conditional.handle  = loop;
+        np.conditional.type    = cudaGraphCondTypeWhile;
+        np.conditional.size    = 1;
+        cudaGraphNode_t node;
+        FPB_CUDA(cudaGraphAddNode(&node, cg, deps, ndeps, &np));
+        FPB_CUDA(cudaStreamUpdateCaptureDependencies(cap, &node, 1, cudaStreamSetCaptureDependencies));
+        FPB_CUDA(cudaStreamBeginCaptureToGraph(cb, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal));
+        in_body = true;
+        k_b_residual<<<(unsigned)res_.total, 256, 0, cb>>>(res_.as<ResSeg>(), res_.pre(), res_.n);
+        FPB_CHECK_LAUNCH();
+        inner(dst_r_, dst_out_r_, false, cb);
+        k_b_add_norms<<<(unsigned)addn_.total, 256, 0, cb>>>(addn_.as<AddSeg>(), addn_.pre(), addn_.n, 0);
+        FPB_CHECK_LAUNCH();
+        const long long nb = (long long)(addp_.bytes() / 16);
+        k_ir_check<<<1, 256, 0, cb>>>(addp_.as<double>(), nb, irst_.as<IrState>(), rel_tol, max_refine, loop);
+        FPB_CHECK_LAUNCH();
+        cudaGraph_t body = nullptr;
+        in_body          = false;
+        FPB_CUDA(cudaStreamEndCapture(cb, &body));
+        in_cap = false;
+        FPB_CUDA(cudaStreamEndCapture(cap, &g));
+        ir_body_ = launches_noted() - before - ir_pro_;
+        note_launches(-(ir_pro_ + ir_body_));  // captured, not executed: counted per run from the steps taken
+        const cudaError_t e = cudaGraphInstantiate(&irgraph_, g, 0);
+        cudaGraphDestroy(g);
+        g = nullptr;
+        FPB_CUDA(e);
+    }
+    catch (...)
+    {
+        cudaGraph_t junk = nullptr;
+        if (in_body) cudaStreamEndCapture(cb, &junk);
+        if (in_cap) cudaStreamEndCapture(cap, &g);
+        if (g) cudaGraphDestroy(g);
+        note_launches(-(launches_noted() - before));
+        irgraph_ = nullptr;
+        if (cb) cudaStreamDestroy(cb);
+        cudaStreamDestroy(cap);
+        throw;
+    }
+    cudaStreamDestroy(cb);
+    cudaStreamDestroy(cap);
+    irfirst_ = first;
+    irmax_   = max_refine;
+    irtol_   = rel_tol;
+    irgen_   = first ? first->assembled_generation() : 0;
+}
+
+// Reads the pinned copy of the refinement state after `runs` graph runs have completed: counts their
+// kernels (the last run's steps for each) and reports a non-finite value met by any of them.
+template <typename TS> int BatchImpl<TS>::ir_outcome(double* rel_change, long long runs)
+{
+    const IrState st = *irhost_;
+    note_launches(runs * (ir_pro_ + ir_body_ * (long long)(st.steps - 1)));
+    if (st.err_sticky)
+    {
+        FPB_CUDA(cudaMemset(&irst_.as<IrState>()->err_sticky, 0, sizeof(int)));
+        irhost_->err_sticky = 0;
+        throw Error(5, "non-finite value in iterative refinement");
+    }
+    last_steps_  = st.steps;
+    last_change_ = st.change;
+    if (rel_change) *rel_change = st.change;
+    return st.steps;
+}
+
+template <typename TS> void BatchImpl<TS>::refine_result(int* steps, double* rel_change)
+{
+    if (!irhost_ || ir_pending_ == 0)
+    {
+        if (steps) *steps = last_steps_;
+        if (rel_change) *rel_change = last_change_;
+        return;
+    }
+    const long long runs = ir_pending_;
+    ir_pending_          = 0;
+    const int st         = ir_outcome(rel_change, runs);
+    if (steps) *steps = st;
 }
 
 template <typename TS>
 int BatchImpl<TS>::refine(double* const* fields, const double* const* ghosts, double rel_tol, int max_refine,
-                         cudaStream_t s, double* rel_change, BatchBase* first)
+                         cudaStream_t s, double* rel_change, BatchBase* first, bool defer)
 {
     if (!fields) throw Error(1, "null field list");
     if (!(rel_tol > 0) || max_refine < 1) throw Error(1, "rel_tol must be > 0 and max_refine >= 1");
     set_user_lists(fields, ghosts, 1);
+    if (max_refine > 1)
+    {
+        const int                  nd = (int)dom_.size();
+        std::vector<const double*> fi(nd);
+        std::vector<double*>       fo(nd);
+        for (int g = 0; g < nd; ++g)
+        {
+            fi[g] = fs_.as<double>() + dom_[g].off;
+            fo[g] = user_ptrs_[g];
+        }
+        if (first) first->prepare_assembled(fi.data(), fo.data());
+        if (!irst_.get())
+        {
+            irst_.alloc(sizeof(IrState));
+            FPB_CUDA(cudaMemset(irst_.get(), 0, sizeof(IrState)));
+            FPB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&irhost_), sizeof(IrState)));
+            *irhost_ = IrState{};
+        }
+        const long long gen = first ? first->assembled_generation() : 0;
+        if (irgraph_ && (irfirst_ != first || irmax_ != max_refine || irtol_ != rel_tol || irgen_ != gen))
+        {
+            cudaGraphExecDestroy(irgraph_);
+            irgraph_ = nullptr;
+        }
+        if (!irgraph_) build_ir_graph(rel_tol, max_refine, first, fi.data(), fo.data());
+        FPB_CUDA(cudaGraphLaunch(irgraph_, s));
+        FPB_CUDA(cudaMemcpyAsync(irhost_, irst_.get(), sizeof(IrState), cudaMemcpyDeviceToHost, s));
+        if (defer)
+        {
+            ++ir_pending_;
+            return -1;
+        }
+        FPB_CUDA(cudaStreamSynchronize(s));
+        const long long runs = ir_pending_ + 1;
+        ir_pending_          = 0;
+        return ir_outcome(rel_change, runs);
+    }
+    // max_refine == 1: one inner solve into r, then u = r through the add pass, whose norms check the values
     k_b_assemble<<<(unsigned)asm_user_.total, 256, 0, s>>>(asm_user_.as<AsmSeg>(), asm_user_.pre(), asm_user_.n);
+    FPB_CHECK_LAUNCH();
+    if (first)
+    {
+        std::vector<const double*> fi(dom_.size());
+        std::vector<double*>       ro(dom_.size());
+        for (size_t g = 0; g < dom_.size(); ++g)
+        {
+            fi[g] = fs_.as<double>() + dom_[g].off;
+            ro[g] = r_.as<double>() + dom_[g].off;
+        }
+        first->solve_assembled(fi.data(), ro.data(), s);
+    }
+    else
+        inner(dst_fs_, dst_out_r_, false, s);
+    k_b_add_norms<<<(unsigned)addn_.total, 256, 0, s>>>(addn_.as<AddSeg>(), addn_.pre(), addn_.n, 1);
     FPB_CHECK_LAUNCH();
     const long long     nb = (long long)(addp_.bytes() / 16);
     std::vector<double> hp((size_t)2 * nb);
-    double              change = 1.0;
-    int                 steps  = 0;
-    // With more than one step allowed, the first solution goes straight into u: its "correction" is the
-    // whole solution (change 1), so the add-and-norms pass would only copy it. With one step the pass
-    // stays, for its check of the solution's values.
-    const bool direct_first = max_refine > 1;
-    while (steps < max_refine)
+    FPB_CUDA(cudaMemcpyAsync(hp.data(), addp_.get(), hp.size() * 8, cudaMemcpyDeviceToHost, s));
+    FPB_CUDA(cudaStreamSynchronize(s));
+    double cn = 0, un = 0;
+    for (long long b = 0; b < nb; ++b)
     {
-        if (steps == 0 && first)
-        {
-            std::vector<const double*> fi(dom_.size());
-            std::vector<double*>       ro(dom_.size());
-            for (size_t g = 0; g < dom_.size(); ++g)
-            {
-                fi[g] = fs_.as<double>() + dom_[g].off;
-                ro[g] = direct_first ? user_ptrs_[g] : r_.as<double>() + dom_[g].off;
-            }
-            first->solve_assembled(fi.data(), ro.data(), s);  // u (or r) <- first solution
-        }
-        else if (steps == 0)
-            inner(dst_fs_, direct_first ? dst_out_u_ : dst_out_r_, false, s);
-        else
-            inner(dst_r_, dst_out_r_, false, s);  // r <- correction
-        if (steps == 0 && direct_first)
-        {
-            ++steps;
-            change = 1.0;
-            k_b_residual<<<(unsigned)res_.total, 256, 0, s>>>(res_.as<ResSeg>(), res_.pre(), res_.n);
-            FPB_CHECK_LAUNCH();
-            continue;
-        }
-        k_b_add_norms<<<(unsigned)addn_.total, 256, 0, s>>>(addn_.as<AddSeg>(), addn_.pre(), addn_.n, steps == 0);
-        FPB_CHECK_LAUNCH();
-        ++steps;
-        FPB_CUDA(cudaMemcpyAsync(hp.data(), addp_.get(), hp.size() * 8, cudaMemcpyDeviceToHost, s));
-        FPB_CUDA(cudaStreamSynchronize(s));
-        double cn = 0, un = 0;
-        for (long long b = 0; b < nb; ++b)
-        {
-            cn += hp[b];
-            un += hp[nb + b];
-        }
-        if (!std::isfinite(cn) || !std::isfinite(un)) throw Error(5, "non-finite value in iterative refinement");
-        const double last = change;
-        change            = un > 0 ? std::sqrt(cn / un) : 0.0;
-        // stop when this correction is below rel_tol, or the observed contraction predicts the error left
-        // after applying it (about change * change / last) is
-        if (change <= rel_tol || (steps >= 2 && last > 0 && change * (change / last) <= rel_tol)) break;
-        if (steps < max_refine)
-        {
-            k_b_residual<<<(unsigned)res_.total, 256, 0, s>>>(res_.as<ResSeg>(), res_.pre(), res_.n);
-            FPB_CHECK_LAUNCH();
-        }
+        cn += hp[b];
+        un += hp[nb + b];
     }
-    if (rel_change) *rel_change = change;
-    return steps;
+    if (!std::isfinite(cn) || !std::isfinite(un)) throw Error(5, "non-finite value in iterative refinement");
+    last_steps_  = 1;
+    last_change_ = un > 0 ? std::sqrt(cn / un) : 0.0;
+    if (rel_change) *rel_change = last_change_;
+    return 1;
 }
 
 template <typename TS>
@@ -2116,11 +2318,17 @@ template <typename TS> void BatchImpl<TS>::autotune(cudaStream_t s)
     build_chase_lists();
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (graph_)
-    {
-        cudaGraphExecDestroy(graph_);
-        graph_ = nullptr;
-    }
+    drop_graphs();
+}
+
+// Captured graphs hold the work lists and launch shapes of their capture; an executable graph still in flight
+// is released when it completes.
+template <typename TS> void BatchImpl<TS>::drop_graphs()
+{
+    if (graph_) cudaGraphExecDestroy(graph_);
+    if (irgraph_) cudaGraphExecDestroy(irgraph_);
+    graph_   = nullptr;
+    irgraph_ = nullptr;
 }
 
 std::unique_ptr<BatchBase> make_batch(const std::vector<BatchProblemDesc>& probs, int precision)

@@ -46,15 +46,27 @@ public:
     virtual void solve_graph(double* const* fields, const double* const* ghosts, int steps, cudaStream_t s) = 0;
     virtual long long graph_kernels() const = 0;  // kernels in the captured graph
     // Iterative refinement until |correction| <= rel_tol |u| over all cells (or the observed contraction
-    // predicts it after the last correction), at most max_refine inner solves; synchronises the stream
-    // after every step. Returns the steps taken; *rel_change the last |correction| / |u|.
+    // predicts it after the last correction), at most max_refine inner solves. Returns the steps taken;
+    // *rel_change the last |correction| / |u|.
     // first: when given, the first inner solve runs on that solver (same problems; e.g. the FP64 solve
     // followed by FP32 corrections).
+    // With max_refine > 1 the whole refinement is one CUDA graph (captured once per field pointers, first
+    // solver and parameters) whose loop over the corrections is a conditional while node: a device kernel
+    // applies the stop rule after every correction, so the host waits once, for the result. With
+    // max_refine == 1 the loop runs on the host. defer: queue the work and return -1 without waiting;
+    // refine_result then gives the outcome once the stream has completed.
     virtual int refine(double* const* fields, const double* const* ghosts, double rel_tol, int max_refine,
-                       cudaStream_t s, double* rel_change, BatchBase* first = nullptr) = 0;
+                       cudaStream_t s, double* rel_change, BatchBase* first = nullptr, bool defer = false) = 0;
+    // Outcome of the deferred refinements queued since the last call (the stream must have completed):
+    // steps and change of the last one. Throws if any of them met a non-finite value.
+    virtual void refine_result(int* steps, double* rel_change) = 0;
     // One inner solve of already assembled, hx^2-scaled right-hand sides `in` (one pointer per subdomain)
     // into `out` (stored, not accumulated); in and out may alias.
     virtual void solve_assembled(const double* const* in, double* const* out, cudaStream_t s) = 0;
+    // The work lists solve_assembled(in, out, .) uses, built now (outside any stream capture); the
+    // generation counts how often they were rebuilt.
+    virtual void      prepare_assembled(const double* const* in, double* const* out) = 0;
+    virtual long long assembled_generation() const = 0;
     // Per-problem |fs - A u| / |fs| (fs: assembled, hx^2-scaled right-hand side); out: host, n_problems.
     virtual void residuals(const double* const* u, const double* const* rhs, const double* const* ghosts,
                            cudaStream_t s, double* out) = 0;

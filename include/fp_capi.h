@@ -183,6 +183,35 @@ int fp_composite_solve_f32ir(fp_composite* c, double* const* fields, const doubl
 int fp_composite_adjoint_f64(fp_composite* c, double* const* fields, int flags, void* stream, fp_solve_info* info);
 int fp_composite_adjoint_f32ir(fp_composite* c, double* const* fields, int flags, void* stream, double rel_tol,
                                int max_refine, fp_solve_info* info);
+/* Pipelined solves of a stream of independent problems with HOST buffers (no counterpart in the reference,
+ * whose ConcatPoissonSolver2D::solve is synchronous): the call queues the host-to-device copy of rhs (and of
+ * the ghost buffers), the solve in the given form and the device-to-host copy of the solution into out, and
+ * returns without waiting; fp_composite_wait waits for every queued call. Consecutive calls overlap: while
+ * one problem is solved, the next one's right-hand sides are copied in and the previous one's solution is
+ * copied out (two device slots, one copy stream each way; the solve runs on `stream`). rhs[d], out[d]: host
+ * arrays of nx*ny doubles per subdomain, out may equal rhs; page-locked host memory lets the copies overlap
+ * the solves (pageable memory gives the same results without the overlap). The host arrays of a queued call
+ * must not be modified or read before fp_composite_wait returns. A call whose rhs or ghost pointer is the out
+ * pointer of a queued call reads it after that call's copy out; other overlaps between calls' host arrays are
+ * the caller's to avoid. Forms:
+ *   FP_FORM_F64      one FP64 solve (fp_composite_solve_f64)
+ *   FP_FORM_F64IR    refinement with FP64 inner solves (fp_composite_solve_f32ir with FP_IR_INNER_F64)
+ *   FP_FORM_F32IR    refinement with FP32 inner solves (fp_composite_solve_f32ir)
+ *   FP_FORM_MIXEDIR  the FP64 solve, then FP32 corrections (fp_composite_solve_f32ir with FP_IR_FIRST_F64)
+ * rel_tol and max_refine as for fp_composite_solve_f32ir (ignored by FP_FORM_F64). On the spectral path
+ * nothing in the call waits for the device (with max_refine > 1 the refinement's loop runs inside a CUDA
+ * graph); on the Schur GMRES path the solve synchronises the stream, so only the copies overlap. Every
+ * other call on this solver first waits for the queued ones. */
+#define FP_FORM_F64 0
+#define FP_FORM_F64IR 1
+#define FP_FORM_F32IR 2
+#define FP_FORM_MIXEDIR 3
+int fp_composite_solve_async(fp_composite* c, const double* const* rhs, double* const* out,
+                             const double* const* ghosts, int form, double rel_tol, int max_refine, void* stream);
+/* Waits for the calls queued by fp_composite_solve_async. info: the last queued call's refinement steps and
+ * change (and GMRES figures on the Schur path). FP_CHECK_CONVERGENCE in flags as for the solves; FP_ERR_NAN if
+ * any queued refinement met a non-finite value. Returns FP_OK at once when nothing is queued. */
+int fp_composite_wait(fp_composite* c, int flags, fp_solve_info* info);
 /* Relative residual |fs - A u| / |fs| of a candidate solution u of the composite problem with right-hand
  * side `rhs` and ghost buffers `ghosts` (fs = their assembled, hx^2-scaled form, the right-hand side
  * ConcatPoissonSolver2D::solve works on; A = its composite 5-point operator). No counterpart in the
