@@ -50,7 +50,7 @@ template <typename T> std::shared_ptr<DevTransform<T>> cached_transform(int kind
     auto                        key = std::make_tuple(dev, kind, n);
     auto                        it  = cache.find(key);
     if (it != cache.end()) return it->second;
-    auto p     = std::make_shared<DevTransform<T>>(kind, n);
+    auto p     = std::make_shared<DevTransform<T>>(kind, n, true, true);
     cache[key] = p;
     return p;
 }

@@ -131,9 +131,13 @@ namespace fpb
 // ---------------------------------------------------------------------------------------------
 constexpr int kChunk = 32;
 
+// cback: the table again, read by the back substitution through a second pointer so that the compiler loads
+// the factors again instead of keeping all 31 forward-sweep factors live in registers (198 registers and one
+// CTA of 256 threads per SM that way; with the reload and a cap of 168 registers, three CTAs of 128 threads).
 template <typename T>
-__global__ void __launch_bounds__(256) k_chase_local(T* __restrict__ f, int nx, int ny, long long batch,
-                                                     const T* __restrict__ ctab, T* __restrict__ zend, int skip_last)
+__global__ void __launch_bounds__(128, 3) k_chase_local(T* __restrict__ f, int nx, int ny, long long batch,
+                                                        const T* __restrict__ ctab, const T* __restrict__ cback,
+                                                        T* __restrict__ zend, int skip_last)
 {
     constexpr int  Li = kChunk - 1;
     const int      P  = nx / kChunk;
@@ -147,6 +151,7 @@ __global__ void __launch_bounds__(256) k_chase_local(T* __restrict__ f, int nx, 
     const int       typ = p == 0 ? 0 : 1;
     T*              col = f + b * (long long)nx * ny + (long long)p * kChunk * ny + j;
     const T*        c   = ctab + (long long)typ * Li * ny + j;
+    const T*        cb  = cback + (long long)typ * Li * ny + j;
     T               y[Li];
 #pragma unroll
     for (int r = 0; r < Li; ++r) y[r] = col[(long long)r * ny];
@@ -158,7 +163,7 @@ __global__ void __launch_bounds__(256) k_chase_local(T* __restrict__ f, int nx, 
         y[r] = prev;
     }
 #pragma unroll
-    for (int r = Li - 2; r >= 0; --r) y[r] = y[r] - __ldg(c + (long long)r * ny) * y[r + 1];
+    for (int r = Li - 2; r >= 0; --r) y[r] = y[r] - __ldg(cb + (long long)r * ny) * y[r + 1];
 #pragma unroll
     for (int r = 0; r < Li; ++r) col[(long long)r * ny] = y[r];
     T* ze                      = zend + ((b * P + p) * 2) * (long long)ny + j;

@@ -43,7 +43,8 @@ struct FftDesc
     int      blue;  // 1: Bluestein
     int      in0, nin;    // Bluestein window: nonzero inputs [in0, in0+nin)
     int      out0, nout;  // and outputs kept [out0, out0+nout); (0, L, 0, L) for a direct transform
-    int      eng;   // 0: the stage engine of this file; 1: the register engine (fp_fft16.cuh, M a power of 2)
+    int      eng;   // 0: the stage engine of this file; 1: the register engine (fp_fft16.cuh, M a power of 2);
+                    // 2: the stage engine on a buffer in global memory (rows too long for shared memory)
     int      pad;   // shared-memory layout: element i in slot i + (i >> pad) (3 here, 4 for the register engine)
     int      lgM;   // log2 M (register engine)
     int      nst;

@@ -138,13 +138,18 @@ template <typename T> struct DevTransform
     FftDesc fd{}, fd_inv{};  // forward / inverse windows of one plan
     DevBuf  tw, chirp, bhat, bhat_inv, perm, stages, ta, tb, tc;
     DevBuf  dargs;  // args(false), args(true) in device memory, for k_b_xform
+    DevBuf  gscratch;  // eng 2: the FFT buffers of gctas CTAs in global memory, gstride elements each
     T       s1 = 0, s2 = 0;
     int     threads = 128;
     size_t  smem    = 0;
+    int     gctas   = 0;
+    long long gstride = 0;
 
     // allow_register false: keep the plan on the stage engine (callers that launch plans of several
-    // lengths with one CTA shape).
-    DevTransform(int kind, int n, bool allow_register = true);
+    // lengths with one CTA shape). allow_global: rows whose FFT buffer exceeds a CTA's shared memory run
+    // with the buffer in global memory (eng 2) instead of being refused (callers that launch this plan
+    // alone).
+    DevTransform(int kind, int n, bool allow_register = true, bool allow_global = false);
     // Everything but the rows for one direction.
     XformArgs<T> args(bool inverse) const;
     // rows = fields * nx contiguous rows of length n; in and out may alias.

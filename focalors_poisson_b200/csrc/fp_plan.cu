@@ -286,7 +286,8 @@ bool plan_register(int L, size_t elem_bytes, size_t smem_limit, const FftWindow&
 }
 }  // namespace
 
-HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftWindow iw, bool allow_register)
+HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftWindow iw, bool allow_register,
+                 bool allow_global)
 {
     HostFft h;
     if (allow_register && register_engine_allowed() && plan_register(L, elem_bytes, smem_limit, fw, iw, h)) return h;
@@ -326,7 +327,12 @@ HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftW
         if (fw.in0 != iw.in0 || fw.nin != iw.nin || fw.out0 != iw.out0 || fw.nout != iw.nout)
             h.bhat_inv = bluestein_kernel(L, best, iw, h.d);
     }
-    if ((size_t)fft_buf_elems(h.d.M) * elem_bytes > smem_limit)
+    if ((size_t)fft_buf_elems(h.d.M) * elem_bytes > smem_limit && allow_global)
+    {
+        h.d.eng     = 2;
+        h.d_inv.eng = 2;
+    }
+    else if ((size_t)fft_buf_elems(h.d.M) * elem_bytes > smem_limit)
         throw std::runtime_error("transform length " + std::to_string(L) + " needs " +
                                  std::to_string((size_t)fft_buf_elems(h.d.M) * elem_bytes) +
                                  " bytes of shared memory, more than this build supports");

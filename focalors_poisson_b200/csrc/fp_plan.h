@@ -74,7 +74,10 @@ struct HostFft
 // and a power-of-two convolution length fits (and allow_register), else on the stage engine
 // (fp_fft.cuh). Throws std::runtime_error if it cannot.
 HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit);
-HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftWindow iw, bool allow_register = true);
+// allow_global: a stage plan whose buffer exceeds smem_limit runs on a buffer in global memory (eng 2)
+// instead of being refused.
+HostFft plan_fft(int L, size_t elem_bytes, size_t smem_limit, FftWindow fw, FftWindow iw, bool allow_register = true,
+                 bool allow_global = false);
 
 // Per-family tables computed with the reference's own double expressions so that the device
 // transform reproduces the reference's values, not merely the exact transform.

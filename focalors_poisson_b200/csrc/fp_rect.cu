@@ -86,19 +86,23 @@ template <typename T2> std::vector<T2> convert_c(const std::vector<std::complex<
 // One run of rows through k_b_xform: one CTA per item on the stage engine; on the register engine as many
 // CTAs as fit on the GPU at once, each looping over items (its tables are loaded once per CTA).
 template <typename T, int K, int I, typename TIO, int ENG>
-void launch_k(const DstSeg& one, const XformArgs<T>* dargs, long long rows, int threads, size_t smem, cudaStream_t s)
+void launch_k(const DstSeg& one, const XformArgs<T>* dargs, long long rows, int threads, size_t smem, cudaStream_t s,
+              long long gctas = 0)
 {
     const void* fn = (const void*)k_b_xform<T, K, I, TIO, TIO, false, ENG>;
     allow_max_dynamic_smem(fn);
     const long long items = FamilyTraits<K, I>::kPairRows ? (rows + 1) / 2 : rows;
     if (items <= 0) return;
-    const long long grid = ENG == 1 ? std::min<long long>(items, resident_ctas(fn, threads, smem)) : items;
+    const long long grid = ENG == 1   ? std::min<long long>(items, resident_ctas(fn, threads, smem))
+                           : ENG == 2 ? std::min<long long>(items, gctas)  // the CTAs the global buffers hold
+                                      : items;
     k_b_xform<T, K, I, TIO, TIO, false, ENG><<<(unsigned)grid, threads, smem, s>>>(nullptr, nullptr, 1, items, dargs, one);
     FPB_CHECK_LAUNCH();
 }
 }  // namespace
 
-template <typename T> DevTransform<T>::DevTransform(int kind_, int n_, bool allow_register) : kind(kind_), n(n_)
+template <typename T>
+DevTransform<T>::DevTransform(int kind_, int n_, bool allow_register, bool allow_global) : kind(kind_), n(n_)
 {
     if (n < 2) throw Error(1, "row length must be at least 2");
     if (kind == K_PP && (n % 2)) throw Error(1, "periodic transform needs an even length");
@@ -107,7 +111,7 @@ template <typename T> DevTransform<T>::DevTransform(int kind_, int n_, bool allo
     try
     {
         h = plan_fft(L, sizeof(T2), max_dynamic_smem(), fft_window(kind, n, false), fft_window(kind, n, true),
-                     allow_register);
+                     allow_register, allow_global);
     }
     catch (const std::runtime_error& e)
     {
@@ -153,6 +157,17 @@ template <typename T> DevTransform<T>::DevTransform(int kind_, int n_, bool allo
         tail    = E - fft_slot(fd.L);
     }
     smem = (size_t)E * sizeof(T2) + ((kind == K_DD && tail < K_scan) ? (size_t)2 * K_scan * sizeof(T) : 0);
+    if (fd.eng == 2)
+    {
+        // per CTA: the buffer, then the DD scan arrays (2K values of T in K + 1 complex slots); two CTAs per SM
+        int dev = 0, sms = 148;
+        FPB_CUDA(cudaGetDevice(&dev));
+        FPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        gstride = ((long long)E + K_scan + 1 + 7) & ~7LL;
+        gctas   = 2 * sms;
+        gscratch.alloc((size_t)gctas * gstride * sizeof(T2));
+        smem = 0;
+    }
     std::vector<XformArgs<T>> both = {args(false), args(true)};
     dargs                          = upload(both);
     if (smem > max_dynamic_smem()) throw Error(3, "transform of length " + std::to_string(n) + " needs more shared memory than a CTA has");
@@ -169,8 +184,10 @@ template <typename T> XformArgs<T> DevTransform<T>::args(bool inverse) const
     a.tc = tc.as<T2>();
     a.ta = ta.as<T>();
     a.tb = tb.as<T>();
-    a.s1 = s1;
-    a.s2 = s2;
+    a.s1      = s1;
+    a.s2      = s2;
+    a.gbuf    = gscratch.as<T2>();
+    a.gstride = gstride;
     return a;
 }
 
@@ -188,6 +205,11 @@ void DevTransform<T>::run_io(const TIO* in, TIO* out, long long rows, bool inver
         {                                                                                                  \
             if (inv) launch_k<T, K, 1, TIO, 1>(a, d, rows, threads, smem, s);                                  \
             else launch_k<T, K, 0, TIO, 1>(a, d, rows, threads, smem, s);                                      \
+        }                                                                                                  \
+        else if (fd.eng == 2)                                                                              \
+        {                                                                                                  \
+            if (inv) launch_k<T, K, 1, TIO, 2>(a, d, rows, threads, smem, s, gctas);                           \
+            else launch_k<T, K, 0, TIO, 2>(a, d, rows, threads, smem, s, gctas);                               \
         }                                                                                                  \
         else if (inv) launch_k<T, K, 1, TIO, 0>(a, d, rows, threads, smem, s);                                 \
         else launch_k<T, K, 0, TIO, 0>(a, d, rows, threads, smem, s);                                          \
@@ -329,7 +351,7 @@ DevRect<T>::DevRect(int nx_, int ny_, double hx_, double hy_, const int* bc_, in
     const bool xp = bc[XNEG] == BC_PERIODIC && bc[XPOS] == BC_PERIODIC;
     if (!xp && (bc[XNEG] == BC_PERIODIC || bc[XPOS] == BC_PERIODIC || bc[XNEG] == BC_NULL || bc[XPOS] == BC_NULL))
         throw Error(1, "unsupported x boundary pair");
-    if (with_transform) tr.reset(new DevTransform<T>(kind, ny));
+    if (with_transform) tr.reset(new DevTransform<T>(kind, ny, true, true));
     singular  = !(dir_like(bc[0]) || dir_like(bc[1]) || dir_like(bc[2]) || dir_like(bc[3]));
     sing_from = ny - 1;
     build_chase_tables(x_diag(ny, hx, hy, bc[YNEG], bc[YPOS]), sep_rows);
@@ -410,7 +432,7 @@ template <typename T> void DevRect<T>::chase(T* f, long long batch, T* scr, cuda
     T*              work = bsep + batch * P * ny;
     const int       skip = singular ? 1 : 0;
     const long long nl   = batch * P * ny;
-    k_chase_local<T><<<(unsigned)((nl + 255) / 256), 256, 0, s>>>(f, nx, ny, batch, cc.as<T>(), zend, skip);
+    k_chase_local<T><<<(unsigned)((nl + 127) / 128), 128, 0, s>>>(f, nx, ny, batch, cc.as<T>(), cc.as<T>(), zend, skip);
     FPB_CHECK_LAUNCH();
     const long long nr = batch * ((ny + 31) / 32);  // CTAs: 32 wavenumbers of one field each
     k_chase_reduced<T><<<(unsigned)nr, 32 * kRedWarps, 0, s>>>(f, nx, ny, batch, cends.as<T>(), dsep.as<T>(),
@@ -432,7 +454,7 @@ template <typename T> void DevRect<T>::solve_mixed(T* f, long long batch, cudaSt
 {
     if (!std::is_same<T, double>::value) throw Error(1, "mixed-precision solve needs an FP64 plan");
     if (batch <= 0) return;
-    if (!tr32) tr32.reset(new DevTransform<float>(tr->kind, ny));
+    if (!tr32) tr32.reset(new DevTransform<float>(tr->kind, ny, true, true));
     tr32->run_io<T>(f, f, batch * nx, false, s);
     const long long need = chase_scratch_elems(batch);
     if (need) scratch.ensure((size_t)need * sizeof(T));

@@ -40,6 +40,8 @@ template <typename T> struct XformArgs
     const T*      tb;  // family table b (ND: sin, PP: sin)
     const T2*     tc;  // NN: exp(-i pi m / 2N)
     T             s1, s2;
+    T2*           gbuf;     // eng 2: CTA b's FFT buffer (and DD scan arrays) at gbuf + b * gstride
+    long long     gstride;
 };
 
 template <int KIND, int INV> struct FamilyTraits
@@ -490,7 +492,7 @@ __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN*
 // threads).
 template <int ENG, typename T> constexpr int xform_maxnreg()
 {
-    return ENG == 1 ? (sizeof(T) == 8 ? 128 : 64) : (sizeof(T) == 8 ? 80 : 64);
+    return ENG == 1 ? (sizeof(T) == 8 ? 128 : 64) : (sizeof(T) == 8 ? 80 : 64);  // ENG 2 as ENG 0
 }
 
 // Largest s with prefix[s] <= x (prefix ascending, prefix[0] = 0).
@@ -526,7 +528,9 @@ struct DstSeg
 // 104-110 registers, which allows only 2 CTAs of 256 threads per SM, and at 80 (16 bytes of spill) three fit,
 // as many as their shared memory allows (see xform_maxnreg).
 // ENG 1 (register engine): every run of one launch has a plan of the same length M (M/16 threads per CTA);
-// the CTA copies a plan's tables into shared memory when its items move to another plan.
+// the CTA copies a plan's tables into shared memory when its items move to another plan. ENG 2 (rows whose
+// FFT buffer does not fit in shared memory): the stage engine's code on a per-CTA buffer in global memory
+// (XformArgs::gbuf, sized for the launch's grid), which the L2 keeps close.
 template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG>
 __global__ void __maxnreg__((xform_maxnreg<ENG, T>()))
     k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg, long long nitems,
@@ -544,6 +548,7 @@ __global__ void __maxnreg__((xform_maxnreg<ENG, T>()))
         const DstSeg        sg = segs ? segs[s] : one;
         const long long     i0 = segs ? prefix[s] : 0;
         const XformArgs<T>& P  = plans[2 * sg.plan + INV];
+        if constexpr (ENG == 2) buf = P.gbuf + blockIdx.x * P.gstride;
         if constexpr (ENG == 1)
         {
             if (sg.plan != loaded)

@@ -45,6 +45,35 @@ def test_transforms_large_vs_oracle(kind, ny):
         assert rel_max(got32, ref) <= 2e-5, (kind, ny, inv, "f32")
 
 
+@pytest.mark.parametrize("kind", list(PAIRS))
+@pytest.mark.parametrize("ny", [7002, 12000, 20000])
+def test_transforms_long_rows_vs_oracle(kind, ny):
+    """Rows whose FFT buffer does not fit in a CTA's shared memory (FP64 ND/DN beyond ~4260, DD beyond ~6400;
+    FP32 at twice those) run with the buffer in global memory: same results as the oracle."""
+    rng = np.random.default_rng(ny + 7)
+    f = rng.standard_normal((3, ny))
+    for inv in (False, True):
+        ref = (O.transform_inverse if inv else O.transform_forward)(kind, f)
+        got = capi.transform(*PAIRS[kind], f, inverse=inv)
+        assert rel_max(got, ref) <= 1e-12, (kind, ny, inv)
+        got32 = capi.transform(*PAIRS[kind], f.astype(np.float32), inverse=inv)
+        assert rel_max(got32, ref) <= 1e-4, (kind, ny, inv, "f32")
+
+
+@pytest.mark.parametrize("bc", [(0, 0, 0, 0), (1, 0, 1, 0), (0, 1, 0, 1), (1, 1, 1, 1), (0, 0, 2, 2)])
+def test_rect_long_rows_vs_oracle(bc):
+    """PoissonSolver2D with ny = 9000 (beyond the shared-memory plans of every family): FP64 solve equals the
+    oracle's."""
+    torch = torch_cuda()
+    nx, ny = 64, 9000
+    rng = np.random.default_rng(5)
+    f = rng.standard_normal((2, nx, ny))
+    ref = np.stack([O.PoissonSolver2D(nx, ny, 1.0 / nx, 1.0 / ny, bc).solve(f[b]) for b in range(2)])
+    t = torch.tensor(f, device="cuda")
+    capi.Rect(nx, ny, 1.0 / nx, 1.0 / ny, bc).solve(t)
+    assert rel_max(t.cpu().numpy(), ref) <= 1e-10, bc
+
+
 def test_poisson_reference_driver_fixture():
     """case/validation/2d/poisson_solver_reference.cpp: 3x4, hx=1, hy=2, all 25 boundary combinations."""
     z = load("poisson.npz")
