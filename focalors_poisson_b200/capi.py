@@ -43,6 +43,11 @@ SIGNATURES = {
     "fp_composite_solve_f32ir": ([_vp, _vp, _vp, _i, _vp, _d, _i, _vp], _i),
     "fp_composite_adjoint_f64": ([_vp, _vp, _i, _vp, _vp], _i),
     "fp_composite_adjoint_f32ir": ([_vp, _vp, _i, _vp, _d, _i, _vp], _i),
+    "fp_composite3d_create": ([_vp, _i, _d, _i, _vp], _i),
+    "fp_composite3d_set_parameter": ([_vp, _i, _d, _i], _i),
+    "fp_composite3d_solve_f64": ([_vp, _vp, _vp, _i, _vp, _vp], _i),
+    "fp_composite3d_tree": ([_vp, _vp, _vp], _i),
+    "fp_composite3d_destroy": ([_vp], _i),
     "fp_composite_solve_async": ([_vp, _vp, _vp, _vp, _i, _d, _i, _vp], _i),
     "fp_composite_wait": ([_vp, _i, _vp], _i),
     "fp_composite_residual": ([_vp, _vp, _vp, _vp, _vp, _vp], _i),
@@ -65,6 +70,14 @@ class Geometry(ctypes.Structure):
 
     _fields_ = [("n_domains", ctypes.c_int), ("nx", _vp), ("ny", _vp), ("hx", _vp), ("hy", _vp), ("bc", _vp),
                 ("n_connections", ctypes.c_int), ("connections", _vp), ("root", ctypes.c_int)]
+
+
+class Geometry3(ctypes.Structure):
+    """struct fp_geometry3"""
+
+    _fields_ = [("n_domains", ctypes.c_int), ("nx", _vp), ("ny", _vp), ("nz", _vp), ("hx", _vp), ("hy", _vp),
+                ("hz", _vp), ("bc", _vp), ("n_connections", ctypes.c_int), ("connections", _vp),
+                ("root", ctypes.c_int)]
 
 
 class SolveInfo(ctypes.Structure):
@@ -206,6 +219,85 @@ class Rect3D:
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
             _lib.fp_rect3d_destroy(self.h)
+            self.h = None
+
+
+class Composite3D:
+    """ConcatPoissonSolver3D on the GPU for a tree of boxes.
+
+    domains: [(nx, ny, nz, hx, hy, hz)], connections: [(a, face of a, b)] (faces 0..5: x-, x+, y-, y+, z-, z+),
+    bc: 6 boundary types per domain (ignored on connected faces)."""
+
+    def __init__(self, domains, connections, bc, m=20, tol=1e-8, max_iter=100, root=-1):
+        nd = len(domains)
+        self.nd = nd
+        self.shapes = [(int(d[0]), int(d[1]), int(d[2])) for d in domains]
+        cols = list(zip(*domains))
+        self._arr = dict(nx=np.ascontiguousarray(cols[0], dtype=np.int32),
+                         ny=np.ascontiguousarray(cols[1], dtype=np.int32),
+                         nz=np.ascontiguousarray(cols[2], dtype=np.int32),
+                         hx=np.ascontiguousarray(cols[3], dtype=np.float64),
+                         hy=np.ascontiguousarray(cols[4], dtype=np.float64),
+                         hz=np.ascontiguousarray(cols[5], dtype=np.float64),
+                         bc=np.ascontiguousarray(np.asarray(bc, dtype=np.int32).reshape(-1)),
+                         conn=np.ascontiguousarray(np.asarray(connections, dtype=np.int32).reshape(-1)))
+        a = self._arr
+        g = Geometry3(nd, a["nx"].ctypes.data, a["ny"].ctypes.data, a["nz"].ctypes.data, a["hx"].ctypes.data,
+                      a["hy"].ctypes.data, a["hz"].ctypes.data, a["bc"].ctypes.data, len(connections),
+                      a["conn"].ctypes.data if len(connections) else None, int(root))
+        h = ctypes.c_void_p()
+        check(lib().fp_composite3d_create(ctypes.byref(g), int(m), float(tol), int(max_iter), ctypes.byref(h)))
+        self.h = h
+
+    def set_parameter(self, m, tol, max_iter):
+        check(lib().fp_composite3d_set_parameter(self.h, int(m), float(tol), int(max_iter)))
+
+    def tree(self):
+        root = ctypes.c_int(0)
+        lv = np.zeros(self.nd, dtype=np.int32)
+        check(lib().fp_composite3d_tree(self.h, ctypes.byref(root), lv.ctypes.data))
+        return root.value, lv
+
+    def solve(self, fields, ghosts=None, check_convergence=False):
+        """ConcatPoissonSolver3D::solve in place. fields: per domain (nx, ny, nz) float64 numpy arrays (host) or
+        CUDA tensors (device); ghosts: None or per domain 6 arrays / None (x faces (ny, nz), y faces (nx, nz),
+        z faces (nx, ny)), on the same side as the fields."""
+        if len(fields) != self.nd:
+            raise ValueError("one field per domain expected")
+        keep, ptrs, flags, stream = [], [], 0, None
+        for f, shp in zip(fields, self.shapes):
+            if tuple(f.shape) != shp:
+                raise ValueError(f"field shape {tuple(f.shape)} != domain shape {shp}")
+            p, fl, st, k = _args(f, np.float64)
+            if not _is_torch(f) and k is not f:
+                raise TypeError("host fields must be contiguous float64 numpy arrays (solved in place)")
+            flags |= fl
+            stream = st if st is not None else stream
+            keep.append(k)
+            ptrs.append(p.value)
+        gp = None
+        if ghosts is not None:
+            gl = []
+            for d in range(self.nd):
+                for face in range(6):
+                    gv = None if ghosts[d] is None else ghosts[d][face]
+                    if gv is None:
+                        gl.append(None)
+                        continue
+                    p, _, _, k = _args(gv, np.float64)
+                    keep.append(k)
+                    gl.append(p.value)
+            gp = (ctypes.c_void_p * (6 * self.nd))(*gl)
+        info = SolveInfo()
+        if check_convergence:
+            flags |= FP_CHECK_CONVERGENCE
+        check(lib().fp_composite3d_solve_f64(self.h, (ctypes.c_void_p * self.nd)(*ptrs), gp, flags, stream,
+                                             ctypes.byref(info)))
+        return Composite._info(info)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fp_composite3d_destroy(self.h)
             self.h = None
 
 

@@ -41,14 +41,15 @@ struct PinnedHost
 };
 }  // namespace
 
-Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root)
+Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root, int faces)
 {
+    if (faces != 4 && faces != 6) throw Error(1, "a tree is built over 4 (2D) or 6 (3D) faces");
     if (nd <= 0) throw Error(1, "geometry has no domains");
-    std::vector<std::array<int, 4>> adj(nd, {-1, -1, -1, -1});
+    std::vector<std::array<int, 6>> adj(nd, {-1, -1, -1, -1, -1, -1});
     for (const auto& c : conns)
     {
         const int a = c[0], loc = c[1], b = c[2];
-        if (a < 0 || a >= nd || b < 0 || b >= nd || a == b || loc < 0 || loc > 3)
+        if (a < 0 || a >= nd || b < 0 || b >= nd || a == b || loc < 0 || loc >= faces)
             throw Error(1, "invalid connection");
         if ((adj[a][loc] != -1 && adj[a][loc] != b) || (adj[b][loc ^ 1] != -1 && adj[b][loc ^ 1] != a))
             throw Error(1, "a face is connected twice");
@@ -58,7 +59,7 @@ Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root)
     // connectivity (Geometry2D::is_single_connected, geometry2d.cpp:109-163) and acyclicity
     long long edges = 0;
     for (int d = 0; d < nd; ++d)
-        for (int f = 0; f < 4; ++f) edges += adj[d][f] >= 0;
+        for (int f = 0; f < faces; ++f) edges += adj[d][f] >= 0;
     edges /= 2;
     {
         std::vector<int> seen(nd, 0);
@@ -69,7 +70,7 @@ Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root)
         {
             int u = q.front();
             q.pop();
-            for (int f = 0; f < 4; ++f)
+            for (int f = 0; f < faces; ++f)
                 if (adj[u][f] >= 0 && !seen[adj[u][f]])
                 {
                     seen[adj[u][f]] = 1;
@@ -90,7 +91,7 @@ Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root)
             std::vector<int> deg(nd, 0), leaves;
             for (int d = 0; d < nd; ++d)
             {
-                for (int f = 0; f < 4; ++f) deg[d] += adj[d][f] >= 0;
+                for (int f = 0; f < faces; ++f) deg[d] += adj[d][f] >= 0;
                 if (deg[d] <= 1) leaves.push_back(d);
             }
             int remaining = nd;
@@ -99,7 +100,7 @@ Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root)
                 remaining -= (int)leaves.size();
                 std::vector<int> next;
                 for (int lf : leaves)
-                    for (int f = 0; f < 4; ++f)
+                    for (int f = 0; f < faces; ++f)
                         if (adj[lf][f] >= 0 && --deg[adj[lf][f]] == 1) next.push_back(adj[lf][f]);
                 leaves.swap(next);
             }
@@ -116,7 +117,7 @@ Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root)
     {
         int u = stack.back();
         stack.pop_back();
-        for (int f = 0; f < 4; ++f)
+        for (int f = 0; f < faces; ++f)
         {
             int v = adj[u][f];
             if (v < 0 || v == par[u]) continue;

@@ -30,8 +30,9 @@ struct Tree
 // Geometry2D::build_tree (base/domain/geometry2d.cpp:165-176) over TreeUtils
 // (base/domain/geometry_tree.hpp:22-200). The root is the tree centre found by leaf stripping; a tie
 // between two centres goes to the lower domain index (the reference compares addresses). Children are
-// listed in face order. Throws on a disconnected or cyclic geometry.
-Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root);
+// listed in face order. Throws on a disconnected or cyclic geometry. faces: 4 (2D, x-, x+, y-, y+) or 6
+// (Geometry3D::build_tree, base/domain/geometry3d.cpp:151-160, adds z-, z+).
+Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root, int faces = 4);
 
 struct GmresInfo
 {

@@ -14,6 +14,7 @@
 // the modes).
 #include "../../include/fp_capi.h"
 #include "fp_internal.h"
+#include "fp_rect3d.h"
 
 #include <cmath>
 #include <memory>
@@ -76,53 +77,45 @@ std::vector<double> cal_lambda3(int n, int bn, int bp)
 }
 }  // namespace
 
-// Device-resident PoissonSolver3D.
-struct DevRect3D
+DevRect3D::DevRect3D(int nx_, int ny_, int nz_, double hx, double hy, double hz, const int* bc)
+    : nx(nx_), ny(ny_), nz(nz_)
 {
-    int                                   nx = 0, ny = 0, nz = 0;
-    std::unique_ptr<DevTransform<double>> tz, ty;
-    std::unique_ptr<DevRect<double>>      chase;  // nz ny combined modes along x
-    mutable DevBuf                        work, scratch;
+    if (nx < 2 || ny < 2 || nz < 2) throw Error(FP_ERR_INVALID, "each direction needs at least 2 cells");
+    if (!(hx > 0) || !(hy > 0) || !(hz > 0)) throw Error(FP_ERR_INVALID, "grid spacings must be positive");
+    const int ky = kind_of(bc[2], bc[3]), kz = kind_of(bc[4], bc[5]);
+    if (ky < 0 || kz < 0) throw Error(FP_ERR_INVALID, "unsupported y or z boundary pair");
+    tz.reset(new DevTransform<double>(kz, nz, true, true));
+    ty.reset(new DevTransform<double>(ky, ny, true, true));
+    const std::vector<double> ly = cal_lambda3(ny, bc[2], bc[3]), lz = cal_lambda3(nz, bc[4], bc[5]);
+    std::vector<double>       d((size_t)ny * nz);
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            d[(size_t)k * ny + j] = -2.0 + hx * hx / hy / hy * ly[j] + hx * hx / hz / hz * lz[k];
+    bool no_dir = true;
+    for (int f = 0; f < 6; ++f) no_dir = no_dir && !dir_like(bc[f]);
+    const bool xp = bc[0] == BC_PERIODIC && bc[1] == BC_PERIODIC;
+    // singular systems without a Dirichlet face (chasing_method3d.cpp:55-90): the last (k, j) pair, or
+    // with periodic x every j of the last k
+    const int sing_from = xp ? (nz - 1) * ny : nz * ny - 1;
+    chase.reset(new DevRect<double>(nx, d, bc[0], bc[1], no_dir, sing_from));
+}
 
-    DevRect3D(int nx_, int ny_, int nz_, double hx, double hy, double hz, const int* bc) : nx(nx_), ny(ny_), nz(nz_)
-    {
-        if (nx < 2 || ny < 2 || nz < 2) throw Error(FP_ERR_INVALID, "each direction needs at least 2 cells");
-        if (!(hx > 0) || !(hy > 0) || !(hz > 0)) throw Error(FP_ERR_INVALID, "grid spacings must be positive");
-        const int ky = kind_of(bc[2], bc[3]), kz = kind_of(bc[4], bc[5]);
-        if (ky < 0 || kz < 0) throw Error(FP_ERR_INVALID, "unsupported y or z boundary pair");
-        tz.reset(new DevTransform<double>(kz, nz));
-        ty.reset(new DevTransform<double>(ky, ny));
-        const std::vector<double> ly = cal_lambda3(ny, bc[2], bc[3]), lz = cal_lambda3(nz, bc[4], bc[5]);
-        std::vector<double>       d((size_t)ny * nz);
-        for (int k = 0; k < nz; ++k)
-            for (int j = 0; j < ny; ++j)
-                d[(size_t)k * ny + j] = -2.0 + hx * hx / hy / hy * ly[j] + hx * hx / hz / hz * lz[k];
-        bool no_dir = true;
-        for (int f = 0; f < 6; ++f) no_dir = no_dir && !dir_like(bc[f]);
-        const bool xp = bc[0] == BC_PERIODIC && bc[1] == BC_PERIODIC;
-        // singular systems without a Dirichlet face (chasing_method3d.cpp:55-90): the last (k, j) pair, or
-        // with periodic x every j of the last k
-        const int sing_from = xp ? (nz - 1) * ny : nz * ny - 1;
-        chase.reset(new DevRect<double>(nx, d, bc[0], bc[1], no_dir, sing_from));
-    }
-
-    void solve(double* f, long long batch, cudaStream_t s) const
-    {
-        if (batch <= 0) return;
-        const long long n = (long long)nx * ny * nz;
-        work.ensure((size_t)(batch * n) * sizeof(double));
-        double* w = work.as<double>();
-        tz->run(f, f, batch * nx * ny, false, s);
-        slab_transpose(f, w, batch * nx, ny, nz, s);
-        ty->run(w, w, batch * nx * nz, false, s);
-        const long long need = chase->chase_scratch_elems(batch);
-        if (need) scratch.ensure((size_t)need * sizeof(double));
-        chase->chase(w, batch, scratch.as<double>(), s);
-        ty->run(w, w, batch * nx * nz, true, s);
-        slab_transpose(w, f, batch * nx, nz, ny, s);
-        tz->run(f, f, batch * nx * ny, true, s);
-    }
-};
+void DevRect3D::solve(double* f, long long batch, cudaStream_t s) const
+{
+    if (batch <= 0) return;
+    const long long n = (long long)nx * ny * nz;
+    work.ensure((size_t)(batch * n) * sizeof(double));
+    double* w = work.as<double>();
+    tz->run(f, f, batch * nx * ny, false, s);
+    slab_transpose(f, w, batch * nx, ny, nz, s);
+    ty->run(w, w, batch * nx * nz, false, s);
+    const long long need = chase->chase_scratch_elems(batch);
+    if (need) scratch.ensure((size_t)need * sizeof(double));
+    chase->chase(w, batch, scratch.as<double>(), s);
+    ty->run(w, w, batch * nx * nz, true, s);
+    slab_transpose(w, f, batch * nx, nz, ny, s);
+    tz->run(f, f, batch * nx * ny, true, s);
+}
 
 }  // namespace fpb
 

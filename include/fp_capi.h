@@ -223,6 +223,45 @@ int fp_composite_tree(const fp_composite* c, int* root, int* level_of);
 int fp_composite_destroy(fp_composite* c);
 
 /* ---------------------------------------------------------------------------------------------------
+ * 3D composite solve: ConcatPoissonSolver3D (reference pe/concat/concat_solver3d.cpp:5-247) over a tree of
+ * boxes connected on whole faces (Geometry3D::connect, base/domain/geometry3d.cpp:27-60), each box solved by
+ * PoissonSolver3D and every box with children by GMRESSolver3D (pe/concat/gmres_solver3d.cpp:155-306) with the
+ * Schur matrices of SchurMat3D_* (pe/concat/schur_mat3d.cpp), built on the device at creation.
+ * A field holds nx*ny*nz doubles, value(i, j, k) = f[(i*ny + j)*nz + k] (base/field/field3.cpp:378-388).
+ * Faces (LocationType order): 0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+. */
+typedef struct fp_geometry3
+{
+    int           n_domains;
+    const int*    nx;          /* per domain */
+    const int*    ny;
+    const int*    nz;
+    const double* hx;          /* per domain (lx / nx) */
+    const double* hy;
+    const double* hz;
+    const int*    bc;          /* 6 per domain (PDEBoundaryType), ignored on connected faces */
+    int           n_connections;
+    const int*    connections; /* 3 per connection: a, face of a, b (Geometry3D::connect(a, face, b));
+                                  the connected faces must have the same cell counts */
+    int           root;        /* -1: the reference's rule (TreeUtils::findOptimalRoot) */
+} fp_geometry3;
+typedef struct fp_composite3d fp_composite3d;
+
+/* Builds the tree, the per-box 3D rectangle plans and every Schur matrix (ConcatPoissonSolver3D constructor
+ * with set_parameter(m, tol, max_iter); the reference's defaults are m = 20, tol = 1e-8, max_iter = 100). */
+int fp_composite3d_create(const fp_geometry3* g, int m, double tol, int max_iter, fp_composite3d** out);
+/* ConcatPoissonSolver3D::set_parameter (concat_solver3d.cpp:5-18): the Schur matrices are built again. */
+int fp_composite3d_set_parameter(fp_composite3d* c, int m, double tol, int max_iter);
+/* ConcatPoissonSolver3D::solve: fields[d] (RHS in, solution out, in place); ghosts[6*d + face]: the Variable3D
+ * ghost planes (NULL = zero), row-major (ny, nz) on x faces, (nx, nz) on y faces, (nx, ny) on z faces. Host
+ * pointers, or device pointers with FP_DEVICE (FP_SYNC, FP_CHECK_CONVERGENCE as for the 2D solves); info: the
+ * root GMRES's iterations, restarts, last residual and convergence. */
+int fp_composite3d_solve_f64(fp_composite3d* c, double* const* fields, const double* const* ghosts, int flags,
+                             void* stream, fp_solve_info* info);
+/* Tree actually used: root index and BFS level of every domain (root = 0). */
+int fp_composite3d_tree(const fp_composite3d* c, int* root, int* level_of);
+int fp_composite3d_destroy(fp_composite3d* c);
+
+/* ---------------------------------------------------------------------------------------------------
  * Batched composite solves: many independent ConcatPoissonSolver2D problems of uneven sizes solved
  * together (pe/concat/concat_solver2d.cpp:101-157 per problem), every stage one launch over all problems.
  * No counterpart in the reference, which solves one geometry per solver object; each problem is what a

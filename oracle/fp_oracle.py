@@ -15,6 +15,9 @@ Every function restates one reference routine (paths relative to the reference p
 * composite solve   pe/concat/concat_solver2d.cpp:48-223
 * tree / root       base/domain/geometry_tree.hpp:22-200 (root tie broken by lower domain index,
                     which equals the reference's lower-address rule for contiguously allocated domains)
+* 3D rectangle      pe/poisson/poisson_solver3d.cpp:49-123, chasing_method3d.cpp:3-103
+* 3D composite      pe/concat/concat_solver3d.cpp:5-247, gmres_solver3d.cpp:20-306,
+                    schur_mat3d.cpp:5-285, base/field/field3.cpp:237-375
 
 FFTW's r2c (the only third-party arithmetic; FFTW3, version unpinned by the reference) is restated by
 numpy.fft.rfft, which has the same unnormalised forward definition. Parity of this module is pinned
@@ -30,12 +33,12 @@ import numpy as np
 
 # PDEBoundaryType (base/location_boundary.h:62-69) and LocationType (:8-16) numbering.
 D, N, P, ADJ, NULL = 0, 1, 2, 3, 4
-XNEG, XPOS, YNEG, YPOS = 0, 1, 2, 3
+XNEG, XPOS, YNEG, YPOS, ZNEG, ZPOS = 0, 1, 2, 3, 4, 5
 PI = 3.14159265358979323846  # base/pch.h:13
 
 
 def opposite(loc: int) -> int:
-    return {XNEG: XPOS, XPOS: XNEG, YNEG: YPOS, YPOS: YNEG}[loc]
+    return {XNEG: XPOS, XPOS: XNEG, YNEG: YPOS, YPOS: YNEG, ZNEG: ZPOS, ZPOS: ZNEG}[loc]
 
 
 def is_dir_like(t: int) -> bool:
@@ -488,8 +491,9 @@ class Tree:
     levels: list  # BFS levels, root first
 
 
-def build_tree(n_domains: int, connections, root: int | None = None) -> Tree:
-    """Geometry2D::build_tree (geometry2d.cpp:165-176) with TreeUtils (geometry_tree.hpp:22-200)."""
+def build_tree(n_domains: int, connections, root: int | None = None, faces=(XNEG, XPOS, YNEG, YPOS)) -> Tree:
+    """Geometry2D::build_tree (geometry2d.cpp:165-176) with TreeUtils (geometry_tree.hpp:22-200); Geometry3D
+    (geometry3d.cpp:151-160) builds its tree the same way over six faces."""
     adj = {i: {} for i in range(n_domains)}
     for a, loc, b in connections:
         adj[a][loc] = b
@@ -515,7 +519,7 @@ def build_tree(n_domains: int, connections, root: int | None = None) -> Tree:
     parent = {}
 
     def rec(cur, par):
-        for loc in (XNEG, XPOS, YNEG, YPOS):
+        for loc in faces:
             nb = adj[cur].get(loc)
             if nb is None or nb == par:
                 continue
@@ -681,3 +685,215 @@ def composite_apply(domains, connections, bc, u):
             lap[:, -1] += (1.0 - r2) * gy1
         out.append(lap)
     return out
+
+
+# ---------------------------------------------------------------------------------------------------
+# 3D composite (ConcatPoissonSolver3D). Fields are (nx, ny, nz) arrays, value(i, j, k) = f[i, j, k]; a face
+# plane is indexed as the reference's Schur matrices index it: x faces (j, k), y faces (i, k), z faces (i, j).
+
+def _plane(f: np.ndarray, face: int, outer: bool) -> np.ndarray:
+    """View of the boundary plane of f on `face` (outer=False: the layer at that face)."""
+    nx, ny, nz = f.shape
+    if face == XNEG:
+        return f[0, :, :]
+    if face == XPOS:
+        return f[nx - 1, :, :]
+    if face == YNEG:
+        return f[:, 0, :]
+    if face == YPOS:
+        return f[:, ny - 1, :]
+    if face == ZNEG:
+        return f[:, :, 0]
+    if face == ZPOS:
+        return f[:, :, nz - 1]
+    raise ValueError(face)
+
+
+def bond_add3(f: np.ndarray, loc: int, a: float, nb: np.ndarray) -> None:
+    """field3::bond_add(LocationType, a, const field3&) -- field3.cpp:306-375 (in place): the layer of f at
+    `loc` gains a times the neighbour's layer on the opposite face."""
+    _plane(f, loc, False)[...] += a * _plane(nb, opposite(loc), False)
+
+
+def schur_matrix3(loc: int, shape, branch_solve) -> np.ndarray:
+    """SchurMat3D_*::construct (schur_mat3d.cpp): column c = the branch's layer facing the node after a solve
+    with a unit impulse at cell c of that layer (row / column index over the plane, row-major)."""
+    face = opposite(loc)  # the branch's face toward the node
+    t = np.zeros(shape)
+    pl = _plane(t, face, False)
+    cn = pl.size
+    S = np.empty((cn, cn))
+    for c in range(cn):
+        t[...] = 0.0
+        pl[np.unravel_index(c, pl.shape)] = 1.0
+        u = branch_solve(t.copy())
+        S[:, c] = _plane(u, face, False).reshape(-1)
+    return S
+
+
+def schur_apply3(loc: int, S: np.ndarray, x: np.ndarray) -> np.ndarray:
+    """SchurMat3D_*::operator* (schur_mat3d.cpp): R zero except its layer at loc = S times x's layer there."""
+    R = np.zeros_like(x)
+    pl = _plane(x, loc, False)
+    _plane(R, loc, False)[...] = (S @ pl.reshape(-1)).reshape(pl.shape)
+    return R
+
+
+class GMRESSolver3D:
+    """GMRESSolver3D (pe/concat/gmres_solver3d.cpp:155-306): restarted GMRES(m) on full 3D fields for
+    (I - A^-1 S) x = A^-1 b, modified Gram-Schmidt, Givens rotations, absolute tolerance on ||r|| (restart test)
+    and |g_{j+1}| (inner test)."""
+
+    def __init__(self, m, tol, max_iter, pe_solve):
+        self.m, self.tol, self.max_iter, self.pe_solve = m, tol, max_iter, pe_solve
+        self.S = []  # (loc, matrix)
+        self.res = []
+
+    def afun(self, x):
+        ft = np.zeros_like(x)
+        for loc, S in self.S:
+            ft = ft + schur_apply3(loc, S, x)
+        ft = self.pe_solve(ft)
+        return x - ft
+
+    def solve(self, b):
+        m, tol = self.m, self.tol
+        b = self.pe_solve(b)
+        self.res = []
+        x = b.copy()
+        for _outer in range(self.max_iter):
+            r = b - self.afun(x)
+            beta = math.sqrt(float(np.dot(r.ravel(), r.ravel())))
+            self.res.append(beta)
+            if beta < tol:
+                return x
+            H = np.zeros((m + 1, m))
+            cs = np.zeros(m)
+            sn = np.zeros(m)
+            g = np.zeros(m + 1)
+            V = [r * (1.0 / beta)]
+            g[0] = beta
+            j = 0
+            while j < m:
+                w = self.afun(V[j])
+                for i in range(j + 1):
+                    H[i, j] = float(np.dot(V[i].ravel(), w.ravel()))
+                    w = w - H[i, j] * V[i]
+                h = math.sqrt(float(np.dot(w.ravel(), w.ravel())))
+                if h < 1e-12:
+                    break
+                H[j + 1, j] = h
+                V.append(w * (1.0 / h))
+                for i in range(j):
+                    t = cs[i] * H[i, j] + sn[i] * H[i + 1, j]
+                    H[i + 1, j] = -sn[i] * H[i, j] + cs[i] * H[i + 1, j]
+                    H[i, j] = t
+                den = math.hypot(H[j, j], H[j + 1, j])
+                cs[j] = H[j, j] / den
+                sn[j] = H[j + 1, j] / den
+                H[j, j] = cs[j] * H[j, j] + sn[j] * H[j + 1, j]
+                H[j + 1, j] = 0.0
+                t = cs[j] * g[j]
+                g[j + 1] = -sn[j] * g[j]
+                g[j] = t
+                if abs(g[j + 1]) < tol:
+                    j += 1
+                    break
+                j += 1
+            y = np.zeros(m)
+            for i in range(j - 1, -1, -1):
+                y[i] = g[i]
+                for k in range(i + 1, j):
+                    y[i] -= H[i, k] * y[k]
+                y[i] /= H[i, i]
+            for i in range(j):
+                x = x + y[i] * V[i]
+        return x
+
+
+@dataclass
+class Domain3:
+    nx: int
+    ny: int
+    nz: int
+    hx: float
+    hy: float
+    hz: float
+    bc: list = dc_field(default_factory=lambda: [D] * 6)  # faces not adjacented
+
+
+class ConcatPoissonSolver3D:
+    """ConcatPoissonSolver3D (pe/concat/concat_solver3d.cpp:5-247). domains[i].bc holds the boundary type of
+    each of the six faces; adjacented faces are overridden from the connections."""
+
+    def __init__(self, domains, connections, m=20, tol=1e-8, max_iter=100, root=None):
+        self.domains = domains
+        self.tree = build_tree(len(domains), connections, root, faces=(XNEG, XPOS, YNEG, YPOS, ZNEG, ZPOS))
+        self.bc = []
+        for i, d in enumerate(domains):
+            b = list(d.bc)
+            for a, loc, bb in connections:
+                if a == i:
+                    b[loc] = ADJ
+                if bb == i:
+                    b[opposite(loc)] = ADJ
+            self.bc.append(b)
+        self.solvers = {}
+        for lvl in reversed(self.tree.levels):  # construct_solver_map, concat_solver3d.cpp:72-98
+            for d in lvl:
+                dom = domains[d]
+                ps = PoissonSolver3D(dom.nx, dom.ny, dom.nz, dom.hx, dom.hy, dom.hz, self.bc[d])
+                if self.tree.children[d]:
+                    g = GMRESSolver3D(m, tol, max_iter, ps.solve)
+                    for loc, c in self.tree.children[d]:
+                        cd_ = domains[c]
+                        g.S.append((loc, schur_matrix3(loc, (cd_.nx, cd_.ny, cd_.nz), self.solvers[c])))
+                    self.solvers[d] = g.solve
+                else:
+                    self.solvers[d] = ps.solve
+
+    def boundary_assembly(self, fields, ghosts):
+        """concat_solver3d.cpp:159-247. ghosts[i][face]: the face's buffer values ((ny, nz), (nx, nz) or
+        (nx, ny); None = zero)."""
+        for i, dom in enumerate(self.domains):
+            f, bt = fields[i], self.bc[i]
+            hs = (dom.hx, dom.hx, dom.hy, dom.hy, dom.hz, dom.hz)
+
+            def g(face):
+                v = ghosts[i][face] if ghosts is not None and ghosts[i] is not None else None
+                return 0.0 if v is None else np.asarray(v, dtype=np.float64)
+
+            for face in range(6):  # Dirichlet faces first, then Neumann faces, as the reference adds them
+                if bt[face] == D:
+                    _plane(f, face, False)[...] += (-1.0 / hs[face] / hs[face]) * g(face)
+            for face in range(6):
+                if bt[face] == N:
+                    _plane(f, face, False)[...] += ((1.0 if face % 2 == 0 else -1.0) / hs[face]) * g(face)
+
+    def solve(self, fields, ghosts=None):
+        """ConcatPoissonSolver3D::solve, concat_solver3d.cpp:100-157. Returns the solution fields."""
+        f = [np.array(x, dtype=np.float64, copy=True) for x in fields]
+        self.boundary_assembly(f, ghosts)
+        for i, dom in enumerate(self.domains):
+            f[i] *= dom.hx * dom.hx
+        T = self.tree
+        temp = {}
+        for lvl in reversed(T.levels[1:]):
+            for d in lvl:
+                temp[d] = f[d].copy()
+                for loc, c in T.children[d]:
+                    bond_add3(temp[d], loc, -1.0, temp[c])
+                    bond_add3(f[d], loc, -1.0, temp[c])
+            for d in lvl:
+                temp[d] = self.solvers[d](temp[d])
+        for loc, c in T.children[T.root]:
+            bond_add3(f[T.root], loc, -1.0, temp[c])
+        f[T.root] = self.solvers[T.root](f[T.root])
+        for lvl in T.levels[1:]:
+            for d in lvl:
+                ploc, par = T.parent[d]
+                bond_add3(f[d], ploc, -1.0, f[par])
+            for d in lvl:
+                f[d] = self.solvers[d](f[d])
+        return f
+

@@ -15,6 +15,8 @@
 //   fpref_concat_*        Geometry2D + Variable2D + ConcatPoissonSolver2D
 //                         (pe/concat/concat_solver2d.cpp:19-223), the case-file flow of
 //                         case/validation/2d/concat_solver_reference.cpp:42-115
+//   fpref_concat3d_*      Geometry3D + Variable3D + ConcatPoissonSolver3D
+//                         (pe/concat/concat_solver3d.cpp:5-247)
 //   fpref_add_random      add_random_number(field2&, ...) (base/math/random.cpp:24-46)
 //   fpref_gmres_mock / fpref_schur_mock
 //                         GMRESSolver2D / SchurMat2D_* with the mock branch solver of
@@ -25,7 +27,11 @@
 #include "base/domain/geometry2d.h"
 #include "base/domain/variable2d.h"
 #include "base/math/random.h"
+#include "base/domain/domain3d.h"
+#include "base/domain/geometry3d.h"
+#include "base/domain/variable3d.h"
 #include "pe/concat/concat_solver2d.h"
+#include "pe/concat/concat_solver3d.h"
 #include "pe/concat/gmres_solver2d.h"
 #include "pe/concat/schur_mat2d.h"
 #include "pe/poisson/poisson_fft2d.h"
@@ -437,5 +443,92 @@ int fpref_add_random(int nx, int ny, double lo, double hi, int seed, double* f)
     copy_out(F, f);
     return 0;
 }
+
+// The 3D composite: domains[i] = Domain3DUniform(nx, ny, nz, lx, ly, lz) allocated contiguously in index
+// order (the address tie-break of TreeUtils::findOptimalRoot then picks the lower index), connect(a, dir, b)
+// in order, bc[6 i + face] on every face that is not adjacented (face order x-, x+, y-, y+, z-, z+), one
+// Variable3D centre field per domain; ConcatPoissonSolver3D(var) with set_parameter(m, tol, maxIter).
+struct Concat3DCase
+{
+    std::vector<Domain3DUniform>           domains;
+    Geometry3D                             geo;
+    std::unique_ptr<Variable3D>            var;
+    std::vector<field3>                    fields;
+    std::unique_ptr<ConcatPoissonSolver3D> solver;
+    double                                 t_construct = 0.0;
+};
+
+void* fpref_concat3d_create(int nd, const int* nx, const int* ny, const int* nz, const double* lx, const double* ly,
+                            const double* lz, int nc, const int* ca, const int* cdir, const int* cb, const int* bc,
+                            int m, double tol, int maxIter)
+{
+    auto* c = new Concat3DCase();
+    c->domains.reserve(nd);
+    for (int i = 0; i < nd; ++i)
+        c->domains.emplace_back(nx[i], ny[i], nz[i], lx[i], ly[i], lz[i], "D" + std::to_string(i));
+    for (int i = 0; i < nd; ++i) c->geo.add_domain(&c->domains[i]);
+    for (int k = 0; k < nc; ++k) c->geo.connect(&c->domains[ca[k]], loc_of(cdir[k]), &c->domains[cb[k]]);
+    c->geo.check();
+    c->geo.solve_prepare();
+    c->var.reset(new Variable3D("v"));
+    c->var->set_geometry(c->geo);
+    c->fields.resize(nd);
+    for (int i = 0; i < nd; ++i) c->var->set_center_field(&c->domains[i], c->fields[i]);
+    for (int i = 0; i < nd; ++i)
+        for (int f = 0; f < 6; ++f)
+        {
+            auto& tm = c->var->boundary_type_map[&c->domains[i]];
+            if (tm.count(loc_of(f)) && tm[loc_of(f)] == PDEBoundaryType::Adjacented) continue;
+            c->var->set_boundary_type(&c->domains[i], loc_of(f), bc_of(bc[6 * i + f]));
+        }
+    auto t0 = std::chrono::steady_clock::now();
+    c->solver.reset(new ConcatPoissonSolver3D(c->var.get()));
+    c->solver->set_parameter(m, tol, maxIter);
+    auto t1        = std::chrono::steady_clock::now();
+    c->t_construct = std::chrono::duration<double>(t1 - t0).count();
+    return c;
+}
+
+int fpref_concat3d_tree(void* h, int* root, int* level_of)
+{
+    auto* c = static_cast<Concat3DCase*>(h);
+    for (size_t i = 0; i < c->domains.size(); ++i)
+        if (&c->domains[i] == c->geo.tree_root) *root = (int)i;
+    for (size_t l = 0; l < c->geo.hierarchical_solve_levels.size(); ++l)
+        for (auto* d : c->geo.hierarchical_solve_levels[l]) level_of[d - c->domains.data()] = (int)l;
+    return 0;
+}
+
+// Fills the fields (value(i, j, k) = rhs[(i ny + j) nz + k]) and the six ghost buffers per domain (x faces
+// ny x nz, y faces nx x nz, z faces nx x ny, row-major; NULL = zero), runs solve(), copies the solution out.
+double fpref_concat3d_solve(void* h, const double* const* rhs, const double* const* ghosts, double* const* out)
+{
+    auto*     c  = static_cast<Concat3DCase*>(h);
+    const int nd = (int)c->domains.size();
+    for (int i = 0; i < nd; ++i)
+    {
+        field3&      F = c->fields[i];
+        const size_t n = (size_t)F.get_nx() * F.get_ny() * F.get_nz();
+        std::memcpy(F.value, rhs[i], n * sizeof(double));
+        for (int f = 0; f < 6; ++f)
+        {
+            field2& b = *c->var->buffer_map[&c->domains[i]][loc_of(f)];
+            for (int p = 0; p < b.get_nx(); ++p)
+                for (int q = 0; q < b.get_ny(); ++q)
+                    b(p, q) = (ghosts && ghosts[6 * i + f]) ? ghosts[6 * i + f][(size_t)p * b.get_ny() + q] : 0.0;
+        }
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    c->solver->solve();
+    auto t1 = std::chrono::steady_clock::now();
+    for (int i = 0; i < nd; ++i)
+    {
+        const field3& F = c->fields[i];
+        std::memcpy(out[i], F.value, (size_t)F.get_nx() * F.get_ny() * F.get_nz() * sizeof(double));
+    }
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+void fpref_concat3d_destroy(void* h) { delete static_cast<Concat3DCase*>(h); }
 
 }  // extern "C"

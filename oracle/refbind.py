@@ -45,6 +45,14 @@ def lib():
         L.fpref_concat_solve.argtypes = [vp, vp, vp, vp, ctypes.c_int]
         L.fpref_concat_solve.restype = ctypes.c_double
         L.fpref_concat_destroy.argtypes = [vp]
+        L.fpref_concat3d_create.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, vp,
+                                            ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        L.fpref_concat3d_create.restype = vp
+        L.fpref_concat3d_tree.argtypes = [vp, ip, vp]
+        L.fpref_concat3d_tree.restype = ctypes.c_int
+        L.fpref_concat3d_solve.argtypes = [vp, vp, vp, vp]
+        L.fpref_concat3d_solve.restype = ctypes.c_double
+        L.fpref_concat3d_destroy.argtypes = [vp]
         L.fpref_gmres_mock.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double, ctypes.c_int, vp]
         L.fpref_schur_mock.argtypes = [ctypes.c_int] * 5 + [vp, vp]
         L.fpref_add_random.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp]
@@ -144,6 +152,63 @@ class ConcatCase:
     def __del__(self):
         if getattr(self, "h", None):
             lib().fpref_concat_destroy(self.h)
+            self.h = None
+
+
+class Concat3DCase:
+    """Geometry3D + Variable3D + ConcatPoissonSolver3D built by the reference (pe/concat/concat_solver3d.cpp).
+    Domains (nx, ny, nz, lx, ly, lz) per index, connections (a, face of a, b), bc: 6 per domain (faces x-, x+,
+    y-, y+, z-, z+; ignored where adjacented)."""
+
+    def __init__(self, nx, ny, nz, lx, ly, lz, connections, bc, m=20, tol=1e-8, max_iter=100):
+        nd = len(nx)
+        self._keep = []
+
+        def arr(x, dt):
+            a = np.ascontiguousarray(np.asarray(x, dtype=dt))
+            self._keep.append(a)
+            return _ptr(a)
+
+        self.h = lib().fpref_concat3d_create(nd, arr(nx, np.int32), arr(ny, np.int32), arr(nz, np.int32),
+                                             arr(lx, np.float64), arr(ly, np.float64), arr(lz, np.float64),
+                                             len(connections), arr([c[0] for c in connections], np.int32),
+                                             arr([c[1] for c in connections], np.int32),
+                                             arr([c[2] for c in connections], np.int32),
+                                             arr(np.asarray(bc).ravel(), np.int32), m, float(tol), max_iter)
+        if not self.h:
+            raise RuntimeError("reference case construction failed")
+        self.nd = nd
+
+    def tree(self):
+        root = ctypes.c_int(0)
+        lv = np.zeros(self.nd, dtype=np.int32)
+        lib().fpref_concat3d_tree(self.h, ctypes.byref(root), _ptr(lv))
+        return root.value, lv
+
+    def solve(self, rhs, ghosts=None):
+        """rhs: per domain (nx, ny, nz) arrays; ghosts: None or per domain 6 arrays / None (x faces (ny, nz),
+        y faces (nx, nz), z faces (nx, ny)). Returns the solution fields and the solve time."""
+        rhs = [np.ascontiguousarray(r, dtype=np.float64) for r in rhs]
+        outs = [np.empty_like(r) for r in rhs]
+        rp = (ctypes.c_void_p * self.nd)(*[r.ctypes.data for r in rhs])
+        op = (ctypes.c_void_p * self.nd)(*[o.ctypes.data for o in outs])
+        gp = None
+        if ghosts is not None:
+            gl = []
+            for i in range(self.nd):
+                for f in range(6):
+                    g = None if ghosts[i] is None else ghosts[i][f]
+                    if g is not None:
+                        g = np.ascontiguousarray(g, dtype=np.float64)
+                        self._keep.append(g)
+                    gl.append(None if g is None else g.ctypes.data)
+            gp = (ctypes.c_void_p * (6 * self.nd))(*gl)
+        t = lib().fpref_concat3d_solve(self.h, rp, gp, op)
+        return outs, t
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().fpref_concat3d_destroy(self.h)
             self.h = None
 
 

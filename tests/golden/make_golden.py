@@ -109,6 +109,57 @@ def poisson3d():
     save("poisson3d.npz", **out)
 
 
+# 3D composite cases: domains (nx, ny, nz, lx, ly, lz), connections (a, face of a, b), outer boundary types per
+# domain (6 faces x-, x+, y-, y+, z-, z+), whether ghost buffers are set.
+CONCAT3D_CASES = {
+    "pair": ([(16, 16, 16, 1.0, 1.0, 1.0), (12, 16, 16, 0.75, 1.0, 1.0)], [(0, 1, 1)],
+             [[D] * 6, [D] * 6], False),
+    "star": ([(12, 10, 8, 1.2, 1.0, 0.8), (8, 10, 8, 0.8, 1.0, 0.8), (12, 6, 8, 1.2, 0.6, 0.8),
+              (12, 10, 5, 1.2, 1.0, 0.5), (12, 10, 4, 1.2, 1.0, 0.4)],
+             [(0, 0, 1), (0, 3, 2), (0, 4, 3), (0, 5, 4)],
+             [[D, N, D, D, D, D], [N, D, D, N, D, D], [D, D, D, N, N, D], [D, D, N, D, D, D], [N, D, D, D, D, N]], True),
+    "chain": ([(6, 6, 6, 1.0, 1.0, 1.0)] * 4, [(0, 1, 1), (1, 1, 2), (2, 1, 3)],
+              [[N, D, D, D, D, D], [D] * 6, [D] * 6, [D, N, N, N, N, N]], True),
+    "periodic_y": ([(10, 8, 6, 1.0, 0.8, 0.6), (14, 8, 6, 1.4, 0.8, 0.6)], [(0, 1, 1)],
+                   [[D, D, P, P, D, D], [D, N, P, P, D, D]], True),
+    "x64": ([(64, 8, 8, 1.0, 0.125, 0.125), (32, 8, 8, 0.5, 0.125, 0.125)], [(0, 0, 1)],
+            [[D, N, D, D, N, N], [D, D, D, D, D, D]], False),
+}
+
+
+def concat3d():
+    """ConcatPoissonSolver3D (pe/concat/concat_solver3d.cpp) of the reference's own sources on seeded random
+    right-hand sides and ghost buffers: two boxes, a star of four children on x-, y+, z- and z+ faces, a chain of
+    four (a tree of depth 2), periodic y faces and a root of 64 cells along x (the partition chase); GMRES(20,
+    1e-12, 100), and the same solve at tol 1e-15 ("tight")."""
+    rng = np.random.default_rng(404)
+    out = {}
+    for name, (doms, conns, bcs, with_ghosts) in CONCAT3D_CASES.items():
+        nx, ny, nz, lx, ly, lz = (list(v) for v in zip(*doms))
+        rhs = [rng.standard_normal((a, b, c)) for a, b, c in zip(nx, ny, nz)]
+        ghosts = None
+        if with_ghosts:
+            ghosts = [[rng.standard_normal(s) for s in ((b, c), (b, c), (a, c), (a, c), (a, b), (a, b))]
+                      for a, b, c in zip(nx, ny, nz)]
+        ref = R.Concat3DCase(nx, ny, nz, lx, ly, lz, conns, bcs, 20, 1e-12, 100)
+        sol, _ = ref.solve(rhs, ghosts)
+        tight, _ = R.Concat3DCase(nx, ny, nz, lx, ly, lz, conns, bcs, 20, 1e-15, 100).solve(rhs, ghosts)
+        root, levels = ref.tree()
+        out[f"{name}_dims"] = np.asarray(doms, dtype=np.float64)
+        out[f"{name}_conns"] = np.asarray(conns, dtype=np.int32)
+        out[f"{name}_bc"] = np.asarray(bcs, dtype=np.int32)
+        out[f"{name}_root"] = np.asarray(root, dtype=np.int32)
+        out[f"{name}_levels"] = levels
+        for i in range(len(doms)):
+            out[f"{name}_rhs_{i}"] = rhs[i]
+            out[f"{name}_out_{i}"] = sol[i]
+            out[f"{name}_tight_{i}"] = tight[i]
+            for f in range(6):
+                if ghosts is not None:
+                    out[f"{name}_ghost_{i}_{f}"] = ghosts[i][f]
+    save("concat3d.npz", **out)
+
+
 def composite(name, g: W.Geometry, rhs, m, tol, max_iter, ghosts=None, extra=None):
     lx = [a * h for a, h in zip(g.nx, g.hx)]
     ly = [b * h for b, h in zip(g.ny, g.hy)]
@@ -233,6 +284,7 @@ if __name__ == "__main__":
     transforms()
     poisson()
     poisson3d()
+    concat3d()
     fixture6()
     cross_config1()
     cross_neumann()

@@ -3,7 +3,7 @@ produced by the reference's own C++ sources (tests/golden/make_golden.py). CPU o
 import numpy as np
 import pytest
 
-from golden_io import COMPOSITE_CASES, composite_case, load, rel_l2
+from golden_io import COMPOSITE_CASES, CONCAT3D_CASES, composite_case, concat3d_case, load, rel_l2
 from oracle import fp_oracle as O
 
 KINDS = ["DD", "NN", "ND", "DN", "PP"]
@@ -97,3 +97,18 @@ def test_poisson3d_matches_reference():
         got = O.PoissonSolver3D(*g.shape, *z[f"{tag}_h"], [int(b) for b in z[f"{tag}_bc"]]).solve(g)
         ref = z[f"{tag}_out"]
         assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), tag
+
+
+@pytest.mark.parametrize("name", CONCAT3D_CASES)
+def test_concat3d_matches_reference(name):
+    """The oracle's ConcatPoissonSolver3D (tree, Schur matrices by impulse solves, GMRES on full fields, the
+    two passes) against the reference's own solve of the same case: same tree, same answer to round-off."""
+    doms, conns, bc, rhs, ghosts, outs, tight, root, levels = concat3d_case(name)
+    D3 = [O.Domain3(*d, list(b)) for d, b in zip(doms, bc)]
+    s = O.ConcatPoissonSolver3D(D3, conns, 20, 1e-12, 100)
+    assert s.tree.root == root
+    for lv, members in enumerate(s.tree.levels):
+        assert all(levels[d] == lv for d in members)
+    got = s.solve(rhs, ghosts)
+    assert rel_l2(got, outs) <= 1e-13, name
+
