@@ -401,7 +401,7 @@ def large_section(args, dev):
     c = capi.Composite(g, 20, 1e-12, 100)
     for w, p in zip(work, pristine):
         w.copy_(p)
-    c.solve(work)  # builds the Schur matrices and interface inverses on first use
+    c.solve(work)  # the Schur matrices and interface inverses are built at creation; first solve warms up
     torch.cuda.synchronize()
     out["setup_s"] = time.perf_counter() - t0
 
@@ -437,6 +437,118 @@ def large_section(args, dev):
     torch.cuda.empty_cache()
     return out
 
+
+
+def star3d(n):
+    """A root box of n^3 cells with four n^3 children on its x-, x+, y- and z+ faces (h = 1/n), Dirichlet outer
+    faces except Neumann x+ on the x+ child: (domains, connections, bc) for capi.Composite3D."""
+    h = 1.0 / n
+    doms = [(n, n, n, h, h, h)] * 5
+    conns = [(0, 0, 1), (0, 1, 2), (0, 2, 3), (0, 5, 4)]
+    bc = [[0] * 6, [0] * 6, [0, 1, 0, 0, 0, 0], [0] * 6, [0] * 6]
+    return doms, conns, bc
+
+
+def threed_section(args, dev, with_cpu):
+    """3D solves. PoissonSolver3D on 256^3 (Dirichlet faces) and ConcatPoissonSolver3D on a star of five 64^3
+    boxes, device-timed with CUDA events (each step refills the right-hand side from a resident copy). Beside
+    them the reference's own 3D solvers (oracle/_ref) on the host cores: the rectangle at the same size, the
+    composite at 32^3 per box (the reference builds its Schur matrices by one impulse solve per face cell)."""
+    import torch
+
+    from focalors_poisson_b200 import capi
+
+    out = {}
+    n = 256
+    h = 1.0 / n
+    bc = (0, 0, 0, 0, 0, 0)
+    f0 = np.random.default_rng(SEED).standard_normal((n, n, n))
+    rect = capi.Rect3D(n, n, n, h, h, h, bc)
+    x = torch.tensor(f0, device=dev)
+    w = torch.empty_like(x)
+
+    def device_time(step, reps):
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def rect_step():
+        w.copy_(x)
+        rect.solve(w)
+
+    ms = device_time(rect_step, max(args.steps, 5))
+    # z-transform, transpose, y-transform, chase (two passes), y-inverse, transpose back, z-inverse: 8 passes
+    # that each read and write the field
+    alg = 16 * n ** 3 * 8
+    peak, peak_kind = measured_peaks()
+    r3 = {"workload": f"PoissonSolver3D {n}^3, Dirichlet faces, h = 1/{n}, N(0,1) right-hand side (seed {SEED})",
+          "solves_per_s": 1e3 / ms, "ms": ms, "algorithmic_bytes": alg, "achieved_gbs": alg / ms / 1e6,
+          "frac_of_hbm": alg / ms / 1e6 / peak, "peak_source": f"{peak_kind} hbm_gbs",
+          "step_note": "each step includes the 134 MB device copy that refills the right-hand side"}
+    if with_cpu:
+        from oracle import refbind as R
+
+        got = w.cpu().numpy()
+        t0 = time.perf_counter()
+        ref, sec = R.poisson3d_solve(f0, h, h, h, bc)
+        r3["cpu_reference"] = {"solves_per_s": 1.0 / sec, "seconds": sec, "cores": os.cpu_count(),
+                               "what": "the reference's PoissonSolver3D::solve on the same field (oracle/_ref)",
+                               "wall_s": time.perf_counter() - t0}
+        r3["rel_l2_vs_reference"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    out["rect3d"] = r3
+    del rect, x, w
+
+    doms, conns, cbc = star3d(64)
+    t0 = time.perf_counter()
+    c3 = capi.Composite3D(doms, conns, cbc, 20, 1e-10, 100)
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    rng = np.random.default_rng(SEED + 1)
+    rhs = [torch.tensor(rng.standard_normal(d[:3]), device=dev) for d in doms]
+    work = [torch.empty_like(r) for r in rhs]
+    info = {}
+
+    def c3_step():
+        for a, b in zip(work, rhs):
+            a.copy_(b)
+        info.update(c3.solve(work))
+
+    ms = device_time(c3_step, 5)
+    c3d = {"workload": "ConcatPoissonSolver3D: root 64^3 with four 64^3 children (x-, x+, y-, z+ faces), "
+                       "GMRES(20, 1e-10, 100), N(0,1) right-hand sides", "solves_per_s": 1e3 / ms, "ms": ms,
+           "setup_s": setup, "gmres_iterations": info.get("iterations")}
+    del c3, rhs, work
+    if with_cpu:
+        from oracle import refbind as R
+
+        doms, conns, cbc = star3d(32)
+        rng = np.random.default_rng(SEED + 2)
+        rhs = [rng.standard_normal(d[:3]) for d in doms]
+        small = capi.Composite3D(doms, conns, cbc, 20, 1e-10, 100)
+        got = [r.copy() for r in rhs]
+        small.solve(got)
+        t0 = time.perf_counter()
+        ref = R.Concat3DCase([d[0] for d in doms], [d[1] for d in doms], [d[2] for d in doms],
+                             [d[0] * d[3] for d in doms], [d[1] * d[4] for d in doms], [d[2] * d[5] for d in doms],
+                             conns, cbc, 20, 1e-10, 100)
+        construct = time.perf_counter() - t0
+        refout, sec = ref.solve(rhs)
+        num = sum(float(((a - b) ** 2).sum()) for a, b in zip(got, refout))
+        den = sum(float((b ** 2).sum()) for b in refout)
+        c3d["reference_32"] = {"what": "the same star at 32^3 per box: the reference's ConcatPoissonSolver3D "
+                                       "(oracle/_ref) on the host cores against this solver",
+                               "cpu_solves_per_s": 1.0 / sec, "cpu_construct_s": construct,
+                               "rel_l2_vs_reference": (num / den) ** 0.5, "cores": os.cpu_count()}
+    out["composite3d"] = c3d
+    torch.cuda.empty_cache()
+    return out
 
 
 # ------------------------------------------------------------------------------------------------
@@ -561,6 +673,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-uneven section")
     ap.add_argument("--no-large", action="store_true", help="skip the 9 x 4096^2 tree section (setup ~2 min)")
+    ap.add_argument("--no-3d", action="store_true", help="skip the 3D rectangle and composite section")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -833,6 +946,8 @@ def main():
         line["batched_uneven"] = batched_section(args, dev, rank, world, dist)
     if not args.no_large and world == 1:
         line["large_tree"] = large_section(args, dev)
+    if not args.no_3d and world == 1:
+        line["three_d"] = threed_section(args, dev, with_cpu=rank == 0 and not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

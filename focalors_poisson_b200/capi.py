@@ -48,6 +48,12 @@ SIGNATURES = {
     "fp_composite3d_solve_f64": ([_vp, _vp, _vp, _i, _vp, _vp], _i),
     "fp_composite3d_tree": ([_vp, _vp, _vp], _i),
     "fp_composite3d_destroy": ([_vp], _i),
+    "fp_composite_part_create": ([_vp, _i, _d, _i, _i, _i, _vp, _vp], _i),
+    "fp_composite_part_schur": ([_vp, _i, _vp, _vp], _i),
+    "fp_composite_set_external_schur": ([_vp, _i, _vp], _i),
+    "fp_composite_part_upward": ([_vp, _vp, _vp, _i, _vp, _vp, _vp], _i),
+    "fp_composite_part_downward": ([_vp, _vp, _i, _vp, _vp, _vp], _i),
+    "fp_composite_root_solve": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp], _i),
     "fp_composite_solve_async": ([_vp, _vp, _vp, _vp, _i, _d, _i, _vp], _i),
     "fp_composite_wait": ([_vp, _i, _vp], _i),
     "fp_composite_residual": ([_vp, _vp, _vp, _vp, _vp, _vp], _i),
@@ -298,6 +304,84 @@ class Composite3D:
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
             _lib.fp_composite3d_destroy(self.h)
+            self.h = None
+
+
+def _cuda_ptrs(tensors, what):
+    ptrs = []
+    for t in tensors:
+        if t is None:
+            ptrs.append(None)
+            continue
+        if not _is_torch(t) or not t.is_cuda or not t.is_contiguous() or str(t.dtype) != "torch.float64":
+            raise TypeError(f"{what}: contiguous float64 CUDA tensors expected")
+        ptrs.append(t.data_ptr())
+    return (ctypes.c_void_p * max(1, len(ptrs)))(*ptrs)
+
+
+class CompositePart:
+    """One part of a subtree decomposition of the composite solve (fp_composite_part_*): a subtree part
+    (geometry of the subtree, its root's face toward the root domain Adjacented, ext_faces empty) or the root
+    part (the root domain alone, ext_faces = the faces of its children in other parts, increasing). All
+    arrays are float64 CUDA tensors; work is queued on torch's current stream."""
+
+    def __init__(self, geo, m=20, tol=1e-8, max_iter=100, root=-1, ext_faces=()):
+        nd = len(geo.nx)
+        self.nd = nd
+        self.shapes = [(int(a), int(b)) for a, b in zip(geo.nx, geo.ny)]
+        self._arr = dict(
+            nx=np.ascontiguousarray(geo.nx, dtype=np.int32), ny=np.ascontiguousarray(geo.ny, dtype=np.int32),
+            hx=np.ascontiguousarray(geo.hx, dtype=np.float64), hy=np.ascontiguousarray(geo.hy, dtype=np.float64),
+            bc=np.ascontiguousarray(np.asarray(geo.bc, dtype=np.int32).reshape(-1)),
+            conn=np.ascontiguousarray(np.asarray(geo.connections, dtype=np.int32).reshape(-1)),
+            ext=np.ascontiguousarray(np.asarray(list(ext_faces), dtype=np.int32)))
+        a = self._arr
+        g = Geometry(nd, a["nx"].ctypes.data, a["ny"].ctypes.data, a["hx"].ctypes.data, a["hy"].ctypes.data,
+                     a["bc"].ctypes.data, len(geo.connections), a["conn"].ctypes.data if len(geo.connections) else None,
+                     int(root))
+        h = ctypes.c_void_p()
+        check(lib().fp_composite_part_create(ctypes.byref(g), int(m), float(tol), int(max_iter), 0, len(ext_faces),
+                                             a["ext"].ctypes.data if len(ext_faces) else None, ctypes.byref(h)))
+        self.h = h
+
+    @staticmethod
+    def _info(info):
+        return Composite._info(info)
+
+    def schur(self, face, S):
+        check(lib().fp_composite_part_schur(self.h, int(face), _cuda_ptrs([S], "S")[0], _stream()))
+
+    def set_external_schur(self, k, S):
+        check(lib().fp_composite_set_external_schur(self.h, int(k), _cuda_ptrs([S], "S")[0]))
+
+    def _ghosts(self, ghosts):
+        if ghosts is None:
+            return None
+        return _cuda_ptrs([None if ghosts[d] is None else ghosts[d][f] for d in range(self.nd) for f in range(4)],
+                          "ghosts")
+
+    def upward(self, fields, ghosts, face, edge_out):
+        info = SolveInfo()
+        check(lib().fp_composite_part_upward(self.h, _cuda_ptrs(fields, "fields"), self._ghosts(ghosts), int(face),
+                                             _cuda_ptrs([edge_out], "edge")[0], _stream(), ctypes.byref(info)))
+        return self._info(info)
+
+    def downward(self, fields, face, parent_edge):
+        info = SolveInfo()
+        check(lib().fp_composite_part_downward(self.h, _cuda_ptrs(fields, "fields"), int(face),
+                                               _cuda_ptrs([parent_edge], "edge")[0], _stream(), ctypes.byref(info)))
+        return self._info(info)
+
+    def root_solve(self, fields, ghosts, child_edges, edges_out):
+        info = SolveInfo()
+        check(lib().fp_composite_root_solve(self.h, _cuda_ptrs(fields, "fields"), self._ghosts(ghosts),
+                                            _cuda_ptrs(child_edges, "child edges"), _cuda_ptrs(edges_out, "edges"),
+                                            _stream(), ctypes.byref(info)))
+        return self._info(info)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fp_composite_destroy(self.h)
             self.h = None
 
 

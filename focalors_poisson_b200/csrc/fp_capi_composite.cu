@@ -60,7 +60,8 @@ struct fp_composite
 
 namespace
 {
-std::unique_ptr<Composite> make_composite(const fp_geometry* g, int m, double tol, int max_iter, int flags)
+std::unique_ptr<Composite> make_composite(const fp_geometry* g, int m, double tol, int max_iter, int flags,
+                                          const std::vector<std::array<int, 2>>& ext = {})
 {
     if (!g || g->n_domains <= 0 || !g->nx || !g->ny || !g->hx || !g->hy || !g->bc)
         throw Error(FP_ERR_INVALID, "incomplete geometry description");
@@ -79,7 +80,7 @@ std::unique_ptr<Composite> make_composite(const fp_geometry* g, int m, double to
         conns[k] = {g->connections[3 * k], g->connections[3 * k + 1], g->connections[3 * k + 2]};
     const int mode = (flags & FP_GMRES_FULLFIELD) ? GMRES_FULLFIELD : GMRES_INTERFACE;
     return std::unique_ptr<Composite>(
-        new Composite(doms, conns, g->root, m, tol, max_iter, mode, (flags & FP_NO_INTERFACE_INVERSE) == 0));
+        new Composite(doms, conns, g->root, m, tol, max_iter, mode, (flags & FP_NO_INTERFACE_INVERSE) == 0, ext));
 }
 }  // namespace
 
@@ -217,6 +218,12 @@ int fp_composite_create(const fp_geometry* g, int m, double tol, int max_iter, i
                 if (e.code != FP_ERR_UNSUPPORTED) throw;
                 h->sp64.reset();  // outside the spectral path's scope: Schur GMRES
             }
+        }
+        // the Schur GMRES path builds its matrices and interface inverses here, so that no solve pays for them
+        if (!h->sp64)
+        {
+            h->c->prepare();
+            FPB_CUDA(cudaDeviceSynchronize());
         }
         *out = h.release();
     });
@@ -464,6 +471,116 @@ int fp_composite_wait(fp_composite* c, int flags, fp_solve_info* info)
         }
     });
     fill_info(info, gi, steps, change);
+    return rc;
+}
+
+int fp_composite_part_create(const fp_geometry* g, int m, double tol, int max_iter, int flags, int n_ext,
+                             const int* ext_faces, fp_composite** out)
+{
+    return guarded([&] {
+        if (!out) throw Error(FP_ERR_INVALID, "null output handle");
+        *out = nullptr;
+        if (n_ext < 0 || (n_ext > 0 && !ext_faces)) throw Error(FP_ERR_INVALID, "bad external child list");
+        if (!g || g->n_domains <= 0 || !g->nx || !g->ny) throw Error(FP_ERR_INVALID, "incomplete geometry description");
+        require_device();
+        const int r = g->root >= 0 ? g->root : 0;
+        if (n_ext > 0 && (g->root < 0 || r >= g->n_domains))
+            throw Error(FP_ERR_INVALID, "a root part names its root domain");
+        std::vector<std::array<int, 2>> ext;
+        for (int k = 0; k < n_ext; ++k)
+        {
+            const int f = ext_faces[k];
+            if (f < 0 || f > 3) throw Error(FP_ERR_INVALID, "external child face out of range");
+            ext.push_back({f, f < 2 ? g->ny[r] : g->nx[r]});
+        }
+        std::unique_ptr<fp_composite> h(new fp_composite());
+        h->c = make_composite(g, m, tol, max_iter, flags & ~FP_GMRES_FULLFIELD, ext);
+        if (n_ext == 0)
+        {
+            h->c->prepare();
+            FPB_CUDA(cudaDeviceSynchronize());
+        }
+        *out = h.release();
+    });
+}
+
+int fp_composite_part_schur(fp_composite* c, int face, double* S, void* stream)
+{
+    return guarded([&] {
+        if (!c || !S) throw Error(FP_ERR_INVALID, "null argument");
+        c->c->part_schur(face, S, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int fp_composite_set_external_schur(fp_composite* c, int k, const double* S)
+{
+    return guarded([&] {
+        if (!c || !S) throw Error(FP_ERR_INVALID, "null argument");
+        c->c->set_external_schur(k, S);
+    });
+}
+
+namespace
+{
+void fill_part_info(fp_solve_info* info, const GmresInfo& gi)
+{
+    if (!info) return;
+    info->gmres_iterations = gi.iterations;
+    info->gmres_restarts   = gi.restarts;
+    info->gmres_residual   = gi.residual;
+    info->converged        = gi.converged ? 1 : 0;
+    info->refinements      = 0;
+    info->rel_change       = 0.0;
+}
+void check_fields(fp_composite* c, double* const* fields)
+{
+    if (!c) throw Error(FP_ERR_INVALID, "null solver");
+    if (!fields) throw Error(FP_ERR_INVALID, "null field list");
+    for (size_t d = 0; d < c->c->domains().size(); ++d)
+        if (!fields[d]) throw Error(FP_ERR_INVALID, "null field pointer");
+}
+}  // namespace
+
+int fp_composite_part_upward(fp_composite* c, double* const* fields, const double* const* ghosts, int face,
+                             double* edge_out, void* stream, fp_solve_info* info)
+{
+    GmresInfo gi;
+    const int rc = guarded([&] {
+        check_fields(c, fields);
+        if (!edge_out) throw Error(FP_ERR_INVALID, "null edge buffer");
+        c->c->part_upward(fields, ghosts, face, edge_out, static_cast<cudaStream_t>(stream), &gi);
+    });
+    fill_part_info(info, gi);
+    return rc;
+}
+
+int fp_composite_part_downward(fp_composite* c, double* const* fields, int face, const double* parent_edge,
+                               void* stream, fp_solve_info* info)
+{
+    GmresInfo gi;
+    const int rc = guarded([&] {
+        check_fields(c, fields);
+        if (!parent_edge) throw Error(FP_ERR_INVALID, "null edge buffer");
+        c->c->part_downward(fields, face, parent_edge, static_cast<cudaStream_t>(stream), &gi);
+    });
+    fill_part_info(info, gi);
+    return rc;
+}
+
+int fp_composite_root_solve(fp_composite* c, double* const* fields, const double* const* ghosts,
+                            const double* const* child_edges, double* const* edges_out, void* stream,
+                            fp_solve_info* info)
+{
+    GmresInfo gi;
+    const int rc = guarded([&] {
+        check_fields(c, fields);
+        const int n = c->c->external_children();
+        for (int k = 0; k < n; ++k)
+            if (!child_edges || !child_edges[k] || !edges_out || !edges_out[k])
+                throw Error(FP_ERR_INVALID, "null edge buffer");
+        c->c->root_solve(fields, ghosts, child_edges, edges_out, static_cast<cudaStream_t>(stream), &gi);
+    });
+    fill_part_info(info, gi);
     return rc;
 }
 

@@ -140,7 +140,8 @@ Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root, 
 }
 
 Composite::Composite(const std::vector<Domain>& doms, const std::vector<std::array<int, 3>>& conns, int root, int m,
-                     double tol, int max_iter, int mode, bool interface_inverse)
+                     double tol, int max_iter, int mode, bool interface_inverse,
+                     const std::vector<std::array<int, 2>>& ext)
     : dom_(doms), m_(m), max_iter_(max_iter), mode_(mode), want_inverse_(interface_inverse), tol_(tol)
 {
     if (m < 1 || m > 200) throw Error(1, "GMRES restart length m must be in [1, 200]");
@@ -156,9 +157,6 @@ Composite::Composite(const std::vector<Domain>& doms, const std::vector<std::arr
         if (xdir ? (a.ny != b.ny) : (a.nx != b.nx))
             throw Error(1, "connected domains must share the interface length");
     }
-    rect_.resize(nd);
-    for (int d = 0; d < nd; ++d)
-        rect_[d].reset(new DevRect<double>(dom_[d].nx, dom_[d].ny, dom_[d].hx, dom_[d].hy, dom_[d].bc));
     temp_.resize(nd);
     for (int d = 0; d < nd; ++d)
         if (d != tree_.root) temp_[d].alloc(dom_[d].cells() * sizeof(double));
@@ -177,11 +175,34 @@ Composite::Composite(const std::vector<Domain>& doms, const std::vector<std::arr
             off += L.cn;
             nd_.kids.push_back(std::move(L));
         }
+        if (d == tree_.root)
+            for (size_t q = 0; q < ext.size(); ++q)  // children in other parts: no local domain, Schur matrix later
+            {
+                const auto& e = ext[q];
+                if (e[0] < 0 || e[0] > 3) throw Error(1, "external child face out of range");
+                if (q > 0 && e[0] <= ext[q - 1][0]) throw Error(1, "external children must be given in face order");
+                for (const auto& k : nd_.kids)
+                    if (k.loc == e[0]) throw Error(1, "external child on a connected face");
+                if (e[1] != edge_length(e[0], dom_[d].nx, dom_[d].ny))
+                    throw Error(1, "external child interface length differs from the root's face");
+                dom_[d].bc[e[0]] = BC_ADJACENTED;
+                Link L;
+                L.loc   = e[0];
+                L.child = -1;
+                L.cn    = e[1];
+                L.off   = off;
+                off += L.cn;
+                nd_.kids.push_back(std::move(L));
+                ++n_ext_;
+            }
         if (nd_.kids.empty()) continue;
         nd_.n_if = off;
         nd_.n    = (mode_ == GMRES_FULLFIELD) ? dom_[d].cells() : (long long)off;
         nd_.R.alloc(dom_[d].cells() * sizeof(double));
     }
+    rect_.resize(nd);  // after the external children's faces became Adjacented
+    for (int d = 0; d < nd; ++d)
+        rect_[d].reset(new DevRect<double>(dom_[d].nx, dom_[d].ny, dom_[d].hx, dom_[d].hy, dom_[d].bc));
     red_.alloc((kRedBlocks + 8) * sizeof(double));
     FPB_CUDA(cudaMemset(red_.get(), 0, red_.bytes()));
     set_parameter(m, tol, max_iter);
@@ -683,6 +704,36 @@ bool Composite::schur_by_spectral(Link& L, cudaStream_t s)
     return true;
 }
 
+// One Schur matrix (SchurMat2D_*::construct, schur_mat2d.cpp:5-106): column i = the child's response along its
+// face toward the parent to a unit impulse at cell i of that face; by batched rectangle solves for a leaf, by
+// the spectral closed form where it applies, else by one subtree solve per impulse.
+void Composite::link_schur(Link& L, cudaStream_t s)
+{
+    const int       c     = L.child;
+    const Domain&   C     = dom_[c];
+    const int       face  = L.loc ^ 1;  // child's face toward its parent
+    const long long cells = C.cells();
+    L.S.alloc((size_t)L.cn * L.cn * sizeof(double));
+    const bool leaf = node_[c].kids.empty();
+    if (!leaf && mode_ != GMRES_FULLFIELD && schur_by_spectral(L, s)) return;
+    long long nb = leaf ? std::max(1LL, std::min<long long>(L.cn, (512LL << 20) / (cells * 8))) : 1;
+    DevBuf    work((size_t)nb * cells * sizeof(double));
+    for (int i0 = 0; i0 < L.cn; i0 += (int)nb)
+    {
+        const int cnt = (int)std::min<long long>(nb, L.cn - i0);
+        FPB_CUDA(cudaMemsetAsync(work.get(), 0, (size_t)cnt * cells * sizeof(double), s));
+        k_impulses<double><<<grid_for(cnt, 128), 128, 0, s>>>(work.as<double>(), C.nx, C.ny, face, i0, cnt);
+        FPB_CHECK_LAUNCH();
+        if (leaf) rect_[c]->solve(work.as<double>(), cnt, s);
+        else
+            for (int b = 0; b < cnt; ++b) node_solve(c, work.as<double>() + (size_t)b * cells, s, nullptr);
+        k_impulse_extract<double><<<grid_for((long long)cnt * L.cn, 256), 256, 0, s>>>(
+            work.as<double>(), C.nx, C.ny, face, L.S.as<double>(), L.cn, i0, cnt);
+        FPB_CHECK_LAUNCH();
+    }
+    FPB_CUDA(cudaStreamSynchronize(s));
+}
+
 void Composite::build_schur()
 {
     cudaStream_t s = 0;
@@ -690,29 +741,8 @@ void Composite::build_schur()
         for (int d : *lv)
             for (Link& L : node_[d].kids)
             {
-                const int       c     = L.child;
-                const Domain&   C     = dom_[c];
-                const int       face  = L.loc ^ 1;  // child's face toward d
-                const long long cells = C.cells();
-                L.S.alloc((size_t)L.cn * L.cn * sizeof(double));
-                const bool leaf = node_[c].kids.empty();
-                if (!leaf && mode_ != GMRES_FULLFIELD && schur_by_spectral(L, s)) continue;
-                long long  nb   = leaf ? std::max(1LL, std::min<long long>(L.cn, (512LL << 20) / (cells * 8))) : 1;
-                DevBuf     work((size_t)nb * cells * sizeof(double));
-                for (int i0 = 0; i0 < L.cn; i0 += (int)nb)
-                {
-                    const int cnt = (int)std::min<long long>(nb, L.cn - i0);
-                    FPB_CUDA(cudaMemsetAsync(work.get(), 0, (size_t)cnt * cells * sizeof(double), s));
-                    k_impulses<double><<<grid_for(cnt, 128), 128, 0, s>>>(work.as<double>(), C.nx, C.ny, face, i0, cnt);
-                    FPB_CHECK_LAUNCH();
-                    if (leaf) rect_[c]->solve(work.as<double>(), cnt, s);
-                    else
-                        for (int b = 0; b < cnt; ++b) node_solve(c, work.as<double>() + (size_t)b * cells, s, nullptr);
-                    k_impulse_extract<double><<<grid_for((long long)cnt * L.cn, 256), 256, 0, s>>>(
-                        work.as<double>(), C.nx, C.ny, face, L.S.as<double>(), L.cn, i0, cnt);
-                    FPB_CHECK_LAUNCH();
-                }
-                FPB_CUDA(cudaStreamSynchronize(s));
+                if (L.child >= 0) link_schur(L, s);
+                else if (!L.S.get()) throw Error(1, "external child's Schur matrix not set");
             }
 }
 
@@ -744,7 +774,8 @@ void Composite::assemble(double* const* fields, const double* const* ghosts, cud
     }
 }
 
-void Composite::eliminate(double* const* fields, cudaStream_t s, GmresInfo* info)
+void Composite::eliminate(double* const* fields, cudaStream_t s, GmresInfo* info, const double* const* child_edges,
+                          double* const* edges_out)
 {
     ensure_built();
     auto bond = [&](double* dst, int dd, int loc, const double* src, int sd) {
@@ -769,7 +800,19 @@ void Composite::eliminate(double* const* fields, cudaStream_t s, GmresInfo* info
         for (int d : T.levels[l]) node_solve(d, temp_[d].as<double>(), s, nullptr);
     }
     for (auto& c : T.children[T.root]) bond(fields[T.root], T.root, c.first, temp_[c.second].as<double>(), c.second);
+    if (n_ext_ > 0 && !child_edges) throw Error(1, "a root part needs its external children's interface values");
+    int e = 0;
+    for (const Link& L : node_[T.root].kids)  // children in other parts: their solved copies' edges
+        if (L.child < 0) edge_axpy(fields[T.root], T.root, L.loc, -1.0, child_edges[e++], s);
     node_solve(T.root, fields[T.root], s, info);
+    e = 0;
+    for (const Link& L : node_[T.root].kids)
+        if (L.child < 0 && edges_out)
+        {
+            const Domain& R = dom_[T.root];
+            k_edge_gather<double><<<grid_for(L.cn, 128), 128, 0, s>>>(edges_out[e++], fields[T.root], R.nx, R.ny, L.loc);
+            FPB_CHECK_LAUNCH();
+        }
     for (size_t l = 1; l < T.levels.size(); ++l)
     {
         for (int d : T.levels[l]) bond(fields[d], d, T.parent[d].first, fields[T.parent[d].second], T.parent[d].second);
@@ -985,6 +1028,127 @@ double Composite::residual_norm(const double* const* u, const double* const* rhs
         fn += hs[2 * d + 1];
     }
     return fn > 0 ? std::sqrt(rn / fn) : std::sqrt(rn);
+}
+
+namespace
+{
+// field.edge(loc)[k] += a * v[k]  (field2::bond_add with a neighbour's edge given as a vector)
+__global__ void k_edge_axpy(double* __restrict__ field, int nx, int ny, int loc, double a, const double* __restrict__ v)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= edge_length(loc, nx, ny)) return;
+    field[edge_index(loc, nx, ny, k)] += a * v[k];
+}
+}  // namespace
+
+void Composite::edge_axpy(double* field, int d, int loc, double a, const double* v, cudaStream_t s)
+{
+    const Domain& D = dom_[d];
+    k_edge_axpy<<<grid_for(edge_length(loc, D.nx, D.ny), 128), 128, 0, s>>>(field, D.nx, D.ny, loc, a, v);
+    FPB_CHECK_LAUNCH();
+}
+
+void Composite::set_external_schur(int k, const double* S_dev)
+{
+    int e = 0;
+    for (Link& L : node_[tree_.root].kids)
+        if (L.child < 0 && e++ == k)
+        {
+            L.S.alloc((size_t)L.cn * L.cn * sizeof(double));
+            FPB_CUDA(cudaMemcpy(L.S.get(), S_dev, L.S.bytes(), cudaMemcpyDeviceToDevice));
+            built_ = false;  // the root's interface inverse is built again with it
+            return;
+        }
+    throw Error(1, "no external child " + std::to_string(k));
+}
+
+void Composite::part_schur(int face, double* S_dev, cudaStream_t s)
+{
+    ensure_built();
+    const int     r = tree_.root;
+    const Domain& R = dom_[r];
+    if (face < 0 || face > 3 || R.bc[face] != BC_ADJACENTED)
+        throw Error(1, "the part's face toward its parent must be an Adjacented face of its root");
+    for (const auto& k : tree_.children[r])
+        if (k.first == face) throw Error(1, "the part's face toward its parent is connected inside the part");
+    Link L;
+    L.child = r;
+    L.loc   = face ^ 1;  // the parent's face toward this part
+    L.cn    = edge_length(face, R.nx, R.ny);
+    link_schur(L, s);
+    FPB_CUDA(cudaMemcpyAsync(S_dev, L.S.get(), L.S.bytes(), cudaMemcpyDeviceToDevice, s));
+    FPB_CUDA(cudaStreamSynchronize(s));
+}
+
+void Composite::part_upward(double* const* fields, const double* const* ghosts, int face, double* edge_out,
+                            cudaStream_t s, GmresInfo* info)
+{
+    ensure_built();
+    mixed_ = false;
+    assemble(fields, ghosts, s);
+    auto bond = [&](double* dst, int dd, int loc, const double* src, int sd) {
+        const Domain &A = dom_[dd], &B = dom_[sd];
+        k_bond_add<double><<<grid_for(edge_length(loc, A.nx, A.ny), 128), 128, 0, s>>>(dst, A.nx, A.ny, loc, -1.0, src,
+                                                                                     B.nx, B.ny);
+        FPB_CHECK_LAUNCH();
+    };
+    const auto& T = tree_;
+    for (int l = (int)T.levels.size() - 1; l >= 1; --l)
+    {
+        for (int d : T.levels[l])
+        {
+            double* td = temp_[d].as<double>();
+            FPB_CUDA(cudaMemcpyAsync(td, fields[d], dom_[d].cells() * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            for (auto& c : T.children[d])
+            {
+                bond(td, d, c.first, temp_[c.second].as<double>(), c.second);
+                bond(fields[d], d, c.first, temp_[c.second].as<double>(), c.second);
+            }
+        }
+        for (int d : T.levels[l]) node_solve(d, temp_[d].as<double>(), s, nullptr);
+    }
+    // the part's root is a non-root domain of the undivided tree: its solved copy goes to the parent
+    const int r = T.root;
+    if (!temp_[r].get()) temp_[r].alloc(dom_[r].cells() * sizeof(double));
+    double* tr = temp_[r].as<double>();
+    FPB_CUDA(cudaMemcpyAsync(tr, fields[r], dom_[r].cells() * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    for (auto& c : T.children[r])
+    {
+        bond(tr, r, c.first, temp_[c.second].as<double>(), c.second);
+        bond(fields[r], r, c.first, temp_[c.second].as<double>(), c.second);
+    }
+    node_solve(r, tr, s, info);
+    const Domain& R = dom_[r];
+    k_edge_gather<double><<<grid_for(edge_length(face, R.nx, R.ny), 128), 128, 0, s>>>(edge_out, tr, R.nx, R.ny, face);
+    FPB_CHECK_LAUNCH();
+}
+
+void Composite::part_downward(double* const* fields, int face, const double* parent_edge, cudaStream_t s,
+                              GmresInfo* info)
+{
+    const auto& T = tree_;
+    const int   r = T.root;
+    edge_axpy(fields[r], r, face, -1.0, parent_edge, s);
+    node_solve(r, fields[r], s, info);
+    for (size_t l = 1; l < T.levels.size(); ++l)
+    {
+        for (int d : T.levels[l])
+        {
+            const Domain &A = dom_[d], &B = dom_[T.parent[d].second];
+            k_bond_add<double><<<grid_for(edge_length(T.parent[d].first, A.nx, A.ny), 128), 128, 0, s>>>(
+                fields[d], A.nx, A.ny, T.parent[d].first, -1.0, fields[T.parent[d].second], B.nx, B.ny);
+            FPB_CHECK_LAUNCH();
+        }
+        for (int d : T.levels[l]) node_solve(d, fields[d], s, nullptr);
+    }
+}
+
+void Composite::root_solve(double* const* fields, const double* const* ghosts, const double* const* child_edges,
+                           double* const* edges_out, cudaStream_t s, GmresInfo* info)
+{
+    mixed_ = false;
+    assemble(fields, ghosts, s);
+    eliminate(fields, s, info, child_edges, edges_out);
 }
 
 }  // namespace fpb

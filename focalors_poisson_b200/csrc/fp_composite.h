@@ -53,8 +53,11 @@ class Composite
 public:
     // interface_inverse: build the inverse of each node's dense interface operator I - P A^-1 S at
     // creation and use it to precondition the interface GMRES (interface mode, n_if <= kMaxInverse).
+    // ext: children of the root that live in other parts of a subtree decomposition, as (root face, its
+    // interface length); their Schur matrices arrive through set_external_schur before the first solve.
     Composite(const std::vector<Domain>& doms, const std::vector<std::array<int, 3>>& conns, int root, int m,
-              double tol, int max_iter, int mode, bool interface_inverse = true);
+              double tol, int max_iter, int mode, bool interface_inverse = true,
+              const std::vector<std::array<int, 2>>& ext = {});
     static constexpr int kMaxInverse = 16384;
     ~Composite();
     void set_parameter(int m, double tol, int max_iter);
@@ -81,6 +84,29 @@ public:
 
     const Tree&                tree() const { return tree_; }
     const std::vector<Domain>& domains() const { return dom_; }
+    // Builds the Schur matrices and interface inverses now rather than on the first solve that needs them.
+    void prepare() { ensure_built(); }
+
+    // Subtree decomposition: the composite solve split into parts solved on different GPUs. The root part
+    // holds the root domain with its children outside (ext at construction); a subtree part holds the subtree
+    // of one child of the root, whose face toward the root is an Adjacented face of the part's geometry. The
+    // parts exchange one interface vector each way per solve; the results equal the undivided solve's.
+    //   part_schur:    the Schur matrix of this part's root toward its parent across `face` (a face of the
+    //                  part's root), cn x cn on the device, as the undivided solver builds it
+    //   part_upward:   assembly, hx^2 scaling and the upward pass including the part's root; edge_out gets
+    //                  the solved copy's values along `face` (for the parent's right-hand side)
+    //   part_downward: the part root's field loses parent_edge along `face`, then the root solve and the
+    //                  downward pass
+    //   root_solve:    assembly, scaling, child_edges[k] subtracted along external child k's face, the root
+    //                  solve (GMRES with the external Schur matrices), edges_out[k] = the solution along face k
+    void set_external_schur(int k, const double* S_dev);
+    void part_schur(int face, double* S_dev, cudaStream_t s);
+    void part_upward(double* const* fields, const double* const* ghosts, int face, double* edge_out, cudaStream_t s,
+                     GmresInfo* info);
+    void part_downward(double* const* fields, int face, const double* parent_edge, cudaStream_t s, GmresInfo* info);
+    void root_solve(double* const* fields, const double* const* ghosts, const double* const* child_edges,
+                    double* const* edges_out, cudaStream_t s, GmresInfo* info);
+    int  external_children() const { return n_ext_; }
 
 private:
     struct Link
@@ -99,11 +125,14 @@ private:
     };
 
     void build_schur();
+    void link_schur(Link& L, cudaStream_t s);
     bool schur_by_spectral(Link& L, cudaStream_t s);
+    void edge_axpy(double* field, int d, int loc, double a, const double* v, cudaStream_t s);
     void ensure_built();
     bool built_ = false;
     void assemble(double* const* fields, const double* const* ghosts, cudaStream_t s);
-    void eliminate(double* const* fields, cudaStream_t s, GmresInfo* info);
+    void eliminate(double* const* fields, cudaStream_t s, GmresInfo* info, const double* const* child_edges = nullptr,
+                   double* const* edges_out = nullptr);
     void rect_solve(int d, double* f, long long batch, cudaStream_t s) const;
     void residual_into(double* const* r, const double* const* fs, const double* const* u, cudaStream_t s);
     void ensure_ir_workspace();
@@ -129,6 +158,7 @@ private:
     DevBuf                                       sums_;    // per-domain reduction results
     bool                                         mixed_ = false;  // inner solve of iterative refinement
     DevBuf                                       red_;     // reduction scratch: partials + ticket + results
+    int                                          n_ext_ = 0;  // external children of the root (subtree parts)
 };
 
 }  // namespace fpb

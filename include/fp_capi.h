@@ -212,6 +212,38 @@ int fp_composite_solve_async(fp_composite* c, const double* const* rhs, double* 
  * change (and GMRES figures on the Schur path). FP_CHECK_CONVERGENCE in flags as for the solves; FP_ERR_NAN if
  * any queued refinement met a non-finite value. Returns FP_OK at once when nothing is queued. */
 int fp_composite_wait(fp_composite* c, int flags, fp_solve_info* info);
+/* Subtree decomposition over GPUs (one process per GPU; the analogue of the reference's MPI decomposition of
+ * the composite solve, pe/concat/concat_solver2d_slab_x.cpp, for a tree): the root domain is one part, and each
+ * subtree under a child of the root is a part of its own, solved by the same algorithm as
+ * ConcatPoissonSolver2D::solve (concat_solver2d.cpp:101-157) split at the root's faces. Per solve every subtree
+ * part sends the root one interface vector (its solved copy along the shared face) and receives one back (the
+ * root's solution along that face); the root part's GMRES needs the children's Schur matrices only, which the
+ * subtree parts compute once (fp_composite_part_schur) and the root part receives at set-up. The results are
+ * those of the undivided Schur GMRES solve (FP_NO_SPECTRAL). Device pointers only; all parts use the same
+ * m, tol, max_iter.
+ *   fp_composite_part_create: a subtree part is the subtree's geometry with its root's face toward the root
+ *     domain marked Adjacented (3) and n_ext = 0; the root part is the root domain alone (root = 0) with its
+ *     n_ext children in other parts given by the root's faces, in increasing face order. */
+int fp_composite_part_create(const fp_geometry* g, int m, double tol, int max_iter, int flags, int n_ext,
+                             const int* ext_faces, fp_composite** out);
+/* Subtree part: S (cn x cn device doubles, cn = the face's length) = the Schur matrix of the part's root toward
+ * the root domain across `face` (SchurMat2D_*::construct, schur_mat2d.cpp:5-106). */
+int fp_composite_part_schur(fp_composite* c, int face, double* S, void* stream);
+/* Root part: the Schur matrix of external child k (index in face order). */
+int fp_composite_set_external_schur(fp_composite* c, int k, const double* S);
+/* Subtree part, first half of a solve: boundary assembly, hx^2 scaling, the upward pass including the part's
+ * root; edge_out (cn doubles) = the part root's solved copy along `face`. */
+int fp_composite_part_upward(fp_composite* c, double* const* fields, const double* const* ghosts, int face,
+                             double* edge_out, void* stream, fp_solve_info* info);
+/* Subtree part, second half: the part root's field loses parent_edge (the root domain's solution along the
+ * shared face) along `face`, then the part root's solve and the downward pass. */
+int fp_composite_part_downward(fp_composite* c, double* const* fields, int face, const double* parent_edge,
+                               void* stream, fp_solve_info* info);
+/* Root part: assembly, scaling, child_edges[k] subtracted along external child k's face, the root's GMRES solve;
+ * edges_out[k] = the root's solution along child k's face (for that child's part_downward). */
+int fp_composite_root_solve(fp_composite* c, double* const* fields, const double* const* ghosts,
+                            const double* const* child_edges, double* const* edges_out, void* stream,
+                            fp_solve_info* info);
 /* Relative residual |fs - A u| / |fs| of a candidate solution u of the composite problem with right-hand
  * side `rhs` and ghost buffers `ghosts` (fs = their assembled, hx^2-scaled form, the right-hand side
  * ConcatPoissonSolver2D::solve works on; A = its composite 5-point operator). No counterpart in the
