@@ -838,6 +838,67 @@ __global__ void __launch_bounds__(256) k_ir_check(const double* __restrict__ par
 }
 
 
+// DST-I of a few rows of one length n as a dense product with the transform's matrix T (n x n, symmetric,
+// T[k][i] = sqrt(2/(n+1)) sin(pi (k+1)(i+1) / (n+1)), the columns the FFT plan produces): one CTA of
+// kEdgeMvThreads per output index k reads T's row k once for all the record's rows (four loads in flight per
+// thread), then a block reduction. For the handful of interface vectors of a single problem this streams T
+// once through the whole GPU where the FFT form runs one CTA per row, latency-bound.
+constexpr int kEdgeMvRows    = 8;
+constexpr int kEdgeMvThreads = 128;
+struct EdgeMv
+{
+    const double* T;
+    int           n, rows;
+    const double* in[kEdgeMvRows];
+    double*       out[kEdgeMvRows];
+};
+__global__ void __launch_bounds__(kEdgeMvThreads) k_edge_dst_mv(const EdgeMv* __restrict__ recs,
+                                                                const long long* __restrict__ prefix, int nrec)
+{
+    __shared__ double sh[kEdgeMvRows][kEdgeMvThreads / 32];
+    const int     s  = seg_of(prefix, nrec, blockIdx.x);
+    const EdgeMv& r  = recs[s];
+    const int     k  = (int)(blockIdx.x - prefix[s]);
+    const double* Tk = r.T + (long long)k * r.n;
+    double        acc[kEdgeMvRows];
+#pragma unroll
+    for (int q = 0; q < kEdgeMvRows; ++q) acc[q] = 0.0;
+    for (int i0 = threadIdx.x; i0 < r.n; i0 += 4 * kEdgeMvThreads)
+    {
+        double t[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+        {
+            const int i = i0 + u * kEdgeMvThreads;
+            t[u]        = i < r.n ? __ldg(Tk + i) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < kEdgeMvRows; ++q)
+            if (q < r.rows)
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                {
+                    const int i = i0 + u * kEdgeMvThreads;
+                    if (i < r.n) acc[q] += t[u] * r.in[q][i];
+                }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < kEdgeMvRows; ++q)
+    {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[q][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < r.rows)
+    {
+        double v = 0.0;
+        for (int w = 0; w < kEdgeMvThreads / 32; ++w) v += sh[threadIdx.x][w];
+        r.out[threadIdx.x][k] = v;
+    }
+}
+
 }  // namespace fpb
 
 // =============================================================================================
@@ -1067,6 +1128,8 @@ private:
     void   chase_run(const Segments& lc, const Segments& red, cudaStream_t s);
     void   inner(const XList& dst_in, const XList& dst_out, bool acc, cudaStream_t s);
     const double* basis_col(int kind, int n, int j);
+    bool   build_edge_mv(const std::vector<DstSeg>& segs, const std::vector<int>& ns, Segments& out);
+    void   edge_mv(const Segments& l, cudaStream_t s);
     void   set_user_lists(double* const* fields, const double* const* ghosts, int steps);
     ResSeg res_seg(size_t g, double* r, const double* fs, const double* const* u_user);
     void   run(int steps, cudaStream_t s);
@@ -1091,6 +1154,9 @@ private:
     Segments                                  l1_lc_, l1_red_, r1_lc_, r1_red_, a2_lc_, a2_red_;
     Segments                                  leaf_rows_, leaf_cols_, root_rows_, root_cols_;
     Segments                                  edst_g_, edst_out_;         // FP64 edge DSTs
+    Segments                                  edge_mv_g_, edge_mv_o_;     // the same as dense products
+    bool                                      mv_g_ = false, mv_o_ = false;
+    std::map<int, DevBuf>                     edge_tab_;                  // DST-I matrices by length
     Segments                                  ifk_, ifym_, ifrow_, ifkw_;  // interface work lists
     Segments                                  ifyyp_, ifyxp_;              // partial-product blocks
     std::vector<DstSeg>                       dst_W_in_rec_, dst_X_out_rec_;
@@ -1497,6 +1563,62 @@ template <typename TS> void BatchImpl<TS>::build_spectral()
 // Column j of the forward y-transform matrix of `kind` at length n (every family is orthonormal with the
 // transpose as inverse, so this is also row j of the inverse): the FP64 transform of the unit vector e_j.
 // Null for DD, whose basis dst_basis() evaluates directly.
+// The edge DSTs of one list as dense products (k_edge_dst_mv) when the matrices they read are small: the rows of
+// each length grouped kEdgeMvRows at a time, every group reading its n x n matrix once. Returns false (the FFT
+// form stays) when the matrices' reads would pass 64 MB, as for the many lengths of a large batch.
+template <typename TS>
+bool BatchImpl<TS>::build_edge_mv(const std::vector<DstSeg>& segs, const std::vector<int>& ns, Segments& out)
+{
+    std::map<int, std::vector<size_t>> by_n;
+    for (size_t q = 0; q < segs.size(); ++q) by_n[ns[q]].push_back(q);
+    long long bytes = 0;
+    for (auto& kv : by_n)
+        bytes += (long long)((kv.second.size() + kEdgeMvRows - 1) / kEdgeMvRows) * kv.first * kv.first * 8;
+    if (segs.empty() || bytes > (64LL << 20)) return false;
+    std::vector<EdgeMv>    recs;
+    std::vector<long long> counts;
+    const long double      pi = 3.141592653589793238462643383279502884L;
+    for (auto& kv : by_n)
+    {
+        const int n = kv.first;
+        if (!edge_tab_.count(n))
+        {
+            const double        sc = std::sqrt(2.0 / (n + 1));
+            std::vector<double> T((size_t)n * n);
+            for (int k = 0; k < n; ++k)
+                for (int i = 0; i < n; ++i)
+                {
+                    const long long q = (long long)(k + 1) * (i + 1) % (2LL * (n + 1));
+                    T[(size_t)k * n + i] = sc * (double)std::sin(pi * (long double)q / (long double)(n + 1));
+                }
+            edge_tab_[n] = upload(T);
+        }
+        for (size_t a = 0; a < kv.second.size(); a += kEdgeMvRows)
+        {
+            EdgeMv r{};
+            r.T = edge_tab_[n].template as<double>();
+            r.n = n;
+            for (size_t b = a; b < kv.second.size() && b < a + kEdgeMvRows; ++b)
+            {
+                const DstSeg& d   = segs[kv.second[b]];
+                r.in[r.rows]      = static_cast<const double*>(d.in);
+                r.out[r.rows]     = static_cast<double*>(d.out);
+                ++r.rows;
+            }
+            recs.push_back(r);
+            counts.push_back(n);
+        }
+    }
+    out.set(recs, counts);
+    return true;
+}
+
+template <typename TS> void BatchImpl<TS>::edge_mv(const Segments& l, cudaStream_t s)
+{
+    k_edge_dst_mv<<<(unsigned)l.total, kEdgeMvThreads, 0, s>>>(l.as<EdgeMv>(), l.pre(), l.n);
+    FPB_CHECK_LAUNCH();
+}
+
 template <typename TS> const double* BatchImpl<TS>::basis_col(int kind, int n, int j)
 {
     auto key = std::make_tuple(kind, n, j);
@@ -1559,6 +1681,7 @@ template <typename TS> void BatchImpl<TS>::build_static_lists()
     std::vector<RowReq<TS>>   lr, rr;
     std::vector<ColReq<TS>>   lc, rc;
     std::vector<DstSeg>       eg, eo;
+    std::vector<int>          eg_n, eo_n;  // their row lengths
     std::vector<BIface>       fk, fy, fr, fw;
     std::vector<long long>    ck, cy, cr, cw, lrc, rrc, lcc, rcc;
     for (int p = 0; p < nP; ++p)
@@ -1593,6 +1716,9 @@ template <typename TS> void BatchImpl<TS>::build_static_lists()
             eg.push_back({ev(p, Y, 1), F.gY + Y * F.nx, 1, eplans_.get(K_DD, F.nx)});
             eo.push_back({F.sY + Y * F.nx, ev(p, Y, 2), 1, eplans_.get(K_DD, F.nx)});
             eo.push_back({F.yY + Y * F.nx, ev(p, Y, 3), 1, eplans_.get(K_DD, F.nx)});
+            eg_n.push_back(F.nx);
+            eo_n.push_back(F.nx);
+            eo_n.push_back(F.nx);
             ChaseSeg<TS> c = base_seg(g, W + L.off, X + L.off);
             c.ncol         = 1;
             c.col_j[0]     = jl;
@@ -1657,6 +1783,8 @@ template <typename TS> void BatchImpl<TS>::build_static_lists()
     std::vector<long long> one_e(eg.size(), 1), one_o(eo.size(), 1);
     edst_g_.set(eg, one_e);
     edst_out_.set(eo, one_o);
+    mv_g_ = build_edge_mv(eg, eg_n, edge_mv_g_);
+    mv_o_ = build_edge_mv(eo, eo_n, edge_mv_o_);
     {
         std::vector<BIface>    py, px;
         std::vector<long long> cy2, cx2;
@@ -1750,7 +1878,8 @@ template <typename TS> void BatchImpl<TS>::inner(const XList& dst_in, const XLis
                                                                          root_cols_.pre(), root_cols_.n);
         FPB_CHECK_LAUNCH();
     }
-    launch_x1<double, K_DD, 0, double, double, false>(edst_g_, eplans_, tm_, s);
+    if (mv_g_) edge_mv(edge_mv_g_, s);
+    else launch_x1<double, K_DD, 0, double, double, false>(edst_g_, eplans_, tm_, s);
     if (ifk_.n)
     {
         k_if_zx<<<grid_of(ifk_.total, 128), 128, 0, s>>>(ifk_.as<BIface>(), ifk_.pre(), ifk_.n);
@@ -1778,7 +1907,8 @@ template <typename TS> void BatchImpl<TS>::inner(const XList& dst_in, const XLis
         k_if_yx<<<grid_of(ifkw_.total, 128), 128, 0, s>>>(ifkw_.as<BIface>(), ifkw_.pre(), ifkw_.n);
         FPB_CHECK_LAUNCH();
     }
-    launch_x1<double, K_DD, 0, double, double, false>(edst_out_, eplans_, tm_, s);
+    if (mv_o_) edge_mv(edge_mv_o_, s);
+    else launch_x1<double, K_DD, 0, double, double, false>(edst_out_, eplans_, tm_, s);
     chase_run(a2_lc_, a2_red_, s);
     if (acc) launch_x<TS, TS, double, true>(dst_out, true, plans_, tm_, s);
     else launch_x<TS, TS, double, false>(dst_out, true, plans_, tm_, s);

@@ -196,6 +196,14 @@ bool register_engine_allowed()
     return !(e && std::string(e) == "stage");
 }
 
+// FP_FFT_ENGINE=register: the register engine takes every Bluestein length it can hold, also where its power
+// of two is longer than the stage engine's choice
+bool register_engine_preferred()
+{
+    const char* e = std::getenv("FP_FFT_ENGINE");
+    return e && std::string(e) == "register";
+}
+
 // The stage engine's Bluestein length for a convolution of at least `need` points: the 7-smooth length in
 // [need, 1.5 need] with the smallest estimated cost (-1 if none).
 int stage_bluestein_length(int need)
@@ -251,7 +259,7 @@ bool plan_register(int L, size_t elem_bytes, size_t smem_limit, const FftWindow&
         // a power of two longer than the stage engine's own choice (ND / DN windows need 3n - 1: 6144 against
         // 8192 at n = 2048) costs more than the register engine saves
         const int stage_M = stage_bluestein_length(need);
-        if (stage_M > 0 && M > stage_M) return false;
+        if (stage_M > 0 && M > stage_M && !register_engine_preferred()) return false;
     }
     if (M > max_M) return false;
     const size_t elems = (size_t)reg_buf_elems(M) + M / 16 + (pow2 ? 0 : reg_chirp_entries(L));
