@@ -11,6 +11,7 @@
 #include "fp_batch.h"
 #include "fp_composite.h"
 #include "fp_ops.cuh"
+#include "fp_gmres.cuh"
 
 #include <cublas_v2.h>
 
@@ -30,15 +31,6 @@ inline unsigned grid_for(long long n, int block, int cap = 4096)
     return (unsigned)std::max(1LL, std::min<long long>(g, cap));
 }
 
-struct PinnedHost
-{
-    double* p = nullptr;
-    explicit PinnedHost(size_t n) { FPB_CUDA(cudaMallocHost(&p, n * sizeof(double))); }
-    ~PinnedHost()
-    {
-        if (p) cudaFreeHost(p);
-    }
-};
 }  // namespace
 
 Tree build_tree(int nd, const std::vector<std::array<int, 3>>& conns, int root, int faces)
@@ -220,7 +212,11 @@ void Composite::ensure_built()
     built_ = true;
 }
 
-Composite::~Composite() = default;
+Composite::~Composite()
+{
+    drop_gmres_graphs();
+    if (gm_host_) cudaFreeHost(gm_host_);
+}
 
 void Composite::set_parameter(int m, double tol, int max_iter)
 {
@@ -229,6 +225,8 @@ void Composite::set_parameter(int m, double tol, int max_iter)
     m_                 = m;
     tol_               = tol;
     max_iter_          = max_iter;
+    gm_graph_.resize(node_.size(), nullptr);
+    drop_gmres_graphs();  // they hold the buffers below and the parameters
     for (auto& nd : node_)
     {
         if (nd.kids.empty()) continue;
@@ -338,9 +336,7 @@ void Composite::node_solve(int d, double* f, cudaStream_t s, GmresInfo* info)
     }
     const Domain& D = dom_[d];
     const long long n = N.n;
-    const int       m = m_;
-    double *V = N.V.as<double>(), *w = N.w.as<double>(), *r = N.r.as<double>(), *x = N.x.as<double>(),
-           *b = N.b.as<double>(), *hcol = N.hcol.as<double>(), *ydev = N.tmp.as<double>();
+    double *        x = N.x.as<double>(), *b = N.b.as<double>();
 
     rect_[d]->solve(f, 1, s);  // b <- A^-1 b (gmres_solver2d.cpp:130)
     if (mode_ == GMRES_FULLFIELD)
@@ -355,113 +351,16 @@ void Composite::node_solve(int d, double* f, cudaStream_t s, GmresInfo* info)
 
     if (N.has_inv && refine_with_inverse(d, f, s, info)) return;
 
-    thread_local std::unique_ptr<PinnedHost> host;
-    if (!host || !host->p) host.reset(new PinnedHost(512));
-    double*             hbuf = host->p;
-    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
-    bool                converged = false;
-    double              last_res  = 0;
-    int                 iters = 0, restarts = 0;
-
-    for (int outer = 0; outer < max_iter_; outer++)
-    {
-        afun(d, x, w, s);
-        k_sub<<<grid_for(n, 256), 256, 0, s>>>(r, b, w, n);
-        FPB_CHECK_LAUNCH();
-        dot(r, r, n, true, s, hcol + m + 1);
-        // Convergence is decided on the reference's full-field residual (gmres_solver2d.cpp:149-160). In
-        // interface mode the iterate is x(y) = A^-1 b + A^-1 S y, whose full-field residual is
-        // A^-1 S rho(y) for the interface residual rho: one more rectangle solve per restart.
-        if (mode_ == GMRES_INTERFACE)
-        {
-            double* R = N.R.as<double>();
-            FPB_CUDA(cudaMemsetAsync(R, 0, D.cells() * sizeof(double), s));
-            schur_apply_into(d, r, false, R, s);
-            rect_[d]->solve(R, 1, s);
-            dot(R, R, D.cells(), true, s, hcol + m);
-        }
-        FPB_CUDA(cudaMemcpyAsync(hbuf, hcol + m, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-        FPB_CUDA(cudaStreamSynchronize(s));
-        const double rho  = hbuf[1];
-        const double beta = (mode_ == GMRES_INTERFACE) ? hbuf[0] : rho;
-        last_res          = beta;
-        if (!std::isfinite(beta) || !std::isfinite(rho)) throw Error(5, "non-finite GMRES residual");
-        if (beta < tol_)
-        {
-            converged = true;
-            break;
-        }
-        // Arnoldi stops on the interface estimate |g_{j+1}|, scaled by the measured ratio of the two norms.
-        const double inner_tol = (mode_ == GMRES_INTERFACE && beta > 0) ? 0.5 * tol_ * (rho / beta) : tol_;
-        restarts++;
-        std::fill(H.begin(), H.end(), 0.0);
-        std::fill(cs.begin(), cs.end(), 0.0);
-        std::fill(sn.begin(), sn.end(), 0.0);
-        std::fill(g.begin(), g.end(), 0.0);
-        k_scale_inv<<<grid_for(n, 256), 256, 0, s>>>(V, r, n, hcol + m + 1);  // V0 = r / ||r||
-        FPB_CHECK_LAUNCH();
-        g[0] = rho;
-        int j = 0;
-        for (; j < m; j++)
-        {
-            double* Vj = V + (size_t)j * n;
-            afun(d, Vj, w, s);
-            for (int i = 0; i <= j; i++)  // modified Gram-Schmidt (gmres_solver2d.cpp:183-187)
-            {
-                const double* Vi = V + (size_t)i * n;
-                dot(Vi, w, n, false, s, hcol + i);
-                k_axpy_dev<<<grid_for(n, 256), 256, 0, s>>>(w, Vi, n, hcol + i, -1.0);
-                FPB_CHECK_LAUNCH();
-            }
-            dot(w, w, n, true, s, hcol + j + 1);
-            FPB_CUDA(cudaMemcpyAsync(hbuf, hcol, (j + 2) * sizeof(double), cudaMemcpyDeviceToHost, s));
-            FPB_CUDA(cudaStreamSynchronize(s));
-            for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = hbuf[i];
-            const double h_j1j = hbuf[j + 1];
-            if (!std::isfinite(h_j1j)) throw Error(5, "non-finite GMRES Arnoldi value");
-            iters++;
-            if (h_j1j < 1e-12) break;
-            H[(size_t)(j + 1) * m + j] = h_j1j;
-            k_scale_inv<<<grid_for(n, 256), 256, 0, s>>>(V + (size_t)(j + 1) * n, w, n, hcol + j + 1);
-            FPB_CHECK_LAUNCH();
-            for (int i = 0; i < j; i++)
-            {
-                const double temp          = cs[i] * H[(size_t)i * m + j] + sn[i] * H[(size_t)(i + 1) * m + j];
-                H[(size_t)(i + 1) * m + j] = -sn[i] * H[(size_t)i * m + j] + cs[i] * H[(size_t)(i + 1) * m + j];
-                H[(size_t)i * m + j]       = temp;
-            }
-            const double hjj   = H[(size_t)j * m + j];
-            const double hj1   = H[(size_t)(j + 1) * m + j];
-            const double denom = std::hypot(hjj, hj1);
-            cs[j]              = hjj / denom;
-            sn[j]              = hj1 / denom;
-            H[(size_t)j * m + j]       = cs[j] * H[(size_t)j * m + j] + sn[j] * H[(size_t)(j + 1) * m + j];
-            H[(size_t)(j + 1) * m + j] = 0.0;
-            const double temp          = cs[j] * g[j];
-            g[j + 1]                   = -sn[j] * g[j];
-            g[j]                       = temp;
-            if (std::fabs(g[j + 1]) < inner_tol)
-            {
-                j++;
-                break;
-            }
-        }
-        std::fill(y.begin(), y.end(), 0.0);
-        for (int i = j - 1; i >= 0; i--)
-        {
-            y[i] = g[i];
-            for (int k = i + 1; k < j; k++) y[i] -= H[(size_t)i * m + k] * y[k];
-            y[i] /= H[(size_t)i * m + i];
-        }
-        if (j > 0)
-        {
-            for (int i = 0; i < j; ++i) hbuf[i] = y[i];
-            FPB_CUDA(cudaMemcpyAsync(ydev, hbuf, j * sizeof(double), cudaMemcpyHostToDevice, s));
-            k_multi_axpy<<<grid_for(n, 256), 256, 0, s>>>(x, V, n, n, ydev, j);
-            FPB_CHECK_LAUNCH();
-            FPB_CUDA(cudaStreamSynchronize(s));  // hbuf is reused next iteration
-        }
-    }
+    // the restart loop (gmres_solver2d.cpp:139-249) as one CUDA graph over the node's buffers (fp_gmres.cuh)
+    if (!gm_graph_[d]) build_gmres_graph(d, s);
+    FPB_CUDA(cudaGraphLaunch(gm_graph_[d], s));
+    FPB_CUDA(cudaMemcpyAsync(gm_host_, N.st.get(), sizeof(GmState), cudaMemcpyDeviceToHost, s));
+    FPB_CUDA(cudaStreamSynchronize(s));
+    const GmState gs = *gm_host_;
+    if (gs.err) throw Error(5, "non-finite GMRES value");
+    const bool   converged = gs.converged != 0;
+    const double last_res  = gs.beta;
+    const int    iters = gs.iters, restarts = gs.restarts;
     if (mode_ == GMRES_FULLFIELD)
     {
         FPB_CUDA(cudaMemcpyAsync(f, x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -482,6 +381,63 @@ void Composite::node_solve(int d, double* f, cudaStream_t s, GmresInfo* info)
         info->residual  = last_res;
         info->converged = info->converged && converged;
     }
+}
+
+void Composite::build_gmres_graph(int d, cudaStream_t s)
+{
+    Node&           N = node_[d];
+    const Domain&   D = dom_[d];
+    const long long n = N.n;
+    const int       m = m_;
+    N.vin.alloc(n * sizeof(double));
+    N.arr.alloc((size_t)((m + 1) * m + 3 * m + 1) * sizeof(double));
+    N.st.alloc(sizeof(GmState));
+    GmBuffers B;
+    B.V        = N.V.as<double>();
+    B.w        = N.w.as<double>();
+    B.r        = N.r.as<double>();
+    B.x        = N.x.as<double>();
+    B.b        = N.b.as<double>();
+    B.vin      = N.vin.as<double>();
+    B.st       = N.st.as<GmState>();
+    B.a.H      = N.arr.as<double>();
+    B.a.cs     = B.a.H + (size_t)(m + 1) * m;
+    B.a.sn     = B.a.cs + m;
+    B.a.g      = B.a.sn + m;
+    B.a.y      = B.a.g + (m + 1);
+    B.a.hcol   = N.hcol.as<double>();
+    B.partials = red_.as<double>();
+    B.ticket   = reinterpret_cast<unsigned*>(B.partials + kRedBlocks);
+    if (!gm_host_) FPB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&gm_host_), sizeof(GmState)));
+    // warm-up outside the capture: the rectangle solves' work buffers are allocated on first use
+    afun(d, B.x, B.w, s);
+    rect_[d]->solve(N.R.as<double>(), 1, s);
+    FPB_CUDA(cudaStreamSynchronize(s));
+    const bool iface = mode_ == GMRES_INTERFACE;
+    gm_graph_[d] = capture_gmres(
+        n, m, tol_, max_iter_, iface, B, [&](const double* in, double* out, cudaStream_t q) { afun(d, in, out, q); },
+        [&](cudaStream_t q) {
+            if (!iface) return;
+            // the reference's test is on the full-field residual A^-1 S rho(y) of the iterate (gmres_solver2d.cpp:149-160)
+            double* R = N.R.as<double>();
+            FPB_CUDA(cudaMemsetAsync(R, 0, D.cells() * sizeof(double), q));
+            schur_apply_into(d, B.r, false, R, q);
+            rect_[d]->solve(R, 1, q);
+            dot(R, R, D.cells(), true, q, B.a.hcol + m);
+        },
+        [&](const double* a, const double* b, long long len, bool sq, double* out, cudaStream_t q) {
+            dot(a, b, len, sq, q, out);
+        });
+}
+
+void Composite::drop_gmres_graphs()
+{
+    for (auto& g : gm_graph_)
+        if (g)
+        {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
 }
 
 namespace

@@ -19,6 +19,8 @@ struct Domain
     long long cells() const { return (long long)nx * ny; }
 };
 
+struct GmState;  // fp_gmres.cuh
+
 struct Tree
 {
     int                                   root = 0;
@@ -121,10 +123,13 @@ private:
         long long         n    = 0;  // Krylov vector length
         DevBuf            V, w, r, x, b, R, hcol, tmp;
         DevBuf            X, Z;  // interface inverse (n_if x n_if) and A^-1 S y workspace
+        DevBuf            vin, arr, st;  // device GMRES loop: step input, Hessenberg storage, state
         bool              has_inv = false;
     };
 
     void build_schur();
+    void build_gmres_graph(int d, cudaStream_t s);
+    void drop_gmres_graphs();
     void link_schur(Link& L, cudaStream_t s);
     bool schur_by_spectral(Link& L, cudaStream_t s);
     void edge_axpy(double* field, int d, int loc, double a, const double* v, cudaStream_t s);
@@ -159,6 +164,8 @@ private:
     bool                                         mixed_ = false;  // inner solve of iterative refinement
     DevBuf                                       red_;     // reduction scratch: partials + ticket + results
     int                                          n_ext_ = 0;  // external children of the root (subtree parts)
+    std::vector<cudaGraphExec_t>                 gm_graph_;   // per node: the GMRES loop (fp_gmres.cuh)
+    GmState*                                     gm_host_ = nullptr;  // pinned copy of a loop's outcome
 };
 
 }  // namespace fpb

@@ -14,6 +14,7 @@
 // index it: x faces (j, k), y faces (i, k), z faces (i, j), row-major.
 #include "../../include/fp_capi.h"
 #include "fp_composite.h"
+#include "fp_gmres.cuh"
 #include "fp_internal.h"
 #include "fp_ops.cuh"
 #include "fp_rect3d.h"
@@ -125,6 +126,21 @@ struct Node3
     std::vector<Child3> kids;
     DevBuf              V, w, r, x, ft, vec, prod;  // GMRES on full fields ((m + 1) x cells for V)
     DevBuf              hd;                         // H column, residual norm, y (m + 2 doubles)
+    DevBuf              b, vin;                     // the solve's A^-1 b and the Arnoldi step's input
+    DevBuf              arr, st;                    // GmArrays storage, GmState
+    cudaGraphExec_t     graph = nullptr;            // the GMRES loop (built on first use per parameters)
+    ~Node3()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+    }
+    Node3() = default;
+    Node3(Node3&& o) noexcept
+        : kids(std::move(o.kids)), V(std::move(o.V)), w(std::move(o.w)), r(std::move(o.r)), x(std::move(o.x)),
+          ft(std::move(o.ft)), vec(std::move(o.vec)), prod(std::move(o.prod)), hd(std::move(o.hd)), b(std::move(o.b)),
+          vin(std::move(o.vin)), arr(std::move(o.arr)), st(std::move(o.st)), graph(o.graph)
+    {
+        o.graph = nullptr;
+    }
 };
 
 }  // namespace
@@ -171,12 +187,12 @@ public:
         }
         red_.alloc((kRedBlocks + 8) * sizeof(double));
         FPB_CUDA(cudaMemset(red_.get(), 0, red_.bytes()));
-        FPB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&hbuf_), (size_t)(kMaxM + 2) * sizeof(double)));
+        FPB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&gmst_), sizeof(GmState)));
         set_parameter(m, tol, max_iter);
     }
     ~Composite3D()
     {
-        if (hbuf_) cudaFreeHost(hbuf_);
+        if (gmst_) cudaFreeHost(gmst_);
     }
 
     // ConcatPoissonSolver3D::set_parameter (concat_solver3d.cpp:5-18): the Schur matrices are built again
@@ -202,6 +218,11 @@ public:
             N.vec.ensure((size_t)cmax * sizeof(double));
             N.prod.ensure((size_t)cmax * sizeof(double));
             N.hd.ensure((size_t)(m_ + 2) * sizeof(double));
+            for (DevBuf* b : {&N.b, &N.vin}) b->ensure(cells * sizeof(double));
+            N.arr.ensure((size_t)((m_ + 1) * m_ + 3 * m_ + 1) * sizeof(double));
+            N.st.ensure(sizeof(GmState));
+            if (N.graph) cudaGraphExecDestroy(N.graph);
+            N.graph = nullptr;
         }
         build_schur();
         built_ = true;
@@ -368,110 +389,69 @@ private:
         FPB_CHECK_LAUNCH();
     }
 
-    // GMRESSolver3D::solve (gmres_solver3d.cpp:155-306) on the full field b, in place
-    void gmres(int d, double* b, cudaStream_t s, GmresInfo* info)
+    GmArrays arrays(int d)
+    {
+        Node3&   N = node_[d];
+        double*  p = N.arr.as<double>();
+        GmArrays a;
+        a.H    = p;
+        a.cs   = a.H + (size_t)(m_ + 1) * m_;
+        a.sn   = a.cs + m_;
+        a.g    = a.sn + m_;
+        a.y    = a.g + (m_ + 1);
+        a.hcol = N.hd.as<double>();
+        return a;
+    }
+
+    // The GMRES loop of box d as one graph (fp_gmres.cuh) on the node's fixed buffers (b, x, V, w, r, vin).
+    void build_gmres_graph(int d, cudaStream_t s)
     {
         Node3&          N = node_[d];
         const long long n = box_[d].cells();
-        const int       m = m_;
-        double *V = N.V.as<double>(), *w = N.w.as<double>(), *r = N.r.as<double>(), *x = N.x.as<double>();
-        double* hd = N.hd.as<double>();  // H column (j + 2 values) / y, and the residual norm at m + 1
-        rect_[d]->solve(b, 1, s);  // b <- A^-1 b
-        FPB_CUDA(cudaMemcpyAsync(x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-        std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
-        int                 iters = 0, restarts = 0;
-        double              beta  = 0;
-        bool                converged = false;
-        for (int outer = 0; outer < max_iter_; outer++)
-        {
-            afun(d, x, w, s);
-            k_sub<<<grid3(n, 256), 256, 0, s>>>(r, b, w, n);
-            FPB_CHECK_LAUNCH();
-            dot(r, r, n, true, hd + m + 1, s);
-            FPB_CUDA(cudaMemcpyAsync(hbuf_, hd + m + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
-            FPB_CUDA(cudaStreamSynchronize(s));
-            beta = hbuf_[0];
-            if (!std::isfinite(beta)) throw Error(FP_ERR_NAN, "non-finite GMRES residual");
-            if (beta < tol_)
-            {
-                converged = true;
-                break;
-            }
-            restarts++;
-            std::fill(H.begin(), H.end(), 0.0);
-            std::fill(cs.begin(), cs.end(), 0.0);
-            std::fill(sn.begin(), sn.end(), 0.0);
-            std::fill(g.begin(), g.end(), 0.0);
-            k_scale_inv<<<grid3(n, 256), 256, 0, s>>>(V, r, n, hd + m + 1);  // V0 = r / beta
-            FPB_CHECK_LAUNCH();
-            g[0]  = beta;
-            int j = 0;
-            for (; j < m; j++)
-            {
-                double* Vj = V + (size_t)j * n;
-                afun(d, Vj, w, s);
-                for (int i = 0; i <= j; i++)  // modified Gram-Schmidt (gmres_solver3d.cpp:221-233)
-                {
-                    const double* Vi = V + (size_t)i * n;
-                    dot(Vi, w, n, false, hd + i, s);
-                    k_axpy_dev<<<grid3(n, 256), 256, 0, s>>>(w, Vi, n, hd + i, -1.0);
-                    FPB_CHECK_LAUNCH();
-                }
-                dot(w, w, n, true, hd + j + 1, s);
-                FPB_CUDA(cudaMemcpyAsync(hbuf_, hd, (j + 2) * sizeof(double), cudaMemcpyDeviceToHost, s));
-                FPB_CUDA(cudaStreamSynchronize(s));
-                for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = hbuf_[i];
-                const double h_j1j = hbuf_[j + 1];
-                if (!std::isfinite(h_j1j)) throw Error(FP_ERR_NAN, "non-finite GMRES Arnoldi value");
-                iters++;
-                if (h_j1j < 1e-12) break;
-                H[(size_t)(j + 1) * m + j] = h_j1j;
-                k_scale_inv<<<grid3(n, 256), 256, 0, s>>>(V + (size_t)(j + 1) * n, w, n, hd + j + 1);
-                FPB_CHECK_LAUNCH();
-                for (int i = 0; i < j; i++)
-                {
-                    const double t             = cs[i] * H[(size_t)i * m + j] + sn[i] * H[(size_t)(i + 1) * m + j];
-                    H[(size_t)(i + 1) * m + j] = -sn[i] * H[(size_t)i * m + j] + cs[i] * H[(size_t)(i + 1) * m + j];
-                    H[(size_t)i * m + j]       = t;
-                }
-                const double hjj = H[(size_t)j * m + j], hj1 = H[(size_t)(j + 1) * m + j];
-                const double den = std::hypot(hjj, hj1);
-                cs[j]            = hjj / den;
-                sn[j]            = hj1 / den;
-                H[(size_t)j * m + j]       = cs[j] * H[(size_t)j * m + j] + sn[j] * H[(size_t)(j + 1) * m + j];
-                H[(size_t)(j + 1) * m + j] = 0.0;
-                const double t             = cs[j] * g[j];
-                g[j + 1]                   = -sn[j] * g[j];
-                g[j]                       = t;
-                if (std::fabs(g[j + 1]) < tol_)
-                {
-                    j++;
-                    break;
-                }
-            }
-            std::fill(y.begin(), y.end(), 0.0);
-            for (int i = j - 1; i >= 0; i--)
-            {
-                y[i] = g[i];
-                for (int k = i + 1; k < j; k++) y[i] -= H[(size_t)i * m + k] * y[k];
-                y[i] /= H[(size_t)i * m + i];
-            }
-            if (j > 0)
-            {
-                for (int i = 0; i < j; ++i) hbuf_[i] = y[i];
-                FPB_CUDA(cudaMemcpyAsync(hd, hbuf_, j * sizeof(double), cudaMemcpyHostToDevice, s));
-                k_multi_axpy<<<grid3(n, 256), 256, 0, s>>>(x, V, n, n, hd, j);
-                FPB_CHECK_LAUNCH();
-                FPB_CUDA(cudaStreamSynchronize(s));  // hbuf_ is reused next
-            }
-        }
-        FPB_CUDA(cudaMemcpyAsync(b, x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        GmBuffers       B;
+        B.V        = N.V.as<double>();
+        B.w        = N.w.as<double>();
+        B.r        = N.r.as<double>();
+        B.x        = N.x.as<double>();
+        B.b        = N.b.as<double>();
+        B.vin      = N.vin.as<double>();
+        B.st       = N.st.as<GmState>();
+        B.a        = arrays(d);
+        B.partials = red_.as<double>();
+        B.ticket   = reinterpret_cast<unsigned*>(B.partials + kRedBlocks);
+        // warm-up outside the capture: the rectangle solve's work buffers are allocated on first use
+        afun(d, B.x, B.w, s);
+        FPB_CUDA(cudaStreamSynchronize(s));
+        N.graph = capture_gmres(
+            n, m_, tol_, max_iter_, false, B, [&](const double* in, double* out, cudaStream_t q) { afun(d, in, out, q); },
+            [](cudaStream_t) {},
+            [&](const double* x, const double* y, long long len, bool sq, double* out, cudaStream_t q) {
+                dot(x, y, len, sq, out, q);
+            });
+    }
+
+    // GMRESSolver3D::solve (gmres_solver3d.cpp:155-306) on the full field f, in place: A^-1 f and the copies into
+    // the node's buffers on the stream, then the loop as one graph launch, one wait for its state
+    void gmres(int d, double* f, cudaStream_t s, GmresInfo* info)
+    {
+        Node3&          N = node_[d];
+        const long long n = box_[d].cells();
+        rect_[d]->solve(f, 1, s);  // b <- A^-1 b
+        FPB_CUDA(cudaMemcpyAsync(N.b.get(), f, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        FPB_CUDA(cudaMemcpyAsync(N.x.get(), f, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        if (!N.graph) build_gmres_graph(d, s);
+        FPB_CUDA(cudaGraphLaunch(N.graph, s));
+        FPB_CUDA(cudaMemcpyAsync(f, N.x.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        FPB_CUDA(cudaMemcpyAsync(gmst_, N.st.get(), sizeof(GmState), cudaMemcpyDeviceToHost, s));
+        FPB_CUDA(cudaStreamSynchronize(s));
+        const GmState st = *gmst_;
+        if (st.err) throw Error(FP_ERR_NAN, "non-finite GMRES value");
         if (info)
         {
-            info->iterations += iters;
-            info->restarts += restarts;
-            info->residual  = beta;
-            info->converged = info->converged && converged;
+            info->iterations += st.iters;
+            info->restarts += st.restarts;
+            info->residual  = st.beta;
+            info->converged = info->converged && st.converged;
         }
     }
 
@@ -481,7 +461,7 @@ private:
     std::vector<Node3>                      node_;
     std::vector<DevBuf>                     temp_;
     DevBuf                                  red_;
-    double*                                 hbuf_  = nullptr;
+    GmState*                                gmst_  = nullptr;  // pinned copy of a GMRES run's state
     int                                     m_     = 0;
     double                                  tol_   = 0;
     int                                     max_iter_ = 0;
