@@ -4,8 +4,8 @@ C++ drop-in interface of focalors_poisson_b200/cpp/ over it) in-tree.
     python -m focalors_poisson_b200.build [--cases <reference case dir>]
 
 Compiles every csrc/*.cu with nvcc for sm_100a (-gencode arch=compute_100a,code=sm_100a) into
-focalors_poisson_b200/_build/ and links focalors_poisson_b200/libfpb200.so; compiles cpp/fp_host.cpp with
-g++ into focalors_poisson_b200/libfocalors_b200.so. With --cases, also compiles the reference's own 2D
+focalors_poisson_b200/_build/ and links focalors_poisson_b200/libfpb200.so; compiles cpp/fp_host.cpp and
+cpp/fp_host3d.cpp with g++ into focalors_poisson_b200/libfocalors_b200.so. With --cases, also compiles the reference's own 2D
 validation drivers (poisson_solver_reference.cpp, concat_solver_reference.cpp), unchanged, against the
 drop-in headers into focalors_poisson_b200/_build/cases/. Rebuilds only what changed.
 """
@@ -90,12 +90,13 @@ def _run(cmd, what):
 
 
 def build_dropin(verbose: bool = False) -> str:
-    """libfocalors_b200.so: Geometry2D / Variable2D / PoissonSolver2D / ConcatPoissonSolver2D over libfpb200."""
+    """libfocalors_b200.so: Geometry2D / Variable2D / PoissonSolver2D / ConcatPoissonSolver2D and their 3D
+    counterparts over libfpb200."""
     build_library()
-    src = os.path.join(CPP, "fp_host.cpp")
-    deps = [src, LIB] + glob.glob(os.path.join(CPP, "**", "*.h*"), recursive=True)
+    srcs = [os.path.join(CPP, "fp_host.cpp"), os.path.join(CPP, "fp_host3d.cpp")]
+    deps = srcs + [LIB] + glob.glob(os.path.join(CPP, "**", "*.h*"), recursive=True)
     if not _newer(DROPIN_LIB, deps):
-        _run([gxx()] + GXX_FLAGS + ["-shared", src, "-o", DROPIN_LIB, "-L" + PKG, "-lfpb200",
+        _run([gxx()] + GXX_FLAGS + ["-shared"] + srcs + ["-o", DROPIN_LIB, "-L" + PKG, "-lfpb200",
                                     "-Wl,-rpath,$ORIGIN"], "g++ (libfocalors_b200.so)")
     if verbose:
         print(DROPIN_LIB)

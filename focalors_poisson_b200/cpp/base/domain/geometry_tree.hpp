@@ -76,14 +76,15 @@ std::unordered_map<DomainT*, std::unordered_map<LocationType, DomainT*>> buildTr
         stack.pop_back();
         tm.try_emplace(cur);
         if (!adj.count(cur)) continue;
-        for (LocationType loc : kBoundaryLocations2D)
+        // children in the adjacency map's own order, as the reference inserts them (the order in which the
+        // levels list them)
+        for (const auto& kv : adj.at(cur))
         {
-            auto it = adj.at(cur).find(loc);
-            if (it == adj.at(cur).end() || it->second == par) continue;
-            if (seen.count(it->second)) throw std::runtime_error("geometry adjacency has a cycle");
-            seen.insert(it->second);
-            tm[cur][loc] = it->second;
-            stack.push_back({it->second, cur});
+            if (kv.second == par) continue;
+            if (seen.count(kv.second)) throw std::runtime_error("geometry adjacency has a cycle");
+            seen.insert(kv.second);
+            tm[cur][kv.first] = kv.second;
+            stack.push_back({kv.second, cur});
         }
     }
     return tm;

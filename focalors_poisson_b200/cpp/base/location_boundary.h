@@ -20,6 +20,9 @@ enum class LocationType : std::uint8_t
 
 constexpr std::array<LocationType, 4> kBoundaryLocations2D = {LocationType::XNegative, LocationType::XPositive,
                                                               LocationType::YNegative, LocationType::YPositive};
+constexpr std::array<LocationType, 6> kBoundaryLocations3D = {LocationType::XNegative, LocationType::XPositive,
+                                                              LocationType::YNegative, LocationType::YPositive,
+                                                              LocationType::ZNegative, LocationType::ZPositive};
 
 inline LocationType opposite(LocationType l)
 {

@@ -280,6 +280,29 @@ def mocks():
     save("mocks.npz", **out)
 
 
+def dropin3d():
+    """tests/cases/variable3d_case.cpp compiled against the reference's own headers and sources and run with
+    "solve": per box the solution's sum, norm, first and last values (ConcatPoissonSolver3D, GMRES(20, 1e-13,
+    100)) in the order the case prints them."""
+    import subprocess
+    import tempfile
+
+    from oracle import refpath
+
+    ref = refpath.reference_dir()
+    src = os.path.join(ROOT, "tests", "cases", "variable3d_case.cpp")
+    lib = os.path.join(ROOT, "oracle", "_ref")
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = os.path.join(tmp, "variable3d_ref")
+        subprocess.run(["g++", "-std=c++17", "-O2", "-fopenmp", "-w", "-I" + os.path.join(ROOT, "oracle", "shim"),
+                        "-I" + ref, "-include", os.path.join(ref, "base", "pch.h"), src, "-o", exe, "-L" + lib,
+                        "-lfpref", "-Wl,-rpath," + lib], check=True)
+        out = subprocess.run([exe, "solve"], check=True, capture_output=True, text=True).stdout
+    rows = [ln.split() for ln in out.splitlines() if ln.startswith("solution ")]
+    save("dropin3d.npz", names=np.array([r[1] for r in rows]),
+         values=np.array([[float(v) for v in r[2:]] for r in rows], dtype=np.float64))
+
+
 if __name__ == "__main__":
     transforms()
     poisson()
@@ -294,3 +317,4 @@ if __name__ == "__main__":
     cross64()
     tree9()
     mocks()
+    dropin3d()

@@ -68,14 +68,16 @@ REFERENCE = refpath.reference_dir()
 @pytest.mark.skipif(not refpath.available() or not os.path.exists(
     os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "libfpref.so")),
     reason="needs the reference sources and the oracle library built from them")
-def test_host_data_model_matches_reference(tmp_path):
-    """Geometry2D / Variable2D host bookkeeping (sizes propagated by connect, axis offsets, tree root,
-    boundary-type overrides, set_value at cell centres, set_buffer at ghost cells) prints identically
-    through the reference's own sources and through the drop-in layer."""
+@pytest.mark.parametrize("case", ["variable_case.cpp", "variable3d_case.cpp"])
+def test_host_data_model_matches_reference(tmp_path, case):
+    """Geometry2D / Variable2D (variable_case.cpp) and Geometry3D / Variable3D (variable3d_case.cpp) host
+    bookkeeping (sizes propagated by connect, axis offsets, tree root and levels, boundary-type overrides and
+    their errors, set_value at cell centres, set_buffer at ghost cells, boundary values, corners) prints
+    identically through the reference's own sources and through the drop-in layer."""
     import subprocess
 
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    src = os.path.join(root, "tests", "cases", "variable_case.cpp")
+    src = os.path.join(root, "tests", "cases", case)
     ours = build.compile_driver(src, str(tmp_path / "ours"))
     refexe = str(tmp_path / "ref")
     lib = os.path.join(root, "oracle", "_ref")

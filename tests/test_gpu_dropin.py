@@ -76,3 +76,19 @@ def test_reference_concat_driver_unchanged():
     for d in range(6):
         np.testing.assert_array_equal(before[d], z[f"rhs_{d}"])
         _printed(after[d], z[f"out_{d}"])
+
+
+def test_dropin_concat3d_case(tmp_path):
+    """tests/cases/variable3d_case.cpp (Geometry3D / Variable3D / ConcatPoissonSolver3D of the reference's API,
+    four boxes in an L with a box on top) solved through the drop-in layer: per box the solution's sum, norm,
+    first and last values equal the reference's own run of the same file (GMRES(20, 1e-13, 100) in both, so the
+    two answers differ by the solvers' residual tolerance, not by round-off)."""
+    src = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cases", "variable3d_case.cpp")
+    exe = build.compile_driver(src, str(tmp_path / "variable3d_case"))
+    r = subprocess.run([exe, "solve"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    rows = [ln.split() for ln in r.stdout.splitlines() if ln.startswith("solution ")]
+    z = load("dropin3d.npz")
+    assert [row[1] for row in rows] == list(z["names"])
+    got = np.array([[float(v) for v in row[2:]] for row in rows])
+    np.testing.assert_allclose(got, z["values"], rtol=1e-9, atol=1e-11)
