@@ -10,6 +10,7 @@
 #include <cmath>
 #include <map>
 #include <numeric>
+#include <type_traits>
 
 namespace fpb
 {
@@ -1126,7 +1127,9 @@ private:
     void   build_static_lists();
     void   build_chase_lists();
     void   chase_run(const Segments& lc, const Segments& red, cudaStream_t s);
-    void   inner(const XList& dst_in, const XList& dst_out, bool acc, cudaStream_t s);
+    void   inner(const XList& dst_in, const XList& dst_out, bool acc, cudaStream_t s, bool inv64 = false);
+    void   first_inner(cudaStream_t s);
+    void   build_plans64();
     const double* basis_col(int kind, int n, int j);
     bool   build_edge_mv(const std::vector<DstSeg>& segs, const std::vector<int>& ns, Segments& out);
     void   edge_mv(const Segments& l, cudaStream_t s);
@@ -1144,6 +1147,11 @@ private:
     long long                                 cells_ = 0;
     PlanSet<TS>                               plans_;
     PlanSet<double>                           eplans_;  // FP64 DSTs of edge vectors (length nx of roots)
+    // FP32 storage: FP64 plans of the same (family, length) at the same indices as plans_, for the first inner
+    // solve's inverse transform, and the list writing its output into the iterate
+    PlanSet<double>                           plans64_;
+    XList                                     dst_out_u64_;
+    BatchTiming                               tm64_;
     std::map<std::pair<int, double>, int>     tab_index_;
     std::vector<std::unique_ptr<DevRect<double>>> tabs_;  // chase tables (FP64 in both storage precisions)
     std::vector<DevBuf>                           tab_back_;  // the back substitution's copy of each cc
@@ -1849,7 +1857,8 @@ template <typename TS> void BatchImpl<TS>::chase_run(const Segments& lc, const S
 }
 
 // One inner solve: dst_in (FP64 rows -> W), ..., X -> dst_out (FP64 rows; += when acc).
-template <typename TS> void BatchImpl<TS>::inner(const XList& dst_in, const XList& dst_out, bool acc, cudaStream_t s)
+template <typename TS>
+void BatchImpl<TS>::inner(const XList& dst_in, const XList& dst_out, bool acc, cudaStream_t s, bool inv64)
 {
     launch_x<TS, double, TS, false>(dst_in, false, plans_, tm_, s);
     chase_run(l1_lc_, l1_red_, s);
@@ -1910,8 +1919,36 @@ template <typename TS> void BatchImpl<TS>::inner(const XList& dst_in, const XLis
     if (mv_o_) edge_mv(edge_mv_o_, s);
     else launch_x1<double, K_DD, 0, double, double, false>(edst_out_, eplans_, tm_, s);
     chase_run(a2_lc_, a2_red_, s);
+    if constexpr (std::is_same<TS, float>::value)
+        if (inv64)
+        {
+            launch_x<double, TS, double, false>(dst_out, true, plans64_, tm64_, s);
+            return;
+        }
     if (acc) launch_x<TS, TS, double, true>(dst_out, true, plans_, tm_, s);
     else launch_x<TS, TS, double, false>(dst_out, true, plans_, tm_, s);
+}
+
+// The first inner solve of a refinement (right-hand sides in fs, solution written into the iterate). With
+// FP32 storage its inverse transform runs in FP64 arithmetic on the FP32 chase output: the DST-I's folding
+// algorithm sums ~n/2 FFT outputs into the odd coefficients, so an FP32 inverse leaves a random-walk error
+// (~3e-6 at n = 2048) that the first correction contracts only to ~6e-10; with the FP64 inverse the first
+// solve is ~8e-8 from the answer and one FP32 correction reaches ~3e-13.
+template <typename TS> void BatchImpl<TS>::first_inner(cudaStream_t s)
+{
+    if (std::is_same<TS, float>::value) inner(dst_fs_, dst_out_u64_, false, s, true);
+    else inner(dst_fs_, dst_out_u_, false, s);
+}
+
+template <typename TS> void BatchImpl<TS>::build_plans64()
+{
+    if (!std::is_same<TS, float>::value || !plans64_.tr.empty()) return;
+    for (auto& D : dom_)
+        if (plans64_.get(D.kind, D.d.ny) != D.plan) throw Error(2, "FP64 plan indices differ from the FP32 plans");
+    plans64_.finish();
+    tm64_                   = tm_;
+    tm64_.dst_threads       = 128;      // the FP64 batch's measured stage-engine shape
+    tm64_.dst_blocks_per_sm = 1 << 20;  // one CTA per work item
 }
 
 template <typename TS>
@@ -1953,6 +1990,11 @@ void BatchImpl<TS>::set_user_lists(double* const* fields, const double* const* g
         std::vector<DstSeg> c = dst_X_out_rec_;
         for (int g = 0; g < nd; ++g) c[g].out = f[g];
         dst_out_u_.set(c, dst_kinds_, plans_);
+        if (std::is_same<TS, float>::value)
+        {
+            build_plans64();
+            dst_out_u64_.set(c, dst_kinds_, plans64_);
+        }
         const long long        nb = (long long)(addp_.bytes() / 16);
         std::vector<AddSeg>    ad;
         std::vector<long long> acn;
@@ -2048,7 +2090,7 @@ template <typename TS> void BatchImpl<TS>::run(int steps, cudaStream_t s)
         inner(dst_user_in_, dst_user_out_, false, s);
         return;
     }
-    inner(dst_fs_, dst_out_u_, false, s);
+    first_inner(s);
     for (int k = 1; k < steps; ++k)
     {
         k_b_residual<<<(unsigned)res_.total, 256, 0, s>>>(res_.as<ResSeg>(), res_.pre(), res_.n);
@@ -2150,7 +2192,7 @@ void BatchImpl<TS>::build_ir_graph(double rel_tol, int max_refine, BatchBase* fi
         k_b_assemble<<<(unsigned)asm_user_.total, 256, 0, cap>>>(asm_user_.as<AsmSeg>(), asm_user_.pre(), asm_user_.n);
         FPB_CHECK_LAUNCH();
         if (first) first->solve_assembled(fi, fo, cap);
-        else inner(dst_fs_, dst_out_u_, false, cap);
+        else first_inner(cap);
         k_ir_init<<<1, 1, 0, cap>>>(irst_.as<IrState>());
         FPB_CHECK_LAUNCH();
         ir_pro_ = launches_noted() - before;
