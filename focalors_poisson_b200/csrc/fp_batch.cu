@@ -979,6 +979,7 @@ struct XList
         int      kind = 0;
         int      eng = 0, threads = 0;  // register engine: threads per CTA (stage engine: autotuned)
         size_t   smem = 0;
+        int      plan = -1;  // the plan of every run, when they share one (launched with it by value)
         Segments seg;
     };
     std::vector<Part> parts;
@@ -998,18 +999,21 @@ struct XList
             {
                 std::vector<DstSeg>    r;
                 std::vector<long long> c;
-                size_t                 sm = 0;
+                size_t                 sm   = 0;
+                int                    plan = recs[g.second[0]].plan;
                 for (size_t i : g.second)
                 {
                     r.push_back(recs[i]);
                     c.push_back((recs[i].rows + 1) / 2);
                     sm = std::max(sm, ps.tr[recs[i].plan]->smem);
+                    if (recs[i].plan != plan) plan = -1;
                 }
                 parts.emplace_back();
                 parts.back().kind    = k;
                 parts.back().eng     = g.first > 0 ? 1 : 0;
                 parts.back().threads = g.first > 0 ? g.first / 16 : 0;
                 parts.back().smem    = sm;
+                parts.back().plan    = plan;
                 parts.back().seg.set(r, c);
             }
         }
@@ -1020,29 +1024,47 @@ template <typename T, int K, int I, typename TIN, typename TOUT, bool ACC> void 
 {
     allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 0>);
     allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 1>);
+    allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 0, true>);
+    allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 1, true, kXformStaticM>);
 }
 
 // Stage engine: the autotuned CTA shape (threads, CTAs per SM); register engine: `threads` per CTA and as
-// many CTAs as are resident at once, each looping over items.
+// many CTAs as are resident at once, each looping over items. plan >= 0: every run uses that plan, whose
+// arguments then go to the kernel by value (stage engine, and register-engine plans of length kXformStaticM
+// with the compile-time instance); otherwise the kernel reads each run's plan from the plan array.
 template <typename T, int K, int I, typename TIN, typename TOUT, bool ACC>
 void launch_x1(const Segments& sg, const PlanSet<T>& ps, const BatchTiming& tm, cudaStream_t s, size_t smem = 0,
-               int eng = 0, int threads = 0)
+               int eng = 0, int threads = 0, int plan = -1)
 {
     if (sg.total == 0) return;
     prep_x<T, K, I, TIN, TOUT, ACC>();
-    const size_t sm = smem ? smem : ps.smem;
+    const size_t        sm = smem ? smem : ps.smem;
+    const XformArgs<T>* pa = ps.dev.template as<XformArgs<T>>();
     if (eng == 1)
     {
+        if (plan >= 0 && ps.tr[plan]->fd.M == kXformStaticM)
+        {
+            const void*     fn   = (const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 1, true, kXformStaticM>;
+            const long long grid = std::min<long long>(sg.total, resident_ctas(fn, threads, sm));
+            k_b_xform<T, K, I, TIN, TOUT, ACC, 1, true, kXformStaticM><<<(unsigned)grid, threads, sm, s>>>(
+                sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, nullptr, DstSeg{}, ps.tr[plan]->hargs[I]);
+            FPB_CHECK_LAUNCH();
+            return;
+        }
         const void*     fn   = (const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 1>;
         const long long grid = std::min<long long>(sg.total, resident_ctas(fn, threads, sm));
         k_b_xform<T, K, I, TIN, TOUT, ACC, 1><<<(unsigned)grid, threads, sm, s>>>(
-            sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, ps.dev.template as<XformArgs<T>>(), DstSeg{});
+            sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, pa, DstSeg{}, XformArgs<T>{});
         FPB_CHECK_LAUNCH();
         return;
     }
     const long long grid = std::min<long long>(sg.total, (long long)sm_count() * tm.dst_blocks_per_sm);
-    k_b_xform<T, K, I, TIN, TOUT, ACC, 0><<<(unsigned)grid, tm.dst_threads, sm, s>>>(
-        sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, ps.dev.template as<XformArgs<T>>(), DstSeg{});
+    if (plan >= 0)
+        k_b_xform<T, K, I, TIN, TOUT, ACC, 0, true><<<(unsigned)grid, tm.dst_threads, sm, s>>>(
+            sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, nullptr, DstSeg{}, ps.tr[plan]->hargs[I]);
+    else
+        k_b_xform<T, K, I, TIN, TOUT, ACC, 0><<<(unsigned)grid, tm.dst_threads, sm, s>>>(
+            sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, pa, DstSeg{}, XformArgs<T>{});
     FPB_CHECK_LAUNCH();
 }
 
@@ -1052,14 +1074,14 @@ void launch_x(const XList& L, bool inverse, const PlanSet<T>& ps, const BatchTim
 {
     for (auto& part : L.parts)
     {
-        const int e = part.eng, th = part.threads;
+        const int e = part.eng, th = part.threads, p = part.plan;
         switch (part.kind)
         {
-            case K_DD: launch_x1<T, K_DD, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th); break;
-            case K_DN: launch_x1<T, K_DN, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th); break;
+            case K_DD: launch_x1<T, K_DD, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th, p); break;
+            case K_DN: launch_x1<T, K_DN, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th, p); break;
             default:
-                if (inverse) launch_x1<T, K_ND, 1, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th);
-                else launch_x1<T, K_ND, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th);
+                if (inverse) launch_x1<T, K_ND, 1, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th, p);
+                else launch_x1<T, K_ND, 0, TIN, TOUT, ACC>(part.seg, ps, tm, s, part.smem, e, th, p);
         }
     }
 }

@@ -137,7 +137,7 @@ template <typename T> struct DevTransform
     int     kind = 0, n = 0;
     FftDesc fd{}, fd_inv{};  // forward / inverse windows of one plan
     DevBuf  tw, chirp, bhat, bhat_inv, perm, stages, ta, tb, tc;
-    DevBuf  dargs;  // args(false), args(true) in device memory, for k_b_xform
+    XformArgs<T> hargs[2]{};  // args(false), args(true), passed by value to k_b_xform (one plan per launch)
     DevBuf  gscratch;  // eng 2: the FFT buffers of gctas CTAs in global memory, gstride elements each
     T       s1 = 0, s2 = 0;
     int     threads = 128;

@@ -83,21 +83,38 @@ template <typename T2> std::vector<T2> convert_c(const std::vector<std::complex<
     return r;
 }
 
-// One run of rows through k_b_xform: one CTA per item on the stage engine; on the register engine as many
-// CTAs as fit on the GPU at once, each looping over items (its tables are loaded once per CTA).
-template <typename T, int K, int I, typename TIO, int ENG>
-void launch_k(const DstSeg& one, const XformArgs<T>* dargs, long long rows, int threads, size_t smem, cudaStream_t s,
-              long long gctas = 0)
+// One run of rows through k_b_xform with the plan's arguments by value (PV): one CTA per item on the stage
+// engine; on the register engine as many CTAs as fit on the GPU at once, each looping over items (its
+// tables are loaded once per CTA), with the compile-time instance for a length of kXformStaticM.
+template <typename T, int K, int I, typename TIO, int ENG, int MC = 0>
+void launch_k1(const DstSeg& one, const XformArgs<T>& ha, long long items, int threads, size_t smem, cudaStream_t s,
+               long long gctas)
 {
-    const void* fn = (const void*)k_b_xform<T, K, I, TIO, TIO, false, ENG>;
+    const void* fn = (const void*)k_b_xform<T, K, I, TIO, TIO, false, ENG, true, MC>;
     allow_max_dynamic_smem(fn);
-    const long long items = FamilyTraits<K, I>::kPairRows ? (rows + 1) / 2 : rows;
-    if (items <= 0) return;
     const long long grid = ENG == 1   ? std::min<long long>(items, resident_ctas(fn, threads, smem))
                            : ENG == 2 ? std::min<long long>(items, gctas)  // the CTAs the global buffers hold
                                       : items;
-    k_b_xform<T, K, I, TIO, TIO, false, ENG><<<(unsigned)grid, threads, smem, s>>>(nullptr, nullptr, 1, items, dargs, one);
+    k_b_xform<T, K, I, TIO, TIO, false, ENG, true, MC>
+        <<<(unsigned)grid, threads, smem, s>>>(nullptr, nullptr, 1, items, nullptr, one, ha);
     FPB_CHECK_LAUNCH();
+}
+
+template <typename T, int K, int I, typename TIO, int ENG>
+void launch_k(const DstSeg& one, const XformArgs<T>& ha, long long rows, int threads, size_t smem, cudaStream_t s,
+              long long gctas = 0)
+{
+    const long long items = FamilyTraits<K, I>::kPairRows ? (rows + 1) / 2 : rows;
+    if (items <= 0) return;
+    if constexpr (ENG == 1)
+    {
+        if (ha.fd.M == kXformStaticM)
+        {
+            launch_k1<T, K, I, TIO, ENG, kXformStaticM>(one, ha, items, threads, smem, s, gctas);
+            return;
+        }
+    }
+    launch_k1<T, K, I, TIO, ENG>(one, ha, items, threads, smem, s, gctas);
 }
 }  // namespace
 
@@ -168,8 +185,8 @@ DevTransform<T>::DevTransform(int kind_, int n_, bool allow_register, bool allow
         gscratch.alloc((size_t)gctas * gstride * sizeof(T2));
         smem = 0;
     }
-    std::vector<XformArgs<T>> both = {args(false), args(true)};
-    dargs                          = upload(both);
+    hargs[0] = args(false);
+    hargs[1] = args(true);
     if (smem > max_dynamic_smem()) throw Error(3, "transform of length " + std::to_string(n) + " needs more shared memory than a CTA has");
 }
 
@@ -197,8 +214,8 @@ void DevTransform<T>::run_io(const TIO* in, TIO* out, long long rows, bool inver
 {
     if (rows > (long long)INT_MAX) throw Error(3, "more than 2^31 rows in one transform call");
     const DstSeg        a{in, out, (int)rows, 0};
-    const XformArgs<T>* d   = dargs.as<XformArgs<T>>();
     const int           inv = inverse ? 1 : 0;
+    const XformArgs<T>& d   = hargs[inv];
 #define FPB_CASE(K)                                                                                        \
     case K:                                                                                                \
         if (fd.eng == 1)                                                                                   \

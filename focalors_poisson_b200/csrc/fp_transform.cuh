@@ -347,7 +347,7 @@ __device__ __forceinline__ void reg_tables_to_smem(const XformArgs<T>& a, typena
 // engine, 1 register engine, whose tables the kernel has already put in shared memory after the buffer).
 // Ends with the CTA synchronised. Every element-wise pass handles kFftBatch elements per thread at a
 // time, loads first.
-template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG = 0>
+template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG = 0, int MC = 0>
 __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN* fa, const TIN* fb, TOUT* oa, TOUT* ob,
                                                bool has_b, typename Cplx<T>::type* buf, T* rowsc)
 {
@@ -375,7 +375,7 @@ __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN*
     if constexpr (ENG == 1)
     {
         const T2* stw = buf + reg_tables_off(a.fd);
-        reg_transform(buf, a.fd, a.ft, stw, stw + (M >> 4), zval);
+        reg_transform<MC>(buf, a.fd, a.ft, stw, stw + (M >> 4), zval);
     }
     else if (a.fd.blue)
     {
@@ -518,25 +518,32 @@ struct DstSeg
 };
 
 // The y-transform kernel of the library, for a single run of rows (the transform and rectangle entry
-// points: segs == nullptr, the run passed by value in `one`, plans = the plan's two argument sets) and for
-// many runs of rows of several lengths in one persistent launch (the batched and composite solvers: a work
-// list segs / prefix). One family and direction per launch; the per-row work is transform_rows.
+// points: segs == nullptr, the run passed by value in `one`) and for many runs of rows of several lengths in
+// one persistent launch (the batched and composite solvers: a work list segs / prefix). One family and
+// direction per launch; the per-row work is transform_rows.
 // One work item = the rows one FFT carries (two for the pairing families) of one run; CTA b takes items
 // b, b + gridDim.x, .... ACC: out (FP64) += result instead of out = result. DD and DN are their own
 // transposes (the batched solver runs their inverse with INV = 0 and the forward arguments).
-// The arguments are read through a global pointer; uncapped, the stage engine's FP64 instances take
-// 104-110 registers, which allows only 2 CTAs of 256 threads per SM, and at 80 (16 bytes of spill) three fit,
-// as many as their shared memory allows (see xform_maxnreg).
-// ENG 1 (register engine): every run of one launch has a plan of the same length M (M/16 threads per CTA);
-// the CTA copies a plan's tables into shared memory when its items move to another plan. ENG 2 (rows whose
-// FFT buffer does not fit in shared memory): the stage engine's code on a per-CTA buffer in global memory
-// (XformArgs::gbuf, sized for the launch's grid), which the L2 keeps close.
-template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG>
+// PV (one plan for every run of the launch): the plan's arguments come by value in `pv`, in parameter space,
+// which no store of the kernel can alias, so they are read as instruction operands instead of being reloaded
+// into registers after the stores (measured on the 2048 x 2048 FP64 DD transform: 94 -> 87 us); otherwise
+// the runs' plans are entries of the global array `plans` (entries 2 plan and 2 plan + 1 are the forward and
+// inverse arguments of plan `plan`).
+// Registers: uncapped, the stage engine's FP64 instances take 104-110, which allows only 2 CTAs of 256
+// threads per SM, and at 80 (16 bytes of spill) three fit, as many as their shared memory allows (see
+// xform_maxnreg).
+// ENG 1 (register engine): every run of one launch has a plan of the same length M (M/16 threads per CTA),
+// MC > 0 when that length is known at compile time; the CTA copies a plan's tables into shared memory when
+// its items move to another plan. ENG 2 (rows whose FFT buffer does not fit in shared memory): the stage
+// engine's code on a per-CTA buffer in global memory (XformArgs::gbuf, sized for the launch's grid), which
+// the L2 keeps close.
+template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG, bool PV = false, int MC = 0>
 __global__ void __maxnreg__((xform_maxnreg<ENG, T>()))
     k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg, long long nitems,
-              const XformArgs<T>* __restrict__ plans, const DstSeg one)
+              const XformArgs<T>* __restrict__ plans, const DstSeg one, const __grid_constant__ XformArgs<T> pv)
 {
     typedef typename Cplx<T>::type T2;
+    static_assert(MC == 0 || ENG == 1, "a compile-time length is a register-engine plan");
     extern __shared__ __align__(16) unsigned char fp_smem_raw[];
     T2*            buf = reinterpret_cast<T2*>(fp_smem_raw);
     __shared__ T   rowsc[2];
@@ -547,14 +554,18 @@ __global__ void __maxnreg__((xform_maxnreg<ENG, T>()))
         const int           s  = segs ? seg_of(prefix, nseg, it) : 0;
         const DstSeg        sg = segs ? segs[s] : one;
         const long long     i0 = segs ? prefix[s] : 0;
-        const XformArgs<T>& P  = plans[2 * sg.plan + INV];
+        const XformArgs<T>* Pp;
+        if constexpr (PV) Pp = &pv;
+        else Pp = plans + 2 * sg.plan + INV;
+        const XformArgs<T>& P = *Pp;
         if constexpr (ENG == 2) buf = P.gbuf + blockIdx.x * P.gstride;
         if constexpr (ENG == 1)
         {
-            if (sg.plan != loaded)
+            const int pid = PV ? 0 : sg.plan;
+            if (pid != loaded)
             {
                 reg_tables_to_smem(P, buf);
-                loaded = sg.plan;
+                loaded = pid;
             }
         }
         const int       n     = P.n;
@@ -564,8 +575,11 @@ __global__ void __maxnreg__((xform_maxnreg<ENG, T>()))
         const TIN*      fb    = has_b ? fa + n : fa;
         TOUT*           oa    = static_cast<TOUT*>(sg.out) + r0 * n;
         TOUT*           ob    = has_b ? oa + n : nullptr;
-        transform_rows<T, KIND, INV, TIN, TOUT, ACC, ENG>(P, fa, fb, oa, ob, has_b, buf, rowsc);
+        transform_rows<T, KIND, INV, TIN, TOUT, ACC, ENG, MC>(P, fa, fb, oa, ob, has_b, buf, rowsc);
     }
 }
+
+// The register-engine lengths with a compile-time instance of k_b_xform (MC); other lengths run with MC = 0.
+constexpr int kXformStaticM = 4096;
 
 }  // namespace fpb
