@@ -325,6 +325,77 @@ __device__ __forceinline__ void put_batch(TOUT* oa, TOUT* ob, const int* idx, co
     }
 }
 
+// Writes the DD output pairs of items k = k0 + u nt (u < U, k < K): out[2k] = ev[u], out[2k+1] = od[u] (2k+1 < n)
+// for row a (.x) and, when ob, row b (.y). vec: n is even and the rows are aligned to a pair, so each pair
+// is one vector store (and one vector load for ACC). ACC adds to the values there in FP64.
+template <typename TOUT> struct Pair;
+template <> struct Pair<double>
+{
+    typedef double2 type;
+};
+template <> struct Pair<float>
+{
+    typedef float2 type;
+};
+template <int U, bool ACC, typename TOUT, typename T2>
+__device__ __forceinline__ void put_pairs(TOUT* oa, TOUT* ob, int k0, int nt, int K, int n, bool vec, const T2* ev,
+                                          const T2* od)
+{
+    typedef typename Pair<TOUT>::type P2;
+    if (vec)
+    {
+        P2 pa[U], pb[U];
+        if (ACC)
+        {
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+            {
+                const int k = k0 + u * nt;
+                if (k >= K) continue;
+                pa[u] = reinterpret_cast<const P2*>(oa)[k];
+                if (ob) pb[u] = reinterpret_cast<const P2*>(ob)[k];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int k = k0 + u * nt;
+            if (k >= K) continue;
+            P2 wa, wb;
+            if (ACC)
+            {
+                wa.x = (TOUT)((double)pa[u].x + (double)ev[u].x);
+                wa.y = (TOUT)((double)pa[u].y + (double)od[u].x);
+                if (ob)
+                {
+                    wb.x = (TOUT)((double)pb[u].x + (double)ev[u].y);
+                    wb.y = (TOUT)((double)pb[u].y + (double)od[u].y);
+                }
+            }
+            else
+            {
+                wa.x = (TOUT)ev[u].x;
+                wa.y = (TOUT)od[u].x;
+                wb.x = (TOUT)ev[u].y;
+                wb.y = (TOUT)od[u].y;
+            }
+            reinterpret_cast<P2*>(oa)[k] = wa;
+            if (ob) reinterpret_cast<P2*>(ob)[k] = wb;
+        }
+        return;
+    }
+    int ie[U], io[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+    {
+        const int k = k0 + u * nt;
+        ie[u]       = k < K ? 2 * k : -1;
+        io[u]       = (k < K && 2 * k + 1 < n) ? 2 * k + 1 : -1;
+    }
+    put_batch<U, ACC>(oa, ob, ie, ev);
+    put_batch<U, ACC>(oa, ob, io, od);
+}
+
 // Shared memory of a register-engine plan: the exchange buffer, then the rotation table (M/16 entries),
 // then the chirp tables (Bluestein plans); in elements of the complex type.
 __host__ __device__ __forceinline__ int reg_tables_off(const FftDesc& d) { return reg_buf_elems(d.M); }
@@ -409,54 +480,45 @@ __device__ __forceinline__ void transform_rows(const XformArgs<T>& a, const TIN*
     const T half = (T)0.5;
     if (KIND == 0)
     {
-        // DD: X_{2k} = -Im Y_k (k >= 1), X_{2k+1} = Re Y_0 / 2 + sum_{q=1..k} Re Y_q; out_m = s1 X_{m+1}
-        const int K  = (n + 1) / 2;  // odd outputs X_1, X_3, ...
+        // DD: X_{2k} = -Im Y_k (k >= 1), X_{2k+1} = Re Y_0 / 2 + sum_{q=1..k} Re Y_q; out_m = s1 X_{m+1}, so
+        // output pair k is out[2k] = s1 X_{2k+1} (k < K) and out[2k+1] = -s1 Im Y_{k+1} (2k+1 < n).
+        const int K  = (n + 1) / 2;
         // scan arrays: the slots past element L-1 when the buffer has K of them, else past the buffer (and
         // the register engine's tables)
         const int lo = fft_slot_d(a.fd, L), hi = ENG == 1 ? reg_smem_elems(a.fd) : fft_buf_elems(M);
         T*        ca = reinterpret_cast<T*>(buf + ((hi - lo >= K) ? lo : hi));
         T*        cb = ca + K;
-        for (int k0 = threadIdx.x; k0 <= n / 2; k0 += U * nt)
+        for (int k = threadIdx.x; k < K; k += nt)
         {
-            int idx[U];
-            T2  v[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-            {
-                const int k = k0 + u * nt;
-                idx[u]      = -1;
-                v[u]        = mk<T2>(0, 0);
-                if (k > n / 2) continue;
-                const T2 Zk = fft_out(buf, a.fd, k);
-                const T2 Zm = fft_out(buf, a.fd, fft_mirror(k, L));
-                if (k < K)
-                {
-                    const T sc = (k == 0) ? (T)0.5 : (T)1;
-                    ca[k]      = sc * (half * (Zk.x + Zm.x));  // Re Y^a_k
-                    cb[k]      = sc * (half * (Zk.y + Zm.y));  // Re Y^b_k
-                }
-                if (k >= 1 && 2 * k <= n)
-                {
-                    idx[u] = 2 * k - 1;
-                    v[u]   = mk<T2>(a.s1 * (-(half * (Zk.y - Zm.y))), a.s1 * (half * (Zk.x - Zm.x)));  // -Im Y^a_k, -Im Y^b_k
-                }
-            }
-            put_batch<U, ACC>(oa, ob, idx, v);
+            const T2 Zk = fft_out(buf, a.fd, k);
+            const T2 Zm = fft_out(buf, a.fd, fft_mirror(k, L));
+            const T  sc = (k == 0) ? (T)0.5 : (T)1;
+            ca[k]       = sc * (half * (Zk.x + Zm.x));  // Re Y^a_k
+            cb[k]       = sc * (half * (Zk.y + Zm.y));  // Re Y^b_k
         }
         __syncthreads();
         block_scan2(ca, cb, K);
+        // Both outputs of a pair in one store where the rows allow it (n even, rows aligned to a pair).
+        const bool vec = (n % 2 == 0) && (reinterpret_cast<uintptr_t>(oa) % (2 * sizeof(TOUT)) == 0);
         for (int k0 = threadIdx.x; k0 < K; k0 += U * nt)
         {
-            int idx[U];
-            T2  v[U];
+            T2 ev[U], od[U];
 #pragma unroll
             for (int u = 0; u < U; ++u)
             {
                 const int k = k0 + u * nt;
-                idx[u]      = (k < K) ? 2 * k : -1;
-                v[u]        = (k < K) ? mk<T2>(a.s1 * ca[k], a.s1 * cb[k]) : mk<T2>(0, 0);
+                ev[u]       = mk<T2>(0, 0);
+                od[u]       = mk<T2>(0, 0);
+                if (k >= K) continue;
+                ev[u] = mk<T2>(a.s1 * ca[k], a.s1 * cb[k]);
+                if (2 * k + 1 < n)
+                {
+                    const T2 Z1 = fft_out(buf, a.fd, k + 1);
+                    const T2 Zm = fft_out(buf, a.fd, fft_mirror(k + 1, L));
+                    od[u] = mk<T2>(a.s1 * (-(half * (Z1.y - Zm.y))), a.s1 * (half * (Z1.x - Zm.x)));  // -Im Y_{k+1}
+                }
             }
-            put_batch<U, ACC>(oa, ob, idx, v);
+            put_pairs<U, ACC>(oa, ob, k0, nt, K, n, vec, ev, od);
         }
         __syncthreads();
         return;
