@@ -1025,13 +1025,13 @@ template <typename T, int K, int I, typename TIN, typename TOUT, bool ACC> void 
     allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 0>);
     allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 1>);
     allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 0, true>);
-    allow_max_dynamic_smem((const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 1, true, kXformStaticM>);
+    allow_max_dynamic_smem((const void*)k_xform_rc<T, K, I, TIN, TOUT, ACC, kXformStaticM>);
 }
 
 // Stage engine: the autotuned CTA shape (threads, CTAs per SM); register engine: `threads` per CTA and as
 // many CTAs as are resident at once, each looping over items. plan >= 0: every run uses that plan, whose
-// arguments then go to the kernel by value (stage engine, and register-engine plans of length kXformStaticM
-// with the compile-time instance); otherwise the kernel reads each run's plan from the plan array.
+// arguments then go to the kernel by value (the stage engine's k_b_xform, and k_xform_rc for register-engine
+// plans of length kXformStaticM); otherwise the kernel reads each run's plan from the plan array.
 template <typename T, int K, int I, typename TIN, typename TOUT, bool ACC>
 void launch_x1(const Segments& sg, const PlanSet<T>& ps, const BatchTiming& tm, cudaStream_t s, size_t smem = 0,
                int eng = 0, int threads = 0, int plan = -1)
@@ -1044,10 +1044,10 @@ void launch_x1(const Segments& sg, const PlanSet<T>& ps, const BatchTiming& tm, 
     {
         if (plan >= 0 && ps.tr[plan]->fd.M == kXformStaticM)
         {
-            const void*     fn   = (const void*)k_b_xform<T, K, I, TIN, TOUT, ACC, 1, true, kXformStaticM>;
+            const void*     fn   = (const void*)k_xform_rc<T, K, I, TIN, TOUT, ACC, kXformStaticM>;
             const long long grid = std::min<long long>(sg.total, resident_ctas(fn, threads, sm));
-            k_b_xform<T, K, I, TIN, TOUT, ACC, 1, true, kXformStaticM><<<(unsigned)grid, threads, sm, s>>>(
-                sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, nullptr, DstSeg{}, ps.tr[plan]->hargs[I]);
+            k_xform_rc<T, K, I, TIN, TOUT, ACC, kXformStaticM><<<(unsigned)grid, threads, sm, s>>>(
+                sg.as<DstSeg>(), sg.pre(), sg.n, sg.total, DstSeg{}, ps.tr[plan]->hargs[I]);
             FPB_CHECK_LAUNCH();
             return;
         }

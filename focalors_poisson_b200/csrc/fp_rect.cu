@@ -85,21 +85,7 @@ template <typename T2> std::vector<T2> convert_c(const std::vector<std::complex<
 
 // One run of rows through k_b_xform with the plan's arguments by value (PV): one CTA per item on the stage
 // engine; on the register engine as many CTAs as fit on the GPU at once, each looping over items (its
-// tables are loaded once per CTA), with the compile-time instance for a length of kXformStaticM.
-template <typename T, int K, int I, typename TIO, int ENG, int MC = 0>
-void launch_k1(const DstSeg& one, const XformArgs<T>& ha, long long items, int threads, size_t smem, cudaStream_t s,
-               long long gctas)
-{
-    const void* fn = (const void*)k_b_xform<T, K, I, TIO, TIO, false, ENG, true, MC>;
-    allow_max_dynamic_smem(fn);
-    const long long grid = ENG == 1   ? std::min<long long>(items, resident_ctas(fn, threads, smem))
-                           : ENG == 2 ? std::min<long long>(items, gctas)  // the CTAs the global buffers hold
-                                      : items;
-    k_b_xform<T, K, I, TIO, TIO, false, ENG, true, MC>
-        <<<(unsigned)grid, threads, smem, s>>>(nullptr, nullptr, 1, items, nullptr, one, ha);
-    FPB_CHECK_LAUNCH();
-}
-
+// tables are loaded once per CTA); a register-engine plan of length kXformStaticM runs k_xform_rc.
 template <typename T, int K, int I, typename TIO, int ENG>
 void launch_k(const DstSeg& one, const XformArgs<T>& ha, long long rows, int threads, size_t smem, cudaStream_t s,
               long long gctas = 0)
@@ -110,11 +96,23 @@ void launch_k(const DstSeg& one, const XformArgs<T>& ha, long long rows, int thr
     {
         if (ha.fd.M == kXformStaticM)
         {
-            launch_k1<T, K, I, TIO, ENG, kXformStaticM>(one, ha, items, threads, smem, s, gctas);
+            const void* fn = (const void*)k_xform_rc<T, K, I, TIO, TIO, false, kXformStaticM>;
+            allow_max_dynamic_smem(fn);
+            const long long grid = std::min<long long>(items, resident_ctas(fn, threads, smem));
+            k_xform_rc<T, K, I, TIO, TIO, false, kXformStaticM>
+                <<<(unsigned)grid, threads, smem, s>>>(nullptr, nullptr, 1, items, one, ha);
+            FPB_CHECK_LAUNCH();
             return;
         }
     }
-    launch_k1<T, K, I, TIO, ENG>(one, ha, items, threads, smem, s, gctas);
+    const void* fn = (const void*)k_b_xform<T, K, I, TIO, TIO, false, ENG, true>;
+    allow_max_dynamic_smem(fn);
+    const long long grid = ENG == 1   ? std::min<long long>(items, resident_ctas(fn, threads, smem))
+                           : ENG == 2 ? std::min<long long>(items, gctas)  // the CTAs the global buffers hold
+                                      : items;
+    k_b_xform<T, K, I, TIO, TIO, false, ENG, true>
+        <<<(unsigned)grid, threads, smem, s>>>(nullptr, nullptr, 1, items, nullptr, one, ha);
+    FPB_CHECK_LAUNCH();
 }
 }  // namespace
 

@@ -594,18 +594,16 @@ struct DstSeg
 // Registers: uncapped, the stage engine's FP64 instances take 104-110, which allows only 2 CTAs of 256
 // threads per SM, and at 80 (16 bytes of spill) three fit, as many as their shared memory allows (see
 // xform_maxnreg).
-// ENG 1 (register engine): every run of one launch has a plan of the same length M (M/16 threads per CTA),
-// MC > 0 when that length is known at compile time; the CTA copies a plan's tables into shared memory when
-// its items move to another plan. ENG 2 (rows whose FFT buffer does not fit in shared memory): the stage
+// ENG 1 (register engine): every run of one launch has a plan of the same length M (M/16 threads per CTA);
+// the CTA copies a plan's tables into shared memory when its items move to another plan. ENG 2 (rows whose FFT buffer does not fit in shared memory): the stage
 // engine's code on a per-CTA buffer in global memory (XformArgs::gbuf, sized for the launch's grid), which
 // the L2 keeps close.
-template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG, bool PV = false, int MC = 0>
+template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG, bool PV = false>
 __global__ void __maxnreg__((xform_maxnreg<ENG, T>()))
     k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg, long long nitems,
               const XformArgs<T>* __restrict__ plans, const DstSeg one, const __grid_constant__ XformArgs<T> pv)
 {
     typedef typename Cplx<T>::type T2;
-    static_assert(MC == 0 || ENG == 1, "a compile-time length is a register-engine plan");
     extern __shared__ __align__(16) unsigned char fp_smem_raw[];
     T2*            buf = reinterpret_cast<T2*>(fp_smem_raw);
     __shared__ T   rowsc[2];
@@ -637,11 +635,49 @@ __global__ void __maxnreg__((xform_maxnreg<ENG, T>()))
         const TIN*      fb    = has_b ? fa + n : fa;
         TOUT*           oa    = static_cast<TOUT*>(sg.out) + r0 * n;
         TOUT*           ob    = has_b ? oa + n : nullptr;
-        transform_rows<T, KIND, INV, TIN, TOUT, ACC, ENG, MC>(P, fa, fb, oa, ob, has_b, buf, rowsc);
+        transform_rows<T, KIND, INV, TIN, TOUT, ACC, ENG>(P, fa, fb, oa, ob, has_b, buf, rowsc);
     }
 }
 
-// The register-engine lengths with a compile-time instance of k_b_xform (MC); other lengths run with MC = 0.
+// The register-engine length with a compile-time kernel (k_xform_rc); other lengths run k_b_xform.
 constexpr int kXformStaticM = 4096;
+
+// CTAs per SM the compile-time register-engine kernel is built for: FP64 2 (128 registers: 16 complex
+// values per thread and no spill), FP32 3 (80 registers: measured on the 2048 x 2048 DD transform, 46 us
+// against 47-48 us at 4 CTAs of 64 registers, which spill about 100 bytes, and 49 us at 2).
+template <typename T> constexpr int xform_rc_ctas() { return sizeof(T) == 8 ? 2 : 3; }
+
+// The register engine with one plan of compile-time length MC (M/16 = MC/16 threads per CTA) for every run
+// of the launch: the plan's arguments by value in parameter space (see k_b_xform), its tables copied into
+// shared memory once per CTA before the item loop, and launch bounds in place of a register cap, so that the
+// compiler knows the CTA size. Runs: the work list segs / prefix, or the single run `one` (segs == nullptr).
+// Measured on the 2048 x 2048 FP64 DD transform: 75 us, against 82-84 us for k_b_xform with the same plan by
+// value (whose general item loop spilled 48 bytes per thread at its register cap).
+template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int MC>
+__global__ void __launch_bounds__(MC / 16, xform_rc_ctas<T>())
+    k_xform_rc(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg, long long nitems,
+               const DstSeg one, const __grid_constant__ XformArgs<T> P)
+{
+    typedef typename Cplx<T>::type T2;
+    extern __shared__ __align__(16) unsigned char fp_smem_raw[];
+    T2*            buf = reinterpret_cast<T2*>(fp_smem_raw);
+    __shared__ T   rowsc[2];
+    constexpr bool kPair = FamilyTraits<KIND, INV>::kPairRows;
+    reg_tables_to_smem(P, buf);
+    const int n = P.n;
+    for (long long it = blockIdx.x; it < nitems; it += gridDim.x)
+    {
+        const int       s     = segs ? seg_of(prefix, nseg, it) : 0;
+        const DstSeg    sg    = segs ? segs[s] : one;
+        const long long i0    = segs ? prefix[s] : 0;
+        const long long r0    = kPair ? 2 * (it - i0) : (it - i0);
+        const bool      has_b = kPair && r0 + 1 < sg.rows;
+        const TIN*      fa    = static_cast<const TIN*>(sg.in) + r0 * n;
+        const TIN*      fb    = has_b ? fa + n : fa;
+        TOUT*           oa    = static_cast<TOUT*>(sg.out) + r0 * n;
+        TOUT*           ob    = has_b ? oa + n : nullptr;
+        transform_rows<T, KIND, INV, TIN, TOUT, ACC, 1, MC>(P, fa, fb, oa, ob, has_b, buf, rowsc);
+    }
+}
 
 }  // namespace fpb
