@@ -672,6 +672,20 @@ __global__ void __launch_bounds__(MC / 16, xform_rc_ctas<T>())
         const long long i0    = segs ? prefix[s] : 0;
         const long long r0    = kPair ? 2 * (it - i0) : (it - i0);
         const bool      has_b = kPair && r0 + 1 < sg.rows;
+        // The rows of this CTA's next item into L2 (one 128-byte line per thread and step), so that its load
+        // phase waits for L2 rather than HBM.
+        const long long nx = it + gridDim.x;
+        if (nx < nitems)
+        {
+            const int       s2  = segs ? seg_of(prefix, nseg, nx) : 0;
+            const DstSeg    sg2 = segs ? segs[s2] : one;
+            const long long q0  = kPair ? 2 * (nx - (segs ? prefix[s2] : 0)) : (nx - (segs ? prefix[s2] : 0));
+            const long long nr  = (kPair && q0 + 1 < sg2.rows) ? 2 : 1;
+            const char*     pb  = reinterpret_cast<const char*>(static_cast<const TIN*>(sg2.in) + q0 * n);
+            const long long nb  = nr * n * (long long)sizeof(TIN);
+            for (long long o = (long long)threadIdx.x * 128; o < nb; o += (long long)blockDim.x * 128)
+                asm volatile("prefetch.L2 [%0];" ::"l"(pb + o));
+        }
         const TIN*      fa    = static_cast<const TIN*>(sg.in) + r0 * n;
         const TIN*      fb    = has_b ? fa + n : fa;
         TOUT*           oa    = static_cast<TOUT*>(sg.out) + r0 * n;
