@@ -37,9 +37,9 @@ N_CELLS = 2048
 GMRES = (20, 1e-14, 100)
 SEED = 2024
 IR_REL_TOL = 1e-11
-# DRAM bytes of one k_b_xform<double, DD> launch on 2048 x 2048 (ncu capture summarised in
-# profiles/k_b_xform_DD_2048x2048_f64.md): the input is read once, the output stays in L2
-DD_TRAFFIC_BYTES = 33.75232e6 + 0.313856e6
+# DRAM bytes of one k_xform_rc<double, DD, 4096> launch on 2048 x 2048 (ncu capture summarised in
+# profiles/k_xform_rc_DD_2048x2048_f64.md): the input is read once, the output stays in L2
+DD_TRAFFIC_BYTES = 33.752576e6 + 0.015104e6
 INNER = {"f64ir": "f64", "f32ir": "f32", "mixedir": "mixed"}
 
 
@@ -871,13 +871,13 @@ def main():
     bytes_launch = 2 * N_CELLS * N_CELLS * 8
     peak, peak_kind = measured_peaks()
     achieved = bytes_launch / t_kernel / 1e9
-    roofline = {"kernel": "k_b_xform<double, DD, 0, double, double, ACC=false, register engine, plan by value, M=4096> "
+    roofline = {"kernel": "k_xform_rc<double, DD, 0, double, double, ACC=false, M=4096> (register engine, plan by value) "
                           "(one run of 2048 rows of 2048, in place, five fields in turn; the instantiation the FP64 "
                           "solve launches)", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} hbm_gbs", "traffic": DD_TRAFFIC_BYTES,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
-                                  "(profiles/k_b_xform_DD_2048x2048_f64.md)",
+                                  "(profiles/k_xform_rc_DD_2048x2048_f64.md)",
                 "algorithmic_bytes_per_launch": bytes_launch, "avg_launch_ms": t_kernel * 1e3}
     # the chase (the solve's other kernel family): the x-direction tridiagonal solves of one 2048^2 FP64
     # subdomain, fp_rect_chase_f64 (local chunk sweeps, separator scan, correction), 2*N*8 bytes algorithmic
