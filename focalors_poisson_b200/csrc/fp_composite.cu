@@ -200,8 +200,9 @@ Composite::Composite(const std::vector<Domain>& doms, const std::vector<std::arr
     set_parameter(m, tol, max_iter);
 }
 
-// Schur matrices and interface inverses are built on the first solve that needs them (a geometry solved by
-// the spectral path never does).
+// Schur matrices and interface inverses: fp_composite_create builds them through prepare() for a geometry
+// outside the spectral path, so that no solve pays for them; a solve that still finds them missing (a
+// geometry that left the spectral path later) builds them first.
 void Composite::ensure_built()
 {
     if (built_) return;
