@@ -595,9 +595,9 @@ struct DstSeg
 // threads per SM, and at 80 (16 bytes of spill) three fit, as many as their shared memory allows (see
 // xform_maxnreg).
 // ENG 1 (register engine): every run of one launch has a plan of the same length M (M/16 threads per CTA);
-// the CTA copies a plan's tables into shared memory when its items move to another plan. ENG 2 (rows whose FFT buffer does not fit in shared memory): the stage
-// engine's code on a per-CTA buffer in global memory (XformArgs::gbuf, sized for the launch's grid), which
-// the L2 keeps close.
+// the CTA copies a plan's tables into shared memory when its items move to another plan. ENG 2 (rows whose
+// FFT buffer does not fit in shared memory): the stage engine's code on a per-CTA buffer in global memory
+// (XformArgs::gbuf, sized for the launch's grid), which the L2 keeps close.
 template <typename T, int KIND, int INV, typename TIN, typename TOUT, bool ACC, int ENG, bool PV = false>
 __global__ void __maxnreg__((xform_maxnreg<ENG, T>()))
     k_b_xform(const DstSeg* __restrict__ segs, const long long* __restrict__ prefix, int nseg, long long nitems,
