@@ -175,11 +175,11 @@ __device__ __forceinline__ void reg_fft(T2 (&v)[kRegE], T2* buf, int M, int lgM,
     }
 }
 
-// The same passes with the length M known at compile time (M = 4096, the Bluestein length of the 2048-row
-// DST-I and the direct length of 4096-row rows): spans, rotation strides and every shared-memory slot become
-// constants or constant offsets from one per-thread base, which takes the slot arithmetic out of the
-// exchanges and frees the registers it held (measured on the 2048 x 2048 FP64 DD transform: 94 -> 87 us
-// with the plan in parameter space either way).
+// The same passes with the length M known at compile time (k_xform_rc instantiates M = 4096: the Bluestein
+// length of DST-I rows of 1025..2048 and the direct length of NN / PP rows of 4096). Spans, rotation strides
+// and every shared-memory slot become constants or constant offsets from one per-thread base, which takes the
+// slot arithmetic out of the exchanges and frees the registers it held (2048 x 2048 FP64 DD transform, plan
+// already passed by value: 87 -> 83 us).
 template <int R, int Ns, int M, typename T2>
 __device__ __forceinline__ void reg_pass_c(T2 (&v)[kRegE], int t, const T2* __restrict__ tw)
 {

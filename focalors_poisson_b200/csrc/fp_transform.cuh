@@ -325,9 +325,9 @@ __device__ __forceinline__ void put_batch(TOUT* oa, TOUT* ob, const int* idx, co
     }
 }
 
-// Writes the DD output pairs of items k = k0 + u nt (u < U, k < K): out[2k] = ev[u], out[2k+1] = od[u] (2k+1 < n)
-// for row a (.x) and, when ob, row b (.y). vec: n is even and the rows are aligned to a pair, so each pair
-// is one vector store (and one vector load for ACC). ACC adds to the values there in FP64.
+// Writes the DD output pairs of items k = k0 + u nt (u < U, k < K): out[2k] = ev[u] and, when 2k+1 < n,
+// out[2k+1] = od[u], for row a (.x) and, when ob, row b (.y). vec: n is even and the rows are aligned to a
+// pair, so each pair is one vector store (and one vector load for ACC). ACC adds to the values there in FP64.
 template <typename TOUT> struct Pair;
 template <> struct Pair<double>
 {
