@@ -924,7 +924,8 @@ def main():
         "roofline_chase": roofline_chase,
         "setup": {"seconds": setup_s, "what": "capi.Composite creation for this workload (plans, chase tables, "
                                                "closed-form interface operators and the reduced-system inverse of "
-                                               "the spectral path; the Schur GMRES path builds lazily), wall clock"},
+                                               "the spectral path; on the Schur GMRES path the Schur matrices and "
+                                               "interface inverses), wall clock"},
     }
     if keep_host:
         from oracle import refsolve as RS
