@@ -215,3 +215,52 @@ def test_engine_choice(driver, kind, n, eng, M):
     the stage engine runs it (ND / DN at 2048: 6144 against 8192)."""
     f = plan(driver, kind, n, "register")["fwd"]
     assert (f["eng"], f["M"]) == (eng, M)
+
+
+def dd_fold_rows(xa, xb):
+    """The DD transform of two rows as the device runs it around its length-(n+1) complex DFT
+    (fp_transform.cuh transform_rows, KIND 0): the folded input z(e) = sin(pi e/L)(x_{e-1} + x_{n-e})
+    + (x_{e-1} - x_{n-e}) / 2 of both rows as one complex sequence, its DFT Z, and the output pass that
+    writes output pair k as out[2k] = s1 (Re Y_0 / 2 + sum_{q=1..k} Re Y_q) and out[2k+1] = -s1 Im Y_{k+1},
+    with Y^a_k = (Z_k + conj Z_{L-k}) / 2, Y^b_k = (Z_k - conj Z_{L-k}) / 2i."""
+    n = len(xa)
+    L = n + 1
+    e = np.arange(1, L)
+    ta = np.sin(np.pi * np.arange(L) / L)
+
+    def fold(x):
+        z = np.zeros(L)
+        z[1:] = ta[1:] * (x[e - 1] + x[n - e]) + 0.5 * (x[e - 1] - x[n - e])
+        return z
+
+    Z = np.fft.fft(fold(xa) + 1j * fold(xb))
+    Zm = Z[(-np.arange(L)) % L]  # Z_{L-k}
+    re_a, re_b = 0.5 * (Z.real + Zm.real), 0.5 * (Z.imag + Zm.imag)
+    im_a, im_b = 0.5 * (Z.imag - Zm.imag), -0.5 * (Z.real - Zm.real)
+    s1 = np.sqrt(2.0 / L)
+    K = (n + 1) // 2
+    outs = []
+    for re, im in ((re_a, im_a), (re_b, im_b)):
+        v = re[:K].copy()
+        v[0] *= 0.5
+        out = np.zeros(n)
+        k = np.arange(K)
+        out[2 * k] = s1 * np.cumsum(v)
+        ko = k[2 * k + 1 < n]
+        out[2 * ko + 1] = -s1 * im[ko + 1]
+        outs.append(out)
+    return outs
+
+
+@pytest.mark.parametrize("n", [2048, 1000, 97, 8, 5])
+def test_dd_fold_output_pairs_replay(n):
+    """The DD fold and its output pairs (even outputs from the prefix sum, odd ones from the imaginary
+    parts), replayed in numpy around an exact DFT, give the orthonormal DST-I of both rows (the reference's
+    PoissonFFT2D_DD, pe/poisson/poisson_fft2d.cpp:19-57), for even and odd row lengths."""
+    scipy_fft = pytest.importorskip("scipy.fft")
+    rng = np.random.default_rng(n)
+    xa, xb = rng.standard_normal(n), rng.standard_normal(n)
+    ga, gb = dd_fold_rows(xa, xb)
+    for x, got in ((xa, ga), (xb, gb)):
+        ref = scipy_fft.dst(x, type=1, norm="ortho")
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), n
