@@ -63,7 +63,7 @@ def _rank(rank, world, port, name, out):
 @pytest.mark.parametrize("name", ["cross", "tree9"])
 def test_decomposed_solve_equals_undivided(name):
     world = 3
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank, args=(world, _free_port(), name, out), nprocs=world, join=True)
         res = dict(out)

@@ -33,7 +33,7 @@ def _rank(rank, world, port, out):
 
 def test_max_over_ranks_and_aggregate_value():
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
         res = dict(out)
@@ -69,7 +69,7 @@ def _shard_rank(rank, world, port, out):
 
 def test_batched_problems_split_between_ranks():
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_shard_rank, args=(world, _free_port(), out), nprocs=world, join=True)
         res = dict(out)
